@@ -1,0 +1,230 @@
+"""ctypes binding of the C ABI in ``include/hignn_b200.h`` (``libhignn_b200.so``).
+
+Tests and the benchmark call the native library through this module. It
+raises at import time when the library has not been built: there is no
+Python or CPU fallback for any operation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhignn_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hignn_b200.build`")
+
+lib = C.CDLL(LIB_PATH)
+
+# parameter keys (enum hignn_param)
+P_EPSILON = 0
+P_ETA = 1
+P_MAX_ITER = 2
+P_MAT_POOL_SIZE_FACTOR = 3
+P_MAX_FAR_DOT_WORK_NODE_SIZE = 4
+P_MAX_RELATIVE_COORD = 5
+P_POST_CHECK_FLAG = 6
+P_USE_SYMMETRY = 7
+P_MAX_FAR_FIELD_DISTANCE = 8
+P_PRECISION = 100
+P_FAR_BATCH_ROWS = 101
+P_TIMING = 102
+P_STUDENT_TOL = 103
+P_FIELDS = 104
+P_RECORD_PIVOTS = 105
+
+ERR_NAMES = {-1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_IO", -5: "ERR_LIMIT", -6: "ERR_NODEV"}
+
+
+class HignnStats(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64), ("num_nodes", C.c_int64), ("num_leaves", C.c_int64), ("num_close", C.c_int64),
+        ("num_far", C.c_int64), ("close_evals", C.c_int64), ("far_evals", C.c_int64), ("far_rank_sum", C.c_int64),
+        ("far_rank_max", C.c_int32), ("far_iterations", C.c_int32), ("student_fallback_blocks", C.c_int64),
+        ("t_build_ms", C.c_double), ("t_close_ms", C.c_double), ("t_far_ms", C.c_double), ("t_dot_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = C.c_void_p
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+
+SIGNATURES = {
+    "hignn_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
+    "hignn_version": ([], C.c_int),
+    "hignn_create": ([_fp, C.c_int64, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "hignn_destroy": ([_P], C.c_int),
+    "hignn_load_two_body": ([_P, C.c_char_p], C.c_int),
+    "hignn_load_two_body_mem": ([_P, C.c_int, C.POINTER(C.c_int32), _fp, C.c_int], C.c_int),
+    "hignn_set_param": ([_P, C.c_int, C.c_double], C.c_int),
+    "hignn_get_param": ([_P, C.c_int, _dp], C.c_int),
+    "hignn_update_coord": ([_P, _fp, C.c_int64], C.c_int),
+    "hignn_dot": ([_P, _fp, _fp, C.c_int64], C.c_int),
+    "hignn_dot_device": ([_P, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "hignn_dense_dot": ([_P, _fp, _fp, C.c_int64], C.c_int),
+    "hignn_dense_rows": ([_P, _dp, _fp, _i64p, C.c_int64, C.c_int], C.c_int),
+    "hignn_two_body_eval": ([_P, C.c_void_p, C.c_void_p, C.c_int64, C.c_int], C.c_int),
+    "hignn_get_stats": ([_P, C.POINTER(HignnStats)], C.c_int),
+    "hignn_get_tree": ([_P, _i64p, _i64p], C.c_int),
+    "hignn_get_lists": ([_P, _i64p, _i64p, _i64p, _i64p], C.c_int),
+    "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
+    "hignn_synchronize": ([_P], C.c_int),
+    "hignn_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
+}
+
+for _name, (_args, _res) in SIGNATURES.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+
+
+class HignnError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    lib.hignn_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise HignnError(status, last_error())
+
+
+def _f32(a, shape=None, writable=False):
+    if writable:
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous and a.flags.writeable):
+            raise TypeError("output must be a writable C-contiguous float32 array")
+        arr = a
+    else:
+        arr = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and arr.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {arr.shape}")
+    return arr
+
+
+def fptr(a):
+    return a.ctypes.data_as(_fp)
+
+
+class Model:
+    """Thin owner of a ``hignn_model*`` (one device, one stream)."""
+
+    def __init__(self, xyz, block_size=128, device=0):
+        x = _f32(xyz)
+        if x.ndim != 2 or x.shape[1] != 3:
+            raise ValueError("coordinates must have shape (n, 3)")
+        self.n = x.shape[0]
+        self._h = _P()
+        check(lib.hignn_create(fptr(x), self.n, int(block_size), int(device), C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hignn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_two_body(self, path):
+        check(lib.hignn_load_two_body(self._h, os.fsencode(path)))
+
+    def set(self, key, value):
+        check(lib.hignn_set_param(self._h, int(key), float(value)))
+
+    def get(self, key):
+        v = C.c_double()
+        check(lib.hignn_get_param(self._h, int(key), C.byref(v)))
+        return v.value
+
+    def update_coord(self, xyz):
+        x = _f32(xyz, (self.n, 3))
+        check(lib.hignn_update_coord(self._h, fptr(x), self.n))
+
+    def dot(self, f, u=None):
+        f = _f32(f, (self.n, 3))
+        if u is None:
+            u = np.empty((self.n, 3), np.float32)
+        _f32(u, (self.n, 3), writable=True)
+        check(lib.hignn_dot(self._h, fptr(u), fptr(f), self.n))
+        return u
+
+    def dot_ptr(self, u_ptr, f_ptr):
+        """Host pointers (e.g. pinned buffers) of (n, 3) float32 arrays."""
+        check(lib.hignn_dot(self._h, C.cast(u_ptr, _fp), C.cast(f_ptr, _fp), self.n))
+
+    def dot_device(self, d_u_ptr, d_f_ptr):
+        check(lib.hignn_dot_device(self._h, C.c_void_p(d_u_ptr), C.c_void_p(d_f_ptr), self.n))
+
+    def dense_dot(self, f):
+        f = _f32(f, (self.n, 3))
+        u = np.empty((self.n, 3), np.float32)
+        check(lib.hignn_dense_dot(self._h, fptr(u), fptr(f), self.n))
+        return u
+
+    def dense_rows(self, f, rows, precision=0):
+        f = _f32(f, (self.n, 3))
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        out = np.empty((rows.shape[0], 3), np.float64)
+        check(lib.hignn_dense_rows(self._h, out.ctypes.data_as(_dp), fptr(f), rows.ctypes.data_as(_i64p),
+                                   rows.shape[0], int(precision)))
+        return out
+
+    def two_body_eval(self, d_r_ptr, d_y_ptr, n, precision=0):
+        check(lib.hignn_two_body_eval(self._h, C.c_void_p(d_r_ptr), C.c_void_p(d_y_ptr), int(n), int(precision)))
+
+    def stats(self):
+        s = HignnStats()
+        check(lib.hignn_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def tree(self):
+        s = self.stats()
+        t = np.empty((s["num_nodes"], 5), np.int64)
+        p = np.empty(self.n, np.int64)
+        check(lib.hignn_get_tree(self._h, t.ctypes.data_as(_i64p), p.ctypes.data_as(_i64p)))
+        return t, p
+
+    def lists(self):
+        s = self.stats()
+        ci = np.empty(s["num_close"], np.int64)
+        cj = np.empty(s["num_close"], np.int64)
+        fi = np.empty(s["num_far"], np.int64)
+        fj = np.empty(s["num_far"], np.int64)
+        check(lib.hignn_get_lists(self._h, ci.ctypes.data_as(_i64p), cj.ctypes.data_as(_i64p),
+                                  fi.ctypes.data_as(_i64p), fj.ctypes.data_as(_i64p)))
+        return ci, cj, fi, fj
+
+    def far_pivots(self):
+        """(ranks, rows, cols) of the last far field; rows/cols are per-block lists."""
+        nf = self.stats()["num_far"]
+        ld = int(self.get(P_MAX_ITER)) + 1
+        rk = np.empty(nf, np.int32)
+        rows = np.empty((nf, ld), np.int32)
+        cols = np.empty((nf, ld), np.int32)
+        i32 = C.POINTER(C.c_int32)
+        check(lib.hignn_get_far_pivots(self._h, rk.ctypes.data_as(i32), rows.ctypes.data_as(i32),
+                                       cols.ctypes.data_as(i32), ld))
+        return rk, [list(rows[b, :rk[b]]) for b in range(nf)], [list(cols[b, :rk[b] + 1]) for b in range(nf)]
+
+    def synchronize(self):
+        check(lib.hignn_synchronize(self._h))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(lib.hignn_get_stream(self._h, C.byref(s)))
+        return s.value

@@ -1,0 +1,873 @@
+// C ABI of the native library: the model object and the HignnModel operations.
+//
+// One model = one device + one stream. The tree and lists are built on the
+// host (hignn::build_tree / build_lists); everything the matvec touches lives
+// in device memory, laid out in tree order:
+//   x4   float4[n]   positions (x, y, z, 0)          -- HignnModel::Reorder(map)
+//   perm int32[n]    tree position -> caller index    -- mReorderedMap
+//   f4   float4[n]   forces, gathered per dot
+//   u    double[3n]  velocity accumulator (FP64, src/HignnModel.cpp:555)
+// Near-field work is a list of PairWork (one per close leaf pair) consumed by a
+// persistent kernel; the far field is cut into ACA batches sized by
+// HIGNN_P_FAR_BATCH_ROWS whose C/Q pools are allocated once and reused.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/hignn_b200.h"
+#include "common.h"
+#include "kernels.h"
+#include "tree.h"
+
+using hignn::Error;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& m) { g_last_error = m; }
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return HIGNN_OK;
+  } catch (const Error& e) {
+    set_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return HIGNN_ERR_ARG;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return HIGNN_ERR_ARG;
+  }
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t b) {
+    if (b <= bytes && p) return;
+    release();
+    if (b == 0) return;
+    HIGNN_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+int host_threads() {
+  int n = 8;
+  if (const char* e = std::getenv("HIGNN_HOST_THREADS")) n = std::max(1, std::atoi(e));
+  return n;
+}
+
+}  // namespace
+
+struct hignn_model {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int64_t n = 0;
+  int block_size = 128;
+  // reference parameters (src/HignnModel.cpp:337-379)
+  double epsilon = 0.05, eta = 1.0, max_far_field_distance = 1000.0;
+  int max_iter = 100, mat_pool_size_factor = 40, max_far_dot_work_node_size = 5000;
+  int64_t max_relative_coord = 500000;
+  bool post_check = false, use_symmetry = true;
+  // this implementation
+  int precision = 0;
+  int64_t far_batch_rows = int64_t(1) << 21;
+  bool timing = false;
+  double student_tol = 1e-3;
+  int fields = 3;
+  bool record_pivots = false;
+  std::vector<int32_t> piv_rank, piv_rows, piv_cols;
+  int piv_ld = 0;
+
+  std::vector<float> xyz;  // caller order
+  hignn::ClusterTree tree;
+  hignn::BlockLists lists;
+  std::vector<float> xt;   // tree order
+  std::vector<int64_t> inv_perm;
+  bool tree_ready = false;
+  bool lists_sym = true;
+  int64_t lists_max_rel = 500000;
+
+  bool has_weights = false;
+  std::vector<float> hw;  // device-layout weights, host copy
+
+  DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, counter;
+  DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
+      far_preI, far_preJ, far_ctr, far_stats;
+  DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
+  int32_t* host_ctr = nullptr;
+
+  // far-field plan
+  struct Batch {
+    int b0, b1;
+  };
+  std::vector<hignn::FarBlock> far_plan;
+  std::vector<Batch> batches;
+  bool plan_ready = false;
+  int plan_max_iter = -1;
+  int64_t plan_rows = -1;
+  int plan_nodes = -1;
+
+  hignn_stats stats{};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  hignn::MlpF32 wdev() const {
+    hignn::MlpF32 w;
+    const float* base = weights.as<float>();
+    w.w1b1 = reinterpret_cast<const float4*>(base);
+    w.w2t = base + 4 * hignn::kH1;
+    w.b2 = w.w2t + hignn::kH1 * hignn::kH2;
+    w.w3 = w.b2 + hignn::kH2;
+    w.b3 = w.w3 + hignn::kOut * hignn::kH2;
+    return w;
+  }
+};
+
+namespace {
+
+void require_device(hignn_model* m) {
+  if (m->device < 0) throw Error(HIGNN_ERR_NODEV, "model was created without a CUDA device (host-only)");
+  HIGNN_CUDA(cudaSetDevice(m->device));
+}
+
+void build_structures(hignn_model* m) {
+  const auto t0 = std::chrono::steady_clock::now();
+  m->tree = hignn::build_tree(m->xyz.data(), m->n, m->block_size, host_threads());
+  m->xt.resize(3 * m->n);
+  m->inv_perm.resize(m->n);
+  for (int64_t i = 0; i < m->n; i++) {
+    const int64_t p = m->tree.perm[i];
+    m->xt[3 * i] = m->xyz[3 * p];
+    m->xt[3 * i + 1] = m->xyz[3 * p + 1];
+    m->xt[3 * i + 2] = m->xyz[3 * p + 2];
+    m->inv_perm[p] = i;
+  }
+  m->lists = hignn::build_lists(m->tree, m->xt.data(), m->max_relative_coord, m->use_symmetry);
+  m->lists_sym = m->use_symmetry;
+  m->lists_max_rel = m->max_relative_coord;
+  m->tree_ready = true;
+  m->plan_ready = false;
+  const auto t1 = std::chrono::steady_clock::now();
+  m->stats.t_build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  m->stats.n = m->n;
+  m->stats.num_nodes = (int64_t)m->tree.nodes.size();
+  m->stats.num_leaves = (int64_t)m->lists.leaves.size();
+  m->stats.num_close = (int64_t)m->lists.closeI.size();
+  m->stats.num_far = (int64_t)m->lists.farI.size();
+  if (m->device < 0) return;
+  // device copies
+  HIGNN_CUDA(cudaSetDevice(m->device));
+  const int64_t n = m->n;
+  std::vector<float4> x4(n);
+  std::vector<int32_t> perm(n);
+  for (int64_t i = 0; i < n; i++) {
+    x4[i] = make_float4(m->xt[3 * i], m->xt[3 * i + 1], m->xt[3 * i + 2], 0.f);
+    perm[i] = (int32_t)m->tree.perm[i];
+  }
+  m->x4.ensure(sizeof(float4) * n);
+  m->perm.ensure(sizeof(int32_t) * n);
+  m->f4.ensure(sizeof(float4) * n);
+  m->u.ensure(sizeof(double) * 3 * n);
+  m->io_f.ensure(sizeof(float) * 3 * n);
+  m->io_u.ensure(sizeof(float) * 3 * n);
+  HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
+  // close work list (src/CloseFarCheck.cpp:298-336 order)
+  std::vector<hignn::PairWork> work(m->lists.closeI.size());
+  int64_t evals = 0;
+  for (size_t q = 0; q < work.size(); q++) {
+    const auto& I = m->tree.nodes[m->lists.closeI[q]];
+    const auto& J = m->tree.nodes[m->lists.closeJ[q]];
+    hignn::PairWork w{};
+    w.sI = (int32_t)I.start;
+    w.nI = (int32_t)(I.end - I.start);
+    w.sJ = (int32_t)J.start;
+    w.nJ = (int32_t)(J.end - J.start);
+    w.flags = (m->use_symmetry && m->lists.closeJ[q] > m->lists.closeI[q]) ? hignn::kPairTransposed : 0;
+    if (w.nI > hignn::kMaxLeaf || w.nJ > hignn::kMaxLeaf)
+      throw Error(HIGNN_ERR_ARG, "leaf larger than " + std::to_string(hignn::kMaxLeaf) +
+                                     " particles; use block_size <= " + std::to_string(hignn::kMaxLeaf));
+    evals += (int64_t)w.nI * w.nJ;
+    work[q] = w;
+  }
+  m->stats.close_evals = evals;
+  m->close_work.ensure(sizeof(hignn::PairWork) * std::max<size_t>(1, work.size()));
+  if (!work.empty())
+    HIGNN_CUDA(cudaMemcpyAsync(m->close_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
+                               cudaMemcpyHostToDevice, m->stream));
+  m->counter.ensure(64);
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+}
+
+void ensure_tree(hignn_model* m) {
+  if (!m->tree_ready || m->lists_sym != m->use_symmetry || m->lists_max_rel != m->max_relative_coord)
+    build_structures(m);
+}
+
+// ACA batches: far pairs in list order, cut when the rows of the batch exceed
+// far_batch_rows or its block count exceeds max_far_dot_work_node_size.
+void ensure_far_plan(hignn_model* m) {
+  if (m->plan_ready && m->plan_max_iter == m->max_iter && m->plan_rows == m->far_batch_rows &&
+      m->plan_nodes == m->max_far_dot_work_node_size)
+    return;
+  const size_t nf = m->lists.farI.size();
+  m->far_plan.assign(nf, hignn::FarBlock{});
+  m->batches.clear();
+  int64_t rows = 0, cE = 0, qE = 0, maxC = 0, maxQ = 0;
+  int32_t rOff = 0, colOff = 0, maxR = 0, maxCol = 0;
+  int b0 = 0, maxNb = 0;
+  for (size_t q = 0; q < nf; q++) {
+    const auto& I = m->tree.nodes[m->lists.farI[q]];
+    const auto& J = m->tree.nodes[m->lists.farJ[q]];
+    const int32_t nI = (int32_t)(I.end - I.start), nJ = (int32_t)(J.end - J.start);
+    const int cnt = (int)q - b0;
+    if (cnt > 0 && (rows + nI + nJ > m->far_batch_rows || cnt >= m->max_far_dot_work_node_size)) {
+      m->batches.push_back({b0, (int)q});
+      maxNb = std::max(maxNb, cnt);
+      b0 = (int)q;
+      rows = cE = qE = 0;
+      rOff = colOff = 0;
+    }
+    hignn::FarBlock fb{};
+    fb.sI = (int32_t)I.start;
+    fb.nI = nI;
+    fb.sJ = (int32_t)J.start;
+    fb.nJ = nJ;
+    fb.kmax = std::max(1, std::min(m->max_iter, std::min(nI, nJ)));
+    fb.cOff = cE;
+    fb.qOff = qE;
+    fb.rOff = rOff;
+    fb.colOff = colOff;
+    cE += (int64_t)fb.kmax * nI;
+    qE += (int64_t)fb.kmax * nJ;
+    rOff += nI;
+    colOff += nJ;
+    rows += nI + nJ;
+    maxC = std::max(maxC, cE);
+    maxQ = std::max(maxQ, qE);
+    maxR = std::max(maxR, rOff);
+    maxCol = std::max(maxCol, colOff);
+    m->far_plan[q] = fb;
+  }
+  if (nf > 0) {
+    m->batches.push_back({b0, (int)nf});
+    maxNb = std::max(maxNb, (int)nf - b0);
+  }
+  if (m->device >= 0 && nf > 0) {
+    m->far_blocks.ensure(sizeof(hignn::FarBlock) * nf);
+    HIGNN_CUDA(cudaMemcpyAsync(m->far_blocks.p, m->far_plan.data(), sizeof(hignn::FarBlock) * nf,
+                               cudaMemcpyHostToDevice, m->stream));
+    const int ldr = m->max_iter + 1;
+    m->far_state.ensure(sizeof(hignn::FarState) * maxNb);
+    m->far_rows.ensure(sizeof(int32_t) * (size_t)maxNb * ldr);
+    m->far_cols.ensure(sizeof(int32_t) * (size_t)maxNb * ldr);
+    m->far_used_row.ensure((size_t)maxR + 16);
+    m->far_used_col.ensure((size_t)maxCol + 16);
+    m->far_C.ensure(sizeof(double) * 9 * (size_t)maxC);
+    m->far_Q.ensure(sizeof(double) * 9 * (size_t)maxQ);
+    m->far_act.ensure(sizeof(int32_t) * (maxNb + 1));
+    m->far_preI.ensure(sizeof(int32_t) * (maxNb + 1));
+    m->far_preJ.ensure(sizeof(int32_t) * (maxNb + 1));
+    m->far_ctr.ensure(sizeof(int32_t) * hignn::kCtrCount);
+    m->far_stats.ensure(sizeof(unsigned long long) * 4);
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  }
+  m->plan_ready = true;
+  m->plan_max_iter = m->max_iter;
+  m->plan_rows = m->far_batch_rows;
+  m->plan_nodes = m->max_far_dot_work_node_size;
+}
+
+void require_weights(hignn_model* m) {
+  if (!m->has_weights) throw Error(HIGNN_ERR_STATE, "no two-body model loaded (call load_two_body_model)");
+}
+
+void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,
+                    const std::vector<int>& dims) {
+  using namespace hignn;
+  if (dims.size() != 4 || dims[0] != 3 || dims[1] != kH1 || dims[2] != kH2 || dims[3] != kOut)
+    throw Error(HIGNN_ERR_ARG, "two-body network must be 3 -> 128 -> 512 -> 9 (tanh)");
+  std::vector<float>& hw = m->hw;
+  hw.assign(4 * kH1 + kH1 * kH2 + kH2 + kOut * kH2 + 16, 0.f);
+  for (int k = 0; k < kH1; k++) {
+    hw[4 * k] = W[0][3 * k];
+    hw[4 * k + 1] = W[0][3 * k + 1];
+    hw[4 * k + 2] = W[0][3 * k + 2];
+    hw[4 * k + 3] = B[0][k];
+  }
+  float* w2t = hw.data() + 4 * kH1;
+  for (int nn = 0; nn < kH2; nn++)
+    for (int k = 0; k < kH1; k++) w2t[(size_t)k * kH2 + nn] = W[1][(size_t)nn * kH1 + k];
+  float* b2 = w2t + kH1 * kH2;
+  for (int nn = 0; nn < kH2; nn++) b2[nn] = B[1][nn];
+  float* w3 = b2 + kH2;
+  for (int q = 0; q < kOut * kH2; q++) w3[q] = W[2][q];
+  float* b3 = w3 + kOut * kH2;
+  for (int q = 0; q < kOut; q++) b3[q] = B[2][q];
+  m->has_weights = true;
+  if (m->device < 0) return;
+  HIGNN_CUDA(cudaSetDevice(m->device));
+  m->weights.ensure(sizeof(float) * hw.size());
+  HIGNN_CUDA(cudaMemcpyAsync(m->weights.p, hw.data(), sizeof(float) * hw.size(), cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+}
+
+void far_field(hignn_model* m) {
+  ensure_far_plan(m);
+  m->stats.far_evals = 0;
+  m->stats.far_rank_sum = 0;
+  m->stats.far_rank_max = 0;
+  m->stats.far_iterations = 0;
+  if (m->batches.empty()) return;
+  HIGNN_CUDA(cudaMemsetAsync(m->far_stats.p, 0, sizeof(unsigned long long) * 4, m->stream));
+  const hignn::MlpF32 w = m->wdev();
+  int iterations = 0;
+  for (const auto& bt : m->batches) {
+    hignn::FarArgs a{};
+    a.blocks = m->far_blocks.as<hignn::FarBlock>() + bt.b0;
+    a.nb = bt.b1 - bt.b0;
+    a.state = m->far_state.as<hignn::FarState>();
+    a.rows = m->far_rows.as<int32_t>();
+    a.cols = m->far_cols.as<int32_t>();
+    a.ldr = m->max_iter + 1;
+    a.usedRow = m->far_used_row.as<uint8_t>();
+    a.usedCol = m->far_used_col.as<uint8_t>();
+    a.C = m->far_C.as<double>();
+    a.Q = m->far_Q.as<double>();
+    a.act = m->far_act.as<int32_t>();
+    a.preI = m->far_preI.as<int32_t>();
+    a.preJ = m->far_preJ.as<int32_t>();
+    a.ctr = m->far_ctr.as<int32_t>();
+    a.rank_sum = m->far_stats.as<unsigned long long>();
+    a.evals = m->far_stats.as<unsigned long long>() + 1;
+    a.x = m->x4.as<float4>();
+    a.f = m->f4.as<float4>();
+    a.u = m->u.as<double>();
+    a.max_iter = m->max_iter;
+    a.eps2 = m->epsilon * m->epsilon;
+    a.use_symmetry = m->use_symmetry ? 1 : 0;
+    const auto& last = m->far_plan[bt.b1 - 1];
+    HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
+    HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
+    hignn::far_batch_plain(a, w, m->num_sms, m->host_ctr, m->stream, &iterations);
+    m->stats.far_rank_max = std::max(m->stats.far_rank_max, m->host_ctr[hignn::kCtrRankMax]);
+    if (m->record_pivots) {
+      const int nb = bt.b1 - bt.b0, ld = a.ldr;
+      if (bt.b0 == 0) {
+        m->piv_ld = ld;
+        m->piv_rank.assign(m->far_plan.size(), 0);
+        m->piv_rows.assign(m->far_plan.size() * (size_t)ld, -1);
+        m->piv_cols.assign(m->far_plan.size() * (size_t)ld, -1);
+      }
+      std::vector<hignn::FarState> st(nb);
+      HIGNN_CUDA(cudaMemcpyAsync(st.data(), a.state, sizeof(hignn::FarState) * nb, cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaMemcpyAsync(m->piv_rows.data() + (size_t)bt.b0 * ld, a.rows, sizeof(int32_t) * nb * ld,
+                                 cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaMemcpyAsync(m->piv_cols.data() + (size_t)bt.b0 * ld, a.cols, sizeof(int32_t) * nb * ld,
+                                 cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+      for (int q = 0; q < nb; q++) m->piv_rank[bt.b0 + q] = st[q].k;
+    }
+  }
+  unsigned long long st[2];
+  HIGNN_CUDA(cudaMemcpyAsync(st, m->far_stats.p, sizeof(st), cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  m->stats.far_rank_sum = (int64_t)st[0];
+  m->stats.far_evals = (int64_t)st[1];
+  m->stats.far_iterations = iterations;
+}
+
+void near_field(hignn_model* m) {
+  hignn::NearArgs a{};
+  a.work = m->close_work.as<hignn::PairWork>();
+  a.nwork = (int)m->lists.closeI.size();
+  a.xI = a.xJ = m->x4.as<float4>();
+  a.fI = a.fJ = m->f4.as<float4>();
+  a.uI = a.uJ = m->u.as<double>();
+  hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+}
+
+// u (tree order, FP64) = M f for f already gathered into f4.
+void matvec_tree_order(hignn_model* m) {
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
+  if (m->fields & 1) near_field(m);
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
+  if (m->fields & 2) far_field(m);
+  if (m->timing) {
+    HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
+    HIGNN_CUDA(cudaEventSynchronize(m->ev[2]));
+    float a = 0, b = 0;
+    HIGNN_CUDA(cudaEventElapsedTime(&a, m->ev[0], m->ev[1]));
+    HIGNN_CUDA(cudaEventElapsedTime(&b, m->ev[1], m->ev[2]));
+    m->stats.t_close_ms = a;
+    m->stats.t_far_ms = b;
+    m->stats.t_dot_ms = a + b;
+  }
+}
+
+void post_check(hignn_model* m);
+
+void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
+  hignn::launch_gather_forces(d_f, m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(), m->n, m->stream);
+  matvec_tree_order(m);
+  if (m->post_check) post_check(m);
+  hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), d_u, m->n, m->stream);
+}
+
+// Dense product over all leaf pairs into m->u (tree order); f4 already gathered.
+void dense_tree_order(hignn_model* m, double* u_out) {
+  const auto& lv = m->lists.leaves;
+  std::vector<hignn::PairWork> work;
+  work.reserve(lv.size() * lv.size());
+  for (int64_t I : lv)
+    for (int64_t J : lv) {
+      const auto& a = m->tree.nodes[I];
+      const auto& b = m->tree.nodes[J];
+      hignn::PairWork w{};
+      w.sI = (int32_t)a.start;
+      w.nI = (int32_t)(a.end - a.start);
+      w.sJ = (int32_t)b.start;
+      w.nJ = (int32_t)(b.end - b.start);
+      w.flags = hignn::kPairSymmetrize;
+      work.push_back(w);
+    }
+  m->tmp_work.ensure(sizeof(hignn::PairWork) * std::max<size_t>(1, work.size()));
+  HIGNN_CUDA(cudaMemcpyAsync(m->tmp_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
+                             cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaMemsetAsync(u_out, 0, sizeof(double) * 3 * m->n, m->stream));
+  hignn::NearArgs a{};
+  a.work = m->tmp_work.as<hignn::PairWork>();
+  a.nwork = (int)work.size();
+  a.xI = a.xJ = m->x4.as<float4>();
+  a.fI = a.fJ = m->f4.as<float4>();
+  a.uI = a.uJ = u_out;
+  hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+}
+
+// PostCheckDot (src/PostCheckDot.cpp:351-377): relative L2 of the H-matrix result vs the dense product.
+void post_check(hignn_model* m) {
+  DevBuf ud;
+  ud.ensure(sizeof(double) * 3 * m->n);
+  dense_tree_order(m, ud.as<double>());
+  std::vector<double> a(3 * m->n), b(3 * m->n);
+  HIGNN_CUDA(cudaMemcpyAsync(a.data(), m->u.p, sizeof(double) * 3 * m->n, cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaMemcpyAsync(b.data(), ud.p, sizeof(double) * 3 * m->n, cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  double num = 0, den = 0;
+  for (size_t i = 0; i < a.size(); i++) {
+    num += (a[i] - b[i]) * (a[i] - b[i]);
+    den += b[i] * b[i];
+  }
+  std::printf("relative error of the H-matrix product vs the dense product: %.6e\n", std::sqrt(num / den));
+  ud.release();
+}
+
+}  // namespace
+
+extern "C" {
+
+int hignn_last_error(char* buf, size_t size) {
+  if (!buf || size == 0) return HIGNN_ERR_ARG;
+  std::snprintf(buf, size, "%s", g_last_error.c_str());
+  return HIGNN_OK;
+}
+
+int hignn_version(void) { return 100; }
+
+int hignn_create(const float* xyz, int64_t n, int block_size, int device, hignn_model** out) {
+  return guard([&] {
+    if (!out) throw Error(HIGNN_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (!xyz || n <= 0) throw Error(HIGNN_ERR_ARG, "coordinates must be a non-empty (n, 3) array");
+    if (n >= (int64_t(1) << 31)) throw Error(HIGNN_ERR_ARG, "n must be below 2^31");
+    if (block_size <= 0) throw Error(HIGNN_ERR_ARG, "block_size must be positive");
+    auto* m = new hignn_model();
+    try {
+      m->n = n;
+      m->block_size = block_size;
+      m->xyz.assign(xyz, xyz + 3 * n);
+      for (float v : m->xyz)
+        if (!std::isfinite(v)) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+      m->device = device;
+      if (device >= 0) {
+        int count = 0;
+        HIGNN_CUDA(cudaGetDeviceCount(&count));
+        if (device >= count) throw Error(HIGNN_ERR_ARG, "no CUDA device " + std::to_string(device));
+        HIGNN_CUDA(cudaSetDevice(device));
+        HIGNN_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        HIGNN_CUDA(cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, device));
+        HIGNN_CUDA(cudaMallocHost((void**)&m->host_ctr, sizeof(int32_t) * hignn::kCtrCount));
+        for (auto& e : m->ev) HIGNN_CUDA(cudaEventCreate(&e));
+      }
+      m->stats.n = n;
+    } catch (...) {
+      hignn_destroy(m);
+      throw;
+    }
+    *out = m;
+  });
+}
+
+int hignn_destroy(hignn_model* m) {
+  if (!m) return HIGNN_OK;
+  if (m->device >= 0) {
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights, &m->counter,
+                      &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
+                      &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
+                      &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
+      b->release();
+    for (auto& e : m->ev)
+      if (e) cudaEventDestroy(e);
+    if (m->host_ctr) cudaFreeHost(m->host_ctr);
+    if (m->stream) cudaStreamDestroy(m->stream);
+  }
+  delete m;
+  return HIGNN_OK;
+}
+
+int hignn_load_two_body(hignn_model* m, const char* path) {
+  return guard([&] {
+    if (!m || !path) throw Error(HIGNN_ERR_ARG, "null argument");
+    std::ifstream fh(path, std::ios::binary);
+    if (!fh) throw Error(HIGNN_ERR_IO, std::string("cannot open weight file ") + path);
+    std::vector<char> data((std::istreambuf_iterator<char>(fh)), std::istreambuf_iterator<char>());
+    auto rd32 = [&](size_t off) {
+      if (off + 4 > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
+      uint32_t v;
+      std::memcpy(&v, data.data() + off, 4);
+      return v;
+    };
+    if (data.size() < 20 || std::memcmp(data.data(), "HGNW", 4) != 0)
+      throw Error(HIGNN_ERR_IO, std::string(path) + " is not an HGNW weight file");
+    if (rd32(4) != 1) throw Error(HIGNN_ERR_IO, "unsupported HGNW version");
+    const uint32_t L = rd32(8), act = rd32(12), wrap = rd32(16);
+    if (act != 1 || wrap != 1) throw Error(HIGNN_ERR_IO, "weight file is not a tanh mobility network");
+    if (L != 3) throw Error(HIGNN_ERR_ARG, "two-body network must have 3 dense layers");
+    std::vector<int> dims;
+    size_t off = 20;
+    std::vector<std::pair<uint32_t, uint32_t>> shp;
+    for (uint32_t l = 0; l < L; l++) {
+      shp.push_back({rd32(off), rd32(off + 4)});
+      off += 8;
+    }
+    dims.push_back((int)shp[0].second);
+    for (auto& s : shp) dims.push_back((int)s.first);
+    std::vector<std::vector<float>> W, B;
+    for (auto& s : shp) {
+      const size_t nw = (size_t)s.first * s.second;
+      if (off + 4 * (nw + s.first) > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
+      std::vector<float> w(nw), b(s.first);
+      std::memcpy(w.data(), data.data() + off, 4 * nw);
+      off += 4 * nw;
+      std::memcpy(b.data(), data.data() + off, 4 * s.first);
+      off += 4 * s.first;
+      W.push_back(std::move(w));
+      B.push_back(std::move(b));
+    }
+    if (off != data.size()) throw Error(HIGNN_ERR_IO, "trailing bytes in weight file");
+    upload_weights(m, W, B, dims);
+  });
+}
+
+int hignn_load_two_body_mem(hignn_model* m, int num_layers, const int32_t* dims, const float* params,
+                            int activation) {
+  return guard([&] {
+    if (!m || !dims || !params) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (activation != 1) throw Error(HIGNN_ERR_ARG, "two-body network activation must be tanh (1)");
+    std::vector<int> d(dims, dims + num_layers + 1);
+    std::vector<std::vector<float>> W, B;
+    const float* p = params;
+    for (int l = 0; l < num_layers; l++) {
+      const size_t o = d[l + 1], i = d[l];
+      W.emplace_back(p, p + o * i);
+      p += o * i;
+      B.emplace_back(p, p + o);
+      p += o;
+    }
+    upload_weights(m, W, B, d);
+  });
+}
+
+int hignn_set_param(hignn_model* m, int key, double v) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    switch (key) {
+      case HIGNN_P_EPSILON: m->epsilon = v; break;
+      case HIGNN_P_ETA: m->eta = v; break;
+      case HIGNN_P_MAX_ITER:
+        if (v < 1 || v > hignn::kMaxIterCap)
+          throw Error(HIGNN_ERR_ARG, "max_iter must be in [1, " + std::to_string(hignn::kMaxIterCap) + "]");
+        m->max_iter = (int)v;
+        break;
+      case HIGNN_P_MAT_POOL_SIZE_FACTOR: m->mat_pool_size_factor = (int)v; break;
+      case HIGNN_P_MAX_FAR_DOT_WORK_NODE_SIZE:
+        if (v < 1) throw Error(HIGNN_ERR_ARG, "max_far_dot_work_node_size must be >= 1");
+        m->max_far_dot_work_node_size = (int)v;
+        break;
+      case HIGNN_P_MAX_RELATIVE_COORD:
+        if (v < 1) throw Error(HIGNN_ERR_ARG, "max_relative_coord must be >= 1");
+        m->max_relative_coord = (int64_t)v;
+        break;
+      case HIGNN_P_POST_CHECK_FLAG: m->post_check = v != 0; break;
+      case HIGNN_P_USE_SYMMETRY: m->use_symmetry = v != 0; break;
+      case HIGNN_P_MAX_FAR_FIELD_DISTANCE: m->max_far_field_distance = v; break;
+      case HIGNN_P_PRECISION:
+        if (v != 0 && v != 1 && v != 2) throw Error(HIGNN_ERR_ARG, "precision must be 0, 1 or 2");
+        m->precision = (int)v;
+        break;
+      case HIGNN_P_FAR_BATCH_ROWS:
+        if (v < 1024) throw Error(HIGNN_ERR_ARG, "far_batch_rows must be >= 1024");
+        m->far_batch_rows = (int64_t)v;
+        break;
+      case HIGNN_P_TIMING: m->timing = v != 0; break;
+      case HIGNN_P_STUDENT_TOL: m->student_tol = v; break;
+      case HIGNN_P_FIELDS:
+        if (v < 0 || v > 3) throw Error(HIGNN_ERR_ARG, "fields must be in [0, 3]");
+        m->fields = (int)v;
+        break;
+      case HIGNN_P_RECORD_PIVOTS: m->record_pivots = v != 0; break;
+      default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
+    }
+  });
+}
+
+int hignn_get_param(hignn_model* m, int key, double* v) {
+  return guard([&] {
+    if (!m || !v) throw Error(HIGNN_ERR_ARG, "null argument");
+    switch (key) {
+      case HIGNN_P_EPSILON: *v = m->epsilon; break;
+      case HIGNN_P_ETA: *v = m->eta; break;
+      case HIGNN_P_MAX_ITER: *v = m->max_iter; break;
+      case HIGNN_P_MAT_POOL_SIZE_FACTOR: *v = m->mat_pool_size_factor; break;
+      case HIGNN_P_MAX_FAR_DOT_WORK_NODE_SIZE: *v = m->max_far_dot_work_node_size; break;
+      case HIGNN_P_MAX_RELATIVE_COORD: *v = (double)m->max_relative_coord; break;
+      case HIGNN_P_POST_CHECK_FLAG: *v = m->post_check; break;
+      case HIGNN_P_USE_SYMMETRY: *v = m->use_symmetry; break;
+      case HIGNN_P_MAX_FAR_FIELD_DISTANCE: *v = m->max_far_field_distance; break;
+      case HIGNN_P_PRECISION: *v = m->precision; break;
+      case HIGNN_P_FAR_BATCH_ROWS: *v = (double)m->far_batch_rows; break;
+      case HIGNN_P_TIMING: *v = m->timing; break;
+      case HIGNN_P_STUDENT_TOL: *v = m->student_tol; break;
+      case HIGNN_P_FIELDS: *v = m->fields; break;
+      case HIGNN_P_RECORD_PIVOTS: *v = m->record_pivots; break;
+      default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
+    }
+  });
+}
+
+int hignn_update_coord(hignn_model* m, const float* xyz, int64_t n) {
+  return guard([&] {
+    if (!m || !xyz) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n)
+      throw Error(HIGNN_ERR_ARG, "update_coord: expected " + std::to_string(m->n) + " particles, got " +
+                                     std::to_string(n));
+    for (int64_t i = 0; i < 3 * n; i++)
+      if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+    m->xyz.assign(xyz, xyz + 3 * n);
+    build_structures(m);
+  });
+}
+
+int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n) {
+  return guard([&] {
+    if (!m || !u || !f) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n) throw Error(HIGNN_ERR_ARG, "dot: size mismatch");
+    require_device(m);
+    require_weights(m);
+    ensure_tree(m);
+    HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, m->stream));
+    dot_impl(m, m->io_u.as<float>(), m->io_f.as<float>());
+    HIGNN_CUDA(cudaMemcpyAsync(u, m->io_u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_dot_device(hignn_model* m, float* d_u, const float* d_f, int64_t n) {
+  return guard([&] {
+    if (!m || !d_u || !d_f) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n) throw Error(HIGNN_ERR_ARG, "dot: size mismatch");
+    require_device(m);
+    require_weights(m);
+    ensure_tree(m);
+    dot_impl(m, d_u, d_f);
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_dense_dot(hignn_model* m, float* u, const float* f, int64_t n) {
+  return guard([&] {
+    if (!m || !u || !f) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n) throw Error(HIGNN_ERR_ARG, "dense_dot: size mismatch");
+    require_device(m);
+    require_weights(m);
+    ensure_tree(m);
+    HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, m->stream));
+    hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
+                                n, m->stream);
+    dense_tree_order(m, m->u.as<double>());
+    hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), n, m->stream);
+    HIGNN_CUDA(cudaMemcpyAsync(u, m->io_u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
+                     int precision) {
+  return guard([&] {
+    if (!m || !u_rows || !f || (!rows && nrows > 0)) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (precision != 0) throw Error(HIGNN_ERR_ARG, "dense_rows on the device supports precision 0 (FP32 network)");
+    require_device(m);
+    require_weights(m);
+    ensure_tree(m);
+    if (nrows <= 0) return;
+    std::vector<int32_t> pos(nrows);
+    for (int64_t q = 0; q < nrows; q++) {
+      if (rows[q] < 0 || rows[q] >= m->n) throw Error(HIGNN_ERR_ARG, "row index out of range");
+      pos[q] = (int32_t)m->inv_perm[rows[q]];
+    }
+    const auto& lv = m->lists.leaves;
+    std::vector<hignn::PairWork> work;
+    for (int64_t c0 = 0; c0 < nrows; c0 += 128)
+      for (int64_t J : lv) {
+        const auto& b = m->tree.nodes[J];
+        hignn::PairWork w{};
+        w.sI = (int32_t)c0;
+        w.nI = (int32_t)std::min<int64_t>(128, nrows - c0);
+        w.sJ = (int32_t)b.start;
+        w.nJ = (int32_t)(b.end - b.start);
+        w.flags = hignn::kPairSymmetrize;
+        work.push_back(w);
+      }
+    m->tmp_pos.ensure(sizeof(int32_t) * nrows);
+    m->tmp_x.ensure(sizeof(float4) * nrows);
+    m->tmp_u.ensure(sizeof(double) * 3 * nrows);
+    m->tmp_work.ensure(sizeof(hignn::PairWork) * work.size());
+    HIGNN_CUDA(cudaMemcpyAsync(m->tmp_pos.p, pos.data(), sizeof(int32_t) * nrows, cudaMemcpyHostToDevice, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(m->tmp_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
+                               cudaMemcpyHostToDevice, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, f, sizeof(float) * 3 * m->n, cudaMemcpyHostToDevice, m->stream));
+    hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
+                                m->n, m->stream);
+    hignn::launch_gather_positions(m->x4.as<float4>(), m->tmp_pos.as<int32_t>(), m->tmp_x.as<float4>(), nrows,
+                                   m->stream);
+    HIGNN_CUDA(cudaMemsetAsync(m->tmp_u.p, 0, sizeof(double) * 3 * nrows, m->stream));
+    hignn::NearArgs a{};
+    a.work = m->tmp_work.as<hignn::PairWork>();
+    a.nwork = (int)work.size();
+    a.xI = m->tmp_x.as<float4>();
+    a.fI = m->tmp_x.as<float4>();  // unused without the transposed update
+    a.uI = m->tmp_u.as<double>();
+    a.xJ = m->x4.as<float4>();
+    a.fJ = m->f4.as<float4>();
+    a.uJ = m->u.as<double>();
+    hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+    HIGNN_CUDA(cudaMemcpyAsync(u_rows, m->tmp_u.p, sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_two_body_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n, int precision) {
+  return guard([&] {
+    if (!m || (!d_r && n > 0) || (!d_y && n > 0)) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (precision != 0) throw Error(HIGNN_ERR_ARG, "unsupported precision");
+    require_device(m);
+    require_weights(m);
+    hignn::launch_eval_simt(d_r, d_y, n, m->wdev(), m->num_sms, m->stream);
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_get_stats(hignn_model* m, hignn_stats* out) {
+  return guard([&] {
+    if (!m || !out) throw Error(HIGNN_ERR_ARG, "null argument");
+    ensure_tree(m);
+    *out = m->stats;
+  });
+}
+
+int hignn_get_tree(hignn_model* m, int64_t* tree5, int64_t* perm) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    ensure_tree(m);
+    if (tree5)
+      for (size_t i = 0; i < m->tree.nodes.size(); i++) {
+        const auto& t = m->tree.nodes[i];
+        tree5[5 * i] = t.child0;
+        tree5[5 * i + 1] = t.child1;
+        tree5[5 * i + 2] = t.start;
+        tree5[5 * i + 3] = t.end;
+        tree5[5 * i + 4] = t.level;
+      }
+    if (perm) std::copy(m->tree.perm.begin(), m->tree.perm.end(), perm);
+  });
+}
+
+int hignn_get_lists(hignn_model* m, int64_t* ci, int64_t* cj, int64_t* fi, int64_t* fj) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    ensure_tree(m);
+    if (ci) std::copy(m->lists.closeI.begin(), m->lists.closeI.end(), ci);
+    if (cj) std::copy(m->lists.closeJ.begin(), m->lists.closeJ.end(), cj);
+    if (fi) std::copy(m->lists.farI.begin(), m->lists.farI.end(), fi);
+    if (fj) std::copy(m->lists.farJ.begin(), m->lists.farJ.end(), fj);
+  });
+}
+
+int hignn_get_far_pivots(hignn_model* m, int32_t* ranks, int32_t* rows, int32_t* cols, int ld) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    if (m->piv_rank.size() != m->lists.farI.size() || m->piv_ld == 0)
+      throw Error(HIGNN_ERR_STATE, "no pivots recorded (set HIGNN_P_RECORD_PIVOTS and run a dot)");
+    if (ld < m->piv_ld) throw Error(HIGNN_ERR_ARG, "ld must be >= max_iter + 1");
+    const size_t nf = m->piv_rank.size();
+    if (ranks) std::copy(m->piv_rank.begin(), m->piv_rank.end(), ranks);
+    for (size_t b = 0; b < nf; b++)
+      for (int l = 0; l < m->piv_ld; l++) {
+        if (rows) rows[b * ld + l] = m->piv_rows[b * m->piv_ld + l];
+        if (cols) cols[b * ld + l] = m->piv_cols[b * m->piv_ld + l];
+      }
+  });
+}
+
+int hignn_synchronize(hignn_model* m) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    if (m->device >= 0) {
+      HIGNN_CUDA(cudaSetDevice(m->device));
+      HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    }
+  });
+}
+
+int hignn_get_stream(hignn_model* m, void** stream) {
+  return guard([&] {
+    if (!m || !stream) throw Error(HIGNN_ERR_ARG, "null argument");
+    *stream = (void*)m->stream;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// Shared definitions of the native library (host and device).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace hignn {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HIGNN_CUDA(call)                                                                              \
+  do {                                                                                                \
+    cudaError_t _e = (call);                                                                          \
+    if (_e != cudaSuccess)                                                                            \
+      throw ::hignn::Error(-2, std::string(#call " failed: ") + cudaGetErrorString(_e) + " at " +   \
+                                   __FILE__ + ":" + std::to_string(__LINE__));                      \
+  } while (0)
+
+#define HIGNN_CHECK_LAUNCH() HIGNN_CUDA(cudaGetLastError())
+
+constexpr int kMaxLeaf = 256;   // largest leaf the near-field kernels stage in shared memory
+constexpr int kH1 = 128;        // two-body network widths (python/convert.py:6-20 over nn/*.pkl)
+constexpr int kH2 = 512;
+constexpr int kOut = 9;
+
+// FP32 weights of the two-body network as the SIMT kernels read them.
+struct MlpF32 {
+  const float4* w1b1;  // [kH1]: (W1[k][0], W1[k][1], W1[k][2], b1[k])
+  const float* w2t;    // [kH1][kH2]: w2t[k*kH2 + n] = W2[n][k]
+  const float* b2;     // [kH2]
+  const float* w3;     // [kOut][kH2]
+  const float* b3;     // [kOut]
+};
+
+// One unit of near-field (or dense) work: target range I against source range J.
+constexpr int32_t kPairTransposed = 1;  // also u_J += M f_I (symmetric close pair, J > I)
+constexpr int32_t kPairSymmetrize = 2;  // use 0.5 (M + M^T) (dense product)
+struct PairWork {
+  int32_t sI, nI, sJ, nJ, flags, pad0, pad1, pad2;
+};
+
+}  // namespace hignn

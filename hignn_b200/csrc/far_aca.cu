@@ -1,0 +1,569 @@
+// Plain FP32 far field: adaptive cross approximation with FP64 bookkeeping.
+//
+// Restates HignnModel::FarDot (src/FarDot.cpp:64-1696). Each admissible block
+// A(i, j) = 0.5 (M + M^T)(x_j - x_i), i in I, j in J, is approximated by
+// sum_l C_l(i) Q_l(j) (3x3 blocks) with the reference's rules:
+//   * first column |J|/2 (:257); column query, symmetrised 3x3 (:348-458);
+//   * C_k -= sum_{l<k} C_l Q_l(jk) (:474-512); row pivot = max signed det over
+//     unused rows (:520-576); C_k <- C_k inv(C_k(ik)) by adjugate (:586-656);
+//   * row query (:672-781); Q_k -= sum_{l<k} C_l(ik) Q_l (:797-841); next
+//     column = max signed det over columns not yet used, current included (:846-903);
+//   * nu2 = ||C_k Q_k||_F^2; mu2 += nu2 + sum_{l<k-1} 2 |C_k^T C_l| |Q_k Q_l^T|
+//     (:919-1078); stop when nu2 < mu2 eps^2, k >= maxIter or k >= min(|I|,|J|);
+//   * apply u_I += sum_l C_l (Q_l f_J), u_J += sum_l Q_l^T (C_l^T f_I) (:1194-1388).
+// The reference compacts converged blocks out of its arrays with O(w^2)
+// launches; here every block carries its own iteration counter and an active
+// list is rebuilt by one CTA per iteration. This file is compiled with
+// -fmad=false so the FP64 determinant, inverse and products round as written.
+#include <cfloat>
+
+#include "common.h"
+#include "kernels.h"
+#include "mlp_simt.cuh"
+
+namespace hignn {
+
+namespace {
+
+constexpr int kPivThreads = 256;
+
+__device__ __forceinline__ double det3(const double* m) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// argmax with the first index winning ties (Kokkos MaxLoc over a strict '>').
+__device__ __forceinline__ void better(double& v, int& i, double v2, int i2) {
+  if (i2 >= 0 && (i < 0 || v2 > v || (v2 == v && i2 < i))) {
+    v = v2;
+    i = i2;
+  }
+}
+
+__device__ void block_argmax(double& v, int& i, double* sv, int* si) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    int i2 = __shfl_down_sync(0xffffffffu, i, o);
+    better(v, i, v2, i2);
+  }
+  if (lane == 0) {
+    sv[wid] = v;
+    si[wid] = i;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bv = sv[0];
+    int bi = si[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) better(bv, bi, sv[w], si[w]);
+    sv[0] = bv;
+    si[0] = bi;
+  }
+  __syncthreads();
+  v = sv[0];
+  i = si[0];
+  __syncthreads();
+}
+
+template <int N>
+__device__ void block_sum(double (&v)[N], double* scratch /* [32][N] */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < N; q++)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < N; q++) scratch[wid * N + q] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int q = 0; q < N; q++) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w * N + q];
+      scratch[q] = s;
+    }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < N; q++) v[q] = scratch[q];
+  __syncthreads();
+}
+
+__global__ void k_far_init(FarArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0) {
+    a.ctr[kCtrRemaining] = a.nb;
+    a.ctr[kCtrError] = 0;
+    a.ctr[kCtrRankMax] = 0;
+  }
+  if (b >= a.nb) return;
+  a.state[b].k = 0;
+  a.state[b].done = 0;
+  a.state[b].mu2 = 0.0;
+  a.state[b].nu2 = 0.0;
+  a.cols[(size_t)b * a.ldr] = a.blocks[b].nJ / 2;
+}
+
+// Active list and prefix sums of |I| and |J| over active blocks (one CTA).
+__global__ void __launch_bounds__(1024) k_far_active(FarArgs a) {
+  __shared__ int sA[32], sI[32], sJ[32];
+  __shared__ int baseA, baseI, baseJ;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  if (t == 0) baseA = baseI = baseJ = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < a.nb; b0 += 1024) {
+    const int b = b0 + t;
+    const bool act = b < a.nb && !a.state[b].done;
+    int vA = act ? 1 : 0, vI = act ? a.blocks[b].nI : 0, vJ = act ? a.blocks[b].nJ : 0;
+    int xA = vA, xI = vI, xJ = vJ;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      int yA = __shfl_up_sync(0xffffffffu, xA, o), yI = __shfl_up_sync(0xffffffffu, xI, o),
+          yJ = __shfl_up_sync(0xffffffffu, xJ, o);
+      if (lane >= o) {
+        xA += yA;
+        xI += yI;
+        xJ += yJ;
+      }
+    }
+    if (lane == 31) {
+      sA[wid] = xA;
+      sI[wid] = xI;
+      sJ[wid] = xJ;
+    }
+    __syncthreads();
+    if (wid == 0) {
+      int zA = sA[lane], zI = sI[lane], zJ = sJ[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        int yA = __shfl_up_sync(0xffffffffu, zA, o), yI = __shfl_up_sync(0xffffffffu, zI, o),
+            yJ = __shfl_up_sync(0xffffffffu, zJ, o);
+        if (lane >= o) {
+          zA += yA;
+          zI += yI;
+          zJ += yJ;
+        }
+      }
+      sA[lane] = zA;
+      sI[lane] = zI;
+      sJ[lane] = zJ;
+    }
+    __syncthreads();
+    const int offA = baseA + (wid ? sA[wid - 1] : 0) + xA - vA;
+    const int offI = baseI + (wid ? sI[wid - 1] : 0) + xI - vI;
+    const int offJ = baseJ + (wid ? sJ[wid - 1] : 0) + xJ - vJ;
+    if (act) {
+      a.act[offA] = b;
+      a.preI[offA] = offI;
+      a.preJ[offA] = offJ;
+    }
+    __syncthreads();
+    if (t == 0) {
+      baseA += sA[31];
+      baseI += sI[31];
+      baseJ += sJ[31];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    a.preI[baseA] = baseI;
+    a.preJ[baseA] = baseJ;
+    a.ctr[kCtrActive] = baseA;
+    a.ctr[kCtrTotI] = baseI;
+    a.ctr[kCtrTotJ] = baseJ;
+  }
+}
+
+struct EvalSmem {
+  simt::Smem mlp;
+  int32_t blk[simt::kTile];
+  int32_t loc[simt::kTile];
+};
+
+// Column (which = 0) or row (which = 1) queries of every active block, 128 per tile.
+__global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF32 w, int which) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  EvalSmem& s = *reinterpret_cast<EvalSmem*>(smem_raw);
+  const int t = threadIdx.x;
+  const int nact = a.ctr[kCtrActive];
+  const int tot = which ? a.ctr[kCtrTotJ] : a.ctr[kCtrTotI];
+  const int32_t* pre = which ? a.preJ : a.preI;
+  if ((int)blockIdx.x * simt::kTile >= tot) return;
+  simt::load_weights(s.mlp, w);
+  for (int tile = blockIdx.x; tile * simt::kTile < tot; tile += gridDim.x) {
+    if (t < simt::kTile) {
+      const int e = tile * simt::kTile + t;
+      if (e < tot) {
+        int lo = 0, hi = nact;  // last active index with pre[idx] <= e
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (pre[mid] <= e)
+            lo = mid;
+          else
+            hi = mid;
+        }
+        const int b = a.act[lo];
+        const int loc = e - pre[lo];
+        const FarBlock bk = a.blocks[b];
+        const int k = a.state[b].k;
+        float4 xi, xj;
+        if (which == 0) {
+          xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
+          xi = a.x[bk.sI + loc];
+        } else {
+          xj = a.x[bk.sJ + loc];
+          xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
+        }
+        s.mlp.r[t] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, 0.f);
+        s.blk[t] = b;
+        s.loc[t] = loc;
+      } else {
+        s.mlp.r[t] = make_float4(1.f, 0.f, 0.f, 0.f);
+        s.blk[t] = -1;
+      }
+    }
+    __syncthreads();
+    simt::mlp_tile(s.mlp, w);
+    if (t < simt::kTile && s.blk[t] >= 0) {
+      const int b = s.blk[t], loc = s.loc[t];
+      const FarBlock bk = a.blocks[b];
+      const int k = a.state[b].k;
+      double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
+                               : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
+      const float* y = s.mlp.y[t];
+      // src/FarDot.cpp:445-456: diagonal copied, off-diagonal 0.5 * (float sum)
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          if (r == c)
+            dst[3 * r + c] = (double)y[3 * r + c];
+          else
+            dst[3 * r + c] = 0.5 * (double)(y[3 * r + c] + y[3 * c + r]);
+        }
+    }
+  }
+  if (t == 0 && blockIdx.x == 0) atomicAdd(a.evals, (unsigned long long)tot);
+}
+
+// Orthogonalise the new column, pick the pivot row, normalise (one CTA per active block).
+__global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
+  extern __shared__ __align__(16) double dsm[];
+  double* qj = dsm;  // [k][9]
+  __shared__ double sv[32], inv[9];
+  __shared__ int si[32];
+  const int ai = blockIdx.x;
+  if (ai >= a.ctr[kCtrActive]) return;
+  const int b = a.act[ai];
+  const FarBlock bk = a.blocks[b];
+  const int k = a.state[b].k;
+  const int jk = a.cols[(size_t)b * a.ldr + k];
+  for (int q = threadIdx.x; q < 9 * k; q += blockDim.x) {
+    const int l = q / 9, e = q - (q / 9) * 9;
+    qj[q] = a.Q[9 * (bk.qOff + (int64_t)l * bk.nJ + jk) + e];
+  }
+  __syncthreads();
+  double best = -DBL_MAX;
+  int bi = -1;
+  double* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
+  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+    double c[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
+    if (k > 0) {
+      double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int l = 0; l < k; l++) {
+        const double* cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+        const double* ql = qj + 9 * l;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+            for (int m = 0; m < 3; m++) s[3 * r + cc] += cl[3 * r + m] * ql[3 * m + cc];
+      }
+#pragma unroll
+      for (int q = 0; q < 9; q++) {
+        c[q] -= s[q];
+        Ck[9 * i + q] = c[q];
+      }
+    }
+    const double d = det3(c);
+    if (!a.usedRow[bk.rOff + i] && (bi < 0 || d > best)) {
+      best = d;
+      bi = i;
+    }
+  }
+  block_argmax(best, bi, sv, si);
+  if (bi < 0) {
+    if (threadIdx.x == 0) {
+      a.ctr[kCtrError] = 1;
+      a.rows[(size_t)b * a.ldr + k] = 0;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    a.rows[(size_t)b * a.ldr + k] = bi;
+    a.usedRow[bk.rOff + bi] = 1;
+    const double* m = Ck + 9 * bi;
+    const double A = m[0], B = m[1], C = m[2], D = m[3], E = m[4], F = m[5], G = m[6], H = m[7], I = m[8];
+    const double det = A * (E * I - F * H) - B * (D * I - F * G) + C * (D * H - E * G);
+    inv[0] = (E * I - F * H) / det;
+    inv[1] = -(B * I - C * H) / det;
+    inv[2] = (B * F - C * E) / det;
+    inv[3] = -(D * I - F * G) / det;
+    inv[4] = (A * I - C * G) / det;
+    inv[5] = -(A * F - C * D) / det;
+    inv[6] = (D * H - E * G) / det;
+    inv[7] = -(A * H - B * G) / det;
+    inv[8] = (A * E - B * D) / det;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+    double c[9], o[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int cc = 0; cc < 3; cc++) {
+        double acc = c[3 * r] * inv[cc];
+        acc = acc + c[3 * r + 1] * inv[3 + cc];
+        acc = acc + c[3 * r + 2] * inv[6 + cc];
+        o[3 * r + cc] = acc;
+      }
+#pragma unroll
+    for (int q = 0; q < 9; q++) Ck[9 * i + q] = o[q];
+  }
+}
+
+// Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
+__global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
+  extern __shared__ __align__(16) double dsm[];
+  double* ci = dsm;                          // [k][9]
+  double* mid = dsm + 9 * kMaxIterCap;       // [rank][3]
+  double* mid2 = mid + 3 * kMaxIterCap;      // [rank][3]
+  __shared__ double sv[32], cross[8][18], red[32 * 12];
+  __shared__ int si[32];
+  __shared__ int s_done, s_rank;
+  const int ai = blockIdx.x;
+  if (ai >= a.ctr[kCtrActive]) return;
+  const int b = a.act[ai];
+  const FarBlock bk = a.blocks[b];
+  const int k = a.state[b].k;
+  const int ik = a.rows[(size_t)b * a.ldr + k];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int q = threadIdx.x; q < 9 * k; q += blockDim.x) {
+    const int l = q / 9, e = q - (q / 9) * 9;
+    ci[q] = a.C[9 * (bk.cOff + (int64_t)l * bk.nI + ik) + e];
+  }
+  if (threadIdx.x == 0) a.usedCol[bk.colOff + a.cols[(size_t)b * a.ldr + k]] = 1;
+  __syncthreads();
+  double best = -DBL_MAX;
+  int bj = -1;
+  double* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
+  for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
+    double q[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) q[e] = Qk[9 * j + e];
+    if (k > 0) {
+      double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int l = 0; l < k; l++) {
+        const double* ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+        const double* cl = ci + 9 * l;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+            for (int m = 0; m < 3; m++) s[3 * r + cc] += cl[3 * r + m] * ql[3 * m + cc];
+      }
+#pragma unroll
+      for (int e = 0; e < 9; e++) {
+        q[e] -= s[e];
+        Qk[9 * j + e] = q[e];
+      }
+    }
+    const double d = det3(q);
+    if (!a.usedCol[bk.colOff + j] && (bj < 0 || d > best)) {
+      best = d;
+      bj = j;
+    }
+  }
+  block_argmax(best, bj, sv, si);  // contains __syncthreads: Q_k writes are visible below
+  // nu2 = ||C_k Q_k||_F^2 from column norms/dots of C_k and row norms/dots of Q_k
+  const double* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
+  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+    const double* c = Ck + 9 * i;
+#pragma unroll
+    for (int cc = 0; cc < 3; cc++) {
+      v[cc] += c[cc] * c[cc] + c[cc + 3] * c[cc + 3] + c[cc + 6] * c[cc + 6];
+      const int c1 = (cc + 1) % 3;
+      v[3 + cc] += c[cc] * c[c1] + c[cc + 3] * c[c1 + 3] + c[cc + 6] * c[c1 + 6];
+    }
+  }
+  for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
+    const double* q = Qk + 9 * j;
+    v[6] += q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    v[7] += q[3] * q[3] + q[4] * q[4] + q[5] * q[5];
+    v[8] += q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
+    v[9] += q[0] * q[3] + q[1] * q[4] + q[2] * q[5];
+    v[10] += q[3] * q[6] + q[4] * q[7] + q[5] * q[8];
+    v[11] += q[6] * q[0] + q[7] * q[1] + q[8] * q[2];
+  }
+  block_sum<12>(v, red);
+  const double nu2 = v[0] * v[6] + v[1] * v[7] + v[2] * v[8] + 2.0 * v[9] * v[3] + 2.0 * v[10] * v[4] +
+                     2.0 * v[11] * v[5];
+  double mu2 = a.state[b].mu2 + nu2;  // every thread tracks the same value; thread 0 stores it
+  // cross terms for l < k - 1 (src/FarDot.cpp:1041-1077), eight l per pass, one warp per l
+  for (int lb = 0; lb < k - 1; lb += 8) {
+    const int l = lb + wid;
+    if (wid < 8 && l < k - 1) {
+      double acc[18];
+#pragma unroll
+      for (int q = 0; q < 18; q++) acc[q] = 0.0;
+      const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
+      const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
+      for (int i = lane; i < bk.nI; i += 32) {
+        const double* c = Ck + 9 * i;
+        const double* d = Cl + 9 * i;
+#pragma unroll
+        for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+          for (int d2 = 0; d2 < 3; d2++)
+            acc[3 * d1 + d2] += c[d1] * d[d2] + c[d1 + 3] * d[d2 + 3] + c[d1 + 6] * d[d2 + 6];
+      }
+      for (int j = lane; j < bk.nJ; j += 32) {
+        const double* q = Qk + 9 * j;
+        const double* p = Ql + 9 * j;
+#pragma unroll
+        for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+          for (int d2 = 0; d2 < 3; d2++)
+            acc[9 + 3 * d1 + d2] += q[3 * d1] * p[3 * d2] + q[3 * d1 + 1] * p[3 * d2 + 1] +
+                                    q[3 * d1 + 2] * p[3 * d2 + 2];
+      }
+#pragma unroll
+      for (int q = 0; q < 18; q++)
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 18; q++) cross[wid][q] = acc[q];
+    }
+    __syncthreads();
+    for (int ww = 0; ww < 8 && lb + ww < k - 1; ww++)
+      for (int q = 0; q < 9; q++) mu2 += 2.0 * fabs(cross[ww][q]) * fabs(cross[ww][9 + q]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int k1 = k + 1;
+    const int mn = bk.nI < bk.nJ ? bk.nI : bk.nJ;
+    int done = (nu2 < mu2 * a.eps2) || k1 >= a.max_iter || k1 >= mn;
+    if (!done && bj < 0) {  // no unused column left: cannot continue
+      done = 1;
+      a.ctr[kCtrError] = 2;
+    }
+    a.state[b].nu2 = nu2;
+    a.state[b].mu2 = mu2;
+    a.state[b].k = k1;
+    if (k1 < a.ldr) a.cols[(size_t)b * a.ldr + k1] = bj < 0 ? 0 : bj;
+    if (done) {
+      a.state[b].done = 1;
+      atomicSub(&a.ctr[kCtrRemaining], 1);
+      atomicMax(&a.ctr[kCtrRankMax], k1);
+      atomicAdd(a.rank_sum, (unsigned long long)k1);
+    }
+    s_done = done;
+    s_rank = k1;
+  }
+  __syncthreads();
+  if (!s_done) return;
+  // ---- apply (src/FarDot.cpp:1225-1387), rank = k + 1 terms
+  const int rank = s_rank;
+  for (int l = wid; l < rank; l += blockDim.x >> 5) {
+    const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
+    const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
+    double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
+    for (int j = lane; j < bk.nJ; j += 32) {
+      const float4 fj = a.f[bk.sJ + j];
+      const double* q = Ql + 9 * j;
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        m[r] += q[3 * r] * (double)fj.x + q[3 * r + 1] * (double)fj.y + q[3 * r + 2] * (double)fj.z;
+    }
+    if (a.use_symmetry)
+      for (int i = lane; i < bk.nI; i += 32) {
+        const float4 fi = a.f[bk.sI + i];
+        const double* c = Cl + 9 * i;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+          m2[r] += c[r] * (double)fi.x + c[3 + r] * (double)fi.y + c[6 + r] * (double)fi.z;
+      }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      for (int o = 16; o > 0; o >>= 1) {
+        m[r] += __shfl_down_sync(0xffffffffu, m[r], o);
+        m2[r] += __shfl_down_sync(0xffffffffu, m2[r], o);
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        mid[3 * l + r] = m[r];
+        mid2[3 * l + r] = m2[r];
+      }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+    double acc[3] = {0, 0, 0};
+    for (int l = 0; l < rank; l++) {
+      const double* c = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        acc[r] += c[3 * r] * mid[3 * l] + c[3 * r + 1] * mid[3 * l + 1] + c[3 * r + 2] * mid[3 * l + 2];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sI + i) + r], acc[r]);
+  }
+  if (a.use_symmetry)
+    for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
+      double acc[3] = {0, 0, 0};
+      for (int l = 0; l < rank; l++) {
+        const double* q = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+          acc[r] += q[r] * mid2[3 * l] + q[3 + r] * mid2[3 * l + 1] + q[6 + r] * mid2[3 * l + 2];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sJ + j) + r], acc[r]);
+    }
+}
+
+}  // namespace
+
+void far_batch_plain(const FarArgs& a, const MlpF32& w, int num_sms, int32_t* host_ctr, cudaStream_t s,
+                     int* iterations) {
+  if (a.nb <= 0) return;
+  const size_t eval_smem = sizeof(EvalSmem);
+  const size_t row_smem = sizeof(double) * (9 + 3 + 3) * kMaxIterCap;
+  const size_t col_smem = sizeof(double) * 9 * kMaxIterCap;
+  HIGNN_CUDA(cudaFuncSetAttribute(k_far_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem));
+  HIGNN_CUDA(cudaFuncSetAttribute(k_far_row_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
+  HIGNN_CUDA(cudaFuncSetAttribute(k_far_col_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+  k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
+  HIGNN_CHECK_LAUNCH();
+  int it = 0;
+  for (; it <= a.max_iter; it++) {
+    k_far_active<<<1, 1024, 0, s>>>(a);
+    k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
+    k_far_col_pivot<<<a.nb, kPivThreads, col_smem, s>>>(a);
+    k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
+    k_far_row_pivot<<<a.nb, kPivThreads, row_smem, s>>>(a);
+    HIGNN_CHECK_LAUNCH();
+    HIGNN_CUDA(cudaMemcpyAsync(host_ctr, a.ctr, sizeof(int32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
+    HIGNN_CUDA(cudaStreamSynchronize(s));
+    if (host_ctr[kCtrError] != 0)
+      throw Error(-5, "ACA: pivot search found no unused row/column (non-finite block entries?)");
+    if (host_ctr[kCtrRemaining] == 0) break;
+  }
+  if (host_ctr[kCtrRemaining] != 0) throw Error(-5, "ACA did not converge within max_iter iterations");
+  if (iterations) *iterations += it + 1;
+}
+
+}  // namespace hignn

@@ -1,0 +1,79 @@
+// Kernel argument blocks and launchers of the native library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace hignn {
+
+constexpr int kMaxIterCap = 512;  // largest ACA iteration cap (set_max_iter) the kernels accept
+
+// ---------------------------------------------------------------- near field / dense
+struct NearArgs {
+  const PairWork* work;
+  int nwork;
+  const float4* xI;  // target positions (x, y, z, 0)
+  const float4* fI;  // target forces
+  double* uI;        // target velocities, (n, 3) FP64
+  const float4* xJ;  // source positions
+  const float4* fJ;
+  double* uJ;
+};
+
+size_t near_simt_smem_bytes();
+void launch_near_simt(const NearArgs& a, const MlpF32& w, int* work_counter, int num_sms, cudaStream_t s);
+
+// ---------------------------------------------------------------- far field (ACA)
+struct FarBlock {
+  int32_t sI, nI, sJ, nJ;
+  int64_t cOff, qOff;      // batch-relative entry offsets into the C / Q pools
+  int32_t rOff, colOff;    // batch-relative offsets into the used-row / used-column flags
+  int32_t kmax, pad;       // min(max_iter, nI, nJ)
+};
+
+struct FarState {
+  int32_t k, done;
+  double mu2, nu2;
+};
+
+// Counters kept on the device per batch.
+enum FarCtr { kCtrActive = 0, kCtrTotI, kCtrTotJ, kCtrRemaining, kCtrError, kCtrRankMax, kCtrCount = 8 };
+
+struct FarArgs {
+  const FarBlock* blocks;
+  int nb;
+  FarState* state;
+  int32_t* rows;      // [nb][ldr]
+  int32_t* cols;      // [nb][ldr]
+  int ldr;            // max_iter + 1
+  uint8_t* usedRow;
+  uint8_t* usedCol;
+  double* C;          // [entries][9]
+  double* Q;
+  int32_t* act;       // active block list
+  int32_t* preI;      // exclusive prefix of nI over active blocks (nact + 1)
+  int32_t* preJ;
+  int32_t* ctr;       // FarCtr counters
+  unsigned long long* rank_sum;
+  unsigned long long* evals;
+  const float4* x;
+  const float4* f;
+  double* u;
+  int max_iter;
+  double eps2;
+  int use_symmetry;
+};
+
+void far_batch_plain(const FarArgs& a, const MlpF32& w, int num_sms, int32_t* host_ctr, cudaStream_t s,
+                     int* iterations);
+
+// ---------------------------------------------------------------- reorder / misc
+void launch_gather_forces(const float* f, const int32_t* perm, float4* f4, double* u, int64_t n, cudaStream_t s);
+void launch_scatter_velocities(const double* u, const int32_t* perm, float* out, int64_t n, cudaStream_t s);
+void launch_eval_simt(const float* r, float* y, int64_t n, const MlpF32& w, int num_sms, cudaStream_t s);
+void launch_gather_positions(const float4* x4, const int32_t* pos, float4* out, int64_t n, cudaStream_t s);
+
+}  // namespace hignn

@@ -1,0 +1,153 @@
+/*
+ * hignn_b200 -- C ABI of the B200-native H-HIGNN mobility matvec U = M(x) F.
+ *
+ * Each entry point replaces a method of the reference's HignnModel, which its
+ * pybind11 module `hignn` exposes (interface/HignnInterface.cpp:17-35). Plain
+ * pointers and sizes only; every call returns an int status (0 = ok, < 0 =
+ * error) and hignn_last_error() gives the message of the calling thread's last
+ * failure. A model owns one CUDA stream on its device; calls on one model are
+ * not thread-safe, calls on different models are. Host arrays are (n, 3)
+ * row-major float32 in the caller's particle order, as the reference's numpy
+ * arrays are (src/HignnModel.cpp:569-570).
+ */
+#ifndef HIGNN_B200_H
+#define HIGNN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HIGNN_OK 0
+#define HIGNN_ERR_ARG (-1)     /* bad argument: null pointer, size mismatch, bad key   */
+#define HIGNN_ERR_CUDA (-2)    /* a CUDA runtime call failed                             */
+#define HIGNN_ERR_STATE (-3)   /* call out of order: no weights, no tree, no device    */
+#define HIGNN_ERR_IO (-4)      /* weight file missing or malformed                       */
+#define HIGNN_ERR_LIMIT (-5)   /* a device loop hit its iteration cap; see message       */
+#define HIGNN_ERR_NODEV (-6)   /* model was created without a device (host-only)        */
+
+typedef struct hignn_model hignn_model;
+
+/* Parameter keys for hignn_set_param / hignn_get_param. The first nine are the
+ * reference's setters (src/HignnModel.cpp:773-874), defaults from its
+ * constructor (src/HignnModel.cpp:337-379). */
+enum hignn_param {
+  HIGNN_P_EPSILON = 0,                    /* ACA tolerance, default 0.05                 */
+  HIGNN_P_ETA = 1,                        /* stored, unused (as in the reference)       */
+  HIGNN_P_MAX_ITER = 2,                   /* ACA iteration cap, default 100              */
+  HIGNN_P_MAT_POOL_SIZE_FACTOR = 3,       /* stored; pools here are sized per batch     */
+  HIGNN_P_MAX_FAR_DOT_WORK_NODE_SIZE = 4, /* max far blocks per ACA batch, default 5000 */
+  HIGNN_P_MAX_RELATIVE_COORD = 5,         /* far-size gate of the close/far check, 500000 */
+  HIGNN_P_POST_CHECK_FLAG = 6,            /* dense re-check after each dot, default 0   */
+  HIGNN_P_USE_SYMMETRY = 7,               /* J >= I lists + transposed update, default 1 */
+  HIGNN_P_MAX_FAR_FIELD_DISTANCE = 8,     /* stored, unused (as in the reference)       */
+  /* keys of this implementation */
+  HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field */
+  HIGNN_P_FAR_BATCH_ROWS = 101,  /* rows (sum of |I|+|J|) per ACA batch, default 1<<21       */
+  HIGNN_P_TIMING = 102,          /* 1 = record per-phase CUDA-event times in hignn_stats     */
+  HIGNN_P_STUDENT_TOL = 103,     /* sampled-residual fallback threshold of the student, 1e-3 */
+  HIGNN_P_FIELDS = 104,          /* bit 0 = near field, bit 1 = far field (default 3), for diagnostics */
+  HIGNN_P_RECORD_PIVOTS = 105    /* 1 = keep every far block's ACA rank and pivots (hignn_get_far_pivots) */
+};
+
+typedef struct hignn_stats {
+  int64_t n;               /* particles                                          */
+  int64_t num_nodes;       /* cluster-tree rows (orphan rows 1, 2 included)      */
+  int64_t num_leaves;
+  int64_t num_close;       /* close leaf pairs in the list (J >= I with symmetry) */
+  int64_t num_far;         /* far node pairs in the list                         */
+  int64_t close_evals;     /* two-body evaluations of the last near field       */
+  int64_t far_evals;       /* two-body evaluations of the last ACA               */
+  int64_t far_rank_sum;    /* sum of ACA ranks of the last far field            */
+  int32_t far_rank_max;
+  int32_t far_iterations;  /* ACA iterations summed over batches                 */
+  int64_t student_fallback_blocks; /* far blocks that fell back to the teacher   */
+  double t_build_ms;       /* host tree + lists of the last update_coord        */
+  double t_close_ms;       /* device time of the last near field (TIMING = 1)   */
+  double t_far_ms;         /* device time of the last far field (TIMING = 1)    */
+  double t_dot_ms;         /* device time of the last dot (TIMING = 1)          */
+} hignn_stats;
+
+/* Message of the calling thread's last error (empty string if none). */
+int hignn_last_error(char* buf, size_t size);
+
+/* Library version, e.g. 100 for 0.1.0. */
+int hignn_version(void);
+
+/* HignnModel(coord, blockSize) -- src/HignnModel.cpp:335-386, plus the first
+ * Update() (src/HignnModel.cpp:457-461) so the model is ready for dot.
+ * device >= 0 selects a CUDA device; device = -1 makes a host-only model whose
+ * tree and lists can be inspected but whose dot calls fail (no CPU fallback). */
+int hignn_create(const float* xyz, int64_t n, int block_size, int device, hignn_model** out);
+
+int hignn_destroy(hignn_model* m);
+
+/* LoadTwoBodyModel -- src/HignnModel.cpp:402-433. `path` names an .hgnw weight
+ * blob (see hignn_b200/weights.py) instead of a TorchScript file. */
+int hignn_load_two_body(hignn_model* m, const char* path);
+
+/* Weights from memory: dims = {3, h1, ..., 9}, w/b concatenated per layer
+ * (row-major out x in, then bias), activation 1 = tanh. */
+int hignn_load_two_body_mem(hignn_model* m, int num_layers, const int32_t* dims, const float* params,
+                            int activation);
+
+/* Setters of src/HignnModel.cpp:773-874 and this implementation's keys. */
+int hignn_set_param(hignn_model* m, int key, double value);
+int hignn_get_param(hignn_model* m, int key, double* value);
+
+/* UpdateCoord -- src/HignnModel.cpp:744-762: copy coordinates, rebuild the tree
+ * (src/Build.cpp:17-265) and the close/far lists (src/CloseFarCheck.cpp:11-465). */
+int hignn_update_coord(hignn_model* m, const float* xyz, int64_t n);
+
+/* Dot -- src/HignnModel.cpp:545-634: u = M(x) f through the H-matrix (close
+ * field + ACA far field). Host pointers; u is written, its input ignored. */
+int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n);
+
+/* Same operation on device pointers (caller's order), stream-ordered on the
+ * model's stream; returns when the result is in d_u. */
+int hignn_dot_device(hignn_model* m, float* d_u, const float* d_f, int64_t n);
+
+/* DenseDot -- src/HignnModel.cpp:660-728 with src/DenseDot.cpp:22-320:
+ * u_i = sum_j 0.5 (M + M^T)(x_j - x_i) f_j over all pairs, FP32 network,
+ * FP64 accumulation. Host pointers. */
+int hignn_dense_dot(hignn_model* m, float* u, const float* f, int64_t n);
+
+/* Dense rows for accuracy checks: for each listed target row (caller's order)
+ * u_row = sum over all j of 0.5 (M + M^T)(x_j - x_row) f_j, accumulated in FP64.
+ * precision 0 = FP32 network, 2 = FP64 network. Host pointers; u_rows is (nrows, 3). */
+int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
+                     int precision);
+
+/* Two-body kernel M(r) on n features (device pointers, r: (n,3), y: (n,9) row-major
+ * 3x3): python/convert.py:11-20. precision 0 = FP32 SIMT, 1 = BF16 tensor cores. */
+int hignn_two_body_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n, int precision);
+
+/* Sizes of the tree and lists built by the last update. */
+int hignn_get_stats(hignn_model* m, hignn_stats* out);
+
+/* Tree rows [child0, child1, start, end, level] (num_nodes x 5) and the
+ * permutation (tree position -> caller index), as src/Build.cpp leaves them. */
+int hignn_get_tree(hignn_model* m, int64_t* tree5, int64_t* perm);
+
+/* Close leaf pairs and far node pairs in the reference's list order
+ * (src/CloseFarCheck.cpp:298-408). Arrays sized from hignn_get_stats. */
+int hignn_get_lists(hignn_model* m, int64_t* close_i, int64_t* close_j, int64_t* far_i, int64_t* far_j);
+
+/* ACA ranks and pivot sequences of the last far field (needs HIGNN_P_RECORD_PIVOTS = 1):
+ * ranks[num_far]; rows / cols [num_far][ld] with ld >= max_iter + 1, block-local indices
+ * (rows[b][l] = pivot row of iteration l, cols[b][l] = its column), in list order. */
+int hignn_get_far_pivots(hignn_model* m, int32_t* ranks, int32_t* rows, int32_t* cols, int ld);
+
+/* Synchronize the model's stream. */
+int hignn_synchronize(hignn_model* m);
+
+/* The model's CUDA stream (cudaStream_t), for callers that order their own work. */
+int hignn_get_stream(hignn_model* m, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIGNN_B200_H */
