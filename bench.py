@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""H-matvec benchmark: particles/s of U = M(x) F at N = 1,048,576 on one B200 per rank.
+
+Workload (seeded, synthetic; no dataset): 1,048,576 unit spheres in a cube at
+volume fraction 0.10, 64 Gaussian clusters (sigma 8 radii) + 50% uniform
+background (seed 2), forces (0,0,-1) + N(0, 0.1^2); leaf size 128, ACA
+tolerance 1e-2 (the reference's production value, python/simulate.py:198),
+max_iter 100, tree prebuilt. One step = one H-matvec (near field + ACA far
+field). Each rank runs an independent replica (weak scaling); `value` is the
+sum of particles/s over ranks, timed on the device (max over ranks).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision P]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+WEIGHTS = os.path.join(REPO, "hignn_b200", "data", "two_body_unbounded.hgnw")
+METRIC = "H-matvec particles/s at N=1M: mixed+batched+student vs plain FP32, err≤1e-3"
+FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)  # 141,056
+PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor", 2: "bf16_tensor+student"}
+PREC_DTYPE = {0: "fp32", 1: "bf16", 2: "bf16"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hignn_b200", choices=["hignn_b200", "reference"])
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1, 2])
+    ap.add_argument("--n", type=int, default=1048576)
+    ap.add_argument("--epsilon", type=float, default=1e-2)
+    ap.add_argument("--check-rows", type=int, default=2048, help="dense target rows for the error check")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload(n):
+    from hignn_b200 import synthetic as S
+
+    x = S.clustered(n, 0.10, 2)
+    f = S.sedimenting_forces(n, 2)
+    return x, f
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if bus_id:
+            cmd += ["-i", bus_id]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return float("nan")
+
+        sm = [num(r[1]) for r in rows]
+        mx = max(num(r[2]) for r in rows)
+        pw = [num(r[3]) for r in rows]
+        load = [i for i in range(len(rows)) if pw[i] > 250 or sm[i] > 0.5 * mx] or list(range(len(rows)))
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for i in load for k in range(4) if rows[i][5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm[i] for i in load), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows), "samples_under_load": len(load),
+                "power_w_max": max(pw)}
+
+
+def cpu_baseline_sample(x, f, eps, close_evals, far_evals, seconds):
+    """Time the oracle port (numpy restatement of the reference path) on a bounded sample.
+
+    Near field: leading close pairs until ~seconds/2 of CPU work; far field: leading ACA
+    blocks for the other half. Evaluations/s of each are extrapolated to the counted
+    evaluations of the full H-matvec.
+    """
+    from oracle import hignn_oracle as O
+
+    net = O.TwoBody.from_hgnw(WEIGHTS)
+    t0 = time.time()
+    tree, rmap = O.build_tree(x, 128)
+    xt = x[rmap]
+    aux = O.compute_aux(tree, xt)
+    ci, cj, fi, fj, _ = O.close_far_lists(tree, aux)
+    t_lists = time.time() - t0
+    ft = f[rmap]
+    sz = tree[:, 3] - tree[:, 2]
+    # near-field sample
+    done_e, t_near, p = 0, 0.0, 0
+    while t_near < seconds / 2 and p < len(ci):
+        q = min(len(ci), p + 64)
+        t = time.time()
+        O.close_dot(tree, xt, ft, ci[p:q], cj[p:q], net)
+        t_near += time.time() - t
+        done_e += int(np.sum(sz[ci[p:q]] * sz[cj[p:q]]))
+        p = q
+    r_near = done_e / t_near
+    # far-field sample
+    far_e, t_far, b = 0, 0.0, 0
+    while t_far < seconds / 2 and b < len(fi):
+        q = min(len(fi), b + 32)
+        t = time.time()
+        col = []
+        O.far_dot(tree, xt, ft, fi[b:q], fj[b:q], net, eps, 100, collect=col)
+        t_far += time.time() - t
+        far_e += sum(c[2] * (sz[c[0]] + sz[c[1]]) for c in col)
+        b = q
+    r_far = far_e / t_far if t_far > 0 else r_near
+    t_dot = close_evals / r_near + far_evals / r_far
+    cores = os.cpu_count() or 1
+    return {"value": len(x) / t_dot, "unit": "particles/s", "cores": cores, "kind": "port",
+            "sample": (f"oracle numpy restatement (BLAS threads = {cores}): {p} close pairs "
+                       f"({done_e:.3g} evals, {r_near:.3g} evals/s) and {b} ACA blocks ({far_e:.3g} evals, "
+                       f"{r_far:.3g} evals/s), extrapolated to {close_evals:.3g} near + {far_evals:.3g} far "
+                       f"evaluations of one H-matvec; tree+lists {t_lists:.1f} s not counted"),
+            "t_dot_s_extrapolated": t_dot}
+
+
+def reference_arm(args, rank, world):
+    """The reference algorithm (restated on the CPU, numpy) on the host cores, bounded samples."""
+    if rank != 0:
+        return 0
+    x, f = workload(args.n)
+    from oracle import hignn_oracle as O
+
+    t0 = time.time()
+    tree, rmap = O.build_tree(x, 128)
+    aux = O.compute_aux(tree, x[rmap])
+    ci, cj, fi, fj, _ = O.close_far_lists(tree, aux)
+    sz = tree[:, 3] - tree[:, 2]
+    close_evals = int(np.sum(sz[ci] * sz[cj]))
+    build_s = time.time() - t0
+    vals = []
+    far_rows = int(np.sum(sz[fi] + sz[fj]))
+    for k in range(args.warmup + args.steps):
+        # far evaluations = mean sampled rank x rows of all far blocks (rank from the sample)
+        s = cpu_baseline_sample(x, f, args.epsilon, close_evals, 0, args.cpu_sample_seconds)
+        net = O.TwoBody.from_hgnw(WEIGHTS)
+        col = []
+        O.far_dot(tree, x[rmap], f[rmap], fi[:64], fj[:64], net, args.epsilon, 100, collect=col)
+        mean_rank = float(np.mean([c[2] for c in col])) if col else 0.0
+        far_evals = mean_rank * far_rows
+        s2 = cpu_baseline_sample(x, f, args.epsilon, close_evals, far_evals, args.cpu_sample_seconds)
+        if k >= args.warmup:
+            vals.append(s2["value"])
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.n / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, "
+                                   "seed 2, leaf 128", "n": args.n, "epsilon": args.epsilon, "max_iter": 100,
+                       "parallelism": "host cores"},
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": s2["cores"], "kind": "port",
+                             "sample": s2["sample"]},
+            "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent); "
+                    f"this arm times its restatement. tree+lists {build_s:.1f} s not counted"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+
+    from hignn_b200 import capi
+
+    x, f = workload(args.n)
+    n = len(x)
+    m = capi.Model(x, 128, device=local)
+    m.load_two_body(WEIGHTS)
+    m.set(capi.P_EPSILON, args.epsilon)
+    m.set(capi.P_MAX_ITER, 100)
+    m.set(capi.P_PRECISION, args.precision)
+    m.set(capi.P_TIMING, 1)
+    st0 = m.stats()  # builds the tree and lists
+    f_d = torch.from_numpy(f).cuda()
+    u_d = torch.empty_like(f_d)
+    stream = torch.cuda.ExternalStream(m.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    for _ in range(args.warmup):
+        m.dot_device(u_d.data_ptr(), f_d.data_ptr())
+    props = torch.cuda.get_device_properties(local)
+    bus = None
+    try:
+        bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+    except AttributeError:
+        pass
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(bus)
+    times, near_ms, far_ms = [], [], []
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.dot_device(u_d.data_ptr(), f_d.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        s = m.stats()
+        near_ms.append(s["t_close_ms"])
+        far_ms.append(s["t_far_ms"])
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+    st = m.stats()
+    ms = float(np.mean(times))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms / 1e3)
+
+    # end to end through the public C ABI from pinned host memory (H2D + matvec + D2H per step)
+    f_h = torch.from_numpy(f).pin_memory()
+    u_h = torch.empty_like(f_h).pin_memory()
+    if not args.no_e2e:
+        m.dot_ptr(u_h.data_ptr(), f_h.data_ptr())
+    else:
+        u_h.copy_(u_d.cpu())
+    e2e_times = []
+    for k in range(0 if args.no_e2e else args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.dot_ptr(u_h.data_ptr(), f_h.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = float(np.mean(e2e_times)) if e2e_times else float("nan")
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # accuracy: dense rows (FP32 network, FP64 accumulation over all N sources)
+    u = u_h.numpy().astype(np.float64)
+    rng = np.random.default_rng(12345)
+    rows = np.sort(rng.choice(n, size=min(args.check_rows, n), replace=False))
+    t0 = time.time()
+    err = None
+    if len(rows):
+        ud = m.dense_rows(f, rows, 0)
+        err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
+    t_check = time.time() - t0
+
+    hbm, bf16, src = peaks()
+    near_s = float(np.mean(near_ms)) / 1e3
+    achieved = st["close_evals"] * FLOP_PER_EVAL / near_s / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": PREC_DTYPE[args.precision], "data": "synthetic",
+        "config": {"workload": "N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, "
+                               "seed 2, leaf 128, tree prebuilt", "n": n, "epsilon": args.epsilon,
+                   "max_iter": 100, "form": PREC_NAME[args.precision],
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "256 MiB buffer written between timed steps"},
+        "roofline": {"bound": "tensor", "kernel": "near field (pair features + two-body MLP + contraction)",
+                     "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                     "peak_source": f"bf16_tflops of {src} MEASURED_PEAKS.json",
+                     "traffic": None,
+                     "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals"},
+        "e2e": {"value": n / (e2e_ms / 1e3) * world, "unit": "particles/s", "h2d_bytes_per_step": 12 * n,
+                "d2h_bytes_per_step": 12 * n, "ms_per_step": e2e_ms},
+        "gpu_launches": int(st["gpu_launches"]),
+        "clocks": ck,
+        "error": {"rel_l2_vs_dense": err, "rows": int(len(rows)),
+                  "oracle": "dense rows on the device, FP32 network, FP64 accumulation over all N sources",
+                  "seconds": t_check},
+        "breakdown_ms": {"near": float(np.mean(near_ms)), "far": float(np.mean(far_ms)),
+                         "build_host": st0["t_build_ms"]},
+        "work": {"close_pairs": st["num_close"], "far_pairs": st["num_far"], "close_evals": st["close_evals"],
+                 "far_evals": st["far_evals"], "far_rank_mean": st["far_rank_sum"] / max(1, st["num_far"]),
+                 "far_rank_max": st["far_rank_max"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(x, f, args.epsilon, st["close_evals"], st["far_evals"],
+                                                   args.cpu_sample_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    m.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

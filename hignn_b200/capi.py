@@ -45,6 +45,7 @@ class HignnStats(C.Structure):
         ("num_far", C.c_int64), ("close_evals", C.c_int64), ("far_evals", C.c_int64), ("far_rank_sum", C.c_int64),
         ("far_rank_max", C.c_int32), ("far_iterations", C.c_int32), ("student_fallback_blocks", C.c_int64),
         ("t_build_ms", C.c_double), ("t_close_ms", C.c_double), ("t_far_ms", C.c_double), ("t_dot_ms", C.c_double),
+        ("gpu_launches", C.c_int64),
     ]
 
     def as_dict(self):

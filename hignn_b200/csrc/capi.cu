@@ -396,6 +396,8 @@ void far_field(hignn_model* m) {
   m->stats.far_rank_sum = (int64_t)st[0];
   m->stats.far_evals = (int64_t)st[1];
   m->stats.far_iterations = iterations;
+  // per batch: one init kernel; per ACA iteration: active list, column eval, column pivot, row eval, row pivot
+  m->stats.gpu_launches += (int64_t)m->batches.size() + 5 * (int64_t)iterations;
 }
 
 void near_field(hignn_model* m) {
@@ -411,7 +413,10 @@ void near_field(hignn_model* m) {
 // u (tree order, FP64) = M f for f already gathered into f4.
 void matvec_tree_order(hignn_model* m) {
   if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
-  if (m->fields & 1) near_field(m);
+  if (m->fields & 1) {
+    near_field(m);
+    if (!m->lists.closeI.empty()) m->stats.gpu_launches += 1;
+  }
   if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
   if (m->fields & 2) far_field(m);
   if (m->timing) {
@@ -429,6 +434,7 @@ void matvec_tree_order(hignn_model* m) {
 void post_check(hignn_model* m);
 
 void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
+  m->stats.gpu_launches = 2;  // gather + scatter
   hignn::launch_gather_forces(d_f, m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(), m->n, m->stream);
   matvec_tree_order(m);
   if (m->post_check) post_check(m);

@@ -68,6 +68,7 @@ typedef struct hignn_stats {
   double t_close_ms;       /* device time of the last near field (TIMING = 1)   */
   double t_far_ms;         /* device time of the last far field (TIMING = 1)    */
   double t_dot_ms;         /* device time of the last dot (TIMING = 1)          */
+  int64_t gpu_launches;    /* kernels launched by the last dot                    */
 } hignn_stats;
 
 /* Message of the calling thread's last error (empty string if none). */

@@ -339,13 +339,38 @@ def is_far(aux, n1, n2):
     return bool(dist > d0 and dist > d1)
 
 
+def _diam2(aux):
+    """Squared box diagonal per node with the float32 operation order of src/HignnModel.cpp:500-504."""
+    d = np.zeros(aux.shape[0], np.float32)
+    with np.errstate(over="ignore", invalid="ignore"):  # unreachable rows 1, 2 hold -FLT_MAX
+        for j in range(3):
+            t = (aux[:, 2 * j] - aux[:, 2 * j + 1]).astype(np.float32)
+            d = (d + (t * t).astype(np.float32)).astype(np.float32)
+    return d
+
+
+def is_far_many(aux, diam2, i, js):
+    """Vectorised HignnModel::CloseFarCheck(aux, i, j) over candidate nodes js (same float32 rounding)."""
+    js = np.asarray(js, np.int64)
+    a, b = aux[i], aux[js]
+    disjoint = ((a[0] > b[:, 1]) | (a[1] < b[:, 0]) | (a[2] > b[:, 3]) | (a[3] < b[:, 2])
+                | (a[4] > b[:, 5]) | (a[5] < b[:, 4]))
+    dist = np.zeros(len(js), np.float32)
+    for j in range(3):
+        t = ((np.float32(a[2 * j] + a[2 * j + 1]) - b[:, 2 * j]).astype(np.float32) - b[:, 2 * j + 1]).astype(np.float32)
+        dist = (dist + (t * t).astype(np.float32)).astype(np.float32)
+    dist = (dist * np.float32(0.25)).astype(np.float32)
+    return disjoint & (dist > diam2[i]) & (dist > diam2[js])
+
+
 def close_far_lists(tree, aux, max_relative_coord=500000, use_symmetry=True):
     """Dual traversal (src/CloseFarCheck.cpp:179-290) and flattening (:292-454).
 
     Returns (closeI, closeJ, farI, farJ, leaf_list) in the reference's order.
     """
     nn = tree.shape[0]
-    size = lambda n: int(tree[n, 3] - tree[n, 2])
+    sizes = (tree[:, 3] - tree[:, 2]).astype(np.int64)
+    d2 = _diam2(aux)
     far = [[] for _ in range(nn)]
     close = [[] for _ in range(nn)]
     close[0] = [0]
@@ -353,11 +378,12 @@ def close_far_lists(tree, aux, max_relative_coord=500000, use_symmetry=True):
     q = deque([0])
     while q:
         i = q.popleft()
+        cand = close[i]
+        fl = is_far_many(aux, d2, i, cand).tolist() if cand else []
         if tree[i, 0] != 0:
             child_close = []
-            for j in close[i]:
-                f = is_far(aux, i, j) and size(i) < max_relative_coord and size(j) < max_relative_coord
-                if f:
+            for j, fr in zip(cand, fl):
+                if fr and sizes[i] < max_relative_coord and sizes[j] < max_relative_coord:
                     far[i].append(j)
                 elif tree[j, 0] != 0:
                     child_close.append(int(tree[j, 0]))
@@ -370,15 +396,15 @@ def close_far_lists(tree, aux, max_relative_coord=500000, use_symmetry=True):
             q.append(int(tree[i, 1]))
         else:
             new_close = []
-            for j in close[i]:
-                if is_far(aux, i, j):
-                    if size(j) < max_relative_coord:
+            for j, fr in zip(cand, fl):
+                if fr:
+                    if sizes[j] < max_relative_coord:
                         far[i].append(j)
                     else:
                         st = [j]
                         while st:
                             c = st.pop()
-                            if size(c) < max_relative_coord:
+                            if sizes[c] < max_relative_coord:
                                 far[i].append(c)
                             else:
                                 st.append(int(tree[c, 0]))
