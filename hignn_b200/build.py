@@ -32,6 +32,7 @@ CU_SOURCES = {
     "near_simt.cu": [],
     "far_aca.cu": ["-fmad=false"],  # FP64 determinants / inverses round as written
     "misc.cu": [],
+    "tc_kernels.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

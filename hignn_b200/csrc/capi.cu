@@ -112,7 +112,7 @@ struct hignn_model {
   bool has_weights = false;
   std::vector<float> hw;  // device-layout weights, host copy
 
-  DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, counter;
+  DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
       far_preI, far_preJ, far_ctr, far_stats;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
@@ -142,6 +142,17 @@ struct hignn_model {
     w.b3 = w.w3 + hignn::kOut * hignn::kH2;
     return w;
   }
+  hignn::TcWeights wtc() const {
+    const hignn::MlpF32 f = wdev();
+    hignn::TcWeights w;
+    w.w2img = weights_tc.as<uint4>();
+    w.w3img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2);
+    w.w1b1 = f.w1b1;
+    w.b2 = f.b2;
+    w.b3 = f.b3;
+    return w;
+  }
+  int* err_flag() const { return counter.as<int>() + 1; }
 };
 
 namespace {
@@ -299,6 +310,31 @@ void ensure_far_plan(hignn_model* m) {
   m->plan_nodes = m->max_far_dot_work_node_size;
 }
 
+// BF16 round-to-nearest-even
+uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+float bf16_value(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+void check_device_error(hignn_model* m) {
+  int e = 0;
+  HIGNN_CUDA(cudaMemcpyAsync(&e, m->err_flag(), sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  if (e != 0) {
+    HIGNN_CUDA(cudaMemsetAsync(m->err_flag(), 0, sizeof(int), m->stream));
+    throw Error(HIGNN_ERR_LIMIT, "tensor-core kernel: a bounded wait timed out (code " + std::to_string(e) + ")");
+  }
+}
+
 void require_weights(hignn_model* m) {
   if (!m->has_weights) throw Error(HIGNN_ERR_STATE, "no two-body model loaded (call load_two_body_model)");
 }
@@ -325,11 +361,33 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
   for (int q = 0; q < kOut * kH2; q++) w3[q] = W[2][q];
   float* b3 = w3 + kOut * kH2;
   for (int q = 0; q < kOut; q++) b3[q] = B[2][q];
+  // tensor-core images: K-major rows of 64 BF16 (128 B) per 64-wide K slab, 8-row groups of
+  // 1024 B, 16-byte chunk c of row r stored at chunk position c ^ (r % 8) (128-byte swizzle)
+  auto swz = [](int row, int k, int rows_per_slab) -> size_t {
+    const int slab = k >> 6, kc = k & 63;
+    return (size_t)slab * rows_per_slab * 128 + (size_t)(row >> 3) * 1024 + (row & 7) * 128 +
+           (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
+  };
+  std::vector<uint8_t> img(kH2 * kH1 * 2 + 32 * kH2 * 2, 0);
+  auto put = [&](size_t off, uint16_t v) { std::memcpy(img.data() + off, &v, 2); };
+  for (int nn = 0; nn < kH2; nn++)
+    for (int k = 0; k < kH1; k++) put(swz(nn, k, kH2), bf16_bits(W[1][(size_t)nn * kH1 + k]));
+  const size_t w3off = (size_t)kH2 * kH1 * 2;
+  for (int o = 0; o < kOut; o++)
+    for (int k = 0; k < kH2; k++) {
+      const float v = W[2][(size_t)o * kH2 + k];
+      const uint16_t hi = bf16_bits(v);
+      const uint16_t lo = bf16_bits(v - bf16_value(hi));
+      put(w3off + swz(o, k, 32), hi);
+      put(w3off + swz(16 + o, k, 32), lo);
+    }
   m->has_weights = true;
   if (m->device < 0) return;
   HIGNN_CUDA(cudaSetDevice(m->device));
   m->weights.ensure(sizeof(float) * hw.size());
   HIGNN_CUDA(cudaMemcpyAsync(m->weights.p, hw.data(), sizeof(float) * hw.size(), cudaMemcpyHostToDevice, m->stream));
+  m->weights_tc.ensure(img.size());
+  HIGNN_CUDA(cudaMemcpyAsync(m->weights_tc.p, img.data(), img.size(), cudaMemcpyHostToDevice, m->stream));
   HIGNN_CUDA(cudaStreamSynchronize(m->stream));
 }
 
@@ -370,7 +428,9 @@ void far_field(hignn_model* m) {
     const auto& last = m->far_plan[bt.b1 - 1];
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
-    hignn::far_batch_plain(a, w, m->num_sms, m->host_ctr, m->stream, &iterations);
+    const hignn::TcWeights tcw = m->wtc();
+    hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, m->err_flag(), m->num_sms, m->host_ctr,
+                           m->stream, &iterations);
     m->stats.far_rank_max = std::max(m->stats.far_rank_max, m->host_ctr[hignn::kCtrRankMax]);
     if (m->record_pivots) {
       const int nb = bt.b1 - bt.b0, ld = a.ldr;
@@ -407,7 +467,10 @@ void near_field(hignn_model* m) {
   a.xI = a.xJ = m->x4.as<float4>();
   a.fI = a.fJ = m->f4.as<float4>();
   a.uI = a.uJ = m->u.as<double>();
-  hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+  if (m->precision >= 1)
+    hignn::launch_near_tc(a, m->wtc(), m->counter.as<int>(), m->err_flag(), m->num_sms, m->stream);
+  else
+    hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
 }
 
 // u (tree order, FP64) = M f for f already gathered into f4.
@@ -439,6 +502,7 @@ void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
   matvec_tree_order(m);
   if (m->post_check) post_check(m);
   hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), d_u, m->n, m->stream);
+  if (m->precision >= 1) check_device_error(m);
 }
 
 // Dense product over all leaf pairs into m->u (tree order); f4 already gathered.
@@ -526,6 +590,8 @@ int hignn_create(const float* xyz, int64_t n, int block_size, int device, hignn_
         HIGNN_CUDA(cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, device));
         HIGNN_CUDA(cudaMallocHost((void**)&m->host_ctr, sizeof(int32_t) * hignn::kCtrCount));
         for (auto& e : m->ev) HIGNN_CUDA(cudaEventCreate(&e));
+        m->counter.ensure(64);
+        HIGNN_CUDA(cudaMemsetAsync(m->counter.p, 0, 64, m->stream));
       }
       m->stats.n = n;
     } catch (...) {
@@ -541,7 +607,8 @@ int hignn_destroy(hignn_model* m) {
   if (m->device >= 0) {
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
-    for (DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights, &m->counter,
+    for (DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
+                      &m->weights_tc, &m->counter,
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
                       &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
@@ -799,10 +866,15 @@ int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64
 int hignn_two_body_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n, int precision) {
   return guard([&] {
     if (!m || (!d_r && n > 0) || (!d_y && n > 0)) throw Error(HIGNN_ERR_ARG, "null argument");
-    if (precision != 0) throw Error(HIGNN_ERR_ARG, "unsupported precision");
+    if (precision != 0 && precision != 1) throw Error(HIGNN_ERR_ARG, "unsupported precision");
     require_device(m);
     require_weights(m);
-    hignn::launch_eval_simt(d_r, d_y, n, m->wdev(), m->num_sms, m->stream);
+    if (precision == 1) {
+      hignn::launch_eval_tc(d_r, d_y, n, m->wtc(), m->err_flag(), m->num_sms, m->stream);
+      check_device_error(m);
+    } else {
+      hignn::launch_eval_simt(d_r, d_y, n, m->wdev(), m->num_sms, m->stream);
+    }
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
   });
 }

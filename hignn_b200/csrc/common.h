@@ -38,6 +38,15 @@ struct MlpF32 {
   const float* b3;     // [kOut]
 };
 
+// Tensor-core weights: swizzled BF16 images of W2 and W3 (hi / residual) plus FP32 biases.
+struct TcWeights {
+  const uint4* w2img;   // 512 x 128 BF16, K-major 128-byte swizzle (131072 B)
+  const uint4* w3img;   // 32 x 512 BF16 (rows 0-8 high part, rows 16-24 residual) (32768 B)
+  const float4* w1b1;   // [128]
+  const float* b2;      // [512]
+  const float* b3;      // [9]
+};
+
 // One unit of near-field (or dense) work: target range I against source range J.
 constexpr int32_t kPairTransposed = 1;  // also u_J += M f_I (symmetric close pair, J > I)
 constexpr int32_t kPairSymmetrize = 2;  // use 0.5 (M + M^T) (dense product)

@@ -67,8 +67,14 @@ struct FarArgs {
   int use_symmetry;
 };
 
-void far_batch_plain(const FarArgs& a, const MlpF32& w, int num_sms, int32_t* host_ctr, cudaStream_t s,
-                     int* iterations);
+// One ACA batch to completion. tcw == nullptr: FP32 SIMT queries; else tensor-core queries.
+void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, int* err, int num_sms,
+                     int32_t* host_ctr, cudaStream_t s, int* iterations);
+
+// tensor-core kernels (tc_kernels.cu); err receives a nonzero code if a bounded wait timed out
+void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, int* err, int num_sms, cudaStream_t s);
+void launch_far_tc(const FarArgs& a, const TcWeights& w, int which, int* err, int num_sms, cudaStream_t s);
+void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int* err, int num_sms, cudaStream_t s);
 
 // ---------------------------------------------------------------- reorder / misc
 void launch_gather_forces(const float* f, const int32_t* perm, float4* f4, double* u, int64_t n, cudaStream_t s);

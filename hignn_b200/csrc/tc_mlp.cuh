@@ -1,0 +1,364 @@
+// Two-body network on the 5th-generation tensor cores (tcgen05, TMEM), 128 evaluations per tile.
+//
+// Mixed precision: layer 1 (3 -> 128) in FP32 on the CUDA cores; layers 2
+// (128 -> 512) and 3 (512 -> 9) as BF16 tcgen05 MMAs with FP32 accumulation in
+// tensor memory; tanh as tanh.approx.bf16x2 (two per MUFU op) on bias-added
+// FP32 accumulators. W3 is split into a BF16 high part and a BF16 residual
+// (rows 0-8 and 16-24 of one N=32 operand): its rounding is the dominant
+// systematic error of a plain BF16 layer 3, and the split removes it for ~6%
+// more tensor work. b1, b2, b3 stay FP32.
+//
+// CTA = 5 warps. Warps 0-3 (128 threads) are the epilogue: thread e owns
+// evaluation e of the tile = row e of every MMA = TMEM lane e. Warp 4 allocates
+// tensor memory and one elected lane issues all MMAs.
+//
+// Tensor memory (512 columns allocated):
+//   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs, the A operand of layer 2
+//   [ 64,448)  three 128-column slots: layer-2 accumulator of one quarter (128
+//              hidden units); after the epilogue reads it, the quarter's
+//              tanh'd BF16 values are written back into the slot's first 64
+//              columns and become the A operand of that quarter's layer-3 MMA
+//   [448,480)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
+// Shared memory: W2 (512 x 128 BF16) and W3 (32 x 512 BF16) in the canonical
+// K-major 128-byte-swizzle layout, loaded once per CTA; mbarriers.
+//
+// Schedule per tile (q = quarter of the 512 hidden units):
+//   epilogue: layer 1 -> A1 ; for q: wait D2(q), tanh -> A2(q) ; wait D3, wrapper
+//   MMA lane: L2(0) L2(1) L2(2) | L3(0) L2(3) | L3(1) | L3(2) | L3(3)
+// Every wait is bounded (about two seconds of clock): on a timeout the CTA
+// records an error, stops issuing work, drains its MMAs and frees its tensor memory.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace hignn {
+namespace tc {
+
+constexpr int kTile = 128;
+constexpr int kEpiThreads = 128;
+constexpr int kThreads = 160;
+constexpr uint32_t kColA1 = 0, kColSlot0 = 64, kColD3 = 448;
+constexpr int kW2Bytes = kH2 * kH1 * 2;   // 131072
+constexpr int kW3Rows = 32;
+constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 32768
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+using hignn::TcWeights;
+
+struct alignas(1024) Smem {
+  uint8_t w2[kW2Bytes];
+  uint8_t w3[kW3Bytes];
+  uint64_t a1_full, a1_free, d3_full, d3_free, drain;
+  uint64_t d2_full[3], a2_full[3], slot_free[3];
+  uint32_t tmem_base;
+  int exit_flag;
+  int abort_flag;
+};
+
+// ------------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false (and raises the CTA abort flag) if the phase never completes.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* abort_flag, int* err, int code) {
+  const long long t0 = clock64();
+  while (!mbar_try(b, parity)) {
+    if (*(volatile int*)abort_flag) return false;
+    if (clock64() - t0 > kWaitCycles) {
+      atomicExch(abort_flag, 1);
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(dst)), "r"(ncols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols));
+}
+
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::f16 (BF16 inputs, FP32 accumulate)
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// D[tmem] (+)= A[tmem] * B[smem desc]^T
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
+      "r"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(saddr(bar))
+               : "memory");
+}
+
+// 32 consecutive 32-bit TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+      "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]),
+      "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]),
+      "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x) {
+  uint32_t y;
+  asm("tanh.approx.bf16x2 %0, %1;\n" : "=r"(y) : "r"(x));
+  return y;
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr_bytes & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused by swizzled K-major): 16 B
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset between 8-row groups
+  d |= (uint64_t)1 << 46;            // descriptor version of sm_100
+  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+  return d;
+}
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// ------------------------------------------------------------------ per-CTA setup / teardown
+__device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
+  const int t = threadIdx.x;
+  // weight images (the host builds them in the swizzled layout)
+  const uint4* src2 = w.w2img;
+  uint4* dst2 = reinterpret_cast<uint4*>(s.w2);
+  for (int i = t; i < kW2Bytes / 16; i += blockDim.x) dst2[i] = src2[i];
+  const uint4* src3 = w.w3img;
+  uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
+  for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
+  if (t == 0) {
+    mbar_init(&s.a1_full, kEpiThreads);
+    mbar_init(&s.a1_free, 1);
+    mbar_init(&s.d3_full, 1);
+    mbar_init(&s.d3_free, kEpiThreads);
+    mbar_init(&s.drain, 1);
+    for (int q = 0; q < 3; q++) {
+      mbar_init(&s.d2_full[q], 1);
+      mbar_init(&s.a2_full[q], kEpiThreads);
+      mbar_init(&s.slot_free[q], 1);
+    }
+    s.exit_flag = 0;
+    s.abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // generic-proxy writes of the weight images must be visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if ((t >> 5) == 4) tmem_alloc(&s.tmem_base, 512);
+  fence_before();
+  __syncthreads();
+  fence_after();
+}
+
+__device__ __forceinline__ void cta_teardown(Smem& s) {
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 4) tmem_dealloc(s.tmem_base, 512);
+}
+
+// ------------------------------------------------------------------ MMA warp (one elected lane)
+// Processes tiles until the epilogue raises exit_flag (or a wait times out).
+__device__ __forceinline__ void mma_loop(Smem& s, int* err) {
+  const uint32_t tbase = s.tmem_base;
+  const uint32_t id_l2 = idesc_bf16(128, 128), id_l3 = idesc_bf16(128, kW3Rows);
+  const uint32_t w2 = saddr(s.w2), w3 = saddr(s.w3);
+  uint32_t tile = 0, gq = 0, pending_l3 = 0;
+  for (;; tile++) {
+    if (!mbar_wait(&s.a1_full, tile & 1, &s.abort_flag, err, 11)) break;
+    fence_after();
+    if (*(volatile int*)&s.exit_flag) break;
+    uint32_t issued = 0;
+    bool ok = true;
+    for (uint32_t q = 0; q < 4 && ok; q++) {
+      while (issued < 4 && issued <= q + 2) {  // layer 2 up to three quarters ahead
+        const uint32_t g = gq + issued, slot = g % 3, use = g / 3;
+        if (use > 0 && !mbar_wait(&s.slot_free[slot], (use - 1) & 1, &s.abort_flag, err, 12)) {
+          ok = false;
+          break;
+        }
+        fence_after();
+        const uint32_t dcol = tbase + kColSlot0 + 128 * slot;
+#pragma unroll
+        for (uint32_t kk = 0; kk < 8; kk++) {
+          // B: rows 128*issued.. of W2, K columns 16*kk..; A: A1 columns 8*kk..
+          const uint32_t b = w2 + (kk >> 2) * (kH2 * 128) + issued * (128 * 128) + (kk & 3) * 32;
+          mma_ts(dcol, tbase + kColA1 + 8 * kk, sdesc(b), id_l2, kk > 0);
+        }
+        mma_commit(&s.d2_full[slot]);
+        if (issued == 3) mma_commit(&s.a1_free);
+        issued++;
+      }
+      if (!ok) break;
+      const uint32_t g = gq + q, slot = g % 3, use = g / 3;
+      if (!mbar_wait(&s.a2_full[slot], use & 1, &s.abort_flag, err, 13)) break;
+      if (q == 0 && tile > 0 && !mbar_wait(&s.d3_free, (tile - 1) & 1, &s.abort_flag, err, 14)) break;
+      fence_after();
+      const uint32_t acol = tbase + kColSlot0 + 128 * slot;
+#pragma unroll
+      for (uint32_t kk = 0; kk < 8; kk++) {
+        const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
+        const uint32_t b = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
+        mma_ts(tbase + kColD3, acol + 8 * kk, sdesc(b), id_l3, (q > 0 || kk > 0) ? 1u : 0u);
+      }
+      mma_commit(&s.slot_free[slot]);
+      if (q == 3) mma_commit(&s.d3_full);
+    }
+    if (*(volatile int*)&s.abort_flag) break;
+    gq += 4;
+  }
+  (void)pending_l3;
+  // drain: every MMA issued so far completes before tensor memory is released
+  mma_commit(&s.drain);
+  const long long t0 = clock64();
+  while (!mbar_try(&s.drain, 0) && clock64() - t0 < kWaitCycles) {
+  }
+}
+
+// ------------------------------------------------------------------ epilogue side
+struct EpiState {
+  uint32_t tile = 0, gq = 0;
+};
+
+// Runs one tile for this thread's evaluation with features r; writes M (row-major 3x3).
+// Returns false if the CTA aborted. All 128 epilogue threads must call it together.
+__device__ __forceinline__ bool run_tile(Smem& s, const TcWeights& w, EpiState& st, float rx, float ry, float rz,
+                                         float (&M)[9], int* err) {
+  const int e = threadIdx.x;                 // 0..127 (warps 0-3)
+  const uint32_t lane_base = (uint32_t)(e & ~31) << 16;
+  const uint32_t tb = s.tmem_base + lane_base;
+  // A1 is free once the previous tile's layer-2 MMAs completed
+  if (st.tile > 0 && !mbar_wait(&s.a1_free, (st.tile - 1) & 1, &s.abort_flag, err, 21)) return false;
+  fence_after();
+  {
+    uint32_t pk[32];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        const float4 w0 = __ldg(&w.w1b1[half * 64 + 2 * c]);
+        const float4 w1 = __ldg(&w.w1b1[half * 64 + 2 * c + 1]);
+        const float z0 = fmaf(w0.z, rz, fmaf(w0.y, ry, fmaf(w0.x, rx, w0.w)));
+        const float z1 = fmaf(w1.z, rz, fmaf(w1.y, ry, fmaf(w1.x, rx, w1.w)));
+        pk[c] = tanh_bf16x2(pack_bf16(z0, z1));
+      }
+      tmem_st32(tb + kColA1 + 32 * half, pk);
+    }
+  }
+  tmem_wait_st();
+  fence_before();
+  mbar_arrive(&s.a1_full);
+  for (uint32_t q = 0; q < 4; q++) {
+    const uint32_t g = st.gq + q, slot = g % 3, use = g / 3;
+    if (!mbar_wait(&s.d2_full[slot], use & 1, &s.abort_flag, err, 22)) return false;
+    fence_after();
+    const uint32_t col = tb + kColSlot0 + 128 * slot;
+    uint32_t out[64];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      uint32_t v[32];
+      tmem_ld32(col + 32 * c, v);
+      tmem_wait_ld();
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const int n = q * 128 + c * 32 + 2 * k;
+        const float a = __uint_as_float(v[2 * k]) + __ldg(&w.b2[n]);
+        const float b = __uint_as_float(v[2 * k + 1]) + __ldg(&w.b2[n + 1]);
+        out[c * 16 + k] = tanh_bf16x2(pack_bf16(a, b));
+      }
+    }
+    tmem_st32(col, out);
+    tmem_st32(col + 32, out + 32);
+    tmem_wait_st();
+    fence_before();
+    mbar_arrive(&s.a2_full[slot]);
+  }
+  if (!mbar_wait(&s.d3_full, st.tile & 1, &s.abort_flag, err, 23)) return false;
+  fence_after();
+  {
+    uint32_t v[32];
+    tmem_ld32(tb + kColD3, v);
+    tmem_wait_ld();
+    fence_before();
+    mbar_arrive(&s.d3_free);
+    const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
+#pragma unroll
+    for (int o = 0; o < 9; o++) {
+      float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + __ldg(&w.b3[o]);
+      const bool dg = (o == 0 || o == 4 || o == 8);
+      if (dg) y += 1.0f;
+      y = y / nr;
+      if (nr < 1e-5f) y = dg ? 1.0f : 0.0f;
+      M[o] = y;
+    }
+  }
+  st.tile++;
+  st.gq += 4;
+  return true;
+}
+
+// Tells the MMA lane to stop (all 128 epilogue threads call it once).
+__device__ __forceinline__ void epi_finish(Smem& s) {
+  if (threadIdx.x == 0) *(volatile int*)&s.exit_flag = 1;
+  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  mbar_arrive(&s.a1_full);
+}
+
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+}  // namespace tc
+}  // namespace hignn
