@@ -36,11 +36,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   NearTcSmem& S = *reinterpret_cast<NearTcSmem*>(align1k(smem_raw));
   tc::cta_setup(S.tcs, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp == 4) {
+  if (warp == tc::kMmaWarp) {
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int e = threadIdx.x;
+    const int e = threadIdx.x;  // 0..255, staging / flush index
+    const int row = tc::epi_row(), h = tc::epi_half();
     tc::EpiState st;
     bool ok = true;
     for (;;) {
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       tc::epi_bar();
       const int total = pw.nI * pw.nJ;
       for (int t0 = 0; t0 < total; t0 += tc::kTile) {
-        const int flat = t0 + e;
+        const int flat = t0 + row;
         const bool valid = flat < total;
         const int i = valid ? flat / pw.nJ : 0;
         const int j = valid ? flat - i * pw.nJ : 0;
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           rz = xj.z - xi.z;
         }
         float M[9];
-        ok = tc::run_tile(S.tcs, w, st, rx, ry, rz, M, err);
+        ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
         if (!ok) break;
         if (valid) {
           if (symm) {
@@ -89,11 +90,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 M[3 * c + r] = v;
               }
           }
-          const float4 fj = S.fJ[j];
-          atomicAdd(&S.uI[i][0], M[0] * fj.x + M[1] * fj.y + M[2] * fj.z);
-          atomicAdd(&S.uI[i][1], M[3] * fj.x + M[4] * fj.y + M[5] * fj.z);
-          atomicAdd(&S.uI[i][2], M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
-          if (trans) {
+          if (h == 0) {  // u_I[i] += M f_J[j]
+            const float4 fj = S.fJ[j];
+            atomicAdd(&S.uI[i][0], M[0] * fj.x + M[1] * fj.y + M[2] * fj.z);
+            atomicAdd(&S.uI[i][1], M[3] * fj.x + M[4] * fj.y + M[5] * fj.z);
+            atomicAdd(&S.uI[i][2], M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
+          } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
             const float4 fi = S.fI[i];
             atomicAdd(&S.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
             atomicAdd(&S.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
@@ -127,16 +129,16 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
   if ((int)blockIdx.x * tc::kTile >= tot) return;  // uniform: before any setup
   tc::cta_setup(S.tcs, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp == 4) {
+  if (warp == tc::kMmaWarp) {
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int e = threadIdx.x;
+    const int row = tc::epi_row(), h = tc::epi_half();
     const int32_t* pre = which ? a.preJ : a.preI;
     tc::EpiState st;
     bool ok = true;
     for (int tile = blockIdx.x; tile * tc::kTile < tot; tile += gridDim.x) {
-      const int g = tile * tc::kTile + e;
+      const int g = tile * tc::kTile + row;
       const bool valid = g < tot;
       float rx = 1.f, ry = 0.f, rz = 0.f;
       int b = 0, loc = 0, k = 0;
@@ -166,17 +168,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
         rz = xj.z - xi.z;
       }
       float M[9];
-      ok = tc::run_tile(S.tcs, w, st, rx, ry, rz, M, err);
+      ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
       if (!ok) break;
-      if (valid) {
+      if (valid) {  // the two threads of a row store alternate entries
         const FarBlock bk = a.blocks[b];
         double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                                  : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
 #pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-          for (int c = 0; c < 3; c++)
-            dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+        for (int q = 0; q < 9; q++) {
+          if ((q & 1) != h) continue;
+          const int r = q / 3, c = q % 3;
+          dst[q] = (r == c) ? (double)M[q] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+        }
       }
     }
     if (ok) tc::epi_finish(S.tcs);
@@ -195,15 +198,15 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   EvalTcSmem& S = *reinterpret_cast<EvalTcSmem*>(align1k(smem_raw));
   tc::cta_setup(S.tcs, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp == 4) {
+  if (warp == tc::kMmaWarp) {
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int e = threadIdx.x;
+    const int row = tc::epi_row(), h = tc::epi_half();
     tc::EpiState st;
     bool ok = true;
     for (int64_t base = (int64_t)blockIdx.x * tc::kTile; base < n; base += (int64_t)gridDim.x * tc::kTile) {
-      const int64_t g = base + e;
+      const int64_t g = base + row;
       float rx = 1.f, ry = 0.f, rz = 0.f;
       if (g < n) {
         rx = r[3 * g];
@@ -211,11 +214,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         rz = r[3 * g + 2];
       }
       float M[9];
-      ok = tc::run_tile(S.tcs, w, st, rx, ry, rz, M, err);
+      ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
       if (!ok) break;
       if (g < n)
 #pragma unroll
-        for (int q = 0; q < 9; q++) y[9 * g + q] = M[q];
+        for (int q = 0; q < 9; q++)
+          if ((q & 1) == h) y[9 * g + q] = M[q];
     }
     if (ok) tc::epi_finish(S.tcs);
   }

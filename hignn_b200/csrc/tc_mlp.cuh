@@ -8,16 +8,19 @@
 // systematic error of a plain BF16 layer 3, and the split removes it for ~6%
 // more tensor work. b1, b2, b3 stay FP32.
 //
-// CTA = 5 warps. Warps 0-3 (128 threads) are the epilogue: thread e owns
-// evaluation e of the tile = row e of every MMA = TMEM lane e. Warp 4 allocates
-// tensor memory and one elected lane issues all MMAs.
+// CTA = 9 warps. Warps 0-7 (256 threads) are the epilogue: warp w reaches TMEM
+// lanes 32*(w%4)..+31, so evaluation (row) e = 32*(w%4) + lane is shared by the
+// threads of warps w%4 and w%4+4, which split every row's columns in halves
+// (h = w/4). Warp 8 allocates tensor memory and one elected lane issues all MMAs.
 //
 // Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs, the A operand of layer 2
 //   [ 64,448)  three 128-column slots: layer-2 accumulator of one quarter (128
 //              hidden units); after the epilogue reads it, the quarter's
-//              tanh'd BF16 values are written back into the slot's first 64
-//              columns and become the A operand of that quarter's layer-3 MMA
+//              tanh'd BF16 values are written back into slot columns [0,32)
+//              (units 0-63, by half h=0) and [64,96) (units 64-127, h=1), each
+//              half writing only columns it read itself, and become the A
+//              operand of that quarter's layer-3 MMA
 //   [448,480)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
 // Shared memory: W2 (512 x 128 BF16) and W3 (32 x 512 BF16) in the canonical
 // K-major 128-byte-swizzle layout, loaded once per CTA; mbarriers.
@@ -39,8 +42,9 @@ namespace hignn {
 namespace tc {
 
 constexpr int kTile = 128;
-constexpr int kEpiThreads = 128;
-constexpr int kThreads = 160;
+constexpr int kEpiThreads = 256;
+constexpr int kThreads = 288;
+constexpr int kMmaWarp = 8;
 constexpr uint32_t kColA1 = 0, kColSlot0 = 64, kColD3 = 448;
 constexpr int kW2Bytes = kH2 * kH1 * 2;   // 131072
 constexpr int kW3Rows = 32;
@@ -57,6 +61,9 @@ struct alignas(1024) Smem {
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
+  alignas(16) float b2[kH2];
+  alignas(16) float4 w1b1[kH1];
+  float b3[16];
 };
 
 // ------------------------------------------------------------------ PTX wrappers
@@ -181,6 +188,9 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   const uint4* src3 = w.w3img;
   uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
   for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
+  for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
+  for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
+  if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t == 0) {
     mbar_init(&s.a1_full, kEpiThreads);
     mbar_init(&s.a1_free, 1);
@@ -198,7 +208,7 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   }
   // generic-proxy writes of the weight images must be visible to the tensor core (async proxy)
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  if ((t >> 5) == 4) tmem_alloc(&s.tmem_base, 512);
+  if ((t >> 5) == kMmaWarp) tmem_alloc(&s.tmem_base, 512);
   fence_before();
   __syncthreads();
   fence_after();
@@ -208,7 +218,7 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
   fence_before();
   __syncthreads();
   fence_after();
-  if ((threadIdx.x >> 5) == 4) tmem_dealloc(s.tmem_base, 512);
+  if ((threadIdx.x >> 5) == kMmaWarp) tmem_dealloc(s.tmem_base, 512);
 }
 
 // ------------------------------------------------------------------ MMA warp (one elected lane)
@@ -253,7 +263,8 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
       for (uint32_t kk = 0; kk < 8; kk++) {
         const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
         const uint32_t b = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-        mma_ts(tbase + kColD3, acol + 8 * kk, sdesc(b), id_l3, (q > 0 || kk > 0) ? 1u : 0u);
+        const uint32_t a_off = kk < 4 ? 8 * kk : 64 + 8 * (kk - 4);  // A2 halves at slot cols 0 and 64
+        mma_ts(tbase + kColD3, acol + a_off, sdesc(b), id_l3, (q > 0 || kk > 0) ? 1u : 0u);
       }
       mma_commit(&s.slot_free[slot]);
       if (q == 3) mma_commit(&s.d3_full);
@@ -274,30 +285,28 @@ struct EpiState {
   uint32_t tile = 0, gq = 0;
 };
 
-// Runs one tile for this thread's evaluation with features r; writes M (row-major 3x3).
-// Returns false if the CTA aborted. All 128 epilogue threads must call it together.
-__device__ __forceinline__ bool run_tile(Smem& s, const TcWeights& w, EpiState& st, float rx, float ry, float rz,
-                                         float (&M)[9], int* err) {
-  const int e = threadIdx.x;                 // 0..127 (warps 0-3)
-  const uint32_t lane_base = (uint32_t)(e & ~31) << 16;
-  const uint32_t tb = s.tmem_base + lane_base;
+// Runs one tile for this thread's evaluation (row) with features r; writes M (row-major 3x3)
+// into both threads of the row. Returns false if the CTA aborted. All 256 epilogue threads
+// must call it together.
+__device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float ry, float rz, float (&M)[9],
+                                         int* err) {
+  const int w = threadIdx.x >> 5;          // 0..7
+  const int h = w >> 2;                     // column half
+  const uint32_t tb = s.tmem_base + ((uint32_t)(32 * (w & 3)) << 16);
   // A1 is free once the previous tile's layer-2 MMAs completed
   if (st.tile > 0 && !mbar_wait(&s.a1_free, (st.tile - 1) & 1, &s.abort_flag, err, 21)) return false;
   fence_after();
   {
     uint32_t pk[32];
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
-#pragma unroll
-      for (int c = 0; c < 32; c++) {
-        const float4 w0 = __ldg(&w.w1b1[half * 64 + 2 * c]);
-        const float4 w1 = __ldg(&w.w1b1[half * 64 + 2 * c + 1]);
-        const float z0 = fmaf(w0.z, rz, fmaf(w0.y, ry, fmaf(w0.x, rx, w0.w)));
-        const float z1 = fmaf(w1.z, rz, fmaf(w1.y, ry, fmaf(w1.x, rx, w1.w)));
-        pk[c] = tanh_bf16x2(pack_bf16(z0, z1));
-      }
-      tmem_st32(tb + kColA1 + 32 * half, pk);
+    for (int c = 0; c < 32; c++) {
+      const float4 w0 = s.w1b1[64 * h + 2 * c];
+      const float4 w1 = s.w1b1[64 * h + 2 * c + 1];
+      const float z0 = fmaf(w0.z, rz, fmaf(w0.y, ry, fmaf(w0.x, rx, w0.w)));
+      const float z1 = fmaf(w1.z, rz, fmaf(w1.y, ry, fmaf(w1.x, rx, w1.w)));
+      pk[c] = tanh_bf16x2(pack_bf16(z0, z1));
     }
+    tmem_st32(tb + kColA1 + 32 * h, pk);
   }
   tmem_wait_st();
   fence_before();
@@ -307,22 +316,27 @@ __device__ __forceinline__ bool run_tile(Smem& s, const TcWeights& w, EpiState& 
     if (!mbar_wait(&s.d2_full[slot], use & 1, &s.abort_flag, err, 22)) return false;
     fence_after();
     const uint32_t col = tb + kColSlot0 + 128 * slot;
-    uint32_t out[64];
+    uint32_t v0[32], v1[32], out[32];
+    tmem_ld32(col + 64 * h, v0);
+    tmem_ld32(col + 64 * h + 32, v1);
+    tmem_wait_ld();
+    const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 64 * h);
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-      uint32_t v[32];
-      tmem_ld32(col + 32 * c, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int k = 0; k < 16; k++) {
-        const int n = q * 128 + c * 32 + 2 * k;
-        const float a = __uint_as_float(v[2 * k]) + __ldg(&w.b2[n]);
-        const float b = __uint_as_float(v[2 * k + 1]) + __ldg(&w.b2[n + 1]);
-        out[c * 16 + k] = tanh_bf16x2(pack_bf16(a, b));
-      }
+    for (int k = 0; k < 8; k++) {
+      const float4 b = bb[k];
+      out[2 * k] = tanh_bf16x2(pack_bf16(__uint_as_float(v0[4 * k]) + b.x, __uint_as_float(v0[4 * k + 1]) + b.y));
+      out[2 * k + 1] =
+          tanh_bf16x2(pack_bf16(__uint_as_float(v0[4 * k + 2]) + b.z, __uint_as_float(v0[4 * k + 3]) + b.w));
     }
-    tmem_st32(col, out);
-    tmem_st32(col + 32, out + 32);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float4 b = bb[8 + k];
+      out[16 + 2 * k] =
+          tanh_bf16x2(pack_bf16(__uint_as_float(v1[4 * k]) + b.x, __uint_as_float(v1[4 * k + 1]) + b.y));
+      out[16 + 2 * k + 1] =
+          tanh_bf16x2(pack_bf16(__uint_as_float(v1[4 * k + 2]) + b.z, __uint_as_float(v1[4 * k + 3]) + b.w));
+    }
+    tmem_st32(col + 64 * h, out);  // only columns this thread read itself
     tmem_wait_st();
     fence_before();
     mbar_arrive(&s.a2_full[slot]);
@@ -338,7 +352,7 @@ __device__ __forceinline__ bool run_tile(Smem& s, const TcWeights& w, EpiState& 
     const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
 #pragma unroll
     for (int o = 0; o < 9; o++) {
-      float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + __ldg(&w.b3[o]);
+      float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + s.b3[o];
       const bool dg = (o == 0 || o == 4 || o == 8);
       if (dg) y += 1.0f;
       y = y / nr;
@@ -351,14 +365,18 @@ __device__ __forceinline__ bool run_tile(Smem& s, const TcWeights& w, EpiState& 
   return true;
 }
 
-// Tells the MMA lane to stop (all 128 epilogue threads call it once).
+// Tells the MMA lane to stop (all 256 epilogue threads call it once).
 __device__ __forceinline__ void epi_finish(Smem& s) {
   if (threadIdx.x == 0) *(volatile int*)&s.exit_flag = 1;
-  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  asm volatile("bar.sync 1, 256;\n" ::: "memory");
   mbar_arrive(&s.a1_full);
 }
 
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+
+// Row (evaluation index within the tile) and column half of the calling epilogue thread.
+__device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
+__device__ __forceinline__ int epi_half() { return threadIdx.x >> 7; }
 
 }  // namespace tc
 }  // namespace hignn

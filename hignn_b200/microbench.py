@@ -1,0 +1,92 @@
+"""Kernel-level timings of the native library (CUDA events), for tuning and profiler captures.
+
+    python -m hignn_b200.microbench eval --n 378880 --precision 1
+    python -m hignn_b200.microbench dot --workload medium --precision 1 --fields 1
+
+Prints one JSON line: milliseconds per call and evaluations per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+WEIGHTS = os.path.join(HERE, "data", "two_body_unbounded.hgnw")
+FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["eval", "dot"])
+    ap.add_argument("--n", type=int, default=148 * 128 * 20)
+    ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m"])
+    ap.add_argument("--fields", type=int, default=3)
+    ap.add_argument("--epsilon", type=float, default=1e-2)
+    a = ap.parse_args()
+
+    import torch
+
+    from hignn_b200 import capi
+    from hignn_b200 import synthetic as S
+
+    out = {"what": a.what, "precision": a.precision}
+    if a.what == "eval":
+        rng = np.random.default_rng(1)
+        v = rng.normal(size=(a.n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        r = (v * np.exp(rng.uniform(np.log(2.0), np.log(300.0), a.n))[:, None]).astype(np.float32)
+        m = capi.Model(rng.uniform(0, 50, (256, 3)), 128, device=0)
+        m.load_two_body(WEIGHTS)
+        rt = torch.from_numpy(r).cuda()
+        y = torch.empty((a.n, 9), device="cuda")
+        stream = torch.cuda.ExternalStream(m.stream())
+        m.two_body_eval(rt.data_ptr(), y.data_ptr(), a.n, a.precision)
+        ts = []
+        for _ in range(a.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            m.two_body_eval(rt.data_ptr(), y.data_ptr(), a.n, a.precision)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.min(ts))
+        out.update(n=a.n, ms=ms, evals_per_s=a.n / ms * 1e3, tflops=a.n * FLOP_PER_EVAL / ms / 1e9)
+    else:
+        if a.workload == "uniform1m":
+            x, f = S.uniform(1048576, 0.1, 2), S.sedimenting_forces(1048576, 2)
+        elif a.workload == "large":
+            x, f = S.clustered(1048576, 0.10, 2), S.sedimenting_forces(1048576, 2)
+        else:
+            x, f, _ = S.workload(a.workload)
+        m = capi.Model(x, 128, device=0)
+        m.load_two_body(WEIGHTS)
+        m.set(capi.P_PRECISION, a.precision)
+        m.set(capi.P_FIELDS, a.fields)
+        m.set(capi.P_EPSILON, a.epsilon)
+        m.set(capi.P_TIMING, 1)
+        m.dot(f)
+        near, far = [], []
+        for _ in range(a.reps):
+            m.dot(f)
+            st = m.stats()
+            near.append(st["t_close_ms"])
+            far.append(st["t_far_ms"])
+        st = m.stats()
+        out.update(workload=a.workload, n=len(x), near_ms=float(np.min(near)), far_ms=float(np.min(far)),
+                   close_evals=st["close_evals"], far_evals=st["far_evals"],
+                   near_evals_per_s=st["close_evals"] / max(1e-9, np.min(near)) * 1e3,
+                   near_tflops=st["close_evals"] * FLOP_PER_EVAL / max(1e-9, np.min(near)) / 1e9,
+                   far_evals_per_s=st["far_evals"] / max(1e-9, np.min(far)) * 1e3 if st["far_evals"] else None,
+                   gpu_launches=st["gpu_launches"])
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
