@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     __syncwarp();
   } else {
     const int e = threadIdx.x;  // 0..255, staging / flush index
-    const int row = tc::epi_row(), h = tc::epi_half();
+    const int row = tc::epi_row(), h = tc::epi_group();
     tc::EpiState st;
     bool ok = true;
     for (;;) {
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             atomicAdd(&S.uI[i][0], M[0] * fj.x + M[1] * fj.y + M[2] * fj.z);
             atomicAdd(&S.uI[i][1], M[3] * fj.x + M[4] * fj.y + M[5] * fj.z);
             atomicAdd(&S.uI[i][2], M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
-          } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
+          } else if (h == 1 && trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
             const float4 fi = S.fI[i];
             atomicAdd(&S.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
             atomicAdd(&S.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_half();
+    const int row = tc::epi_row(), h = tc::epi_group();
     const int32_t* pre = which ? a.preJ : a.preI;
     tc::EpiState st;
     bool ok = true;
@@ -170,13 +170,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
       float M[9];
       ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
       if (!ok) break;
-      if (valid) {  // the two threads of a row store alternate entries
+      if (valid) {  // the four threads of a row store interleaved entries
         const FarBlock bk = a.blocks[b];
         double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                                  : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
 #pragma unroll
         for (int q = 0; q < 9; q++) {
-          if ((q & 1) != h) continue;
+          if ((q & 3) != h) continue;
           const int r = q / 3, c = q % 3;
           dst[q] = (r == c) ? (double)M[q] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
         }
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_half();
+    const int row = tc::epi_row(), h = tc::epi_group();
     tc::EpiState st;
     bool ok = true;
     for (int64_t base = (int64_t)blockIdx.x * tc::kTile; base < n; base += (int64_t)gridDim.x * tc::kTile) {
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       if (g < n)
 #pragma unroll
         for (int q = 0; q < 9; q++)
-          if ((q & 1) == h) y[9 * g + q] = M[q];
+          if ((q & 3) == h) y[9 * g + q] = M[q];
     }
     if (ok) tc::epi_finish(S.tcs);
   }

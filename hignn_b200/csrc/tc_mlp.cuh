@@ -8,19 +8,19 @@
 // systematic error of a plain BF16 layer 3, and the split removes it for ~6%
 // more tensor work. b1, b2, b3 stay FP32.
 //
-// CTA = 9 warps. Warps 0-7 (256 threads) are the epilogue: warp w reaches TMEM
+// CTA = 17 warps. Warps 0-15 (512 threads) are the epilogue: warp w reaches TMEM
 // lanes 32*(w%4)..+31, so evaluation (row) e = 32*(w%4) + lane is shared by the
-// threads of warps w%4 and w%4+4, which split every row's columns in halves
-// (h = w/4). Warp 8 allocates tensor memory and one elected lane issues all MMAs.
+// threads of warps w%4 + 4g (g = 0..3), which split every row's columns in four
+// groups of 32. Warp 16 allocates tensor memory and one elected lane issues all MMAs.
 //
 // Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs, the A operand of layer 2
 //   [ 64,448)  three 128-column slots: layer-2 accumulator of one quarter (128
 //              hidden units); after the epilogue reads it, the quarter's
-//              tanh'd BF16 values are written back into slot columns [0,32)
-//              (units 0-63, by half h=0) and [64,96) (units 64-127, h=1), each
-//              half writing only columns it read itself, and become the A
-//              operand of that quarter's layer-3 MMA
+//              tanh'd BF16 values (units 32g..32g+31 of group g) are written
+//              back into slot columns [32g, 32g+16), inside the range the
+//              group itself read, and become the A operand of that quarter's
+//              layer-3 MMA (K-step kk at column 32*(kk/2) + 8*(kk%2))
 //   [448,480)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
 // Shared memory: W2 (512 x 128 BF16) and W3 (32 x 512 BF16) in the canonical
 // K-major 128-byte-swizzle layout, loaded once per CTA; mbarriers.
@@ -42,9 +42,9 @@ namespace hignn {
 namespace tc {
 
 constexpr int kTile = 128;
-constexpr int kEpiThreads = 256;
-constexpr int kThreads = 288;
-constexpr int kMmaWarp = 8;
+constexpr int kEpiThreads = 512;
+constexpr int kThreads = 544;
+constexpr int kMmaWarp = 16;
 constexpr uint32_t kColA1 = 0, kColSlot0 = 64, kColD3 = 448;
 constexpr int kW2Bytes = kH2 * kH1 * 2;   // 131072
 constexpr int kW3Rows = 32;
@@ -61,7 +61,7 @@ struct alignas(1024) Smem {
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
-  alignas(16) float b2[kH2];
+  alignas(16) uint32_t b2p[kH2 / 2];  // b2 as packed BF16 pairs
   alignas(16) float4 w1b1[kH1];
   float b3[16];
 };
@@ -152,6 +152,21 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
       : "memory");
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+
+__device__ __forceinline__ uint32_t add_bf16x2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("add.rn.bf16x2 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   uint32_t r;
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
@@ -188,7 +203,7 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   const uint4* src3 = w.w3img;
   uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
   for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
-  for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
+  for (int i = t; i < kH2 / 2; i += blockDim.x) s.b2p[i] = pack_bf16(w.b2[2 * i], w.b2[2 * i + 1]);
   for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t == 0) {
@@ -263,7 +278,7 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
       for (uint32_t kk = 0; kk < 8; kk++) {
         const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
         const uint32_t b = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-        const uint32_t a_off = kk < 4 ? 8 * kk : 64 + 8 * (kk - 4);  // A2 halves at slot cols 0 and 64
+        const uint32_t a_off = 32 * (kk >> 1) + 8 * (kk & 1);  // group g's A2 at slot cols 32g..32g+15
         mma_ts(tbase + kColD3, acol + a_off, sdesc(b), id_l3, (q > 0 || kk > 0) ? 1u : 0u);
       }
       mma_commit(&s.slot_free[slot]);
@@ -286,57 +301,49 @@ struct EpiState {
 };
 
 // Runs one tile for this thread's evaluation (row) with features r; writes M (row-major 3x3)
-// into both threads of the row. Returns false if the CTA aborted. All 256 epilogue threads
-// must call it together.
+// into all four threads of the row. Returns false if the CTA aborted. All 512 epilogue
+// threads must call it together.
 __device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float ry, float rz, float (&M)[9],
                                          int* err) {
-  const int w = threadIdx.x >> 5;          // 0..7
-  const int h = w >> 2;                     // column half
+  const int w = threadIdx.x >> 5;          // 0..15
+  const int g = w >> 2;                     // column group
   const uint32_t tb = s.tmem_base + ((uint32_t)(32 * (w & 3)) << 16);
   // A1 is free once the previous tile's layer-2 MMAs completed
   if (st.tile > 0 && !mbar_wait(&s.a1_free, (st.tile - 1) & 1, &s.abort_flag, err, 21)) return false;
   fence_after();
   {
-    uint32_t pk[32];
+    uint32_t pk[16];
 #pragma unroll
-    for (int c = 0; c < 32; c++) {
-      const float4 w0 = s.w1b1[64 * h + 2 * c];
-      const float4 w1 = s.w1b1[64 * h + 2 * c + 1];
+    for (int c = 0; c < 16; c++) {
+      const float4 w0 = s.w1b1[32 * g + 2 * c];
+      const float4 w1 = s.w1b1[32 * g + 2 * c + 1];
       const float z0 = fmaf(w0.z, rz, fmaf(w0.y, ry, fmaf(w0.x, rx, w0.w)));
       const float z1 = fmaf(w1.z, rz, fmaf(w1.y, ry, fmaf(w1.x, rx, w1.w)));
       pk[c] = tanh_bf16x2(pack_bf16(z0, z1));
     }
-    tmem_st32(tb + kColA1 + 32 * h, pk);
+    tmem_st16(tb + kColA1 + 16 * g, pk);
   }
   tmem_wait_st();
   fence_before();
   mbar_arrive(&s.a1_full);
   for (uint32_t q = 0; q < 4; q++) {
-    const uint32_t g = st.gq + q, slot = g % 3, use = g / 3;
+    const uint32_t gg = st.gq + q, slot = gg % 3, use = gg / 3;
     if (!mbar_wait(&s.d2_full[slot], use & 1, &s.abort_flag, err, 22)) return false;
     fence_after();
     const uint32_t col = tb + kColSlot0 + 128 * slot;
-    uint32_t v0[32], v1[32], out[32];
-    tmem_ld32(col + 64 * h, v0);
-    tmem_ld32(col + 64 * h + 32, v1);
+    uint32_t v[32], out[16];
+    tmem_ld32(col + 32 * g, v);
     tmem_wait_ld();
-    const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 64 * h);
+    const uint4* bb = reinterpret_cast<const uint4*>(s.b2p + q * 64 + 16 * g);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const float4 b = bb[k];
-      out[2 * k] = tanh_bf16x2(pack_bf16(__uint_as_float(v0[4 * k]) + b.x, __uint_as_float(v0[4 * k + 1]) + b.y));
-      out[2 * k + 1] =
-          tanh_bf16x2(pack_bf16(__uint_as_float(v0[4 * k + 2]) + b.z, __uint_as_float(v0[4 * k + 3]) + b.w));
+    for (int k = 0; k < 4; k++) {
+      const uint4 b = bb[k];
+      out[4 * k + 0] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 0]), __uint_as_float(v[8 * k + 1])), b.x));
+      out[4 * k + 1] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 2]), __uint_as_float(v[8 * k + 3])), b.y));
+      out[4 * k + 2] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5])), b.z));
+      out[4 * k + 3] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])), b.w));
     }
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const float4 b = bb[8 + k];
-      out[16 + 2 * k] =
-          tanh_bf16x2(pack_bf16(__uint_as_float(v1[4 * k]) + b.x, __uint_as_float(v1[4 * k + 1]) + b.y));
-      out[16 + 2 * k + 1] =
-          tanh_bf16x2(pack_bf16(__uint_as_float(v1[4 * k + 2]) + b.z, __uint_as_float(v1[4 * k + 3]) + b.w));
-    }
-    tmem_st32(col + 64 * h, out);  // only columns this thread read itself
+    tmem_st16(col + 32 * g, out);  // inside the columns this thread read itself
     tmem_wait_st();
     fence_before();
     mbar_arrive(&s.a2_full[slot]);
@@ -365,18 +372,18 @@ __device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float 
   return true;
 }
 
-// Tells the MMA lane to stop (all 256 epilogue threads call it once).
+// Tells the MMA lane to stop (all 512 epilogue threads call it once).
 __device__ __forceinline__ void epi_finish(Smem& s) {
   if (threadIdx.x == 0) *(volatile int*)&s.exit_flag = 1;
-  asm volatile("bar.sync 1, 256;\n" ::: "memory");
+  asm volatile("bar.sync 1, 512;\n" ::: "memory");
   mbar_arrive(&s.a1_full);
 }
 
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
 
 // Row (evaluation index within the tile) and column half of the calling epilogue thread.
 __device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
-__device__ __forceinline__ int epi_half() { return threadIdx.x >> 7; }
+__device__ __forceinline__ int epi_group() { return threadIdx.x >> 7; }
 
 }  // namespace tc
 }  // namespace hignn
