@@ -1,12 +1,14 @@
 // Tensor-core (tcgen05) forms of the near field, the ACA queries and the stand-alone evaluation.
 //
-// All three kernels are persistent (one CTA per SM, ~190 KB shared memory, 512
-// TMEM columns) and share the tile engine of tc_mlp.cuh; they differ only in
-// where an evaluation's features come from and where its 3x3 goes:
-//   k_near_tc : close pair (I, J) flattened into 128-evaluation tiles; the
-//               contraction u_I += M f_J (and u_J += M f_I for J > I) is reduced
-//               per particle in shared memory and flushed with one FP64 atomic
-//               per particle and component per pair (src/CloseDot.cpp:245-299).
+// All three kernels are persistent (one CTA per SM, up to ~213 KB shared
+// memory, 512 TMEM columns) and share the tile engine of tc_mlp.cuh. Each CTA
+// runs two independent epilogue groups (tile contexts); every group walks its
+// own share of the work:
+//   k_near_tc : close pairs (I, J) fetched from a global counter, flattened into
+//               128-evaluation tiles; the contraction u_I += M f_J (and u_J +=
+//               M f_I for J > I) is reduced per particle in shared memory and
+//               flushed with one FP64 atomic per particle and component per pair
+//               (src/CloseDot.cpp:245-299).
 //   k_far_tc  : column / row queries of all active ACA blocks, symmetrised into
 //               the FP64 C / Q pools (src/FarDot.cpp:348-458, 672-781).
 //   k_eval_tc : M(r) for an array of features.
@@ -23,12 +25,46 @@ __device__ __forceinline__ uint8_t* align1k(uint8_t* p) {
   return p + ((1024u - (a & 1023u)) & 1023u);
 }
 
-struct NearTcSmem {
-  tc::Smem tcs;
+struct NearStage {
   float4 xI[kMaxLeaf], xJ[kMaxLeaf], fI[kMaxLeaf], fJ[kMaxLeaf];
   float uI[kMaxLeaf][3], uJ[kMaxLeaf][3];
   int item;
 };
+
+struct NearTcSmem {
+  tc::Smem tcs;
+  NearStage st[2];
+};
+
+// u_I[i] += v for the rows of a warp: rows of a tile share few i (contiguous), so lanes with
+// equal i are summed by a segmented shuffle reduction and only segment heads add to shared memory.
+__device__ __forceinline__ void add_segmented(float (*uI)[3], int i, float v0, float v1, float v2) {
+  const unsigned act = __activemask();
+  if (act == 0xffffffffu) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float t0 = __shfl_down_sync(act, v0, o), t1 = __shfl_down_sync(act, v1, o),
+                  t2 = __shfl_down_sync(act, v2, o);
+      const int ko = __shfl_down_sync(act, i, o);
+      if (lane + o < 32 && ko == i) {
+        v0 += t0;
+        v1 += t1;
+        v2 += t2;
+      }
+    }
+    const int kp = __shfl_up_sync(act, i, 1);
+    if (lane == 0 || kp != i) {
+      atomicAdd(&uI[i][0], v0);
+      atomicAdd(&uI[i][1], v1);
+      atomicAdd(&uI[i][2], v2);
+    }
+  } else {
+    atomicAdd(&uI[i][0], v0);
+    atomicAdd(&uI[i][1], v1);
+    atomicAdd(&uI[i][2], v2);
+  }
+}
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
     k_near_tc(NearArgs a, TcWeights w, int* work_counter, int* err) {
@@ -40,27 +76,28 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int e = threadIdx.x;  // 0..255, staging / flush index
-    const int row = tc::epi_row(), h = tc::epi_group();
+    NearStage& G = S.st[tc::epi_group()];
+    const int e = tc::epi_gthread();  // staging / flush index within the group
+    const int row = tc::epi_row(), h = tc::epi_half();
     tc::EpiState st;
     bool ok = true;
     for (;;) {
-      if (e == 0) S.item = atomicAdd(work_counter, 1);
+      if (e == 0) G.item = atomicAdd(work_counter, 1);
       tc::epi_bar();
-      const int item = S.item;
+      const int item = G.item;
       if (item >= a.nwork) break;
       const PairWork pw = a.work[item];
       const bool trans = (pw.flags & kPairTransposed) != 0;
       const bool symm = (pw.flags & kPairSymmetrize) != 0;
-      for (int i = e; i < pw.nI; i += tc::kEpiThreads) {
-        S.xI[i] = a.xI[pw.sI + i];
-        S.fI[i] = a.fI[pw.sI + i];
-        S.uI[i][0] = S.uI[i][1] = S.uI[i][2] = 0.f;
+      for (int i = e; i < pw.nI; i += tc::kGroupThreads) {
+        G.xI[i] = a.xI[pw.sI + i];
+        G.fI[i] = a.fI[pw.sI + i];
+        G.uI[i][0] = G.uI[i][1] = G.uI[i][2] = 0.f;
       }
-      for (int j = e; j < pw.nJ; j += tc::kEpiThreads) {
-        S.xJ[j] = a.xJ[pw.sJ + j];
-        S.fJ[j] = a.fJ[pw.sJ + j];
-        S.uJ[j][0] = S.uJ[j][1] = S.uJ[j][2] = 0.f;
+      for (int j = e; j < pw.nJ; j += tc::kGroupThreads) {
+        G.xJ[j] = a.xJ[pw.sJ + j];
+        G.fJ[j] = a.fJ[pw.sJ + j];
+        G.uJ[j][0] = G.uJ[j][1] = G.uJ[j][2] = 0.f;
       }
       tc::epi_bar();
       const int total = pw.nI * pw.nJ;
@@ -71,7 +108,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int j = valid ? flat - i * pw.nJ : 0;
         float rx = 1.f, ry = 0.f, rz = 0.f;
         if (valid) {
-          const float4 xi = S.xI[i], xj = S.xJ[j];
+          const float4 xi = G.xI[i], xj = G.xJ[j];
           rx = xj.x - xi.x;
           ry = xj.y - xi.y;
           rz = xj.z - xi.z;
@@ -91,25 +128,24 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
               }
           }
           if (h == 0) {  // u_I[i] += M f_J[j]
-            const float4 fj = S.fJ[j];
-            atomicAdd(&S.uI[i][0], M[0] * fj.x + M[1] * fj.y + M[2] * fj.z);
-            atomicAdd(&S.uI[i][1], M[3] * fj.x + M[4] * fj.y + M[5] * fj.z);
-            atomicAdd(&S.uI[i][2], M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
-          } else if (h == 1 && trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
-            const float4 fi = S.fI[i];
-            atomicAdd(&S.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
-            atomicAdd(&S.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
-            atomicAdd(&S.uJ[j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
+            const float4 fj = G.fJ[j];
+            add_segmented(G.uI, i, M[0] * fj.x + M[1] * fj.y + M[2] * fj.z, M[3] * fj.x + M[4] * fj.y + M[5] * fj.z,
+                          M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
+          } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
+            const float4 fi = G.fI[i];
+            atomicAdd(&G.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
+            atomicAdd(&G.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
+            atomicAdd(&G.uJ[j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
           }
         }
       }
       if (!ok) break;
       tc::epi_bar();
-      for (int q = e; q < 3 * pw.nI; q += tc::kEpiThreads)
-        atomicAdd(&a.uI[3 * (size_t)pw.sI + q], (double)(&S.uI[0][0])[q]);
+      for (int q = e; q < 3 * pw.nI; q += tc::kGroupThreads)
+        atomicAdd(&a.uI[3 * (size_t)pw.sI + q], (double)(&G.uI[0][0])[q]);
       if (trans)
-        for (int q = e; q < 3 * pw.nJ; q += tc::kEpiThreads)
-          atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&S.uJ[0][0])[q]);
+        for (int q = e; q < 3 * pw.nJ; q += tc::kGroupThreads)
+          atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&G.uJ[0][0])[q]);
       tc::epi_bar();
     }
     if (ok) tc::epi_finish(S.tcs);
@@ -126,18 +162,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
   FarTcSmem& S = *reinterpret_cast<FarTcSmem*>(align1k(smem_raw));
   const int nact = a.ctr[kCtrActive];
   const int tot = which ? a.ctr[kCtrTotJ] : a.ctr[kCtrTotI];
-  if ((int)blockIdx.x * tc::kTile >= tot) return;  // uniform: before any setup
+  if (2 * (int)blockIdx.x * tc::kTile >= tot) return;  // uniform: before any setup
   tc::cta_setup(S.tcs, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == tc::kMmaWarp) {
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_group();
+    const int row = tc::epi_row(), h = tc::epi_half();
     const int32_t* pre = which ? a.preJ : a.preI;
     tc::EpiState st;
     bool ok = true;
-    for (int tile = blockIdx.x; tile * tc::kTile < tot; tile += gridDim.x) {
+    for (int tile = 2 * blockIdx.x + tc::epi_group(); tile * tc::kTile < tot; tile += 2 * gridDim.x) {
       const int g = tile * tc::kTile + row;
       const bool valid = g < tot;
       float rx = 1.f, ry = 0.f, rz = 0.f;
@@ -170,13 +206,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
       float M[9];
       ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
       if (!ok) break;
-      if (valid) {  // the four threads of a row store interleaved entries
+      if (valid) {  // the two threads of a row store alternate entries
         const FarBlock bk = a.blocks[b];
         double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                                  : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
 #pragma unroll
         for (int q = 0; q < 9; q++) {
-          if ((q & 3) != h) continue;
+          if ((q & 1) != h) continue;
           const int r = q / 3, c = q % 3;
           dst[q] = (r == c) ? (double)M[q] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
         }
@@ -202,11 +238,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_group();
+    const int row = tc::epi_row(), h = tc::epi_half();
     tc::EpiState st;
     bool ok = true;
-    for (int64_t base = (int64_t)blockIdx.x * tc::kTile; base < n; base += (int64_t)gridDim.x * tc::kTile) {
-      const int64_t g = base + row;
+    for (int64_t tile = 2 * (int64_t)blockIdx.x + tc::epi_group(); tile * tc::kTile < n;
+         tile += 2 * (int64_t)gridDim.x) {
+      const int64_t g = tile * tc::kTile + row;
       float rx = 1.f, ry = 0.f, rz = 0.f;
       if (g < n) {
         rx = r[3 * g];
@@ -219,7 +256,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       if (g < n)
 #pragma unroll
         for (int q = 0; q < 9; q++)
-          if ((q & 3) == h) y[9 * g + q] = M[q];
+          if ((q & 1) == h) y[9 * g + q] = M[q];
     }
     if (ok) tc::epi_finish(S.tcs);
   }
@@ -259,7 +296,8 @@ void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int
   const size_t smem = sizeof(EvalTcSmem) + 1024;
   set_smem(k_eval_tc, smem);
   const int64_t tiles = (n + tc::kTile - 1) / tc::kTile;
-  const int grid = (int)(tiles < num_sms ? tiles : num_sms);
+  const int64_t pairs = (tiles + 1) / 2;
+  const int grid = (int)(pairs < num_sms ? pairs : num_sms);
   k_eval_tc<<<grid, tc::kThreads, smem, s>>>(r, y, n, w, err);
   HIGNN_CHECK_LAUNCH();
 }

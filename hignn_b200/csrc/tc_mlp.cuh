@@ -2,34 +2,37 @@
 //
 // Mixed precision: layer 1 (3 -> 128) in FP32 on the CUDA cores; layers 2
 // (128 -> 512) and 3 (512 -> 9) as BF16 tcgen05 MMAs with FP32 accumulation in
-// tensor memory; tanh as tanh.approx.bf16x2 (two per MUFU op) on bias-added
-// FP32 accumulators. W3 is split into a BF16 high part and a BF16 residual
-// (rows 0-8 and 16-24 of one N=32 operand): its rounding is the dominant
-// systematic error of a plain BF16 layer 3, and the split removes it for ~6%
-// more tensor work. b1, b2, b3 stay FP32.
+// tensor memory; tanh as tanh.approx.bf16x2 (two per MUFU op) on the
+// accumulators rounded to BF16 plus the BF16 bias. W3 is split into a BF16
+// high part and a BF16 residual (rows 0-8 and 16-24 of one N=32 operand): its
+// rounding is the dominant systematic error of a plain BF16 layer 3, and the
+// split removes it for ~6% more tensor work. b1 and b3 stay FP32.
 //
-// CTA = 17 warps. Warps 0-15 (512 threads) are the epilogue: warp w reaches TMEM
-// lanes 32*(w%4)..+31, so evaluation (row) e = 32*(w%4) + lane is shared by the
-// threads of warps w%4 + 4g (g = 0..3), which split every row's columns in four
-// groups of 32. Warp 16 allocates tensor memory and one elected lane issues all MMAs.
-//
-// Tensor memory (512 columns allocated):
-//   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs, the A operand of layer 2
-//   [ 64,448)  three 128-column slots: layer-2 accumulator of one quarter (128
-//              hidden units); after the epilogue reads it, the quarter's
-//              tanh'd BF16 values (units 32g..32g+31 of group g) are written
-//              back into slot columns [32g, 32g+16), inside the range the
-//              group itself read, and become the A operand of that quarter's
-//              layer-3 MMA (K-step kk at column 32*(kk/2) + 8*(kk%2))
-//   [448,480)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
+// Two tile contexts per CTA so that tanh work of one overlaps the MMAs of the
+// other. CTA = 17 warps:
+//   warps 0-7   epilogue group 0 (context 0), warps 8-15 epilogue group 1;
+//               warp w reaches TMEM lanes 32*(w%4)..+31, so the evaluation (row)
+//               e = 32*(w%4) + lane of a context is handled by two threads
+//               (warps w and w+4 of the group), each owning one half of every
+//               row's columns;
+//   warp 16     allocates tensor memory; one lane issues every MMA, serving the
+//               two contexts as their operands become ready.
+// Tensor memory (512 columns allocated), per context c at column 224c:
+//   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs (A operand of layer 2)
+//   [ 64,192)  slot: layer-2 accumulator of one quarter (128 hidden units);
+//              after the epilogue reads it, the quarter's tanh'd BF16 pairs
+//              are written back into slot columns [0,32) (units 0-63, half 0)
+//              and [64,96) (units 64-127, half 1) -- each half writes only
+//              columns it read itself -- and are the A operand of layer 3
+//   [192,224)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
 // Shared memory: W2 (512 x 128 BF16) and W3 (32 x 512 BF16) in the canonical
-// K-major 128-byte-swizzle layout, loaded once per CTA; mbarriers.
+// K-major 128-byte-swizzle layout, loaded once per CTA; biases; mbarriers.
 //
-// Schedule per tile (q = quarter of the 512 hidden units):
-//   epilogue: layer 1 -> A1 ; for q: wait D2(q), tanh -> A2(q) ; wait D3, wrapper
-//   MMA lane: L2(0) L2(1) L2(2) | L3(0) L2(3) | L3(1) | L3(2) | L3(3)
-// Every wait is bounded (about two seconds of clock): on a timeout the CTA
-// records an error, stops issuing work, drains its MMAs and frees its tensor memory.
+// Per context and tile: epilogue layer 1 -> A1; then for each quarter q:
+// MMA L2(q) -> slot, epilogue tanh -> A2(q) in the slot, MMA L3(q) -> D3; the
+// next L2 waits until L3(q) has read the slot. Every wait is bounded (about two
+// seconds of clock): on a timeout the CTA records an error, stops issuing
+// work, drains its MMAs and frees its tensor memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,25 +44,31 @@
 namespace hignn {
 namespace tc {
 
+using hignn::TcWeights;
+
 constexpr int kTile = 128;
+constexpr int kGroupThreads = 256;
 constexpr int kEpiThreads = 512;
 constexpr int kThreads = 544;
 constexpr int kMmaWarp = 16;
-constexpr uint32_t kColA1 = 0, kColSlot0 = 64, kColD3 = 448;
+constexpr uint32_t kCtxCols = 224, kOffA1 = 0, kOffSlot = 64, kOffD3 = 192;
 constexpr int kW2Bytes = kH2 * kH1 * 2;   // 131072
 constexpr int kW3Rows = 32;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 32768
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
-using hignn::TcWeights;
+struct CtxBars {
+  uint64_t a1_full, a1_free, d2_full, a2_full, slot_free, d3_full, d3_free;
+  int exit_flag;
+  int pad;
+};
 
 struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
   uint8_t w3[kW3Bytes];
-  uint64_t a1_full, a1_free, d3_full, d3_free, drain;
-  uint64_t d2_full[3], a2_full[3], slot_free[3];
+  CtxBars ctx[2];
+  uint64_t drain;
   uint32_t tmem_base;
-  int exit_flag;
   int abort_flag;
   alignas(16) uint32_t b2p[kH2 / 2];  // b2 as packed BF16 pairs
   alignas(16) float4 w1b1[kH1];
@@ -111,14 +120,7 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols));
 }
 
-// D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::f16 (BF16 inputs, FP32 accumulate)
-__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-// D[tmem] (+)= A[tmem] * B[smem desc]^T
+// D[tmem] (+)= A[tmem] * B[smem desc]^T, kind::f16 (BF16 inputs, FP32 accumulate)
 __device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
@@ -152,24 +154,14 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(
-          taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
-      : "memory");
-}
-
-__device__ __forceinline__ uint32_t add_bf16x2(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("add.rn.bf16x2 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(b));
-  return r;
-}
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   uint32_t r;
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ uint32_t add_bf16x2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("add.rn.bf16x2 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(b));
   return r;
 }
 __device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x) {
@@ -196,7 +188,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 // ------------------------------------------------------------------ per-CTA setup / teardown
 __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   const int t = threadIdx.x;
-  // weight images (the host builds them in the swizzled layout)
   const uint4* src2 = w.w2img;
   uint4* dst2 = reinterpret_cast<uint4*>(s.w2);
   for (int i = t; i < kW2Bytes / 16; i += blockDim.x) dst2[i] = src2[i];
@@ -207,17 +198,18 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t == 0) {
-    mbar_init(&s.a1_full, kEpiThreads);
-    mbar_init(&s.a1_free, 1);
-    mbar_init(&s.d3_full, 1);
-    mbar_init(&s.d3_free, kEpiThreads);
-    mbar_init(&s.drain, 1);
-    for (int q = 0; q < 3; q++) {
-      mbar_init(&s.d2_full[q], 1);
-      mbar_init(&s.a2_full[q], kEpiThreads);
-      mbar_init(&s.slot_free[q], 1);
+    for (int c = 0; c < 2; c++) {
+      CtxBars& b = s.ctx[c];
+      mbar_init(&b.a1_full, kGroupThreads);
+      mbar_init(&b.a1_free, 1);
+      mbar_init(&b.d2_full, 1);
+      mbar_init(&b.a2_full, kGroupThreads);
+      mbar_init(&b.slot_free, 1);
+      mbar_init(&b.d3_full, 1);
+      mbar_init(&b.d3_free, kGroupThreads);
+      b.exit_flag = 0;
     }
-    s.exit_flag = 0;
+    mbar_init(&s.drain, 1);
     s.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -236,58 +228,87 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
   if ((threadIdx.x >> 5) == kMmaWarp) tmem_dealloc(s.tmem_base, 512);
 }
 
-// ------------------------------------------------------------------ MMA warp (one elected lane)
-// Processes tiles until the epilogue raises exit_flag (or a wait times out).
+// ------------------------------------------------------------------ MMA lane
+// Non-blocking state machine per context; mma_loop returns when both epilogue groups
+// raised their exit flags (or the CTA aborted / nothing progressed for kWaitCycles).
+struct MmaCtx {
+  uint32_t tile = 0, q = 0, state = 0, l2s = 0, l3s = 0;
+  bool done = false;
+};
+
+__device__ __forceinline__ bool mma_step(Smem& s, MmaCtx& x, uint32_t c, uint32_t tbase, uint32_t w2, uint32_t w3) {
+  CtxBars& b = s.ctx[c];
+  const uint32_t base = tbase + c * kCtxCols;
+  const uint32_t id_l2 = idesc_bf16(128, 128), id_l3 = idesc_bf16(128, kW3Rows);
+  if (x.state == 0) {  // waiting for A1 of the next tile (or the exit signal)
+    if (!mbar_try(&b.a1_full, x.tile & 1)) return false;
+    fence_after();
+    if (*(volatile int*)&b.exit_flag) {
+      x.done = true;
+      return true;
+    }
+    x.q = 0;
+    x.state = 1;
+    return true;
+  }
+  if (x.state == 1) {  // layer 2 of quarter q, once layer 3 of the previous quarter released the slot
+    if (x.l3s > 0 && !mbar_try(&b.slot_free, (x.l3s - 1) & 1)) return false;
+    fence_after();
+#pragma unroll
+    for (uint32_t kk = 0; kk < 8; kk++) {
+      const uint32_t bb = w2 + (kk >> 2) * (kH2 * 128) + x.q * (128 * 128) + (kk & 3) * 32;
+      mma_ts(base + kOffSlot, base + kOffA1 + 8 * kk, sdesc(bb), id_l2, kk > 0);
+    }
+    mma_commit(&b.d2_full);
+    if (x.q == 3) mma_commit(&b.a1_free);
+    x.l2s++;
+    x.state = 2;
+    return true;
+  }
+  // state 2: layer 3 of quarter q, once the epilogue wrote A2 (and, for q = 0, read the last D3)
+  if (!mbar_try(&b.a2_full, (x.l2s - 1) & 1)) return false;
+  if (x.q == 0 && x.tile > 0 && !mbar_try(&b.d3_free, (x.tile - 1) & 1)) return false;
+  fence_after();
+#pragma unroll
+  for (uint32_t kk = 0; kk < 8; kk++) {
+    const uint32_t kg = x.q * 128 + kk * 16;  // global K of layer 3
+    const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
+    const uint32_t a_off = kk < 4 ? 8 * kk : 64 + 8 * (kk - 4);  // A2 halves at slot columns 0 and 64
+    mma_ts(base + kOffD3, base + kOffSlot + a_off, sdesc(bb), id_l3, (x.q > 0 || kk > 0) ? 1u : 0u);
+  }
+  mma_commit(&b.slot_free);
+  x.l3s++;
+  if (x.q == 3) {
+    mma_commit(&b.d3_full);
+    x.tile++;
+    x.state = 0;
+  } else {
+    x.q++;
+    x.state = 1;
+  }
+  return true;
+}
+
 __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
   const uint32_t tbase = s.tmem_base;
-  const uint32_t id_l2 = idesc_bf16(128, 128), id_l3 = idesc_bf16(128, kW3Rows);
   const uint32_t w2 = saddr(s.w2), w3 = saddr(s.w3);
-  uint32_t tile = 0, gq = 0, pending_l3 = 0;
-  for (;; tile++) {
-    if (!mbar_wait(&s.a1_full, tile & 1, &s.abort_flag, err, 11)) break;
-    fence_after();
-    if (*(volatile int*)&s.exit_flag) break;
-    uint32_t issued = 0;
-    bool ok = true;
-    for (uint32_t q = 0; q < 4 && ok; q++) {
-      while (issued < 4 && issued <= q + 2) {  // layer 2 up to three quarters ahead
-        const uint32_t g = gq + issued, slot = g % 3, use = g / 3;
-        if (use > 0 && !mbar_wait(&s.slot_free[slot], (use - 1) & 1, &s.abort_flag, err, 12)) {
-          ok = false;
-          break;
-        }
-        fence_after();
-        const uint32_t dcol = tbase + kColSlot0 + 128 * slot;
-#pragma unroll
-        for (uint32_t kk = 0; kk < 8; kk++) {
-          // B: rows 128*issued.. of W2, K columns 16*kk..; A: A1 columns 8*kk..
-          const uint32_t b = w2 + (kk >> 2) * (kH2 * 128) + issued * (128 * 128) + (kk & 3) * 32;
-          mma_ts(dcol, tbase + kColA1 + 8 * kk, sdesc(b), id_l2, kk > 0);
-        }
-        mma_commit(&s.d2_full[slot]);
-        if (issued == 3) mma_commit(&s.a1_free);
-        issued++;
+  MmaCtx x[2];
+  long long last = clock64();
+  while (!(x[0].done && x[1].done)) {
+    bool prog = false;
+    if (!x[0].done) prog |= mma_step(s, x[0], 0, tbase, w2, w3);
+    if (!x[1].done) prog |= mma_step(s, x[1], 1, tbase, w2, w3);
+    if (prog) {
+      last = clock64();
+    } else {
+      if (*(volatile int*)&s.abort_flag) break;
+      if (clock64() - last > kWaitCycles) {
+        atomicExch(&s.abort_flag, 1);
+        atomicCAS(err, 0, 11);
+        break;
       }
-      if (!ok) break;
-      const uint32_t g = gq + q, slot = g % 3, use = g / 3;
-      if (!mbar_wait(&s.a2_full[slot], use & 1, &s.abort_flag, err, 13)) break;
-      if (q == 0 && tile > 0 && !mbar_wait(&s.d3_free, (tile - 1) & 1, &s.abort_flag, err, 14)) break;
-      fence_after();
-      const uint32_t acol = tbase + kColSlot0 + 128 * slot;
-#pragma unroll
-      for (uint32_t kk = 0; kk < 8; kk++) {
-        const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
-        const uint32_t b = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-        const uint32_t a_off = 32 * (kk >> 1) + 8 * (kk & 1);  // group g's A2 at slot cols 32g..32g+15
-        mma_ts(tbase + kColD3, acol + a_off, sdesc(b), id_l3, (q > 0 || kk > 0) ? 1u : 0u);
-      }
-      mma_commit(&s.slot_free[slot]);
-      if (q == 3) mma_commit(&s.d3_full);
     }
-    if (*(volatile int*)&s.abort_flag) break;
-    gq += 4;
   }
-  (void)pending_l3;
   // drain: every MMA issued so far completes before tensor memory is released
   mma_commit(&s.drain);
   const long long t0 = clock64();
@@ -297,65 +318,80 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
 
 // ------------------------------------------------------------------ epilogue side
 struct EpiState {
-  uint32_t tile = 0, gq = 0;
+  uint32_t tile = 0, quarters = 0;
 };
 
-// Runs one tile for this thread's evaluation (row) with features r; writes M (row-major 3x3)
-// into all four threads of the row. Returns false if the CTA aborted. All 512 epilogue
-// threads must call it together.
+__device__ __forceinline__ int epi_group() { return threadIdx.x >> 8; }                      // context 0 / 1
+__device__ __forceinline__ int epi_gthread() { return threadIdx.x & 255; }                   // 0..255 in group
+__device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
+__device__ __forceinline__ int epi_half() { return (threadIdx.x >> 7) & 1; }                 // column half
+__device__ __forceinline__ void epi_bar() {
+  if (epi_group() == 0)
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+  else
+    asm volatile("bar.sync 2, 256;\n" ::: "memory");
+}
+
+// One tile for this thread's evaluation (row) with features r; writes M (row-major 3x3) into
+// both threads of the row. Returns false if the CTA aborted. All 256 threads of the group
+// call it together.
 __device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float ry, float rz, float (&M)[9],
                                          int* err) {
-  const int w = threadIdx.x >> 5;          // 0..15
-  const int g = w >> 2;                     // column group
-  const uint32_t tb = s.tmem_base + ((uint32_t)(32 * (w & 3)) << 16);
-  // A1 is free once the previous tile's layer-2 MMAs completed
-  if (st.tile > 0 && !mbar_wait(&s.a1_free, (st.tile - 1) & 1, &s.abort_flag, err, 21)) return false;
+  const int c = epi_group(), h = epi_half();
+  CtxBars& b = s.ctx[c];
+  const uint32_t tb = s.tmem_base + c * kCtxCols + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16);
+  if (st.tile > 0 && !mbar_wait(&b.a1_free, (st.tile - 1) & 1, &s.abort_flag, err, 21)) return false;
   fence_after();
   {
-    uint32_t pk[16];
+    uint32_t pk[32];
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
-      const float4 w0 = s.w1b1[32 * g + 2 * c];
-      const float4 w1 = s.w1b1[32 * g + 2 * c + 1];
+    for (int k = 0; k < 32; k++) {
+      const float4 w0 = s.w1b1[64 * h + 2 * k];
+      const float4 w1 = s.w1b1[64 * h + 2 * k + 1];
       const float z0 = fmaf(w0.z, rz, fmaf(w0.y, ry, fmaf(w0.x, rx, w0.w)));
       const float z1 = fmaf(w1.z, rz, fmaf(w1.y, ry, fmaf(w1.x, rx, w1.w)));
-      pk[c] = tanh_bf16x2(pack_bf16(z0, z1));
+      pk[k] = tanh_bf16x2(pack_bf16(z0, z1));
     }
-    tmem_st16(tb + kColA1 + 16 * g, pk);
+    tmem_st32(tb + kOffA1 + 32 * h, pk);
   }
   tmem_wait_st();
   fence_before();
-  mbar_arrive(&s.a1_full);
+  mbar_arrive(&b.a1_full);
   for (uint32_t q = 0; q < 4; q++) {
-    const uint32_t gg = st.gq + q, slot = gg % 3, use = gg / 3;
-    if (!mbar_wait(&s.d2_full[slot], use & 1, &s.abort_flag, err, 22)) return false;
+    if (!mbar_wait(&b.d2_full, st.quarters & 1, &s.abort_flag, err, 22)) return false;
     fence_after();
-    const uint32_t col = tb + kColSlot0 + 128 * slot;
-    uint32_t v[32], out[16];
-    tmem_ld32(col + 32 * g, v);
-    tmem_wait_ld();
-    const uint4* bb = reinterpret_cast<const uint4*>(s.b2p + q * 64 + 16 * g);
+    const uint32_t col = tb + kOffSlot + 64 * h;
+    uint32_t out[32];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint4 b = bb[k];
-      out[4 * k + 0] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 0]), __uint_as_float(v[8 * k + 1])), b.x));
-      out[4 * k + 1] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 2]), __uint_as_float(v[8 * k + 3])), b.y));
-      out[4 * k + 2] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5])), b.z));
-      out[4 * k + 3] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])), b.w));
+    for (int part = 0; part < 2; part++) {
+      uint32_t v[32];
+      tmem_ld32(col + 32 * part, v);
+      tmem_wait_ld();
+      const uint4* bb = reinterpret_cast<const uint4*>(s.b2p + q * 64 + 32 * h + 16 * part);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint4 bv = bb[k];
+        uint32_t* o = out + 16 * part + 4 * k;
+        o[0] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 0]), __uint_as_float(v[8 * k + 1])), bv.x));
+        o[1] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 2]), __uint_as_float(v[8 * k + 3])), bv.y));
+        o[2] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5])), bv.z));
+        o[3] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])), bv.w));
+      }
     }
-    tmem_st16(col + 32 * g, out);  // inside the columns this thread read itself
+    tmem_st32(col, out);  // inside the columns this thread read itself
     tmem_wait_st();
     fence_before();
-    mbar_arrive(&s.a2_full[slot]);
+    mbar_arrive(&b.a2_full);
+    st.quarters++;
   }
-  if (!mbar_wait(&s.d3_full, st.tile & 1, &s.abort_flag, err, 23)) return false;
+  if (!mbar_wait(&b.d3_full, st.tile & 1, &s.abort_flag, err, 23)) return false;
   fence_after();
   {
     uint32_t v[32];
-    tmem_ld32(tb + kColD3, v);
+    tmem_ld32(tb + kOffD3, v);
     tmem_wait_ld();
     fence_before();
-    mbar_arrive(&s.d3_free);
+    mbar_arrive(&b.d3_free);
     const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
 #pragma unroll
     for (int o = 0; o < 9; o++) {
@@ -368,22 +404,16 @@ __device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float 
     }
   }
   st.tile++;
-  st.gq += 4;
   return true;
 }
 
-// Tells the MMA lane to stop (all 512 epilogue threads call it once).
+// Tells the MMA lane that this group has no more tiles (all 256 threads of the group call it).
 __device__ __forceinline__ void epi_finish(Smem& s) {
-  if (threadIdx.x == 0) *(volatile int*)&s.exit_flag = 1;
-  asm volatile("bar.sync 1, 512;\n" ::: "memory");
-  mbar_arrive(&s.a1_full);
+  CtxBars& b = s.ctx[epi_group()];
+  if (epi_gthread() == 0) *(volatile int*)&b.exit_flag = 1;
+  epi_bar();
+  mbar_arrive(&b.a1_full);
 }
-
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
-
-// Row (evaluation index within the tile) and column half of the calling epilogue thread.
-__device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
-__device__ __forceinline__ int epi_group() { return threadIdx.x >> 7; }
 
 }  // namespace tc
 }  // namespace hignn
