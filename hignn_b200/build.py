@@ -33,6 +33,7 @@ CU_SOURCES = {
     "far_aca.cu": ["-fmad=false"],  # FP64 determinants / inverses round as written
     "misc.cu": [],
     "tc_kernels.cu": [],
+    "noalloc.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

@@ -71,6 +71,7 @@ SIGNATURES = {
     "hignn_dot_device": ([_P, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "hignn_dense_dot": ([_P, _fp, _fp, C.c_int64], C.c_int),
     "hignn_dense_rows": ([_P, _dp, _fp, _i64p, C.c_int64, C.c_int], C.c_int),
+    "hignn_dense_rows_noalloc": ([_P, _dp, _fp, _i64p, C.c_int64, C.c_int], C.c_int),
     "hignn_two_body_eval": ([_P, C.c_void_p, C.c_void_p, C.c_int64, C.c_int], C.c_int),
     "hignn_get_stats": ([_P, C.POINTER(HignnStats)], C.c_int),
     "hignn_get_tree": ([_P, _i64p, _i64p], C.c_int),
@@ -183,6 +184,15 @@ class Model:
         out = np.empty((rows.shape[0], 3), np.float64)
         check(lib.hignn_dense_rows(self._h, out.ctypes.data_as(_dp), fptr(f), rows.ctypes.data_as(_i64p),
                                    rows.shape[0], int(precision)))
+        return out
+
+    def dense_rows_noalloc(self, f, rows, precision=0):
+        """hignn_dense_rows without device allocation (scratch in a static device array)."""
+        f = _f32(f, (self.n, 3))
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        out = np.empty((rows.shape[0], 3), np.float64)
+        check(lib.hignn_dense_rows_noalloc(self._h, out.ctypes.data_as(_dp), fptr(f), rows.ctypes.data_as(_i64p),
+                                           rows.shape[0], int(precision)))
         return out
 
     def two_body_eval(self, d_r_ptr, d_y_ptr, n, precision=0):

@@ -23,6 +23,7 @@
 #include "../../include/hignn_b200.h"
 #include "common.h"
 #include "kernels.h"
+#include "model_view.h"
 #include "tree.h"
 
 using hignn::Error;
@@ -555,6 +556,31 @@ void post_check(hignn_model* m) {
 }
 
 }  // namespace
+
+namespace hignn {
+
+void model_view(hignn_model* m, ModelView& v) {
+  v = ModelView{};
+  if (!m) return;
+  v.device = m->device;
+  v.stream = m->stream;
+  v.num_sms = m->num_sms;
+  v.n = m->n;
+  v.ready = m->device >= 0 && m->has_weights && m->tree_ready && m->x4.p && m->f4.p && m->io_f.p;
+  if (!v.ready) return;
+  v.x4 = m->x4.as<float4>();
+  v.f4 = m->f4.as<float4>();
+  v.perm = m->perm.as<int32_t>();
+  v.io_f = m->io_f.as<float>();
+  v.w = m->wdev();
+  v.nodes = &m->tree.nodes;
+  v.leaves = &m->lists.leaves;
+  v.inv_perm = &m->inv_perm;
+}
+
+void set_last_error(const char* msg) { set_error(msg); }
+
+}  // namespace hignn
 
 extern "C" {
 

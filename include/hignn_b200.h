@@ -121,6 +121,24 @@ int hignn_dense_dot(hignn_model* m, float* u, const float* f, int64_t n);
 int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
                      int precision);
 
+/* Allocation-free variant of hignn_dense_rows (same arguments and results); it has
+ * no counterpart in the reference. It serves callers that cannot allocate device
+ * memory once they are running -- a time-stepping code whose device-memory budget
+ * is fixed at start-up, or a host framework whose own caching allocator owns the
+ * GPU: it calls no cudaMalloc, cudaFree or allocating library routine. Its per-call
+ * scratch lives in one static device array of about 6.3 MB that every GPU which
+ * loads this library holds until the process exits. Limits: nrows <=
+ * HIGNN_NOALLOC_MAX_ROWS and a tree of at most HIGNN_NOALLOC_MAX_LEAVES leaves
+ * (larger sizes return HIGNN_ERR_ARG); precision 0 only. The model must already
+ * hold weights and a built tree (hignn_update_coord or hignn_dot once: those may
+ * allocate). The first call on a device looks up the array's address; make it
+ * before any stream capture. All calls share the array: calls whose GPU work
+ * overlaps race. */
+#define HIGNN_NOALLOC_MAX_ROWS 131072
+#define HIGNN_NOALLOC_MAX_LEAVES 65536
+int hignn_dense_rows_noalloc(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
+                             int precision);
+
 /* Two-body kernel M(r) on n features (device pointers, r: (n,3), y: (n,9) row-major
  * 3x3): python/convert.py:11-20. precision 0 = FP32 SIMT, 1 = BF16 tensor cores. */
 int hignn_two_body_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n, int precision);
