@@ -5,9 +5,12 @@ Workload (seeded, synthetic; no dataset): 1,048,576 unit spheres in a cube at
 volume fraction 0.10, 64 Gaussian clusters (sigma 8 radii) + 50% uniform
 background (seed 2), forces (0,0,-1) + N(0, 0.1^2); leaf size 128, ACA
 tolerance 1e-2 (the reference's production value, python/simulate.py:198),
-max_iter 100, tree prebuilt. One step = one H-matvec (near field + ACA far
-field). Each rank runs an independent replica (weak scaling); `value` is the
-sum of particles/s over ranks, timed on the device (max over ranks).
+max_iter 100, tree prebuilt (its host build time is reported apart). One step =
+one H-matvec (near field + ACA far field). Each rank runs an independent replica
+(weak scaling); `value` is the sum of particles/s over ranks, timed on the device
+(max over ranks). The plain FP32 form is timed once in the same run for the
+mixed-vs-plain ratio of the metric; both forms are checked against the dense
+product on sampled target rows.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision P]
     python bench.py --impl reference ...   # the reference algorithm on the host cores
@@ -30,8 +33,10 @@ sys.path.insert(0, REPO)
 WEIGHTS = os.path.join(REPO, "hignn_b200", "data", "two_body_unbounded.hgnw")
 METRIC = "H-matvec particles/s at N=1M: mixed+batched+student vs plain FP32, err≤1e-3"
 FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)  # 141,056
-PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor", 2: "bf16_tensor+student"}
+PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor_cores", 2: "bf16_tensor_cores+student_far_field"}
 PREC_DTYPE = {0: "fp32", 1: "bf16", 2: "bf16"}
+WORKLOAD = ("N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, seed 2, "
+            "leaf 128, eps 1e-2, max_iter 100, tree prebuilt")
 
 
 def parse():
@@ -40,10 +45,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hignn_b200", choices=["hignn_b200", "reference"])
-    ap.add_argument("--precision", type=int, default=0, choices=[0, 1, 2])
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1, 2])
     ap.add_argument("--n", type=int, default=1048576)
     ap.add_argument("--epsilon", type=float, default=1e-2)
     ap.add_argument("--check-rows", type=int, default=2048, help="dense target rows for the error check")
+    ap.add_argument("--no-plain", action="store_true", help="do not time the plain FP32 form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
@@ -53,9 +59,7 @@ def parse():
 def workload(n):
     from hignn_b200 import synthetic as S
 
-    x = S.clustered(n, 0.10, 2)
-    f = S.sedimenting_forces(n, 2)
-    return x, f
+    return S.clustered(n, 0.10, 2), S.sedimenting_forces(n, 2)
 
 
 def peaks():
@@ -92,11 +96,8 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.p.kill()
         self.f.flush()
-        rows = []
-        for line in open(self.f.name):
-            parts = [s.strip() for s in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        rows = [[s.strip() for s in line.split(",")] for line in open(self.f.name)]
+        rows = [r for r in rows if len(r) >= 9]
         os.unlink(self.f.name)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
@@ -114,16 +115,16 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for i in load for k in range(4) if rows[i][5 + k].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm[i] for i in load), "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows), "samples_under_load": len(load),
-                "power_w_max": max(pw)}
+                "samples": len(rows), "samples_under_load": len(load), "power_w_max": max(pw)}
 
 
-def cpu_baseline_sample(x, f, eps, close_evals, far_evals, seconds):
-    """Time the oracle port (numpy restatement of the reference path) on a bounded sample.
+def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
+    """The oracle port (numpy restatement of the reference path) timed on a bounded sample.
 
-    Near field: leading close pairs until ~seconds/2 of CPU work; far field: leading ACA
+    Near field: leading close pairs for ~seconds/2 of CPU work; far field: leading ACA
     blocks for the other half. Evaluations/s of each are extrapolated to the counted
-    evaluations of the full H-matvec.
+    evaluations of one full H-matvec (far evaluations from the sampled mean rank when
+    not given).
     """
     from oracle import hignn_oracle as O
 
@@ -136,7 +137,8 @@ def cpu_baseline_sample(x, f, eps, close_evals, far_evals, seconds):
     t_lists = time.time() - t0
     ft = f[rmap]
     sz = tree[:, 3] - tree[:, 2]
-    # near-field sample
+    if close_evals is None:
+        close_evals = int(np.sum(sz[ci] * sz[cj]))
     done_e, t_near, p = 0, 0.0, 0
     while t_near < seconds / 2 and p < len(ci):
         q = min(len(ci), p + 64)
@@ -146,8 +148,7 @@ def cpu_baseline_sample(x, f, eps, close_evals, far_evals, seconds):
         done_e += int(np.sum(sz[ci[p:q]] * sz[cj[p:q]]))
         p = q
     r_near = done_e / t_near
-    # far-field sample
-    far_e, t_far, b = 0, 0.0, 0
+    far_e, t_far, b, ranks = 0, 0.0, 0, []
     while t_far < seconds / 2 and b < len(fi):
         q = min(len(fi), b + 32)
         t = time.time()
@@ -155,16 +156,18 @@ def cpu_baseline_sample(x, f, eps, close_evals, far_evals, seconds):
         O.far_dot(tree, xt, ft, fi[b:q], fj[b:q], net, eps, 100, collect=col)
         t_far += time.time() - t
         far_e += sum(c[2] * (sz[c[0]] + sz[c[1]]) for c in col)
+        ranks += [c[2] for c in col]
         b = q
     r_far = far_e / t_far if t_far > 0 else r_near
+    if far_evals is None:
+        far_evals = float(np.mean(ranks)) * float(np.sum(sz[fi] + sz[fj])) if ranks else 0.0
     t_dot = close_evals / r_near + far_evals / r_far
     cores = os.cpu_count() or 1
     return {"value": len(x) / t_dot, "unit": "particles/s", "cores": cores, "kind": "port",
-            "sample": (f"oracle numpy restatement (BLAS threads = {cores}): {p} close pairs "
-                       f"({done_e:.3g} evals, {r_near:.3g} evals/s) and {b} ACA blocks ({far_e:.3g} evals, "
-                       f"{r_far:.3g} evals/s), extrapolated to {close_evals:.3g} near + {far_evals:.3g} far "
-                       f"evaluations of one H-matvec; tree+lists {t_lists:.1f} s not counted"),
-            "t_dot_s_extrapolated": t_dot}
+            "sample": (f"oracle numpy restatement on {cores} host threads: {p} close pairs ({done_e:.3g} evals, "
+                       f"{r_near:.3g} evals/s) and {b} ACA blocks ({far_e:.3g} evals, {r_far:.3g} evals/s), "
+                       f"extrapolated to {close_evals:.3g} near + {far_evals:.3g} far evaluations of one "
+                       f"H-matvec; tree+lists ({t_lists:.1f} s) not counted")}
 
 
 def reference_arm(args, rank, world):
@@ -172,42 +175,44 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return 0
     x, f = workload(args.n)
-    from oracle import hignn_oracle as O
-
-    t0 = time.time()
-    tree, rmap = O.build_tree(x, 128)
-    aux = O.compute_aux(tree, x[rmap])
-    ci, cj, fi, fj, _ = O.close_far_lists(tree, aux)
-    sz = tree[:, 3] - tree[:, 2]
-    close_evals = int(np.sum(sz[ci] * sz[cj]))
-    build_s = time.time() - t0
     vals = []
-    far_rows = int(np.sum(sz[fi] + sz[fj]))
     for k in range(args.warmup + args.steps):
-        # far evaluations = mean sampled rank x rows of all far blocks (rank from the sample)
-        s = cpu_baseline_sample(x, f, args.epsilon, close_evals, 0, args.cpu_sample_seconds)
-        net = O.TwoBody.from_hgnw(WEIGHTS)
-        col = []
-        O.far_dot(tree, x[rmap], f[rmap], fi[:64], fj[:64], net, args.epsilon, 100, collect=col)
-        mean_rank = float(np.mean([c[2] for c in col])) if col else 0.0
-        far_evals = mean_rank * far_rows
-        s2 = cpu_baseline_sample(x, f, args.epsilon, close_evals, far_evals, args.cpu_sample_seconds)
+        s = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds)
         if k >= args.warmup:
-            vals.append(s2["value"])
+            vals.append(s["value"])
     v = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.n / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": "N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, "
-                                   "seed 2, leaf 128", "n": args.n, "epsilon": args.epsilon, "max_iter": 100,
-                       "parallelism": "host cores"},
-            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": s2["cores"], "kind": "port",
-                             "sample": s2["sample"]},
+            "config": {"workload": WORKLOAD, "n": args.n, "epsilon": args.epsilon, "parallelism": "host cores"},
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": s["cores"], "kind": "port",
+                             "sample": s["sample"]},
             "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent); "
-                    f"this arm times its restatement. tree+lists {build_s:.1f} s not counted"}
+            "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent; "
+                    "not pip-installable); this arm times its restatement on the host cores"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def timed(m, stream, flush, steps, fn):
+    """Per-step device time (CUDA events on the model's stream), L2 flushed between steps."""
+    import torch
+
+    times, near, far = [], [], []
+    for k in range(steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        s = m.stats()
+        near.append(s["t_close_ms"])
+        far.append(s["t_far_ms"])
+    return times, near, far
 
 
 def main():
@@ -228,6 +233,13 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
     from hignn_b200 import capi
 
@@ -256,66 +268,50 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(bus)
-    times, near_ms, far_ms = [], [], []
-    for k in range(args.steps):
-        flush.fill_(k & 0xFF)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        m.dot_device(u_d.data_ptr(), f_d.data_ptr())
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-        s = m.stats()
-        near_ms.append(s["t_close_ms"])
-        far_ms.append(s["t_far_ms"])
+    times, near_ms, far_ms = timed(m, stream, flush, args.steps,
+                                   lambda: m.dot_device(u_d.data_ptr(), f_d.data_ptr()))
     torch.cuda.synchronize()
     ck = clocks.stop()
     if dist:
         dist.barrier()
     st = m.stats()
-    ms = float(np.mean(times))
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(np.mean(times)))
     value = world * n / (ms / 1e3)
 
     # end to end through the public C ABI from pinned host memory (H2D + matvec + D2H per step)
     f_h = torch.from_numpy(f).pin_memory()
     u_h = torch.empty_like(f_h).pin_memory()
-    if not args.no_e2e:
-        m.dot_ptr(u_h.data_ptr(), f_h.data_ptr())
-    else:
+    if args.no_e2e:
         u_h.copy_(u_d.cpu())
-    e2e_times = []
-    for k in range(0 if args.no_e2e else args.steps):
-        flush.fill_(k & 0xFF)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        m.dot_ptr(u_h.data_ptr(), f_h.data_ptr())
-        e1.record(stream)
-        e1.synchronize()
-        e2e_times.append(e0.elapsed_time(e1))
-    e2e_ms = float(np.mean(e2e_times)) if e2e_times else float("nan")
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = float("nan")
+    else:
+        e2e_times, _, _ = timed(m, stream, flush, args.steps, lambda: m.dot_ptr(u_h.data_ptr(), f_h.data_ptr()))
+        e2e_ms = max_over_ranks(float(np.mean(e2e_times)))
+    u = u_h.numpy().astype(np.float64)
 
     # accuracy: dense rows (FP32 network, FP64 accumulation over all N sources)
-    u = u_h.numpy().astype(np.float64)
     rng = np.random.default_rng(12345)
     rows = np.sort(rng.choice(n, size=min(args.check_rows, n), replace=False))
+    err = err_plain = None
     t0 = time.time()
-    err = None
-    if len(rows):
-        ud = m.dense_rows(f, rows, 0)
-        err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
+    ud = m.dense_rows(f, rows, 0) if len(rows) else None
     t_check = time.time() - t0
+    if ud is not None:
+        err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
+
+    plain = None
+    if args.precision != 0 and not args.no_plain:
+        m.set(capi.P_PRECISION, 0)
+        up_d = torch.empty_like(f_d)
+        pt, pn, pf = timed(m, stream, flush, 1, lambda: m.dot_device(up_d.data_ptr(), f_d.data_ptr()))
+        m.set(capi.P_PRECISION, args.precision)
+        pms = max_over_ranks(float(np.mean(pt)))
+        up = up_d.cpu().numpy().astype(np.float64)
+        if ud is not None:
+            err_plain = float(np.linalg.norm(up[rows] - ud) / np.linalg.norm(ud))
+        plain = {"form": "plain_fp32", "ms_per_step": pms, "value": world * n / (pms / 1e3),
+                 "near_ms": float(pn[0]), "far_ms": float(pf[0]), "rel_l2_vs_dense": err_plain,
+                 "steps": 1, "speedup_of_headline": (world * n / (ms / 1e3)) / (world * n / (pms / 1e3))}
 
     hbm, bf16, src = peaks()
     near_s = float(np.mean(near_ms)) / 1e3
@@ -324,23 +320,22 @@ def main():
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": PREC_DTYPE[args.precision], "data": "synthetic",
-        "config": {"workload": "N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, "
-                               "seed 2, leaf 128, tree prebuilt", "n": n, "epsilon": args.epsilon,
-                   "max_iter": 100, "form": PREC_NAME[args.precision],
+        "config": {"workload": WORKLOAD, "n": n, "epsilon": args.epsilon, "max_iter": 100,
+                   "form": PREC_NAME[args.precision],
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "256 MiB buffer written between timed steps"},
-        "roofline": {"bound": "tensor", "kernel": "near field (pair features + two-body MLP + contraction)",
+        "roofline": {"bound": "tensor", "kernel": "near field (features + two-body network + contraction)",
                      "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
                      "peak_source": f"bf16_tflops of {src} MEASURED_PEAKS.json",
                      "traffic": None,
-                     "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals"},
-        "e2e": {"value": n / (e2e_ms / 1e3) * world, "unit": "particles/s", "h2d_bytes_per_step": 12 * n,
+                     "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals / near-field time"},
+        "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 12 * n, "ms_per_step": e2e_ms},
         "gpu_launches": int(st["gpu_launches"]),
         "clocks": ck,
-        "error": {"rel_l2_vs_dense": err, "rows": int(len(rows)),
-                  "oracle": "dense rows on the device, FP32 network, FP64 accumulation over all N sources",
-                  "seconds": t_check},
+        "error": {"rel_l2_vs_dense": err, "rows": int(len(rows)), "seconds": t_check,
+                  "oracle": "dense rows on the device, FP32 network, FP64 accumulation over all N sources"},
+        "plain_fp32": plain,
         "breakdown_ms": {"near": float(np.mean(near_ms)), "far": float(np.mean(far_ms)),
                          "build_host": st0["t_build_ms"]},
         "work": {"close_pairs": st["num_close"], "far_pairs": st["num_far"], "close_evals": st["close_evals"],
@@ -348,8 +343,8 @@ def main():
                  "far_rank_max": st["far_rank_max"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(x, f, args.epsilon, st["close_evals"], st["far_evals"],
-                                                   args.cpu_sample_seconds)
+        line["cpu_baseline"] = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds, st["close_evals"],
+                                            st["far_evals"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     m.close()

@@ -35,7 +35,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_NTHREADS = max(1, min(8, os.cpu_count() or 1))
+_NTHREADS = max(1, os.cpu_count() or 1)
 _POOL = None
 
 
