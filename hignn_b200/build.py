@@ -34,6 +34,7 @@ CU_SOURCES = {
     "misc.cu": [],
     "tc_kernels.cu": [],
     "noalloc.cu": [],
+    "student.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

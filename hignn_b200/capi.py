@@ -36,6 +36,8 @@ P_STUDENT_TOL = 103
 P_FIELDS = 104
 P_RECORD_PIVOTS = 105
 
+STUDENT_PARAMS = 2537
+
 ERR_NAMES = {-1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_IO", -5: "ERR_LIMIT", -6: "ERR_NODEV"}
 
 
@@ -76,6 +78,11 @@ SIGNATURES = {
     "hignn_get_stats": ([_P, C.POINTER(HignnStats)], C.c_int),
     "hignn_get_tree": ([_P, _i64p, _i64p], C.c_int),
     "hignn_get_lists": ([_P, _i64p, _i64p, _i64p, _i64p], C.c_int),
+    "hignn_train_student": ([_P, C.c_int, C.c_int, C.c_int64, C.c_double, C.c_uint64, _dp], C.c_int),
+    "hignn_set_student": ([_P, _fp, C.c_int], C.c_int),
+    "hignn_get_student": ([_P, _fp, C.c_int], C.c_int),
+    "hignn_student_eval": ([_P, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "hignn_student_grad": ([_P, C.c_void_p, C.c_void_p, C.c_int64, _fp, _dp], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
     "hignn_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
@@ -219,6 +226,32 @@ class Model:
         check(lib.hignn_get_lists(self._h, ci.ctypes.data_as(_i64p), cj.ctypes.data_as(_i64p),
                                   fi.ctypes.data_as(_i64p), fj.ctypes.data_as(_i64p)))
         return ci, cj, fi, fj
+
+    # ---- far-field student network
+    def train_student(self, steps=20000, batch=65536, nsamples=10_000_000, lr=1e-3, seed=1):
+        loss = C.c_double()
+        check(lib.hignn_train_student(self._h, int(steps), int(batch), int(nsamples), float(lr), int(seed),
+                                      C.byref(loss)))
+        return loss.value
+
+    def set_student(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        check(lib.hignn_set_student(self._h, fptr(p), p.size))
+
+    def get_student(self):
+        p = np.empty(STUDENT_PARAMS, np.float32)
+        check(lib.hignn_get_student(self._h, fptr(p), p.size))
+        return p
+
+    def student_eval(self, d_r_ptr, d_y_ptr, n):
+        check(lib.hignn_student_eval(self._h, C.c_void_p(d_r_ptr), C.c_void_p(d_y_ptr), int(n)))
+
+    def student_grad(self, d_r_ptr, d_t_ptr, n):
+        g = np.empty(STUDENT_PARAMS, np.float32)
+        loss = C.c_double()
+        check(lib.hignn_student_grad(self._h, C.c_void_p(d_r_ptr), C.c_void_p(d_t_ptr), int(n), fptr(g),
+                                     C.byref(loss)))
+        return g, loss.value
 
     def far_pivots(self):
         """(ranks, rows, cols) of the last far field; rows/cols are per-block lists."""

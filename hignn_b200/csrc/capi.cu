@@ -112,6 +112,8 @@ struct hignn_model {
 
   bool has_weights = false;
   std::vector<float> hw;  // device-layout weights, host copy
+  bool has_student = false;
+  DevBuf student;         // 2537 FP32 parameters of the far-field student network
 
   DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
@@ -336,6 +338,11 @@ void check_device_error(hignn_model* m) {
   }
 }
 
+void require_student_if_needed(hignn_model* m) {
+  if (m->precision == 2 && !m->has_student)
+    throw Error(HIGNN_ERR_STATE, "precision 2 needs a student network (hignn_train_student or hignn_set_student)");
+}
+
 void require_weights(hignn_model* m) {
   if (!m->has_weights) throw Error(HIGNN_ERR_STATE, "no two-body model loaded (call load_two_body_model)");
 }
@@ -430,7 +437,8 @@ void far_field(hignn_model* m) {
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
     const hignn::TcWeights tcw = m->wtc();
-    hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, m->err_flag(), m->num_sms, m->host_ctr,
+    const float* student = (m->precision == 2 && m->has_student) ? m->student.as<float>() : nullptr;
+    hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, student, m->err_flag(), m->num_sms, m->host_ctr,
                            m->stream, &iterations);
     m->stats.far_rank_max = std::max(m->stats.far_rank_max, m->host_ctr[hignn::kCtrRankMax]);
     if (m->record_pivots) {
@@ -634,7 +642,7 @@ int hignn_destroy(hignn_model* m) {
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
-                      &m->weights_tc, &m->counter,
+                      &m->weights_tc, &m->counter, &m->student,
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
                       &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
@@ -797,6 +805,7 @@ int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n) {
     if (n != m->n) throw Error(HIGNN_ERR_ARG, "dot: size mismatch");
     require_device(m);
     require_weights(m);
+    require_student_if_needed(m);
     ensure_tree(m);
     HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, m->stream));
     dot_impl(m, m->io_u.as<float>(), m->io_f.as<float>());
@@ -811,6 +820,7 @@ int hignn_dot_device(hignn_model* m, float* d_u, const float* d_f, int64_t n) {
     if (n != m->n) throw Error(HIGNN_ERR_ARG, "dot: size mismatch");
     require_device(m);
     require_weights(m);
+    require_student_if_needed(m);
     ensure_tree(m);
     dot_impl(m, d_u, d_f);
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
@@ -938,6 +948,129 @@ int hignn_get_lists(hignn_model* m, int64_t* ci, int64_t* cj, int64_t* fi, int64
     if (cj) std::copy(m->lists.closeJ.begin(), m->lists.closeJ.end(), cj);
     if (fi) std::copy(m->lists.farI.begin(), m->lists.farI.end(), fi);
     if (fj) std::copy(m->lists.farJ.begin(), m->lists.farJ.end(), fj);
+  });
+}
+
+int hignn_set_student(hignn_model* m, const float* params, int nparams) {
+  return guard([&] {
+    if (!m || !params) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (nparams != hignn::kStudentParams)
+      throw Error(HIGNN_ERR_ARG, "student network has " + std::to_string(hignn::kStudentParams) + " parameters");
+    require_device(m);
+    m->student.ensure(sizeof(float) * hignn::kStudentParams);
+    HIGNN_CUDA(cudaMemcpyAsync(m->student.p, params, sizeof(float) * hignn::kStudentParams, cudaMemcpyHostToDevice,
+                               m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    m->has_student = true;
+  });
+}
+
+int hignn_get_student(hignn_model* m, float* params, int nparams) {
+  return guard([&] {
+    if (!m || !params) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (nparams != hignn::kStudentParams)
+      throw Error(HIGNN_ERR_ARG, "student network has " + std::to_string(hignn::kStudentParams) + " parameters");
+    if (!m->has_student) throw Error(HIGNN_ERR_STATE, "no student network (train or set one first)");
+    require_device(m);
+    HIGNN_CUDA(cudaMemcpyAsync(params, m->student.p, sizeof(float) * hignn::kStudentParams, cudaMemcpyDeviceToHost,
+                               m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_student_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n) {
+  return guard([&] {
+    if (!m || (n > 0 && (!d_r || !d_y))) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (!m->has_student) throw Error(HIGNN_ERR_STATE, "no student network (train or set one first)");
+    require_device(m);
+    hignn::launch_student_eval(m->student.as<float>(), d_r, d_y, n, m->num_sms, m->stream);
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_student_grad(hignn_model* m, const float* d_r, const float* d_t, int64_t n, float* grad, double* loss) {
+  return guard([&] {
+    if (!m || !d_r || !d_t || !grad || n <= 0) throw Error(HIGNN_ERR_ARG, "null argument or empty batch");
+    if (!m->has_student) throw Error(HIGNN_ERR_STATE, "no student network (train or set one first)");
+    require_device(m);
+    const int nparts = (int)((n + 127) / 128);
+    DevBuf partial, lpart, g, l;
+    partial.ensure(sizeof(float) * (size_t)nparts * hignn::kStudentParams);
+    lpart.ensure(sizeof(float) * nparts);
+    g.ensure(sizeof(float) * hignn::kStudentParams);
+    l.ensure(sizeof(float));
+    hignn::launch_student_grad(m->student.as<float>(), d_r, d_t, n, n, 0, partial.as<float>(), lpart.as<float>(),
+                               g.as<float>(), l.as<float>(), m->stream);
+    float lh = 0.f;
+    HIGNN_CUDA(cudaMemcpyAsync(grad, g.p, sizeof(float) * hignn::kStudentParams, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(&lh, l.p, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    if (loss) *loss = (double)lh / (9.0 * (double)n);
+    for (DevBuf* b : {&partial, &lpart, &g, &l}) b->release();
+  });
+}
+
+int hignn_train_student(hignn_model* m, int steps, int batch, int64_t nsamples, double lr, uint64_t seed,
+                        double* final_loss) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    if (steps < 0 || batch < 128 || nsamples < batch || lr <= 0)
+      throw Error(HIGNN_ERR_ARG, "train_student: need steps >= 0, batch >= 128, nsamples >= batch, lr > 0");
+    require_device(m);
+    require_weights(m);
+    using hignn::kStudentParams;
+    // initial parameters: uniform Glorot weights from the seed, zero biases, small last layer
+    std::vector<float> p(kStudentParams, 0.f);
+    uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto rnd = [&]() {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      return (float)((st >> 40) * (1.0 / 16777216.0)) * 2.f - 1.f;
+    };
+    const int offs[4] = {0, 128, 1184, 2240}, fin[4] = {3, 32, 32, 32}, fout[4] = {32, 32, 32, 9};
+    for (int l = 0; l < 4; l++) {
+      const float a = std::sqrt(6.f / (fin[l] + fout[l])) * (l == 3 ? 0.1f : 1.f);
+      for (int q = 0; q < fin[l] * fout[l]; q++) p[offs[l] + q] = a * rnd();
+    }
+    m->student.ensure(sizeof(float) * kStudentParams);
+    HIGNN_CUDA(cudaMemcpyAsync(m->student.p, p.data(), sizeof(float) * kStudentParams, cudaMemcpyHostToDevice,
+                               m->stream));
+    DevBuf r, t, partial, lpart, g, m1, m2, l;
+    r.ensure(sizeof(float) * 3 * (size_t)nsamples);
+    t.ensure(sizeof(float) * 9 * (size_t)nsamples);
+    const int nparts = (batch + 127) / 128;
+    partial.ensure(sizeof(float) * (size_t)nparts * kStudentParams);
+    lpart.ensure(sizeof(float) * nparts);
+    g.ensure(sizeof(float) * kStudentParams);
+    m1.ensure(sizeof(float) * kStudentParams);
+    m2.ensure(sizeof(float) * kStudentParams);
+    l.ensure(sizeof(float));
+    HIGNN_CUDA(cudaMemsetAsync(m1.p, 0, sizeof(float) * kStudentParams, m->stream));
+    HIGNN_CUDA(cudaMemsetAsync(m2.p, 0, sizeof(float) * kStudentParams, m->stream));
+    // teacher evaluations at admissible separations (FP32 network), as residuals of the RPY tensor
+    hignn::launch_student_samples(r.as<float>(), nsamples, seed ^ 0x5EEDull, 4.0f, 400.0f, m->stream);
+    hignn::launch_eval_simt(r.as<float>(), t.as<float>(), nsamples, m->wdev(), m->num_sms, m->stream);
+    hignn::launch_student_targets(r.as<float>(), t.as<float>(), nsamples, m->stream);
+    double b1t = 1.0, b2t = 1.0;
+    for (int k = 0; k < steps; k++) {
+      const double lrk = lr * (0.01 + 0.99 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * k / std::max(1, steps))));
+      hignn::launch_student_grad(m->student.as<float>(), r.as<float>(), t.as<float>(), nsamples, batch,
+                                 (seed + 1) * 0x9E3779B97F4A7C15ull + (uint64_t)k + 1, partial.as<float>(),
+                                 lpart.as<float>(), g.as<float>(), nullptr, m->stream);
+      b1t *= 0.9;
+      b2t *= 0.999;
+      hignn::launch_student_adam(m->student.as<float>(), g.as<float>(), m1.as<float>(), m2.as<float>(), (float)lrk,
+                                 (float)b1t, (float)b2t, m->stream);
+    }
+    // loss on one more random batch
+    hignn::launch_student_grad(m->student.as<float>(), r.as<float>(), t.as<float>(), nsamples, batch,
+                               seed * 31 + 7, partial.as<float>(), lpart.as<float>(), g.as<float>(), l.as<float>(),
+                               m->stream);
+    float lh = 0.f;
+    HIGNN_CUDA(cudaMemcpyAsync(&lh, l.p, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    if (final_loss) *final_loss = (double)lh / (9.0 * (double)batch);
+    for (DevBuf* b : {&r, &t, &partial, &lpart, &g, &m1, &m2, &l}) b->release();
+    m->has_student = true;
   });
 }
 

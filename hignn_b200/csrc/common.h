@@ -28,6 +28,7 @@ constexpr int kMaxLeaf = 256;   // largest leaf the near-field kernels stage in 
 constexpr int kH1 = 128;        // two-body network widths (python/convert.py:6-20 over nn/*.pkl)
 constexpr int kH2 = 512;
 constexpr int kOut = 9;
+constexpr int kStudentParams = 2537;  // 3-32-32-32-9 student network (weights + biases)
 
 // FP32 weights of the two-body network as the SIMT kernels read them.
 struct MlpF32 {

@@ -537,8 +537,8 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
 
 }  // namespace
 
-void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, int* err, int num_sms,
-                     int32_t* host_ctr, cudaStream_t s, int* iterations) {
+void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                     int num_sms, int32_t* host_ctr, cudaStream_t s, int* iterations) {
   if (a.nb <= 0) return;
   const size_t eval_smem = sizeof(EvalSmem);
   const size_t row_smem = sizeof(double) * (9 + 3 + 3) * kMaxIterCap;
@@ -551,12 +551,16 @@ void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, in
   int it = 0;
   for (; it <= a.max_iter; it++) {
     k_far_active<<<1, 1024, 0, s>>>(a);
-    if (tcw)
+    if (student)
+      launch_far_student(a, student, 0, num_sms, s);
+    else if (tcw)
       launch_far_tc(a, *tcw, 0, err, num_sms, s);
     else
       k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
     k_far_col_pivot<<<a.nb, kPivThreads, col_smem, s>>>(a);
-    if (tcw)
+    if (student)
+      launch_far_student(a, student, 1, num_sms, s);
+    else if (tcw)
       launch_far_tc(a, *tcw, 1, err, num_sms, s);
     else
       k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);

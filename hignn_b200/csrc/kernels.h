@@ -67,9 +67,22 @@ struct FarArgs {
   int use_symmetry;
 };
 
-// One ACA batch to completion. tcw == nullptr: FP32 SIMT queries; else tensor-core queries.
-void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, int* err, int num_sms,
-                     int32_t* host_ctr, cudaStream_t s, int* iterations);
+// One ACA batch to completion. Queries: student != nullptr -> student network; else
+// tcw != nullptr -> teacher on the tensor cores; else teacher FP32 SIMT.
+void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                     int num_sms, int32_t* host_ctr, cudaStream_t s, int* iterations);
+
+// student network (student.cu)
+size_t student_grad_smem();
+void launch_student_samples(float* r, int64_t n, uint64_t seed, float rmin, float rmax, cudaStream_t s);
+void launch_student_targets(const float* r, float* t, int64_t n, cudaStream_t s);
+void launch_student_grad(const float* params, const float* r, const float* t, int64_t nsamples, int64_t batch,
+                         uint64_t step_seed, float* partial, float* loss_partial, float* grad, float* loss,
+                         cudaStream_t s);
+void launch_student_adam(float* p, const float* g, float* m1, float* m2, float lr, float b1t, float b2t,
+                         cudaStream_t s);
+void launch_student_eval(const float* params, const float* r, float* y, int64_t n, int num_sms, cudaStream_t s);
+void launch_far_student(const FarArgs& a, const float* params, int which, int num_sms, cudaStream_t s);
 
 // tensor-core kernels (tc_kernels.cu); err receives a nonzero code if a bounded wait timed out
 void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, int* err, int num_sms, cudaStream_t s);

@@ -2,8 +2,8 @@
 //
 // Mixed precision: layer 1 (3 -> 128) in FP32 on the CUDA cores; layers 2
 // (128 -> 512) and 3 (512 -> 9) as BF16 tcgen05 MMAs with FP32 accumulation in
-// tensor memory; tanh as tanh.approx.bf16x2 (two per MUFU op) on the
-// accumulators rounded to BF16 plus the BF16 bias. W3 is split into a BF16
+// tensor memory; tanh as tanh.approx.bf16x2 (two per MUFU op) on the FP32
+// accumulator plus FP32 bias, rounded to BF16 once. W3 is split into a BF16
 // high part and a BF16 residual (rows 0-8 and 16-24 of one N=32 operand): its
 // rounding is the dominant systematic error of a plain BF16 layer 3, and the
 // split removes it for ~6% more tensor work. b1 and b3 stay FP32.
@@ -70,7 +70,7 @@ struct alignas(1024) Smem {
   uint64_t drain;
   uint32_t tmem_base;
   int abort_flag;
-  alignas(16) uint32_t b2p[kH2 / 2];  // b2 as packed BF16 pairs
+  alignas(16) float b2[kH2];          // FP32 layer-2 bias, added before rounding to BF16
   alignas(16) float4 w1b1[kH1];
   float b3[16];
 };
@@ -194,7 +194,7 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   const uint4* src3 = w.w3img;
   uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
   for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
-  for (int i = t; i < kH2 / 2; i += blockDim.x) s.b2p[i] = pack_bf16(w.b2[2 * i], w.b2[2 * i + 1]);
+  for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
   for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t == 0) {
@@ -367,15 +367,13 @@ __device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float 
       uint32_t v[32];
       tmem_ld32(col + 32 * part, v);
       tmem_wait_ld();
-      const uint4* bb = reinterpret_cast<const uint4*>(s.b2p + q * 64 + 32 * h + 16 * part);
+      const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 64 * h + 32 * part);
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const uint4 bv = bb[k];
-        uint32_t* o = out + 16 * part + 4 * k;
-        o[0] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 0]), __uint_as_float(v[8 * k + 1])), bv.x));
-        o[1] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 2]), __uint_as_float(v[8 * k + 3])), bv.y));
-        o[2] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5])), bv.z));
-        o[3] = tanh_bf16x2(add_bf16x2(pack_bf16(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])), bv.w));
+      for (int k = 0; k < 8; k++) {
+        const float4 bv = bb[k];
+        uint32_t* o = out + 16 * part + 2 * k;
+        o[0] = tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
+        o[1] = tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
       }
     }
     tmem_st32(col, out);  // inside the columns this thread read itself

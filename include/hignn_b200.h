@@ -143,6 +143,29 @@ int hignn_dense_rows_noalloc(hignn_model* m, double* u_rows, const float* f, con
  * 3x3): python/convert.py:11-20. precision 0 = FP32 SIMT, 1 = BF16 tensor cores. */
 int hignn_two_body_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n, int precision);
 
+/* Far-field student network (no counterpart in the reference; the student is new work).
+ * A 3-32-32-32-9 SiLU network on x = r_hat ln(|r|/2) predicting the teacher's inner
+ * output minus the Rotne-Prager-Yamakawa tensor; used for the ACA queries of
+ * admissible blocks when HIGNN_P_PRECISION = 2. Parameters (2537 floats): W1 (32x3),
+ * b1, W2 (32x32), b2, W3 (32x32), b3, W4 (9x32), b4, row-major. */
+#define HIGNN_STUDENT_PARAMS 2537
+
+/* Trains the student on the device from teacher evaluations at separations drawn
+ * log-uniform in [4, 400] with uniform directions: nsamples teacher samples, Adam
+ * (cosine-decayed from lr), mini-batches of `batch`. final_loss: mean squared error
+ * of the inner output on one more batch. */
+int hignn_train_student(hignn_model* m, int steps, int batch, int64_t nsamples, double lr, uint64_t seed,
+                        double* final_loss);
+int hignn_set_student(hignn_model* m, const float* params, int nparams);
+int hignn_get_student(hignn_model* m, float* params, int nparams);
+
+/* Student M(r) on n features (device pointers, r: (n,3), y: (n,9)). */
+int hignn_student_eval(hignn_model* m, const float* d_r, float* d_y, int64_t n);
+
+/* Gradient (host array of HIGNN_STUDENT_PARAMS floats) and loss of mean((net(x(r)) - t)^2)
+ * over a batch of features d_r (n,3) and residual targets d_t (n,9), device pointers. */
+int hignn_student_grad(hignn_model* m, const float* d_r, const float* d_t, int64_t n, float* grad, double* loss);
+
 /* Sizes of the tree and lists built by the last update. */
 int hignn_get_stats(hignn_model* m, hignn_stats* out);
 
