@@ -73,7 +73,9 @@ def test_student_gradient_matches_autograd():
     n = 1000  # several CTAs of 128 and a partial one
     r = features(n, 3)
     t = (rng.normal(size=(n, 9)) * 0.01).astype(np.float32)
-    g_dev, loss_dev = m.student_grad(torch.from_numpy(r).cuda().data_ptr(), torch.from_numpy(t).cuda().data_ptr(), n)
+    # keep the device copies alive: a temporary's memory goes back to the caching allocator at once
+    rd, td = torch.from_numpy(r).cuda(), torch.from_numpy(t).cuda()
+    g_dev, loss_dev = m.student_grad(rd.data_ptr(), td.data_ptr(), n)
     p, fwd = student_torch(params)
     loss = ((fwd(r) - torch.as_tensor(t, dtype=torch.float64)) ** 2).mean()
     loss.backward()
@@ -88,7 +90,8 @@ def test_student_eval_matches_cpu_forward():
     m.set_student(params)
     r = features(4096, 4)
     y = torch.empty((4096, 9), device="cuda")
-    m.student_eval(torch.from_numpy(r).cuda().data_ptr(), y.data_ptr(), 4096)
+    rd = torch.from_numpy(r).cuda()
+    m.student_eval(rd.data_ptr(), y.data_ptr(), 4096)
     _, fwd = student_torch(params)
     d = np.linalg.norm(r.astype(np.float64), axis=1, keepdims=True)
     rh = r / d
@@ -115,7 +118,8 @@ def test_student_training_fits_teacher(trained, oracle_net):
     m.set_student(params)
     r = features(8192, 11)
     y = torch.empty((8192, 9), device="cuda")
-    m.student_eval(torch.from_numpy(r).cuda().data_ptr(), y.data_ptr(), 8192)
+    rd = torch.from_numpy(r).cuda()
+    m.student_eval(rd.data_ptr(), y.data_ptr(), 8192)
     ref = oracle_net.eval64(r)
     err = np.linalg.norm(y.cpu().numpy() - ref, axis=1) / np.linalg.norm(ref, axis=1)
     assert np.median(err) < 6e-3 and np.percentile(err, 99) < 2e-2, (np.median(err), np.percentile(err, 99))
