@@ -29,6 +29,7 @@ def main():
     ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
+    ap.add_argument("--student-steps", type=int, default=4000, help="training steps when --precision 2")
     a = ap.parse_args()
 
     import torch
@@ -71,6 +72,9 @@ def main():
         m.set(capi.P_FIELDS, a.fields)
         m.set(capi.P_EPSILON, a.epsilon)
         m.set(capi.P_TIMING, 1)
+        if a.precision == 2:
+            out["student_loss"] = m.train_student(steps=a.student_steps, batch=16384, nsamples=2_000_000, lr=1e-3,
+                                                  seed=3)
         m.dot(f)
         near, far = [], []
         for _ in range(a.reps):
@@ -84,7 +88,8 @@ def main():
                    near_evals_per_s=st["close_evals"] / max(1e-9, np.min(near)) * 1e3,
                    near_tflops=st["close_evals"] * FLOP_PER_EVAL / max(1e-9, np.min(near)) / 1e9,
                    far_evals_per_s=st["far_evals"] / max(1e-9, np.min(far)) * 1e3 if st["far_evals"] else None,
-                   gpu_launches=st["gpu_launches"])
+                   far_iterations=st["far_iterations"], far_rank_max=st["far_rank_max"],
+                   student_fallback_blocks=st["student_fallback_blocks"], gpu_launches=st["gpu_launches"])
     print(json.dumps(out), flush=True)
 
 
