@@ -299,15 +299,14 @@ class ExplicitRk4 : public TimeIntegrator {
         }
         err = 0.0;
         for (size_t i = 0; i < n_; i++) {
-          double e2 = 0.0;
+          float ve[3];
           for (int d = 0; d < 3; d++) {
             const size_t q = 3 * i + d;
-            const float ve = (k[1][q] * dc1 + k[3][q] * dc3 + k[4][q] * dc4 + k[5][q] * dc5 + k[6][q] * dc6 +
-                              k[7][q] * dc7) *
-                             (float)dt;
-            e2 += (double)ve * ve;
+            ve[d] = (k[1][q] * dc1 + k[3][q] * dc3 + k[4][q] * dc4 + k[5][q] * dc5 + k[6][q] * dc6 +
+                     k[7][q] * dc7) *
+                    (float)dt;
           }
-          err += e2;
+          err += (double)(ve[0] * ve[0] + ve[1] * ve[1] + ve[2] * ve[2]);  // Vec3::SquareMag is float
         }
         err = std::sqrt(err);
         if (err > thr_) {

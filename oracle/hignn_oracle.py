@@ -743,3 +743,106 @@ class OracleModel:
         u = np.empty_like(ut)
         u[self.rmap] = ut  # BackwardReorder: vCopy(map(i)) = v(i)
         return u.astype(np.float32)
+
+
+# ----------------------------------------------------------------------------------------------
+# Time integration: include/TimeIntegrator.hpp (float positions, double t and dt)
+# ----------------------------------------------------------------------------------------------
+def _periodic_offsets(x, lo, hi):
+    """Per-component offset that wraps a position back into [lo, hi] (TimeIntegrator.hpp:105-115)."""
+    off = np.zeros_like(x)
+    span = (np.asarray(lo, np.float32) - np.asarray(hi, np.float32)).astype(np.float32)
+    off = np.where(x > np.asarray(hi, np.float32), span, off)
+    off = np.where(x < np.asarray(lo, np.float32), -span, off)
+    return off.astype(np.float32)
+
+
+def euler_run(x0, velocity, dt, tf, lim=None, output=None, output_step=1):
+    """ExplicitEuler::Run (include/TimeIntegrator.hpp:431-488), float32 positions.
+
+    ``velocity(t, pos6)`` gets t rounded to float32 and an (n, 6) array (positions wrapped
+    into the box when ``lim`` = (lo, hi) is given; angles zero) and returns (n, 3).
+    ``output(pos, vel)`` is called every ``output_step`` steps before the wrap is
+    applied to the stored positions, as the reference does.
+    """
+    x = np.array(x0, np.float32, copy=True)
+    n = len(x)
+    t, count = 0.0, 0
+    while t < tf - 1e-5:
+        h = min(dt, tf - t)
+        inp = np.zeros((n, 6), np.float32)
+        inp[:, :3] = x if lim is None else x + _periodic_offsets(x, *lim)
+        v = np.asarray(velocity(float(np.float32(t + h)), inp), np.float32)[:, :3]  # t passed as float
+        x = (x + v * np.float32(h)).astype(np.float32)
+        off = None if lim is None else _periodic_offsets(x, *lim)
+        t += h
+        if output is not None and count % output_step == 0:
+            output(x.copy(), v.copy())
+        if off is not None:
+            x = (x + off).astype(np.float32)
+        count += 1
+    return x, count
+
+
+def dp45_run(x0, velocity, dt, tf, threshold=1e-3, output=None, output_step=1):
+    """ExplicitRk4::Run (include/TimeIntegrator.hpp:602-860): adaptive Dormand-Prince 5(4)
+    with FSAL, float32 stage arithmetic, no periodic box.
+
+    Reproduced quirks: k1 is zero on the first step (the initial evaluation writes the
+    velocity, :608); the step size grown at the end of a step is discarded because the
+    next step starts from min(h0, tf - t) (:616).
+    """
+    f32 = np.float32
+    a = {
+        21: f32(1) / f32(5), 31: f32(3) / f32(40), 32: f32(9) / f32(40),
+        41: f32(44) / f32(45), 42: f32(-56) / f32(15), 43: f32(32) / f32(9),
+        51: f32(19372) / f32(6561), 52: f32(-25360) / f32(2187), 53: f32(64448) / f32(6561),
+        54: f32(-212) / f32(729),
+        61: f32(9017) / f32(3168), 62: f32(-355) / f32(33), 63: f32(46732) / f32(5247), 64: f32(49) / f32(176),
+        65: f32(-5103) / f32(18656),
+    }
+    b1, b3, b4 = f32(35) / f32(384), f32(500) / f32(1113), f32(125) / f32(192)
+    b5, b6 = f32(-2187) / f32(6784), f32(11) / f32(84)
+    dc = [b1 - f32(5179) / f32(57600), None, b3 - f32(7571) / f32(16695), b4 - f32(393) / f32(640),
+          b5 - f32(-92097) / f32(339200), b6 - f32(187) / f32(2100), f32(-1) / f32(40)]
+    c = [f32(0), f32(1) / f32(5), f32(3) / f32(10), f32(4) / f32(5), f32(8) / f32(9), f32(1), f32(1)]
+    rows = {1: [(1, a[21])], 2: [(1, a[31]), (2, a[32])], 3: [(1, a[41]), (2, a[42]), (3, a[43])],
+            4: [(1, a[51]), (2, a[52]), (3, a[53]), (4, a[54])],
+            5: [(1, a[61]), (2, a[62]), (3, a[63]), (4, a[64]), (5, a[65])],
+            6: [(1, b1), (3, b3), (4, b4), (5, b5), (6, b6)]}
+    x = np.array(x0, np.float32, copy=True)
+    n = len(x)
+    k = {i: np.zeros((n, 3), np.float32) for i in range(1, 8)}
+
+    def vel(t, p):
+        inp = np.zeros((n, 6), np.float32)
+        inp[:, :3] = p
+        return np.asarray(velocity(float(np.float32(t)), inp), np.float32)[:, :3]  # t passed as float
+
+    v = vel(0.0, x)
+    t, count = 0.0, 0
+    while t < tf - 1e-5:
+        h = min(dt, tf - t)
+        x0s = x.copy()
+        err = 100.0
+        while err > threshold:
+            for i in range(1, 7):
+                p = x0s.copy()
+                for j, coef in rows[i]:
+                    p = (p + k[j] * f32(float(coef) * h)).astype(np.float32)  # (a_ij * dt) in double, then float
+                x = p
+                v = vel(t + float(c[i]) * h, x)
+                k[i + 1] = v
+            ve = (k[1] * dc[0] + k[3] * dc[2] + k[4] * dc[3] + k[5] * dc[4] + k[6] * dc[5] + k[7] * dc[6])
+            ve = (ve.astype(np.float32) * f32(h)).astype(np.float32)
+            sq = (ve[:, 0] * ve[:, 0] + ve[:, 1] * ve[:, 1] + ve[:, 2] * ve[:, 2]).astype(np.float32)
+            err = math.sqrt(float(np.sum(sq.astype(np.float64))))
+            if err > threshold:
+                h = h * max(0.8 * (err / threshold) ** -0.2, 0.1)
+                h = max(h, 1e-6)
+        t += h
+        if output is not None and count % output_step == 0:
+            output(x.copy(), v.copy())
+        k[1] = k[7].copy()
+        count += 1
+    return x, count
