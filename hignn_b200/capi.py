@@ -35,6 +35,8 @@ P_TIMING = 102
 P_STUDENT_TOL = 103
 P_FIELDS = 104
 P_RECORD_PIVOTS = 105
+P_FAR_POOL_MB = 106
+P_RANK_HINT_OFFSET = 107
 
 STUDENT_PARAMS = 2537
 
@@ -83,6 +85,8 @@ SIGNATURES = {
     "hignn_get_student": ([_P, _fp, C.c_int], C.c_int),
     "hignn_student_eval": ([_P, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "hignn_student_grad": ([_P, C.c_void_p, C.c_void_p, C.c_int64, _fp, _dp], C.c_int),
+    "hignn_set_shard": ([_P, C.c_int, C.c_int], C.c_int),
+    "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
     "hignn_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
@@ -226,6 +230,16 @@ class Model:
         check(lib.hignn_get_lists(self._h, ci.ctypes.data_as(_i64p), cj.ctypes.data_as(_i64p),
                                   fi.ctypes.data_as(_i64p), fj.ctypes.data_as(_i64p)))
         return ci, cj, fi, fj
+
+    def set_shard(self, rank, world):
+        """Compute only shard `rank` of `world` of the block lists; dot then returns partial velocities."""
+        check(lib.hignn_set_shard(self._h, int(rank), int(world)))
+
+    def shard(self):
+        """(close begin, close end, far begin, far end) of this model's shard, in list order."""
+        r = np.empty(4, np.int64)
+        check(lib.hignn_get_shard(self._h, r.ctypes.data_as(_i64p)))
+        return tuple(int(v) for v in r)
 
     # ---- far-field student network
     def train_student(self, steps=20000, batch=65536, nsamples=10_000_000, lr=1e-3, seed=1):

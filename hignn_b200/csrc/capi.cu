@@ -8,8 +8,8 @@
 //   f4   float4[n]   forces, gathered per dot
 //   u    double[3n]  velocity accumulator (FP64, src/HignnModel.cpp:555)
 // Near-field work is a list of PairWork (one per close leaf pair) consumed by a
-// persistent kernel; the far field is cut into ACA batches sized by
-// HIGNN_P_FAR_BATCH_ROWS whose C/Q pools are allocated once and reused.
+// persistent kernel; the far field is cut into ACA batches whose C/Q pools fit
+// HIGNN_P_FAR_POOL_MB (allocated once and reused).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -93,7 +93,14 @@ struct hignn_model {
   bool post_check = false, use_symmetry = true;
   // this implementation
   int precision = 0;
-  int64_t far_batch_rows = int64_t(1) << 21;
+  int64_t far_batch_rows = int64_t(1) << 26;
+  int64_t far_pool_bytes = int64_t(24) << 30;  // C + Q pool memory of one ACA batch
+  int rank_hint_offset = 0;                      // added to recorded ranks when planning (tests)
+  // shard of the block lists this model computes (hignn_set_shard): close pairs [sh_c0, sh_c1),
+  // far pairs [sh_f0, sh_f1) of the lists
+  int shard_rank = 0, shard_world = 1;
+  int64_t sh_c0 = 0, sh_c1 = 0, sh_f0 = 0, sh_f1 = 0;
+  bool shard_ready = false;
   bool timing = false;
   double student_tol = 1e-3;
   int fields = 3;
@@ -117,20 +124,26 @@ struct hignn_model {
 
   DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
-      far_preI, far_preJ, far_ctr, far_stats;
+      far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
   int32_t* host_ctr = nullptr;
 
-  // far-field plan
+  // far-field plan: blocks in batch order; iters > 0 when every block's rank is known
   struct Batch {
-    int b0, b1;
+    int b0, b1, iters;
   };
   std::vector<hignn::FarBlock> far_plan;
   std::vector<Batch> batches;
   bool plan_ready = false;
+  bool plan_hinted = false;
   int plan_max_iter = -1;
-  int64_t plan_rows = -1;
-  int plan_nodes = -1;
+  int64_t plan_rows = -1, plan_pool = -1;
+  int plan_offset = 0;
+  // ACA ranks of the last far field (far-list order), valid for the same tree and settings
+  std::vector<int32_t> rank_hint;
+  bool hint_valid = false;
+  int hint_precision = -1, hint_max_iter = -1;
+  double hint_epsilon = -1.0;
 
   hignn_stats stats{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -150,7 +163,8 @@ struct hignn_model {
     hignn::TcWeights w;
     w.w2img = weights_tc.as<uint4>();
     w.w3img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2);
-    w.w1b1 = f.w1b1;
+    w.w1img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2 +
+                                             32 * hignn::kH2 * 2);
     w.b2 = f.b2;
     w.b3 = f.b3;
     return w;
@@ -182,6 +196,8 @@ void build_structures(hignn_model* m) {
   m->lists_max_rel = m->max_relative_coord;
   m->tree_ready = true;
   m->plan_ready = false;
+  m->hint_valid = false;
+  m->shard_ready = false;
   const auto t1 = std::chrono::steady_clock::now();
   m->stats.t_build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   m->stats.n = m->n;
@@ -239,59 +255,106 @@ void ensure_tree(hignn_model* m) {
     build_structures(m);
 }
 
-// ACA batches: far pairs in list order, cut when the rows of the batch exceed
-// far_batch_rows or its block count exceeds max_far_dot_work_node_size.
-void ensure_far_plan(hignn_model* m) {
-  if (m->plan_ready && m->plan_max_iter == m->max_iter && m->plan_rows == m->far_batch_rows &&
-      m->plan_nodes == m->max_far_dot_work_node_size)
-    return;
-  const size_t nf = m->lists.farI.size();
-  m->far_plan.assign(nf, hignn::FarBlock{});
-  m->batches.clear();
+// Contiguous range of `cost` owned by `rank` of `world` with about equal cost per rank.
+void balanced_range(const std::vector<double>& cost, int rank, int world, int64_t* lo, int64_t* hi) {
+  const size_t n = cost.size();
+  std::vector<double> pre(n + 1, 0.0);
+  for (size_t q = 0; q < n; q++) pre[q + 1] = pre[q] + cost[q];
+  auto cut = [&](int r) -> int64_t {
+    if (r <= 0) return 0;
+    if (r >= world) return (int64_t)n;
+    const double target = pre[n] * r / world;
+    return (int64_t)(std::lower_bound(pre.begin(), pre.end(), target) - pre.begin());
+  };
+  *lo = std::min<int64_t>(cut(rank), (int64_t)n);
+  *hi = std::max(*lo, std::min<int64_t>(cut(rank + 1), (int64_t)n));
+}
+
+// The shard of this model: close pairs balanced by |I||J| evaluations, far pairs by
+// (|I| + |J|) min(kmax, 32) (query rows times a typical rank), contiguous in list order as the
+// reference's ranks take interleaved shares of the same lists (src/CloseFarCheck.cpp:309,394).
+void ensure_shard(hignn_model* m) {
+  if (m->shard_ready) return;
+  std::vector<double> cc(m->lists.closeI.size()), fc(m->lists.farI.size());
+  for (size_t q = 0; q < cc.size(); q++) {
+    const auto& I = m->tree.nodes[m->lists.closeI[q]];
+    const auto& J = m->tree.nodes[m->lists.closeJ[q]];
+    cc[q] = (double)(I.end - I.start) * (double)(J.end - J.start);
+  }
+  for (size_t q = 0; q < fc.size(); q++) {
+    const auto& I = m->tree.nodes[m->lists.farI[q]];
+    const auto& J = m->tree.nodes[m->lists.farJ[q]];
+    const int64_t nI = I.end - I.start, nJ = J.end - J.start;
+    fc[q] = (double)(nI + nJ) * (double)std::min<int64_t>(std::min<int64_t>(m->max_iter, std::min(nI, nJ)), 32);
+  }
+  balanced_range(cc, m->shard_rank, m->shard_world, &m->sh_c0, &m->sh_c1);
+  balanced_range(fc, m->shard_rank, m->shard_world, &m->sh_f0, &m->sh_f1);
+  int64_t evals = 0;
+  for (int64_t q = m->sh_c0; q < m->sh_c1; q++) evals += (int64_t)cc[q];
+  m->stats.close_evals = evals;
+  m->shard_ready = true;
+}
+
+bool hints_usable(const hignn_model* m) {
+  return m->hint_valid && m->hint_precision == m->precision && m->hint_epsilon == m->epsilon &&
+         m->hint_max_iter == m->max_iter && m->rank_hint.size() == m->lists.farI.size();
+}
+
+// Lays out far blocks `idx` (far-list positions) with pool capacities `kcap` into ACA batches:
+// a batch is cut when its C + Q pools (9 doubles per particle and term) would exceed
+// far_pool_bytes or its rows (sum of |I| + |J|) far_batch_rows. Grows the device buffers to
+// the largest batch. Returns the blocks in batch order.
+std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<int>& idx, const std::vector<int>& kcap,
+                                            bool known, std::vector<hignn_model::Batch>& batches) {
+  std::vector<hignn::FarBlock> out(idx.size());
+  batches.clear();
   int64_t rows = 0, cE = 0, qE = 0, maxC = 0, maxQ = 0;
   int32_t rOff = 0, colOff = 0, maxR = 0, maxCol = 0;
-  int b0 = 0, maxNb = 0;
-  for (size_t q = 0; q < nf; q++) {
+  int b0 = 0, maxNb = 0, iters = 0;
+  for (size_t p = 0; p < idx.size(); p++) {
+    const int q = idx[p];
     const auto& I = m->tree.nodes[m->lists.farI[q]];
     const auto& J = m->tree.nodes[m->lists.farJ[q]];
     const int32_t nI = (int32_t)(I.end - I.start), nJ = (int32_t)(J.end - J.start);
-    const int cnt = (int)q - b0;
-    if (cnt > 0 && (rows + nI + nJ > m->far_batch_rows || cnt >= m->max_far_dot_work_node_size)) {
-      m->batches.push_back({b0, (int)q});
+    const int cnt = (int)p - b0;
+    const int64_t add = (int64_t)kcap[p] * (nI + nJ) * 9 * (int64_t)sizeof(double);
+    if (cnt > 0 && ((cE + qE) * 9 * (int64_t)sizeof(double) + add > m->far_pool_bytes ||
+                    rows + nI + nJ > m->far_batch_rows)) {
+      batches.push_back({b0, (int)p, known ? iters : 0});
       maxNb = std::max(maxNb, cnt);
-      b0 = (int)q;
+      b0 = (int)p;
       rows = cE = qE = 0;
       rOff = colOff = 0;
+      iters = 0;
     }
     hignn::FarBlock fb{};
     fb.sI = (int32_t)I.start;
     fb.nI = nI;
     fb.sJ = (int32_t)J.start;
     fb.nJ = nJ;
-    fb.kmax = std::max(1, std::min(m->max_iter, std::min(nI, nJ)));
+    fb.kcap = kcap[p];
+    fb.list_idx = q;
     fb.cOff = cE;
     fb.qOff = qE;
     fb.rOff = rOff;
     fb.colOff = colOff;
-    cE += (int64_t)fb.kmax * nI;
-    qE += (int64_t)fb.kmax * nJ;
+    cE += (int64_t)fb.kcap * nI;
+    qE += (int64_t)fb.kcap * nJ;
     rOff += nI;
     colOff += nJ;
     rows += nI + nJ;
+    iters = std::max(iters, fb.kcap);
     maxC = std::max(maxC, cE);
     maxQ = std::max(maxQ, qE);
     maxR = std::max(maxR, rOff);
     maxCol = std::max(maxCol, colOff);
-    m->far_plan[q] = fb;
+    out[p] = fb;
   }
-  if (nf > 0) {
-    m->batches.push_back({b0, (int)nf});
-    maxNb = std::max(maxNb, (int)nf - b0);
+  if (!idx.empty()) {
+    batches.push_back({b0, (int)idx.size(), known ? iters : 0});
+    maxNb = std::max(maxNb, (int)idx.size() - b0);
   }
-  if (m->device >= 0 && nf > 0) {
-    m->far_blocks.ensure(sizeof(hignn::FarBlock) * nf);
-    HIGNN_CUDA(cudaMemcpyAsync(m->far_blocks.p, m->far_plan.data(), sizeof(hignn::FarBlock) * nf,
-                               cudaMemcpyHostToDevice, m->stream));
+  if (m->device >= 0 && !idx.empty()) {
     const int ldr = m->max_iter + 1;
     m->far_state.ensure(sizeof(hignn::FarState) * maxNb);
     m->far_rows.ensure(sizeof(int32_t) * (size_t)maxNb * ldr);
@@ -305,12 +368,57 @@ void ensure_far_plan(hignn_model* m) {
     m->far_preJ.ensure(sizeof(int32_t) * (maxNb + 1));
     m->far_ctr.ensure(sizeof(int32_t) * hignn::kCtrCount);
     m->far_stats.ensure(sizeof(unsigned long long) * 4);
+    m->far_rank.ensure(sizeof(int32_t) * std::max<size_t>(1, m->lists.farI.size()));
+  }
+  return out;
+}
+
+// ACA plan of the far list. Without rank information every block gets the pool capacity
+// min(max_iter, |I|, |J|) and the batches follow the list order (src/FarDot.cpp:191-340
+// batches the list in order). When the previous far field on the same tree and settings
+// recorded every block's rank, each block gets exactly that capacity, the blocks are sorted by
+// rank (batches of similar ranks need fewer iterations) and each batch runs its known
+// iteration count without reading counters back; a block that would need more terms than
+// recorded is deferred and rerun with the full capacity, so the result never depends on the
+// hint.
+void ensure_far_plan(hignn_model* m) {
+  ensure_shard(m);
+  const bool use_hints = hints_usable(m);
+  if (m->plan_ready && m->plan_hinted == use_hints && m->plan_max_iter == m->max_iter &&
+      m->plan_rows == m->far_batch_rows && m->plan_pool == m->far_pool_bytes &&
+      m->plan_offset == m->rank_hint_offset)
+    return;
+  const size_t nf = (size_t)(m->sh_f1 - m->sh_f0);
+  std::vector<int> idx(nf), kcap(nf);
+  std::vector<int> full(m->lists.farI.size());
+  for (size_t p = 0; p < nf; p++) {
+    const size_t q = (size_t)m->sh_f0 + p;
+    const auto& I = m->tree.nodes[m->lists.farI[q]];
+    const auto& J = m->tree.nodes[m->lists.farJ[q]];
+    const int nI = (int)(I.end - I.start), nJ = (int)(J.end - J.start);
+    full[q] = std::max(1, std::min(m->max_iter, std::min(nI, nJ)));
+    idx[p] = (int)q;
+  }
+  if (use_hints) {
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return m->rank_hint[x] > m->rank_hint[y]; });
+    for (size_t p = 0; p < nf; p++)
+      kcap[p] = std::max(1, std::min(full[idx[p]], m->rank_hint[idx[p]] + m->rank_hint_offset));
+  } else {
+    for (size_t p = 0; p < nf; p++) kcap[p] = full[idx[p]];
+  }
+  m->far_plan = layout_batches(m, idx, kcap, use_hints, m->batches);
+  if (m->device >= 0 && nf > 0) {
+    m->far_blocks.ensure(sizeof(hignn::FarBlock) * nf);
+    HIGNN_CUDA(cudaMemcpyAsync(m->far_blocks.p, m->far_plan.data(), sizeof(hignn::FarBlock) * nf,
+                               cudaMemcpyHostToDevice, m->stream));
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
   }
   m->plan_ready = true;
+  m->plan_hinted = use_hints;
   m->plan_max_iter = m->max_iter;
   m->plan_rows = m->far_batch_rows;
-  m->plan_nodes = m->max_far_dot_work_node_size;
+  m->plan_pool = m->far_pool_bytes;
+  m->plan_offset = m->rank_hint_offset;
 }
 
 // BF16 round-to-nearest-even
@@ -376,7 +484,8 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
     return (size_t)slab * rows_per_slab * 128 + (size_t)(row >> 3) * 1024 + (row & 7) * 128 +
            (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
   };
-  std::vector<uint8_t> img(kH2 * kH1 * 2 + 32 * kH2 * 2, 0);
+  const size_t w1off = (size_t)kH2 * kH1 * 2 + 32 * kH2 * 2;
+  std::vector<uint8_t> img(w1off + (size_t)kH1 * 64 * 2, 0);
   auto put = [&](size_t off, uint16_t v) { std::memcpy(img.data() + off, &v, 2); };
   for (int nn = 0; nn < kH2; nn++)
     for (int k = 0; k < kH1; k++) put(swz(nn, k, kH2), bf16_bits(W[1][(size_t)nn * kH1 + k]));
@@ -389,7 +498,24 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
       put(w3off + swz(o, k, 32), hi);
       put(w3off + swz(16 + o, k, 32), lo);
     }
+  // layer 1 as one K = 16 MMA on split operands: row n = [W_hi(3), W_hi(3), W_lo(3), b1_hi, b1_lo, 0 x 5]
+  // against the feature row [r_hi(3), r_lo(3), r_hi(3), 1, 1, 0 x 5]
+  for (int nn = 0; nn < kH1; nn++) {
+    uint16_t row[16] = {0};
+    for (int d = 0; d < 3; d++) {
+      const float v = W[0][3 * nn + d];
+      const uint16_t hi = bf16_bits(v);
+      row[d] = hi;
+      row[3 + d] = hi;
+      row[6 + d] = bf16_bits(v - bf16_value(hi));
+    }
+    const uint16_t bh = bf16_bits(B[0][nn]);
+    row[9] = bh;
+    row[10] = bf16_bits(B[0][nn] - bf16_value(bh));
+    for (int k = 0; k < 16; k++) put(w1off + swz(nn, k, kH1), row[k]);
+  }
   m->has_weights = true;
+  m->hint_valid = false;  // ACA ranks depend on the network
   if (m->device < 0) return;
   HIGNN_CUDA(cudaSetDevice(m->device));
   m->weights.ensure(sizeof(float) * hw.size());
@@ -399,19 +525,26 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
   HIGNN_CUDA(cudaStreamSynchronize(m->stream));
 }
 
-void far_field(hignn_model* m) {
-  ensure_far_plan(m);
-  m->stats.far_evals = 0;
-  m->stats.far_rank_sum = 0;
-  m->stats.far_rank_max = 0;
-  m->stats.far_iterations = 0;
-  if (m->batches.empty()) return;
-  HIGNN_CUDA(cudaMemsetAsync(m->far_stats.p, 0, sizeof(unsigned long long) * 4, m->stream));
+struct FarOutcome {
+  std::vector<int> deferred;  // far-list positions that outgrew their pool capacity
+  std::vector<int> fallback;  // far-list positions the student check sent to the teacher
+};
+
+// Runs the ACA batches of `plan` (device copy at d_blocks). student_pass: queries by the
+// student network, each converged block applied only after its sampled residual against the
+// teacher passed (student_tol); otherwise queries by the teacher (tensor cores from precision 1
+// on, FP32 SIMT at precision 0).
+FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& plan,
+                           const std::vector<hignn_model::Batch>& batches, const hignn::FarBlock* d_blocks,
+                           bool student_pass, int* iterations) {
   const hignn::MlpF32 w = m->wdev();
-  int iterations = 0;
-  for (const auto& bt : m->batches) {
+  const hignn::TcWeights tcw = m->wtc();
+  const float* student = student_pass ? m->student.as<float>() : nullptr;
+  FarOutcome out;
+  std::vector<int>& deferred = out.deferred;
+  for (const auto& bt : batches) {
     hignn::FarArgs a{};
-    a.blocks = m->far_blocks.as<hignn::FarBlock>() + bt.b0;
+    a.blocks = d_blocks + bt.b0;
     a.nb = bt.b1 - bt.b0;
     a.state = m->far_state.as<hignn::FarState>();
     a.rows = m->far_rows.as<int32_t>();
@@ -427,37 +560,115 @@ void far_field(hignn_model* m) {
     a.ctr = m->far_ctr.as<int32_t>();
     a.rank_sum = m->far_stats.as<unsigned long long>();
     a.evals = m->far_stats.as<unsigned long long>() + 1;
+    a.rank_out = m->far_rank.as<int32_t>();
     a.x = m->x4.as<float4>();
     a.f = m->f4.as<float4>();
     a.u = m->u.as<double>();
     a.max_iter = m->max_iter;
     a.eps2 = m->epsilon * m->epsilon;
     a.use_symmetry = m->use_symmetry ? 1 : 0;
-    const auto& last = m->far_plan[bt.b1 - 1];
+    a.defer_apply = student_pass ? 1 : 0;
+    const auto& last = plan[bt.b1 - 1];
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
-    const hignn::TcWeights tcw = m->wtc();
-    const float* student = (m->precision == 2 && m->has_student) ? m->student.as<float>() : nullptr;
-    hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, student, m->err_flag(), m->num_sms, m->host_ctr,
-                           m->stream, &iterations);
+    const int nd = hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, student, m->err_flag(),
+                                          m->num_sms, m->host_ctr, m->stream, bt.iters, iterations);
     m->stats.far_rank_max = std::max(m->stats.far_rank_max, m->host_ctr[hignn::kCtrRankMax]);
-    if (m->record_pivots) {
-      const int nb = bt.b1 - bt.b0, ld = a.ldr;
-      if (bt.b0 == 0) {
-        m->piv_ld = ld;
-        m->piv_rank.assign(m->far_plan.size(), 0);
-        m->piv_rows.assign(m->far_plan.size() * (size_t)ld, -1);
-        m->piv_cols.assign(m->far_plan.size() * (size_t)ld, -1);
-      }
-      std::vector<hignn::FarState> st(nb);
-      HIGNN_CUDA(cudaMemcpyAsync(st.data(), a.state, sizeof(hignn::FarState) * nb, cudaMemcpyDeviceToHost, m->stream));
-      HIGNN_CUDA(cudaMemcpyAsync(m->piv_rows.data() + (size_t)bt.b0 * ld, a.rows, sizeof(int32_t) * nb * ld,
-                                 cudaMemcpyDeviceToHost, m->stream));
-      HIGNN_CUDA(cudaMemcpyAsync(m->piv_cols.data() + (size_t)bt.b0 * ld, a.cols, sizeof(int32_t) * nb * ld,
-                                 cudaMemcpyDeviceToHost, m->stream));
-      HIGNN_CUDA(cudaStreamSynchronize(m->stream));
-      for (int q = 0; q < nb; q++) m->piv_rank[bt.b0 + q] = st[q].k;
+    m->stats.gpu_launches += 1;
+    const int nb = bt.b1 - bt.b0, ld = a.ldr;
+    int nfail = 0;
+    if (student_pass) {
+      const size_t ns = (size_t)nb * hignn::kFarSamples;
+      m->far_check.ensure(sizeof(float) * ns * 21 + 64);
+      float* feat = m->far_check.as<float>();
+      // The student cannot represent the teacher's fine texture (its residual from the RPY tensor has
+      // ~3e-3 relative amplitude and a correlation length of 1-2 radii at every distance), so a
+      // block is sent back to the teacher when the student's sampled error exceeds the accuracy
+      // the ACA block is held to anyway: the larger of student_tol and epsilon.
+      const float tol = (float)std::max(m->student_tol, m->epsilon);
+      nfail = hignn::far_student_check(a, tcw, student, tol, feat, feat + 3 * ns, feat + 12 * ns,
+                                       reinterpret_cast<int*>(feat + 21 * ns), m->err_flag(), m->num_sms, m->stream);
+      m->stats.student_fallback_blocks += nfail;
+      m->stats.gpu_launches += 5;
     }
+    std::vector<hignn::FarState> st;
+    if (nd > 0 || nfail > 0 || m->record_pivots) {
+      st.resize(nb);
+      HIGNN_CUDA(cudaMemcpyAsync(st.data(), a.state, sizeof(hignn::FarState) * nb, cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+      for (int q = 0; q < nb; q++) {
+        if (st[q].done == 2) deferred.push_back(plan[bt.b0 + q].list_idx);
+        if (st[q].done == 3) out.fallback.push_back(plan[bt.b0 + q].list_idx);
+      }
+    }
+    if (m->record_pivots) {
+      std::vector<int32_t> rows((size_t)nb * ld), cols((size_t)nb * ld);
+      HIGNN_CUDA(cudaMemcpyAsync(rows.data(), a.rows, sizeof(int32_t) * nb * ld, cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaMemcpyAsync(cols.data(), a.cols, sizeof(int32_t) * nb * ld, cudaMemcpyDeviceToHost, m->stream));
+      HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+      for (int q = 0; q < nb; q++) {
+        if (st[q].done != 1) continue;
+        const int li = plan[bt.b0 + q].list_idx;
+        m->piv_rank[li] = st[q].k;
+        std::copy(rows.begin() + (size_t)q * ld, rows.begin() + (size_t)(q + 1) * ld,
+                  m->piv_rows.begin() + (size_t)li * ld);
+        std::copy(cols.begin() + (size_t)q * ld, cols.begin() + (size_t)(q + 1) * ld,
+                  m->piv_cols.begin() + (size_t)li * ld);
+      }
+    }
+  }
+  return out;
+}
+
+// Full-capacity plan of the given far-list positions (deferred blocks, student fallbacks).
+void run_far_subset(hignn_model* m, const std::vector<int>& subset, bool student_pass, int* iterations,
+                    FarOutcome* out) {
+  std::vector<int> kcap(subset.size());
+  for (size_t p = 0; p < subset.size(); p++) {
+    const auto& I = m->tree.nodes[m->lists.farI[subset[p]]];
+    const auto& J = m->tree.nodes[m->lists.farJ[subset[p]]];
+    kcap[p] = std::max(1, std::min(m->max_iter, (int)std::min(I.end - I.start, J.end - J.start)));
+  }
+  std::vector<hignn_model::Batch> rb;
+  const std::vector<hignn::FarBlock> rplan = layout_batches(m, subset, kcap, false, rb);
+  m->far_retry.ensure(sizeof(hignn::FarBlock) * rplan.size());
+  HIGNN_CUDA(cudaMemcpyAsync(m->far_retry.p, rplan.data(), sizeof(hignn::FarBlock) * rplan.size(),
+                             cudaMemcpyHostToDevice, m->stream));
+  *out = run_far_batches(m, rplan, rb, m->far_retry.as<hignn::FarBlock>(), student_pass, iterations);
+}
+
+void far_field(hignn_model* m) {
+  ensure_far_plan(m);
+  m->stats.far_evals = 0;
+  m->stats.far_rank_sum = 0;
+  m->stats.far_rank_max = 0;
+  m->stats.far_iterations = 0;
+  if (m->batches.empty()) return;
+  const size_t nf = m->lists.farI.size();  // pivots and ranks are kept in far-list order
+  if (m->record_pivots) {
+    m->piv_ld = m->max_iter + 1;
+    m->piv_rank.assign(nf, 0);
+    m->piv_rows.assign(nf * (size_t)m->piv_ld, -1);
+    m->piv_cols.assign(nf * (size_t)m->piv_ld, -1);
+  }
+  HIGNN_CUDA(cudaMemsetAsync(m->far_stats.p, 0, sizeof(unsigned long long) * 4, m->stream));
+  m->stats.student_fallback_blocks = 0;
+  int iterations = 0;
+  const bool student_pass = m->precision == 2 && m->has_student;
+  FarOutcome res =
+      run_far_batches(m, m->far_plan, m->batches, m->far_blocks.as<hignn::FarBlock>(), student_pass, &iterations);
+  const bool had_deferred = !res.deferred.empty();
+  std::vector<int> fallback = res.fallback;
+  if (had_deferred) {  // blocks that outgrew their recorded rank: rerun with the full capacity
+    FarOutcome r2;
+    run_far_subset(m, res.deferred, student_pass, &iterations, &r2);
+    if (!r2.deferred.empty()) throw Error(HIGNN_ERR_LIMIT, "ACA: a block was deferred at its full capacity");
+    fallback.insert(fallback.end(), r2.fallback.begin(), r2.fallback.end());
+  }
+  if (!fallback.empty()) {  // student residual above tolerance: the teacher network for these blocks
+    FarOutcome r3;
+    run_far_subset(m, fallback, false, &iterations, &r3);
+    if (!r3.deferred.empty()) throw Error(HIGNN_ERR_LIMIT, "ACA: a block was deferred at its full capacity");
   }
   unsigned long long st[2];
   HIGNN_CUDA(cudaMemcpyAsync(st, m->far_stats.p, sizeof(st), cudaMemcpyDeviceToHost, m->stream));
@@ -465,14 +676,25 @@ void far_field(hignn_model* m) {
   m->stats.far_rank_sum = (int64_t)st[0];
   m->stats.far_evals = (int64_t)st[1];
   m->stats.far_iterations = iterations;
-  // per batch: one init kernel; per ACA iteration: active list, column eval, column pivot, row eval, row pivot
-  m->stats.gpu_launches += (int64_t)m->batches.size() + 5 * (int64_t)iterations;
+  // per ACA iteration: active list, column eval, column pivot, row eval, row pivot
+  m->stats.gpu_launches += 5 * (int64_t)iterations;
+  if (!m->plan_hinted || had_deferred) {  // record the ranks for the next far field on this tree
+    m->rank_hint.resize(nf);
+    HIGNN_CUDA(cudaMemcpyAsync(m->rank_hint.data(), m->far_rank.p, sizeof(int32_t) * nf, cudaMemcpyDeviceToHost,
+                               m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    m->hint_valid = true;
+    m->hint_precision = m->precision;
+    m->hint_epsilon = m->epsilon;
+    m->hint_max_iter = m->max_iter;
+  }
 }
 
 void near_field(hignn_model* m) {
   hignn::NearArgs a{};
-  a.work = m->close_work.as<hignn::PairWork>();
-  a.nwork = (int)m->lists.closeI.size();
+  ensure_shard(m);
+  a.work = m->close_work.as<hignn::PairWork>() + m->sh_c0;
+  a.nwork = (int)(m->sh_c1 - m->sh_c0);
   a.xI = a.xJ = m->x4.as<float4>();
   a.fI = a.fJ = m->f4.as<float4>();
   a.uI = a.uJ = m->u.as<double>();
@@ -750,6 +972,11 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         if (v < 1024) throw Error(HIGNN_ERR_ARG, "far_batch_rows must be >= 1024");
         m->far_batch_rows = (int64_t)v;
         break;
+      case HIGNN_P_FAR_POOL_MB:
+        if (v < 1) throw Error(HIGNN_ERR_ARG, "far_pool_mb must be >= 1");
+        m->far_pool_bytes = (int64_t)(v * 1048576.0);
+        break;
+      case HIGNN_P_RANK_HINT_OFFSET: m->rank_hint_offset = (int)v; break;
       case HIGNN_P_TIMING: m->timing = v != 0; break;
       case HIGNN_P_STUDENT_TOL: m->student_tol = v; break;
       case HIGNN_P_FIELDS:
@@ -777,6 +1004,8 @@ int hignn_get_param(hignn_model* m, int key, double* v) {
       case HIGNN_P_MAX_FAR_FIELD_DISTANCE: *v = m->max_far_field_distance; break;
       case HIGNN_P_PRECISION: *v = m->precision; break;
       case HIGNN_P_FAR_BATCH_ROWS: *v = (double)m->far_batch_rows; break;
+      case HIGNN_P_FAR_POOL_MB: *v = (double)m->far_pool_bytes / 1048576.0; break;
+      case HIGNN_P_RANK_HINT_OFFSET: *v = m->rank_hint_offset; break;
       case HIGNN_P_TIMING: *v = m->timing; break;
       case HIGNN_P_STUDENT_TOL: *v = m->student_tol; break;
       case HIGNN_P_FIELDS: *v = m->fields; break;
@@ -951,6 +1180,29 @@ int hignn_get_lists(hignn_model* m, int64_t* ci, int64_t* cj, int64_t* fi, int64
   });
 }
 
+int hignn_set_shard(hignn_model* m, int rank, int world) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null model");
+    if (world < 1 || rank < 0 || rank >= world) throw Error(HIGNN_ERR_ARG, "shard: need 0 <= rank < world");
+    m->shard_rank = rank;
+    m->shard_world = world;
+    m->shard_ready = false;
+    m->plan_ready = false;
+  });
+}
+
+int hignn_get_shard(hignn_model* m, int64_t* ranges) {
+  return guard([&] {
+    if (!m || !ranges) throw Error(HIGNN_ERR_ARG, "null argument");
+    ensure_tree(m);
+    ensure_shard(m);
+    ranges[0] = m->sh_c0;
+    ranges[1] = m->sh_c1;
+    ranges[2] = m->sh_f0;
+    ranges[3] = m->sh_f1;
+  });
+}
+
 int hignn_set_student(hignn_model* m, const float* params, int nparams) {
   return guard([&] {
     if (!m || !params) throw Error(HIGNN_ERR_ARG, "null argument");
@@ -962,6 +1214,7 @@ int hignn_set_student(hignn_model* m, const float* params, int nparams) {
                                m->stream));
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
     m->has_student = true;
+    m->hint_valid = false;
   });
 }
 
@@ -1071,6 +1324,7 @@ int hignn_train_student(hignn_model* m, int steps, int batch, int64_t nsamples, 
     if (final_loss) *final_loss = (double)lh / (9.0 * (double)batch);
     for (DevBuf* b : {&r, &t, &partial, &lpart, &g, &m1, &m2, &l}) b->release();
     m->has_student = true;
+    m->hint_valid = false;
   });
 }
 

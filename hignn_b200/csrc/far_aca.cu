@@ -93,6 +93,7 @@ __global__ void k_far_init(FarArgs a) {
     a.ctr[kCtrRemaining] = a.nb;
     a.ctr[kCtrError] = 0;
     a.ctr[kCtrRankMax] = 0;
+    a.ctr[kCtrDeferred] = 0;
   }
   if (b >= a.nb) return;
   a.state[b].k = 0;
@@ -248,8 +249,8 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
   double* qj = dsm;  // [k][9]
   __shared__ double sv[32], inv[9];
   __shared__ int si[32];
-  const int ai = blockIdx.x;
-  if (ai >= a.ctr[kCtrActive]) return;
+  const int nact = a.ctr[kCtrActive];
+  for (int ai = blockIdx.x; ai < nact; ai += gridDim.x) {
   const int b = a.act[ai];
   const FarBlock bk = a.blocks[b];
   const int k = a.state[b].k;
@@ -291,12 +292,13 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
     }
   }
   block_argmax(best, bi, sv, si);
-  if (bi < 0) {
+  if (bi < 0) {  // CTA-uniform
     if (threadIdx.x == 0) {
       a.ctr[kCtrError] = 1;
       a.rows[(size_t)b * a.ldr + k] = 0;
     }
-    return;
+    __syncthreads();
+    continue;
   }
   if (threadIdx.x == 0) {
     a.rows[(size_t)b * a.ldr + k] = bi;
@@ -331,19 +333,83 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
 #pragma unroll
     for (int q = 0; q < 9; q++) Ck[9 * i + q] = o[q];
   }
+  __syncthreads();  // shared state is reused by the next active block
+  }
+}
+
+// u_I += sum_l C_l (Q_l f_J) and, with symmetry, u_J += sum_l Q_l^T (C_l^T f_I) for one
+// converged block (src/FarDot.cpp:1225-1387); all threads of the CTA call it.
+__device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, double* mid, double* mid2) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int l = wid; l < rank; l += blockDim.x >> 5) {
+    const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
+    const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
+    double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
+    for (int j = lane; j < bk.nJ; j += 32) {
+      const float4 fj = a.f[bk.sJ + j];
+      const double* q = Ql + 9 * j;
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        m[r] += q[3 * r] * (double)fj.x + q[3 * r + 1] * (double)fj.y + q[3 * r + 2] * (double)fj.z;
+    }
+    if (a.use_symmetry)
+      for (int i = lane; i < bk.nI; i += 32) {
+        const float4 fi = a.f[bk.sI + i];
+        const double* c = Cl + 9 * i;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+          m2[r] += c[r] * (double)fi.x + c[3 + r] * (double)fi.y + c[6 + r] * (double)fi.z;
+      }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      for (int o = 16; o > 0; o >>= 1) {
+        m[r] += __shfl_down_sync(0xffffffffu, m[r], o);
+        m2[r] += __shfl_down_sync(0xffffffffu, m2[r], o);
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        mid[3 * l + r] = m[r];
+        mid2[3 * l + r] = m2[r];
+      }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+    double acc[3] = {0, 0, 0};
+    for (int l = 0; l < rank; l++) {
+      const double* c = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        acc[r] += c[3 * r] * mid[3 * l] + c[3 * r + 1] * mid[3 * l + 1] + c[3 * r + 2] * mid[3 * l + 2];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sI + i) + r], acc[r]);
+  }
+  if (a.use_symmetry)
+    for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
+      double acc[3] = {0, 0, 0};
+      for (int l = 0; l < rank; l++) {
+        const double* q = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+          acc[r] += q[r] * mid2[3 * l] + q[3 + r] * mid2[3 * l + 1] + q[6 + r] * mid2[3 * l + 2];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sJ + j) + r], acc[r]);
+    }
 }
 
 // Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
 __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* ci = dsm;                          // [k][9]
-  double* mid = dsm + 9 * kMaxIterCap;       // [rank][3]
-  double* mid2 = mid + 3 * kMaxIterCap;      // [rank][3]
+  double* mid = dsm + 9 * a.ldr;            // [rank][3]
+  double* mid2 = mid + 3 * a.ldr;            // [rank][3]
   __shared__ double sv[32], cross[8][18], red[32 * 12];
   __shared__ int si[32];
   __shared__ int s_done, s_rank;
-  const int ai = blockIdx.x;
-  if (ai >= a.ctr[kCtrActive]) return;
+  const int nact = a.ctr[kCtrActive];
+  for (int ai = blockIdx.x; ai < nact; ai += gridDim.x) {
   const int b = a.act[ai];
   const FarBlock bk = a.blocks[b];
   const int k = a.state[b].k;
@@ -464,116 +530,169 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
     a.state[b].mu2 = mu2;
     a.state[b].k = k1;
     if (k1 < a.ldr) a.cols[(size_t)b * a.ldr + k1] = bj < 0 ? 0 : bj;
+    int deferred = 0;
+    if (!done && k1 >= bk.kcap) {  // the next term would not fit this block's pool share
+      deferred = 1;
+      a.state[b].done = 2;
+      atomicSub(&a.ctr[kCtrRemaining], 1);
+      atomicAdd(&a.ctr[kCtrDeferred], 1);
+    }
     if (done) {
       a.state[b].done = 1;
       atomicSub(&a.ctr[kCtrRemaining], 1);
       atomicMax(&a.ctr[kCtrRankMax], k1);
       atomicAdd(a.rank_sum, (unsigned long long)k1);
+      if (a.rank_out) a.rank_out[bk.list_idx] = k1;
     }
-    s_done = done;
+    s_done = done && !deferred;
     s_rank = k1;
   }
   __syncthreads();
-  if (!s_done) return;
-  // ---- apply (src/FarDot.cpp:1225-1387), rank = k + 1 terms
-  const int rank = s_rank;
-  for (int l = wid; l < rank; l += blockDim.x >> 5) {
-    const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
-    const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
-    double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
-    for (int j = lane; j < bk.nJ; j += 32) {
-      const float4 fj = a.f[bk.sJ + j];
-      const double* q = Ql + 9 * j;
-#pragma unroll
-      for (int r = 0; r < 3; r++)
-        m[r] += q[3 * r] * (double)fj.x + q[3 * r + 1] * (double)fj.y + q[3 * r + 2] * (double)fj.z;
-    }
-    if (a.use_symmetry)
-      for (int i = lane; i < bk.nI; i += 32) {
-        const float4 fi = a.f[bk.sI + i];
-        const double* c = Cl + 9 * i;
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-          m2[r] += c[r] * (double)fi.x + c[3 + r] * (double)fi.y + c[6 + r] * (double)fi.z;
-      }
+  if (!s_done) continue;  // CTA-uniform; the loop-end barrier protects the shared state
+  if (!a.defer_apply) apply_block(a, bk, s_rank, mid, mid2);
+  __syncthreads();
+  }
+}
+
+// Applies every converged block of the batch (state done == 1): the student path defers the
+// apply until the sampled residual check has accepted the block.
+__global__ void __launch_bounds__(kPivThreads) k_far_apply(FarArgs a) {
+  extern __shared__ __align__(16) double dsm[];
+  double* mid = dsm;
+  double* mid2 = dsm + 3 * a.ldr;
+  for (int b = blockIdx.x; b < a.nb; b += gridDim.x) {
+    if (a.state[b].done != 1) continue;  // CTA-uniform
+    const FarBlock bk = a.blocks[b];
+    apply_block(a, bk, a.state[b].k, mid, mid2);
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint64_t mix_hash(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// kFarSamples entries (i, j) per converged block, drawn by a hash of the block's far-list
+// position: features x_j - x_i for the teacher / student residual check.
+__global__ void k_far_samples(FarArgs a, float* __restrict__ feat) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)a.nb * kFarSamples) return;
+  const int b = (int)(g / kFarSamples), q = (int)(g % kFarSamples);
+  const FarBlock bk = a.blocks[b];
+  const uint64_t h = mix_hash(((uint64_t)bk.list_idx << 8) ^ (uint64_t)q);
+  const int i = (int)((h & 0xffffffffull) % (uint64_t)bk.nI), j = (int)((h >> 32) % (uint64_t)bk.nJ);
+  const float4 xi = a.x[bk.sI + i], xj = a.x[bk.sJ + j];
+  feat[3 * g] = xj.x - xi.x;
+  feat[3 * g + 1] = xj.y - xi.y;
+  feat[3 * g + 2] = xj.z - xi.z;
+}
+
+// One warp per block: relative Frobenius residual of the student against the teacher over the
+// block's samples (symmetrised 3x3 blocks, as the far field uses them). A converged block whose
+// residual exceeds tol is marked for the teacher (done = 3).
+__global__ void k_far_check(FarArgs a, const float* __restrict__ yt, const float* __restrict__ ys, float tol2,
+                            int* nfail) {
+  const int lane = threadIdx.x & 31;
+  const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  if (b >= a.nb) return;
+  if (a.state[b].done != 1) return;  // warp-uniform
+  float e2 = 0.f, t2 = 0.f;
+  for (int q = lane; q < kFarSamples; q += 32) {
+    const float* t = yt + 9 * ((int64_t)b * kFarSamples + q);
+    const float* st = ys + 9 * ((int64_t)b * kFarSamples + q);
 #pragma unroll
     for (int r = 0; r < 3; r++)
-      for (int o = 16; o > 0; o >>= 1) {
-        m[r] += __shfl_down_sync(0xffffffffu, m[r], o);
-        m2[r] += __shfl_down_sync(0xffffffffu, m2[r], o);
-      }
-    if (lane == 0)
 #pragma unroll
-      for (int r = 0; r < 3; r++) {
-        mid[3 * l + r] = m[r];
-        mid2[3 * l + r] = m2[r];
+      for (int c = 0; c < 3; c++) {
+        const float tv = 0.5f * (t[3 * r + c] + t[3 * c + r]);
+        const float sv = 0.5f * (st[3 * r + c] + st[3 * c + r]);
+        e2 += (sv - tv) * (sv - tv);
+        t2 += tv * tv;
       }
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
-    double acc[3] = {0, 0, 0};
-    for (int l = 0; l < rank; l++) {
-      const double* c = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
-#pragma unroll
-      for (int r = 0; r < 3; r++)
-        acc[r] += c[3 * r] * mid[3 * l] + c[3 * r + 1] * mid[3 * l + 1] + c[3 * r + 2] * mid[3 * l + 2];
-    }
-#pragma unroll
-    for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sI + i) + r], acc[r]);
+  for (int o = 16; o > 0; o >>= 1) {
+    e2 += __shfl_down_sync(0xffffffffu, e2, o);
+    t2 += __shfl_down_sync(0xffffffffu, t2, o);
   }
-  if (a.use_symmetry)
-    for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
-      double acc[3] = {0, 0, 0};
-      for (int l = 0; l < rank; l++) {
-        const double* q = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-          acc[r] += q[r] * mid2[3 * l] + q[3 + r] * mid2[3 * l + 1] + q[6 + r] * mid2[3 * l + 2];
-      }
-#pragma unroll
-      for (int r = 0; r < 3; r++) atomicAdd(&a.u[3 * (size_t)(bk.sJ + j) + r], acc[r]);
-    }
+  if (lane == 0 && !(e2 <= tol2 * t2)) {
+    a.state[b].done = 3;
+    atomicAdd(nfail, 1);
+  }
 }
 
 }  // namespace
 
-void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
-                     int num_sms, int32_t* host_ctr, cudaStream_t s, int* iterations) {
-  if (a.nb <= 0) return;
+int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations) {
+  if (a.nb <= 0) return 0;
   const size_t eval_smem = sizeof(EvalSmem);
-  const size_t row_smem = sizeof(double) * (9 + 3 + 3) * kMaxIterCap;
-  const size_t col_smem = sizeof(double) * 9 * kMaxIterCap;
+  const size_t row_smem = sizeof(double) * (9 + 3 + 3) * a.ldr;
+  const size_t col_smem = sizeof(double) * 9 * a.ldr;
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem));
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_row_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_col_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+  const int piv_grid = a.nb < 8 * num_sms ? a.nb : 8 * num_sms;  // grid-stride over active blocks
   k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   HIGNN_CHECK_LAUNCH();
+  // Without a known bound the counters are read back every kCheck iterations; the kernels of
+  // an iteration with no active block return at once.
+  constexpr int kCheck = 4;
+  const int limit = known_iters > 0 ? known_iters : a.max_iter + 1;
   int it = 0;
-  for (; it <= a.max_iter; it++) {
-    k_far_active<<<1, 1024, 0, s>>>(a);
-    if (student)
-      launch_far_student(a, student, 0, num_sms, s);
-    else if (tcw)
-      launch_far_tc(a, *tcw, 0, err, num_sms, s);
-    else
-      k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
-    k_far_col_pivot<<<a.nb, kPivThreads, col_smem, s>>>(a);
-    if (student)
-      launch_far_student(a, student, 1, num_sms, s);
-    else if (tcw)
-      launch_far_tc(a, *tcw, 1, err, num_sms, s);
-    else
-      k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
-    k_far_row_pivot<<<a.nb, kPivThreads, row_smem, s>>>(a);
-    HIGNN_CHECK_LAUNCH();
+  bool finished = false;
+  while (it < limit && !finished) {
+    const int span = known_iters > 0 ? limit : (it + kCheck < limit ? kCheck : limit - it);
+    for (int q = 0; q < span; q++, it++) {
+      k_far_active<<<1, 1024, 0, s>>>(a);
+      if (student)
+        launch_far_student(a, student, 0, num_sms, s);
+      else if (tcw)
+        launch_far_tc(a, *tcw, 0, err, num_sms, s);
+      else
+        k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
+      k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
+      if (student)
+        launch_far_student(a, student, 1, num_sms, s);
+      else if (tcw)
+        launch_far_tc(a, *tcw, 1, err, num_sms, s);
+      else
+        k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
+      k_far_row_pivot<<<piv_grid, kPivThreads, row_smem, s>>>(a);
+      HIGNN_CHECK_LAUNCH();
+    }
     HIGNN_CUDA(cudaMemcpyAsync(host_ctr, a.ctr, sizeof(int32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
     HIGNN_CUDA(cudaStreamSynchronize(s));
     if (host_ctr[kCtrError] != 0)
       throw Error(-5, "ACA: pivot search found no unused row/column (non-finite block entries?)");
-    if (host_ctr[kCtrRemaining] == 0) break;
+    finished = host_ctr[kCtrRemaining] == 0;
   }
-  if (host_ctr[kCtrRemaining] != 0) throw Error(-5, "ACA did not converge within max_iter iterations");
-  if (iterations) *iterations += it + 1;
+  if (!finished) throw Error(-5, "ACA did not converge within max_iter iterations");
+  if (iterations) *iterations += it;
+  return host_ctr[kCtrDeferred];
+}
+
+int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat, float* yt,
+                      float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s) {
+  if (a.nb <= 0) return 0;
+  const int64_t ns = (int64_t)a.nb * kFarSamples;
+  HIGNN_CUDA(cudaMemsetAsync(nfail_dev, 0, sizeof(int), s));
+  k_far_samples<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(a, feat);
+  HIGNN_CHECK_LAUNCH();
+  launch_student_eval(student, feat, ys, ns, num_sms, s);
+  launch_eval_tc(feat, yt, ns, tcw, err, num_sms, s);
+  k_far_check<<<(unsigned)((a.nb * 32 + 255) / 256), 256, 0, s>>>(a, yt, ys, tol * tol, nfail_dev);
+  HIGNN_CHECK_LAUNCH();
+  const size_t smem = sizeof(double) * 6 * a.ldr;
+  const int grid = a.nb < 8 * num_sms ? a.nb : 8 * num_sms;
+  k_far_apply<<<grid, kPivThreads, smem, s>>>(a);
+  HIGNN_CHECK_LAUNCH();
+  int nfail = 0;
+  HIGNN_CUDA(cudaMemcpyAsync(&nfail, nfail_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HIGNN_CUDA(cudaStreamSynchronize(s));
+  return nfail;
 }
 
 }  // namespace hignn

@@ -31,16 +31,19 @@ struct FarBlock {
   int32_t sI, nI, sJ, nJ;
   int64_t cOff, qOff;      // batch-relative entry offsets into the C / Q pools
   int32_t rOff, colOff;    // batch-relative offsets into the used-row / used-column flags
-  int32_t kmax, pad;       // min(max_iter, nI, nJ)
+  int32_t kcap;            // pool capacity in ACA terms, <= min(max_iter, nI, nJ)
+  int32_t list_idx;        // position in the far list (ranks are recorded there)
 };
 
+// done: 0 = iterating, 1 = converged (applied to u), 2 = deferred (reached its pool
+// capacity kcap before the stopping rule; not applied, to be rerun with a larger pool)
 struct FarState {
   int32_t k, done;
   double mu2, nu2;
 };
 
 // Counters kept on the device per batch.
-enum FarCtr { kCtrActive = 0, kCtrTotI, kCtrTotJ, kCtrRemaining, kCtrError, kCtrRankMax, kCtrCount = 8 };
+enum FarCtr { kCtrActive = 0, kCtrTotI, kCtrTotJ, kCtrRemaining, kCtrError, kCtrRankMax, kCtrDeferred, kCtrCount = 8 };
 
 struct FarArgs {
   const FarBlock* blocks;
@@ -59,18 +62,33 @@ struct FarArgs {
   int32_t* ctr;       // FarCtr counters
   unsigned long long* rank_sum;
   unsigned long long* evals;
+  int32_t* rank_out;  // [far list size]: ACA rank of each converged block
   const float4* x;
   const float4* f;
   double* u;
   int max_iter;
   double eps2;
   int use_symmetry;
+  int defer_apply;  // 1: converged blocks are applied later by far_student_check
 };
 
+constexpr int kFarSamples = 64;  // sampled entries per block in the student residual check
+
 // One ACA batch to completion. Queries: student != nullptr -> student network; else
-// tcw != nullptr -> teacher on the tensor cores; else teacher FP32 SIMT.
-void far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
-                     int num_sms, int32_t* host_ctr, cudaStream_t s, int* iterations);
+// tcw != nullptr -> teacher on the tensor cores; else teacher FP32 SIMT. known_iters > 0:
+// every block stops (converges or is deferred) within that many iterations, so they are
+// launched without reading the counters back in between; 0: counters are read every
+// few iterations. Returns the number of deferred blocks.
+int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations);
+
+// Student residual check of a finished batch run with defer_apply = 1: kFarSamples entries per
+// converged block are evaluated by the student and by the teacher (tensor cores); blocks whose
+// relative residual exceeds tol are marked done = 3 (to be rerun with the teacher), the others
+// are applied to u. feat / yt / ys: device scratch of nb * kFarSamples * (3 / 9 / 9) floats.
+// Returns the number of marked blocks.
+int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat, float* yt,
+                      float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s);
 
 // student network (student.cu)
 size_t student_grad_smem();

@@ -35,6 +35,7 @@ struct NearTcSmem {
   tc::Smem tcs;
   NearStage st[2];
 };
+static_assert(sizeof(NearTcSmem) + 1024 <= 232448, "near-field shared memory exceeds 227 KB per CTA");
 
 // u_I[i] += v for the rows of a warp: rows of a tile share few i (contiguous), so lanes with
 // equal i are summed by a segmented shuffle reduction and only segment heads add to shared memory.

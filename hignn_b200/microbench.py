@@ -30,6 +30,10 @@ def main():
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
     ap.add_argument("--student-steps", type=int, default=4000, help="training steps when --precision 2")
+    ap.add_argument("--student-batch", type=int, default=16384)
+    ap.add_argument("--student-samples", type=int, default=2_000_000)
+    ap.add_argument("--student-tol", type=float, nargs="*", default=[1e-3],
+                    help="sampled-residual tolerances to time (precision 2)")
     a = ap.parse_args()
 
     import torch
@@ -73,9 +77,23 @@ def main():
         m.set(capi.P_EPSILON, a.epsilon)
         m.set(capi.P_TIMING, 1)
         if a.precision == 2:
-            out["student_loss"] = m.train_student(steps=a.student_steps, batch=16384, nsamples=2_000_000, lr=1e-3,
-                                                  seed=3)
+            import time
+
+            t0 = time.time()
+            out["student_loss"] = m.train_student(steps=a.student_steps, batch=a.student_batch,
+                                                  nsamples=a.student_samples, lr=1e-3, seed=3)
+            out["student_train_s"] = time.time() - t0
+            out["per_tol"] = {}
+            for tol in a.student_tol:
+                m.set(capi.P_STUDENT_TOL, tol)
+                m.dot(f)
+                m.dot(f)
+                st = m.stats()
+                out["per_tol"][str(tol)] = {"far_ms": st["t_far_ms"], "fallback_blocks": st["student_fallback_blocks"],
+                                            "num_far": st["num_far"], "far_iterations": st["far_iterations"]}
+            m.set(capi.P_STUDENT_TOL, a.student_tol[-1])
         m.dot(f)
+        first = m.stats()
         near, far = [], []
         for _ in range(a.reps):
             m.dot(f)
@@ -83,13 +101,16 @@ def main():
             near.append(st["t_close_ms"])
             far.append(st["t_far_ms"])
         st = m.stats()
+        out["first_far_ms"] = first["t_far_ms"]
+        out["first_far_iterations"] = first["far_iterations"]
         out.update(workload=a.workload, n=len(x), near_ms=float(np.min(near)), far_ms=float(np.min(far)),
                    close_evals=st["close_evals"], far_evals=st["far_evals"],
                    near_evals_per_s=st["close_evals"] / max(1e-9, np.min(near)) * 1e3,
                    near_tflops=st["close_evals"] * FLOP_PER_EVAL / max(1e-9, np.min(near)) / 1e9,
                    far_evals_per_s=st["far_evals"] / max(1e-9, np.min(far)) * 1e3 if st["far_evals"] else None,
                    far_iterations=st["far_iterations"], far_rank_max=st["far_rank_max"],
-                   student_fallback_blocks=st["student_fallback_blocks"], gpu_launches=st["gpu_launches"])
+                   student_fallback_blocks=st["student_fallback_blocks"], gpu_launches=st["gpu_launches"],
+                   num_far=st["num_far"])
     print(json.dumps(out), flush=True)
 
 

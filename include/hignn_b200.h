@@ -38,18 +38,23 @@ enum hignn_param {
   HIGNN_P_ETA = 1,                        /* stored, unused (as in the reference)       */
   HIGNN_P_MAX_ITER = 2,                   /* ACA iteration cap, default 100              */
   HIGNN_P_MAT_POOL_SIZE_FACTOR = 3,       /* stored; pools here are sized per batch     */
-  HIGNN_P_MAX_FAR_DOT_WORK_NODE_SIZE = 4, /* max far blocks per ACA batch, default 5000 */
+  HIGNN_P_MAX_FAR_DOT_WORK_NODE_SIZE = 4, /* stored; batches are sized by pool memory    */
   HIGNN_P_MAX_RELATIVE_COORD = 5,         /* far-size gate of the close/far check, 500000 */
   HIGNN_P_POST_CHECK_FLAG = 6,            /* dense re-check after each dot, default 0   */
   HIGNN_P_USE_SYMMETRY = 7,               /* J >= I lists + transposed update, default 1 */
   HIGNN_P_MAX_FAR_FIELD_DISTANCE = 8,     /* stored, unused (as in the reference)       */
   /* keys of this implementation */
   HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field */
-  HIGNN_P_FAR_BATCH_ROWS = 101,  /* rows (sum of |I|+|J|) per ACA batch, default 1<<21       */
+  HIGNN_P_FAR_BATCH_ROWS = 101,  /* max rows (sum of |I|+|J|) per ACA batch, default 1<<26   */
   HIGNN_P_TIMING = 102,          /* 1 = record per-phase CUDA-event times in hignn_stats     */
-  HIGNN_P_STUDENT_TOL = 103,     /* sampled-residual fallback threshold of the student, 1e-3 */
+  HIGNN_P_STUDENT_TOL = 103,     /* student fallback: a far block whose 64 sampled entries differ from
+                                    the teacher by more than max(this, epsilon) relative (Frobenius)
+                                    is recomputed with the teacher; default 1e-3                   */
   HIGNN_P_FIELDS = 104,          /* bit 0 = near field, bit 1 = far field (default 3), for diagnostics */
-  HIGNN_P_RECORD_PIVOTS = 105    /* 1 = keep every far block's ACA rank and pivots (hignn_get_far_pivots) */
+  HIGNN_P_RECORD_PIVOTS = 105,   /* 1 = keep every far block's ACA rank and pivots (hignn_get_far_pivots) */
+  HIGNN_P_FAR_POOL_MB = 106,     /* C + Q pool memory of one ACA batch in MiB, default 24576   */
+  HIGNN_P_RANK_HINT_OFFSET = 107 /* added to the recorded ACA ranks when planning (default 0; a
+                                    negative value exercises the deferral path in tests)        */
 };
 
 typedef struct hignn_stats {
@@ -176,6 +181,18 @@ int hignn_get_tree(hignn_model* m, int64_t* tree5, int64_t* perm);
 /* Close leaf pairs and far node pairs in the reference's list order
  * (src/CloseFarCheck.cpp:298-408). Arrays sized from hignn_get_stats. */
 int hignn_get_lists(hignn_model* m, int64_t* close_i, int64_t* close_j, int64_t* far_i, int64_t* far_j);
+
+/* Shard of the block lists for one of `world` processes (one GPU each), no counterpart
+ * of its own in the reference: there MPI ranks take interleaved shares of the close and far
+ * lists (src/CloseFarCheck.cpp:309,323,394,401) and all-reduce u (src/HignnModel.cpp:602).
+ * Here each rank takes a contiguous, cost-balanced range of each list; hignn_dot and
+ * hignn_dot_device then return this rank's partial velocities, which the caller sums over
+ * the ranks (an NCCL all-reduce of the (n, 3) float32 result). rank = 0, world = 1 (the
+ * default) is the whole product. */
+int hignn_set_shard(hignn_model* m, int rank, int world);
+
+/* The shard's ranges: ranges[4] = {close begin, close end, far begin, far end} in list order. */
+int hignn_get_shard(hignn_model* m, int64_t* ranges);
 
 /* ACA ranks and pivot sequences of the last far field (needs HIGNN_P_RECORD_PIVOTS = 1):
  * ranks[num_far]; rows / cols [num_far][ld] with ld >= max_iter + 1, block-local indices
