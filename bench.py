@@ -1,16 +1,21 @@
 #!/usr/bin/env python
-"""H-matvec benchmark: particles/s of U = M(x) F at N = 1,048,576 on one B200 per rank.
+"""H-matvec benchmark: particles/s of U = M(x) F at N = 1,048,576 on B200s.
 
 Workload (seeded, synthetic; no dataset): 1,048,576 unit spheres in a cube at
 volume fraction 0.10, 64 Gaussian clusters (sigma 8 radii) + 50% uniform
 background (seed 2), forces (0,0,-1) + N(0, 0.1^2); leaf size 128, ACA
 tolerance 1e-2 (the reference's production value, python/simulate.py:198),
 max_iter 100, tree prebuilt (its host build time is reported apart). One step =
-one H-matvec (near field + ACA far field). Each rank runs an independent replica
-(weak scaling); `value` is the sum of particles/s over ranks, timed on the device
-(max over ranks). The plain FP32 form is timed once in the same run for the
-mixed-vs-plain ratio of the metric; both forms are checked against the dense
-product on sampled target rows.
+one H-matvec (near field + ACA far field). The headline form is BF16 tensor
+cores + rank-planned ACA batches + the far-field student network (trained on
+the device before timing; its training time is reported apart); the plain FP32
+form is timed in the same run for the mixed-vs-plain ratio of the metric, and
+both are checked against the dense product on sampled target rows.
+
+With N GPUs (torchrun, one rank per GPU) every rank builds the same tree and
+computes a cost-balanced shard of the close and far block lists; the partial
+velocities are summed by one NCCL all-reduce per step, inside the timed region
+(strong scaling: the same N=1M product on every GPU count).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision P]
     python bench.py --impl reference ...   # the reference algorithm on the host cores
@@ -33,6 +38,7 @@ sys.path.insert(0, REPO)
 WEIGHTS = os.path.join(REPO, "hignn_b200", "data", "two_body_unbounded.hgnw")
 METRIC = "H-matvec particles/s at N=1M: mixed+batched+student vs plain FP32, err≤1e-3"
 FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)  # 141,056
+TANH_PER_EVAL = 128 + 512
 PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor_cores", 2: "bf16_tensor_cores+student_far_field"}
 PREC_DTYPE = {0: "fp32", 1: "bf16", 2: "bf16"}
 WORKLOAD = ("N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, seed 2, "
@@ -45,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hignn_b200", choices=["hignn_b200", "reference"])
-    ap.add_argument("--precision", type=int, default=1, choices=[0, 1, 2])
+    ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2])
+    ap.add_argument("--student-steps", type=int, default=20000)
+    ap.add_argument("--student-batch", type=int, default=65536)
+    ap.add_argument("--student-samples", type=int, default=10_000_000)
     ap.add_argument("--n", type=int, default=1048576)
     ap.add_argument("--epsilon", type=float, default=1e-2)
     ap.add_argument("--check-rows", type=int, default=2048, help="dense target rows for the error check")
@@ -249,15 +258,46 @@ def main():
     m.load_two_body(WEIGHTS)
     m.set(capi.P_EPSILON, args.epsilon)
     m.set(capi.P_MAX_ITER, 100)
-    m.set(capi.P_PRECISION, args.precision)
     m.set(capi.P_TIMING, 1)
+    if world > 1:
+        m.set_shard(rank, world)
     st0 = m.stats()  # builds the tree and lists
+    student = None
+    if args.precision == 2:  # the far-field student network, trained on the device from teacher samples
+        t0 = time.time()
+        loss = m.train_student(steps=args.student_steps, batch=args.student_batch, nsamples=args.student_samples,
+                               lr=1e-3, seed=3)
+        student = {"steps": args.student_steps, "batch": args.student_batch, "teacher_samples": args.student_samples,
+                   "final_mse": loss, "train_seconds": time.time() - t0}
+    m.set(capi.P_PRECISION, args.precision)
     f_d = torch.from_numpy(f).cuda()
     u_d = torch.empty_like(f_d)
     stream = torch.cuda.ExternalStream(m.stream())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step_device(out):
+        m.dot_device(out.data_ptr(), f_d.data_ptr())
+        if dist:  # partial velocities of this rank's shard -> the whole product on every rank
+            with torch.cuda.stream(stream):
+                dist.all_reduce(out)
+
+    f_h = torch.from_numpy(f).pin_memory()
+    u_h = torch.empty_like(f_h).pin_memory()
+    fe_d = torch.empty_like(f_d)
+
+    def step_e2e():
+        if not dist:
+            m.dot_ptr(u_h.data_ptr(), f_h.data_ptr())  # the C ABI's host-pointer call (H2D, matvec, D2H)
+            return
+        with torch.cuda.stream(stream):  # the model's stream: copies, matvec and all-reduce in order
+            fe_d.copy_(f_h, non_blocking=True)
+        m.dot_device(u_d.data_ptr(), fe_d.data_ptr())
+        with torch.cuda.stream(stream):
+            dist.all_reduce(u_d)
+            u_h.copy_(u_d, non_blocking=True)
+
     for _ in range(args.warmup):
-        m.dot_device(u_d.data_ptr(), f_d.data_ptr())
+        step_device(u_d)
     props = torch.cuda.get_device_properties(local)
     bus = None
     try:
@@ -268,24 +308,22 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(bus)
-    times, near_ms, far_ms = timed(m, stream, flush, args.steps,
-                                   lambda: m.dot_device(u_d.data_ptr(), f_d.data_ptr()))
+    times, near_ms, far_ms = timed(m, stream, flush, args.steps, lambda: step_device(u_d))
     torch.cuda.synchronize()
     ck = clocks.stop()
     if dist:
         dist.barrier()
     st = m.stats()
     ms = max_over_ranks(float(np.mean(times)))
-    value = world * n / (ms / 1e3)
+    value = n / (ms / 1e3)
 
     # end to end through the public C ABI from pinned host memory (H2D + matvec + D2H per step)
-    f_h = torch.from_numpy(f).pin_memory()
-    u_h = torch.empty_like(f_h).pin_memory()
     if args.no_e2e:
         u_h.copy_(u_d.cpu())
         e2e_ms = float("nan")
     else:
-        e2e_times, _, _ = timed(m, stream, flush, args.steps, lambda: m.dot_ptr(u_h.data_ptr(), f_h.data_ptr()))
+        e2e_times, _, _ = timed(m, stream, flush, args.steps, step_e2e)
+        torch.cuda.synchronize()
         e2e_ms = max_over_ranks(float(np.mean(e2e_times)))
     u = u_h.numpy().astype(np.float64)
 
@@ -294,7 +332,7 @@ def main():
     rows = np.sort(rng.choice(n, size=min(args.check_rows, n), replace=False))
     err = err_plain = None
     t0 = time.time()
-    ud = m.dense_rows(f, rows, 0) if len(rows) else None
+    ud = m.dense_rows(f, rows, 0) if len(rows) and rank == 0 else None
     t_check = time.time() - t0
     if ud is not None:
         err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
@@ -303,44 +341,58 @@ def main():
     if args.precision != 0 and not args.no_plain:
         m.set(capi.P_PRECISION, 0)
         up_d = torch.empty_like(f_d)
-        pt, pn, pf = timed(m, stream, flush, 1, lambda: m.dot_device(up_d.data_ptr(), f_d.data_ptr()))
+        step_device(up_d)  # warm-up: records the plain form's ACA ranks for its plan
+        pt, pn, pf = timed(m, stream, flush, 1, lambda: step_device(up_d))
         m.set(capi.P_PRECISION, args.precision)
         pms = max_over_ranks(float(np.mean(pt)))
         up = up_d.cpu().numpy().astype(np.float64)
         if ud is not None:
             err_plain = float(np.linalg.norm(up[rows] - ud) / np.linalg.norm(ud))
-        plain = {"form": "plain_fp32", "ms_per_step": pms, "value": world * n / (pms / 1e3),
+        plain = {"form": "plain_fp32", "ms_per_step": pms, "value": n / (pms / 1e3),
                  "near_ms": float(pn[0]), "far_ms": float(pf[0]), "rel_l2_vs_dense": err_plain,
-                 "steps": 1, "speedup_of_headline": (world * n / (ms / 1e3)) / (world * n / (pms / 1e3))}
+                 "steps": 1, "warmup": 1, "speedup_of_headline": pms / ms}
 
     hbm, bf16, src = peaks()
     near_s = float(np.mean(near_ms)) / 1e3
     achieved = st["close_evals"] * FLOP_PER_EVAL / near_s / 1e12
+    # the MUFU roofline of the same kernel: 640 tanh per evaluation at 16 tanh per clock per SM
+    # (tanh.approx.bf16x2 issues at half the rate of tanh.approx.f32; measured on this B200)
+    sm_mhz = ck.get("sm_mhz") or 1965.0  # clocks.max.sm of this B200 when nvidia-smi gave nothing
+    mufu_peak = props.multi_processor_count * 16 * sm_mhz * 1e6 / TANH_PER_EVAL
+    near_eps = st["close_evals"] / near_s
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None, "dtype": PREC_DTYPE[args.precision], "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "epsilon": args.epsilon, "max_iter": 100,
                    "form": PREC_NAME[args.precision],
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "256 MiB buffer written between timed steps"},
-        "roofline": {"bound": "tensor", "kernel": "near field (features + two-body network + contraction)",
+                   "parallelism": f"list shards x{world} + NCCL all-reduce of u" if world > 1 else "single GPU",
+                   "l2": "256 MiB buffer written between timed steps",
+                   "aca_plan": "ranks recorded by the warm-up H-matvec on the same tree"},
+        "roofline": {"bound": "tensor", "kernel": "k_near_tc (features + two-body network + contraction)",
                      "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
                      "peak_source": f"bf16_tflops of {src} MEASURED_PEAKS.json",
                      "traffic": None,
-                     "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals / near-field time"},
-        "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": 12 * n,
+                     "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals / near-field time",
+                     "mufu": {"achieved_evals_per_s": near_eps, "peak_evals_per_s": mufu_peak,
+                              "frac": near_eps / mufu_peak,
+                              "peak_source": f"16 tanh/clk/SM x {props.multi_processor_count} SMs x {sm_mhz:.0f} MHz "
+                                             f"/ {TANH_PER_EVAL} tanh per evaluation"}},
+        "e2e": {"value": n / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 12 * n, "ms_per_step": e2e_ms},
         "gpu_launches": int(st["gpu_launches"]),
         "clocks": ck,
         "error": {"rel_l2_vs_dense": err, "rows": int(len(rows)), "seconds": t_check,
                   "oracle": "dense rows on the device, FP32 network, FP64 accumulation over all N sources"},
         "plain_fp32": plain,
+        "student": student,
         "breakdown_ms": {"near": float(np.mean(near_ms)), "far": float(np.mean(far_ms)),
                          "build_host": st0["t_build_ms"]},
         "work": {"close_pairs": st["num_close"], "far_pairs": st["num_far"], "close_evals": st["close_evals"],
                  "far_evals": st["far_evals"], "far_rank_mean": st["far_rank_sum"] / max(1, st["num_far"]),
-                 "far_rank_max": st["far_rank_max"]},
+                 "far_rank_max": st["far_rank_max"], "far_iterations": st["far_iterations"],
+                 "student_fallback_blocks": st["student_fallback_blocks"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds, st["close_evals"],

@@ -317,8 +317,8 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
     const auto& J = m->tree.nodes[m->lists.farJ[q]];
     const int32_t nI = (int32_t)(I.end - I.start), nJ = (int32_t)(J.end - J.start);
     const int cnt = (int)p - b0;
-    const int64_t add = (int64_t)kcap[p] * (nI + nJ) * 9 * (int64_t)sizeof(double);
-    if (cnt > 0 && ((cE + qE) * 9 * (int64_t)sizeof(double) + add > m->far_pool_bytes ||
+    const int64_t add = (int64_t)kcap[p] * (nI + nJ) * 9 * (int64_t)sizeof(hignn::pool_t);
+    if (cnt > 0 && ((cE + qE) * 9 * (int64_t)sizeof(hignn::pool_t) + add > m->far_pool_bytes ||
                     rows + nI + nJ > m->far_batch_rows)) {
       batches.push_back({b0, (int)p, known ? iters : 0});
       maxNb = std::max(maxNb, cnt);
@@ -361,8 +361,8 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
     m->far_cols.ensure(sizeof(int32_t) * (size_t)maxNb * ldr);
     m->far_used_row.ensure((size_t)maxR + 16);
     m->far_used_col.ensure((size_t)maxCol + 16);
-    m->far_C.ensure(sizeof(double) * 9 * (size_t)maxC);
-    m->far_Q.ensure(sizeof(double) * 9 * (size_t)maxQ);
+    m->far_C.ensure(sizeof(hignn::pool_t) * 9 * (size_t)maxC);
+    m->far_Q.ensure(sizeof(hignn::pool_t) * 9 * (size_t)maxQ);
     m->far_act.ensure(sizeof(int32_t) * (maxNb + 1));
     m->far_preI.ensure(sizeof(int32_t) * (maxNb + 1));
     m->far_preJ.ensure(sizeof(int32_t) * (maxNb + 1));
@@ -552,8 +552,8 @@ FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& p
     a.ldr = m->max_iter + 1;
     a.usedRow = m->far_used_row.as<uint8_t>();
     a.usedCol = m->far_used_col.as<uint8_t>();
-    a.C = m->far_C.as<double>();
-    a.Q = m->far_Q.as<double>();
+    a.C = m->far_C.as<hignn::pool_t>();
+    a.Q = m->far_Q.as<hignn::pool_t>();
     a.act = m->far_act.as<int32_t>();
     a.preI = m->far_preI.as<int32_t>();
     a.preJ = m->far_preJ.as<int32_t>();

@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF3
       const int b = s.blk[t], loc = s.loc[t];
       const FarBlock bk = a.blocks[b];
       const int k = a.state[b].k;
-      double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
+      pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                                : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
       const float* y = s.mlp.y[t];
       // src/FarDot.cpp:445-456: diagonal copied, off-diagonal 0.5 * (float sum)
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
   __syncthreads();
   double best = -DBL_MAX;
   int bi = -1;
-  double* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
+  pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
     double c[9];
 #pragma unroll
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
     if (k > 0) {
       double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int l = 0; l < k; l++) {
-        const double* cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+        const pool_t* cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
         const double* ql = qj + 9 * l;
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -280,9 +280,9 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
             for (int m = 0; m < 3; m++) s[3 * r + cc] += cl[3 * r + m] * ql[3 * m + cc];
       }
 #pragma unroll
-      for (int q = 0; q < 9; q++) {
-        c[q] -= s[q];
-        Ck[9 * i + q] = c[q];
+      for (int q = 0; q < 9; q++) {  // stored rounded; the pivot search sees the stored value
+        c[q] = (double)(pool_t)(c[q] - s[q]);
+        Ck[9 * i + q] = (pool_t)c[q];
       }
     }
     const double d = det3(c);
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
   if (threadIdx.x == 0) {
     a.rows[(size_t)b * a.ldr + k] = bi;
     a.usedRow[bk.rOff + bi] = 1;
-    const double* m = Ck + 9 * bi;
+    const pool_t* m = Ck + 9 * bi;
     const double A = m[0], B = m[1], C = m[2], D = m[3], E = m[4], F = m[5], G = m[6], H = m[7], I = m[8];
     const double det = A * (E * I - F * H) - B * (D * I - F * G) + C * (D * H - E * G);
     inv[0] = (E * I - F * H) / det;
@@ -342,12 +342,12 @@ __global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
 __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, double* mid, double* mid2) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int l = wid; l < rank; l += blockDim.x >> 5) {
-    const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
-    const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
+    const pool_t* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
+    const pool_t* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
     double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
     for (int j = lane; j < bk.nJ; j += 32) {
       const float4 fj = a.f[bk.sJ + j];
-      const double* q = Ql + 9 * j;
+      const pool_t* q = Ql + 9 * j;
 #pragma unroll
       for (int r = 0; r < 3; r++)
         m[r] += q[3 * r] * (double)fj.x + q[3 * r + 1] * (double)fj.y + q[3 * r + 2] * (double)fj.z;
@@ -355,7 +355,7 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
     if (a.use_symmetry)
       for (int i = lane; i < bk.nI; i += 32) {
         const float4 fi = a.f[bk.sI + i];
-        const double* c = Cl + 9 * i;
+        const pool_t* c = Cl + 9 * i;
 #pragma unroll
         for (int r = 0; r < 3; r++)
           m2[r] += c[r] * (double)fi.x + c[3 + r] * (double)fi.y + c[6 + r] * (double)fi.z;
@@ -377,7 +377,7 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
     double acc[3] = {0, 0, 0};
     for (int l = 0; l < rank; l++) {
-      const double* c = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+      const pool_t* c = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
 #pragma unroll
       for (int r = 0; r < 3; r++)
         acc[r] += c[3 * r] * mid[3 * l] + c[3 * r + 1] * mid[3 * l + 1] + c[3 * r + 2] * mid[3 * l + 2];
@@ -389,7 +389,7 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
     for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
       double acc[3] = {0, 0, 0};
       for (int l = 0; l < rank; l++) {
-        const double* q = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+        const pool_t* q = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
 #pragma unroll
         for (int r = 0; r < 3; r++)
           acc[r] += q[r] * mid2[3 * l] + q[3 + r] * mid2[3 * l + 1] + q[6 + r] * mid2[3 * l + 2];
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
   __syncthreads();
   double best = -DBL_MAX;
   int bj = -1;
-  double* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
+  pool_t* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
   for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
     double q[9];
 #pragma unroll
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
     if (k > 0) {
       double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int l = 0; l < k; l++) {
-        const double* ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+        const pool_t* ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
         const double* cl = ci + 9 * l;
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -441,9 +441,9 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
             for (int m = 0; m < 3; m++) s[3 * r + cc] += cl[3 * r + m] * ql[3 * m + cc];
       }
 #pragma unroll
-      for (int e = 0; e < 9; e++) {
-        q[e] -= s[e];
-        Qk[9 * j + e] = q[e];
+      for (int e = 0; e < 9; e++) {  // stored rounded; the pivot search sees the stored value
+        q[e] = (double)(pool_t)(q[e] - s[e]);
+        Qk[9 * j + e] = (pool_t)q[e];
       }
     }
     const double d = det3(q);
@@ -454,10 +454,12 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
   }
   block_argmax(best, bj, sv, si);  // contains __syncthreads: Q_k writes are visible below
   // nu2 = ||C_k Q_k||_F^2 from column norms/dots of C_k and row norms/dots of Q_k
-  const double* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
+  const pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
   double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
-    const double* c = Ck + 9 * i;
+    double c[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) c[e] = Ck[9 * i + e];
 #pragma unroll
     for (int cc = 0; cc < 3; cc++) {
       v[cc] += c[cc] * c[cc] + c[cc + 3] * c[cc + 3] + c[cc + 6] * c[cc + 6];
@@ -466,7 +468,9 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
     }
   }
   for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
-    const double* q = Qk + 9 * j;
+    double q[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) q[e] = Qk[9 * j + e];
     v[6] += q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
     v[7] += q[3] * q[3] + q[4] * q[4] + q[5] * q[5];
     v[8] += q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
@@ -485,11 +489,15 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
       double acc[18];
 #pragma unroll
       for (int q = 0; q < 18; q++) acc[q] = 0.0;
-      const double* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
-      const double* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
+      const pool_t* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
+      const pool_t* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
       for (int i = lane; i < bk.nI; i += 32) {
-        const double* c = Ck + 9 * i;
-        const double* d = Cl + 9 * i;
+        double c[9], d[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+          c[e] = Ck[9 * i + e];
+          d[e] = Cl[9 * i + e];
+        }
 #pragma unroll
         for (int d1 = 0; d1 < 3; d1++)
 #pragma unroll
@@ -497,8 +505,12 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
             acc[3 * d1 + d2] += c[d1] * d[d2] + c[d1 + 3] * d[d2 + 3] + c[d1 + 6] * d[d2 + 6];
       }
       for (int j = lane; j < bk.nJ; j += 32) {
-        const double* q = Qk + 9 * j;
-        const double* p = Ql + 9 * j;
+        double q[9], p[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+          q[e] = Qk[9 * j + e];
+          p[e] = Ql[9 * j + e];
+        }
 #pragma unroll
         for (int d1 = 0; d1 < 3; d1++)
 #pragma unroll

@@ -11,6 +11,13 @@ namespace hignn {
 
 constexpr int kMaxIterCap = 512;  // largest ACA iteration cap (set_max_iter) the kernels accept
 
+// Storage type of the ACA factors C_l, Q_l (9 entries per particle and term). The reference keeps
+// them in FP64 (src/FarDot.cpp:104-107); here they are stored in FP32 and every operation on them
+// (orthogonalisation, pivot determinants and inverses, the stopping norms, the apply) is carried
+// out in FP64: the factors are the bulk of the far field's memory traffic, and their FP32 rounding
+// (1e-7 relative) is far below the ACA tolerance.
+using pool_t = float;
+
 // ---------------------------------------------------------------- near field / dense
 struct NearArgs {
   const PairWork* work;
@@ -54,8 +61,8 @@ struct FarArgs {
   int ldr;            // max_iter + 1
   uint8_t* usedRow;
   uint8_t* usedCol;
-  double* C;          // [entries][9]
-  double* Q;
+  pool_t* C;          // [entries][9]
+  pool_t* Q;
   int32_t* act;       // active block list
   int32_t* preI;      // exclusive prefix of nI over active blocks (nact + 1)
   int32_t* preJ;

@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) k_far_student(FarArgs a, const float* 
     }
     float M[9];
     student_forward(p, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, M);
-    double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
+    pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                              : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
 #pragma unroll
     for (int r = 0; r < 3; r++)

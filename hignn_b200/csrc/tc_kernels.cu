@@ -1,14 +1,15 @@
 // Tensor-core (tcgen05) forms of the near field, the ACA queries and the stand-alone evaluation.
 //
-// All three kernels are persistent (one CTA per SM, up to ~213 KB shared
-// memory, 512 TMEM columns) and share the tile engine of tc_mlp.cuh. Each CTA
-// runs two independent epilogue groups (tile contexts); every group walks its
-// own share of the work:
-//   k_near_tc : close pairs (I, J) fetched from a global counter, flattened into
-//               128-evaluation tiles; the contraction u_I += M f_J (and u_J +=
-//               M f_I for J > I) is reduced per particle in shared memory and
-//               flushed with one FP64 atomic per particle and component per pair
-//               (src/CloseDot.cpp:245-299).
+// All three kernels are persistent (one CTA per SM, up to ~227 KB shared
+// memory, 512 TMEM columns) and drive the tile engine of tc_mlp.cuh with a
+// stream of 128-evaluation tiles; the epilogue threads compute the features of
+// the next tile before the engine retires the current one:
+//   k_near_tc : close pairs (I, J) fetched from a global counter, staged in
+//               shared memory (two buffers: the pair being retired and the next)
+//               and flattened into tiles; the contraction u_I += M f_J (and
+//               u_J += M f_I for J > I) is reduced per particle in shared memory
+//               and flushed with one FP64 atomic per particle and component per
+//               pair (src/CloseDot.cpp:245-299).
 //   k_far_tc  : column / row queries of all active ACA blocks, symmetrised into
 //               the FP64 C / Q pools (src/FarDot.cpp:348-458, 672-781).
 //   k_eval_tc : M(r) for an array of features.
@@ -28,12 +29,12 @@ __device__ __forceinline__ uint8_t* align1k(uint8_t* p) {
 struct NearStage {
   float4 xI[kMaxLeaf], xJ[kMaxLeaf], fI[kMaxLeaf], fJ[kMaxLeaf];
   float uI[kMaxLeaf][3], uJ[kMaxLeaf][3];
-  int item;
 };
 
 struct NearTcSmem {
   tc::Smem tcs;
   NearStage st[2];
+  int item[2];
 };
 static_assert(sizeof(NearTcSmem) + 1024 <= 232448, "near-field shared memory exceeds 227 KB per CTA");
 
@@ -67,6 +68,58 @@ __device__ __forceinline__ void add_segmented(float (*uI)[3], int i, float v0, f
   }
 }
 
+// Position of one 128-evaluation tile in the near-field stream.
+struct NearCursor {
+  int buf, item, t0;
+  PairWork pw;
+};
+
+// Next close pair from the global counter, staged into buffer b (all epilogue threads).
+__device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int* counter, int b, NearCursor& c) {
+  const int e = threadIdx.x;
+  if (e == 0) S.item[b] = atomicAdd(counter, 1);
+  tc::epi_bar();  // also: every thread is done with the pair last staged in buffer b
+  const int item = S.item[b];
+  if (item >= a.nwork) return false;
+  const PairWork pw = a.work[item];
+  NearStage& G = S.st[b];
+  for (int i = e; i < pw.nI; i += tc::kEpiThreads) {
+    G.xI[i] = a.xI[pw.sI + i];
+    G.fI[i] = a.fI[pw.sI + i];
+    G.uI[i][0] = G.uI[i][1] = G.uI[i][2] = 0.f;
+  }
+  for (int j = e; j < pw.nJ; j += tc::kEpiThreads) {
+    G.xJ[j] = a.xJ[pw.sJ + j];
+    G.fJ[j] = a.fJ[pw.sJ + j];
+    G.uJ[j][0] = G.uJ[j][1] = G.uJ[j][2] = 0.f;
+  }
+  tc::epi_bar();
+  c.buf = b;
+  c.item = item;
+  c.t0 = 0;
+  c.pw = pw;
+  return true;
+}
+
+// This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
+__device__ __forceinline__ bool near_row(const NearTcSmem& S, const NearCursor& c, int row, int& i, int& j,
+                                         float (&r)[3]) {
+  const int total = c.pw.nI * c.pw.nJ;
+  const int flat = c.t0 + row;
+  const bool valid = flat < total;
+  i = valid ? flat / c.pw.nJ : 0;
+  j = valid ? flat - i * c.pw.nJ : 0;
+  r[0] = 1.f;
+  r[1] = r[2] = 0.f;
+  if (valid) {
+    const float4 xi = S.st[c.buf].xI[i], xj = S.st[c.buf].xJ[j];
+    r[0] = xj.x - xi.x;
+    r[1] = xj.y - xi.y;
+    r[2] = xj.z - xi.z;
+  }
+  return valid;
+}
+
 __global__ void __launch_bounds__(tc::kThreads, 1)
     k_near_tc(NearArgs a, TcWeights w, int* work_counter, int* err) {
   extern __shared__ uint8_t smem_raw[];
@@ -77,79 +130,68 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    NearStage& G = S.st[tc::epi_group()];
-    const int e = tc::epi_gthread();  // staging / flush index within the group
-    const int row = tc::epi_row(), h = tc::epi_half();
-    tc::EpiState st;
-    bool ok = true;
-    for (;;) {
-      if (e == 0) G.item = atomicAdd(work_counter, 1);
-      tc::epi_bar();
-      const int item = G.item;
-      if (item >= a.nwork) break;
-      const PairWork pw = a.work[item];
-      const bool trans = (pw.flags & kPairTransposed) != 0;
-      const bool symm = (pw.flags & kPairSymmetrize) != 0;
-      for (int i = e; i < pw.nI; i += tc::kGroupThreads) {
-        G.xI[i] = a.xI[pw.sI + i];
-        G.fI[i] = a.fI[pw.sI + i];
-        G.uI[i][0] = G.uI[i][1] = G.uI[i][2] = 0.f;
-      }
-      for (int j = e; j < pw.nJ; j += tc::kGroupThreads) {
-        G.xJ[j] = a.xJ[pw.sJ + j];
-        G.fJ[j] = a.fJ[pw.sJ + j];
-        G.uJ[j][0] = G.uJ[j][1] = G.uJ[j][2] = 0.f;
-      }
-      tc::epi_bar();
-      const int total = pw.nI * pw.nJ;
-      for (int t0 = 0; t0 < total; t0 += tc::kTile) {
-        const int flat = t0 + row;
-        const bool valid = flat < total;
-        const int i = valid ? flat / pw.nJ : 0;
-        const int j = valid ? flat - i * pw.nJ : 0;
-        float rx = 1.f, ry = 0.f, rz = 0.f;
-        if (valid) {
-          const float4 xi = G.xI[i], xj = G.xJ[j];
-          rx = xj.x - xi.x;
-          ry = xj.y - xi.y;
-          rz = xj.z - xi.z;
-        }
-        float M[9];
-        ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
-        if (!ok) break;
-        if (valid) {
-          if (symm) {
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-              for (int c = r + 1; c < 3; c++) {
-                const float v = 0.5f * (M[3 * r + c] + M[3 * c + r]);
-                M[3 * r + c] = v;
-                M[3 * c + r] = v;
-              }
-          }
-          if (h == 0) {  // u_I[i] += M f_J[j]
-            const float4 fj = G.fJ[j];
-            add_segmented(G.uI, i, M[0] * fj.x + M[1] * fj.y + M[2] * fj.z, M[3] * fj.x + M[4] * fj.y + M[5] * fj.z,
-                          M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
-          } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
-            const float4 fi = G.fI[i];
-            atomicAdd(&G.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
-            atomicAdd(&G.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
-            atomicAdd(&G.uJ[j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
-          }
-        }
-      }
+    const int e = threadIdx.x, row = tc::epi_row(), p = tc::epi_part();
+    tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
+    NearCursor cur;
+    bool have = near_fetch(S, a, work_counter, 0, cur);
+    int i = 0, j = 0;
+    float r[3];
+    bool valid = have && near_row(S, cur, row, i, j, r);
+    eng.start(have, r[0], r[1], r[2]);
+    while (have) {
+      // the next tile: the rest of this pair, or the next pair staged into the other buffer
+      NearCursor nxt = cur;
+      nxt.t0 += tc::kTile;
+      const bool last = nxt.t0 >= cur.pw.nI * cur.pw.nJ;
+      bool has_next = true;
+      if (last) has_next = near_fetch(S, a, work_counter, cur.buf ^ 1, nxt);
+      int ni = 0, nj = 0;
+      float nr[3] = {1.f, 0.f, 0.f};
+      const bool nvalid = has_next && near_row(S, nxt, row, ni, nj, nr);
+      float M[9];
+      const bool ok = tc::epi_all(eng.step(has_next, nr[0], nr[1], nr[2], r[0], r[1], r[2], M));
       if (!ok) break;
-      tc::epi_bar();
-      for (int q = e; q < 3 * pw.nI; q += tc::kGroupThreads)
-        atomicAdd(&a.uI[3 * (size_t)pw.sI + q], (double)(&G.uI[0][0])[q]);
-      if (trans)
-        for (int q = e; q < 3 * pw.nJ; q += tc::kGroupThreads)
-          atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&G.uJ[0][0])[q]);
-      tc::epi_bar();
+      NearStage& G = S.st[cur.buf];
+      const bool trans = (cur.pw.flags & kPairTransposed) != 0;
+      if (valid && p < 2) {
+        if (cur.pw.flags & kPairSymmetrize) {
+#pragma unroll
+          for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int c = q + 1; c < 3; c++) {
+              const float v = 0.5f * (M[3 * q + c] + M[3 * c + q]);
+              M[3 * q + c] = v;
+              M[3 * c + q] = v;
+            }
+        }
+        if (p == 0) {  // u_I[i] += M f_J[j]
+          const float4 fj = G.fJ[j];
+          add_segmented(G.uI, i, M[0] * fj.x + M[1] * fj.y + M[2] * fj.z, M[3] * fj.x + M[4] * fj.y + M[5] * fj.z,
+                        M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
+        } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
+          const float4 fi = G.fI[i];
+          atomicAdd(&G.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
+          atomicAdd(&G.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
+          atomicAdd(&G.uJ[j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
+        }
+      }
+      if (last) {  // the pair is complete: flush its velocities
+        tc::epi_bar();
+        for (int q = e; q < 3 * cur.pw.nI; q += tc::kEpiThreads)
+          atomicAdd(&a.uI[3 * (size_t)cur.pw.sI + q], (double)(&G.uI[0][0])[q]);
+        if (trans)
+          for (int q = e; q < 3 * cur.pw.nJ; q += tc::kEpiThreads)
+            atomicAdd(&a.uJ[3 * (size_t)cur.pw.sJ + q], (double)(&G.uJ[0][0])[q]);
+      }
+      if (!has_next) break;
+      cur = nxt;
+      i = ni;
+      j = nj;
+      valid = nvalid;
+      r[0] = nr[0];
+      r[1] = nr[1];
+      r[2] = nr[2];
     }
-    if (ok) tc::epi_finish(S.tcs);
   }
   tc::cta_teardown(S.tcs);
 }
@@ -158,68 +200,87 @@ struct FarTcSmem {
   tc::Smem tcs;
 };
 
+// This thread's row of far tile `tile`: block b, local index loc, term k, feature r.
+__device__ __forceinline__ bool far_row(const FarArgs& a, int which, int nact, int tot, int tile, int row, int& b,
+                                        int& loc, int& k, float (&r)[3]) {
+  const int g = tile * tc::kTile + row;
+  r[0] = 1.f;
+  r[1] = r[2] = 0.f;
+  if (g >= tot) return false;
+  const int32_t* pre = which ? a.preJ : a.preI;
+  int lo = 0, hi = nact;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  b = a.act[lo];
+  loc = g - pre[lo];
+  const FarBlock bk = a.blocks[b];
+  k = a.state[b].k;
+  float4 xi, xj;
+  if (which == 0) {
+    xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
+    xi = a.x[bk.sI + loc];
+  } else {
+    xj = a.x[bk.sJ + loc];
+    xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
+  }
+  r[0] = xj.x - xi.x;
+  r[1] = xj.y - xi.y;
+  r[2] = xj.z - xi.z;
+  return true;
+}
+
 __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
   extern __shared__ uint8_t smem_raw[];
   FarTcSmem& S = *reinterpret_cast<FarTcSmem*>(align1k(smem_raw));
   const int nact = a.ctr[kCtrActive];
   const int tot = which ? a.ctr[kCtrTotJ] : a.ctr[kCtrTotI];
-  if (2 * (int)blockIdx.x * tc::kTile >= tot) return;  // uniform: before any setup
+  if ((int)blockIdx.x * tc::kTile >= tot) return;  // uniform: before any setup
   tc::cta_setup(S.tcs, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == tc::kMmaWarp) {
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_half();
-    const int32_t* pre = which ? a.preJ : a.preI;
-    tc::EpiState st;
-    bool ok = true;
-    for (int tile = 2 * blockIdx.x + tc::epi_group(); tile * tc::kTile < tot; tile += 2 * gridDim.x) {
-      const int g = tile * tc::kTile + row;
-      const bool valid = g < tot;
-      float rx = 1.f, ry = 0.f, rz = 0.f;
-      int b = 0, loc = 0, k = 0;
-      if (valid) {
-        int lo = 0, hi = nact;
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (pre[mid] <= g)
-            lo = mid;
-          else
-            hi = mid;
-        }
-        b = a.act[lo];
-        loc = g - pre[lo];
-        const FarBlock bk = a.blocks[b];
-        k = a.state[b].k;
-        float4 xi, xj;
-        if (which == 0) {
-          xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
-          xi = a.x[bk.sI + loc];
-        } else {
-          xj = a.x[bk.sJ + loc];
-          xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
-        }
-        rx = xj.x - xi.x;
-        ry = xj.y - xi.y;
-        rz = xj.z - xi.z;
-      }
+    const int row = tc::epi_row(), p = tc::epi_part();
+    tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
+    int tile = blockIdx.x, b = 0, loc = 0, k = 0;
+    float r[3];
+    bool valid = far_row(a, which, nact, tot, tile, row, b, loc, k, r);
+    eng.start(true, r[0], r[1], r[2]);
+    for (;;) {
+      const int nt = tile + gridDim.x;
+      const bool has_next = nt * tc::kTile < tot;
+      int nb = 0, nloc = 0, nk = 0;
+      float nr[3] = {1.f, 0.f, 0.f};
+      const bool nvalid = has_next && far_row(a, which, nact, tot, nt, row, nb, nloc, nk, nr);
       float M[9];
-      ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
-      if (!ok) break;
-      if (valid) {  // the two threads of a row store alternate entries
+      if (!tc::epi_all(eng.step(has_next, nr[0], nr[1], nr[2], r[0], r[1], r[2], M))) break;
+      if (valid && p < 2) {  // the two threads of a row store alternate entries
         const FarBlock bk = a.blocks[b];
-        double* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
+        pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
                                  : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
 #pragma unroll
         for (int q = 0; q < 9; q++) {
-          if ((q & 1) != h) continue;
-          const int r = q / 3, c = q % 3;
-          dst[q] = (r == c) ? (double)M[q] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+          if ((q & 1) != p) continue;
+          const int rr = q / 3, c = q % 3;
+          dst[q] = (rr == c) ? (double)M[q] : 0.5 * (double)(M[3 * rr + c] + M[3 * c + rr]);
         }
       }
+      if (!has_next) break;
+      tile = nt;
+      b = nb;
+      loc = nloc;
+      k = nk;
+      valid = nvalid;
+      r[0] = nr[0];
+      r[1] = nr[1];
+      r[2] = nr[2];
     }
-    if (ok) tc::epi_finish(S.tcs);
   }
   tc::cta_teardown(S.tcs);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(a.evals, (unsigned long long)tot);
@@ -228,6 +289,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
 struct EvalTcSmem {
   tc::Smem tcs;
 };
+
+__device__ __forceinline__ bool eval_row(const float* __restrict__ r, int64_t n, int64_t tile, int row,
+                                         float (&f)[3]) {
+  const int64_t g = tile * tc::kTile + row;
+  f[0] = 1.f;
+  f[1] = f[2] = 0.f;
+  if (g >= n) return false;
+  f[0] = r[3 * g];
+  f[1] = r[3 * g + 1];
+  f[2] = r[3 * g + 2];
+  return true;
+}
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
     k_eval_tc(const float* __restrict__ r, float* __restrict__ y, int64_t n, TcWeights w, int* err) {
@@ -239,27 +312,32 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int row = tc::epi_row(), h = tc::epi_half();
-    tc::EpiState st;
-    bool ok = true;
-    for (int64_t tile = 2 * (int64_t)blockIdx.x + tc::epi_group(); tile * tc::kTile < n;
-         tile += 2 * (int64_t)gridDim.x) {
-      const int64_t g = tile * tc::kTile + row;
-      float rx = 1.f, ry = 0.f, rz = 0.f;
-      if (g < n) {
-        rx = r[3 * g];
-        ry = r[3 * g + 1];
-        rz = r[3 * g + 2];
-      }
+    const int row = tc::epi_row(), p = tc::epi_part();
+    tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
+    int64_t tile = blockIdx.x;
+    float f[3];
+    bool valid = eval_row(r, n, tile, row, f);
+    eng.start(true, f[0], f[1], f[2]);
+    for (;;) {
+      const int64_t nt = tile + gridDim.x;
+      const bool has_next = nt * tc::kTile < n;
+      float nf[3] = {1.f, 0.f, 0.f};
+      const bool nvalid = has_next && eval_row(r, n, nt, row, nf);
       float M[9];
-      ok = tc::run_tile(S.tcs, st, rx, ry, rz, M, err);
-      if (!ok) break;
-      if (g < n)
+      if (!tc::epi_all(eng.step(has_next, nf[0], nf[1], nf[2], f[0], f[1], f[2], M))) break;
+      if (valid && p < 2) {
+        const int64_t g = tile * tc::kTile + row;
 #pragma unroll
         for (int q = 0; q < 9; q++)
-          if ((q & 1) == h) y[9 * g + q] = M[q];
+          if ((q & 1) == p) y[9 * g + q] = M[q];
+      }
+      if (!has_next) break;
+      tile = nt;
+      valid = nvalid;
+      f[0] = nf[0];
+      f[1] = nf[1];
+      f[2] = nf[2];
     }
-    if (ok) tc::epi_finish(S.tcs);
   }
   tc::cta_teardown(S.tcs);
 }
@@ -297,8 +375,7 @@ void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int
   const size_t smem = sizeof(EvalTcSmem) + 1024;
   set_smem(k_eval_tc, smem);
   const int64_t tiles = (n + tc::kTile - 1) / tc::kTile;
-  const int64_t pairs = (tiles + 1) / 2;
-  const int grid = (int)(pairs < num_sms ? pairs : num_sms);
+  const int grid = (int)(tiles < num_sms ? tiles : num_sms);
   k_eval_tc<<<grid, tc::kThreads, smem, s>>>(r, y, n, w, err);
   HIGNN_CHECK_LAUNCH();
 }

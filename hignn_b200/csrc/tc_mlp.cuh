@@ -10,37 +10,40 @@
 //       (rows 0-8) and a BF16 residual (rows 16-24): W3 rounding is the dominant
 //       systematic error of a plain BF16 layer 3, and the split removes it.
 // Between layers the epilogue warps read the accumulator (tcgen05.ld), add the
-// FP32 layer-2 bias, round to BF16 pairs and apply tanh.approx.bf16x2 (two per
-// MUFU op), and write the pairs back into tensor memory as the next A operand.
+// FP32 layer-2 bias, round to BF16 pairs and apply tanh.approx.bf16x2, and write
+// the pairs back into tensor memory as the next A operand.
 //
-// Two tile contexts per CTA so that tanh work of one overlaps the MMAs of the
-// other. CTA = 17 warps:
-//   warps 0-7   epilogue group 0 (context 0), warps 8-15 epilogue group 1;
-//               warp w reaches TMEM lanes 32*(w%4)..+31, so the evaluation (row)
-//               e = 32*(w%4) + lane of a context is handled by two threads
-//               (warps w and w+4 of the group), each owning one half of every
-//               row's columns;
-//   warp 16     allocates tensor memory; one lane issues every MMA, serving the
-//               two contexts as their operands become ready (non-blocking
-//               mbarrier tests, so one context never holds up the other).
-// Tensor memory (512 columns allocated), per context c at column 256c:
+// The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM
+// (tanh.approx.bf16x2 issues at half the rate of tanh.approx.f32, so packing
+// saves issue slots, not MUFU time), i.e. 40 clocks per evaluation per SM,
+// twice the tensor-core time of the three layers. The pipeline is therefore
+// built to keep the MUFU busy: one tile stream per CTA, two FP32 accumulator
+// slots, and an MMA lane that runs one quarter ahead of the epilogue, so the
+// tanh of one quarter overlaps the layer-2 MMA of the next.
+//
+// CTA = 17 warps:
+//   warps 0-15  epilogue; warp w reaches TMEM lanes 32 (w % 4) .. + 31, so the
+//               evaluation (row) e = 32 (w % 4) + lane is handled by four
+//               threads (part p = w / 4 owns columns 32p .. 32p + 31 of every
+//               128-column accumulator);
+//   warp 16     allocates tensor memory; one lane issues every MMA.
+// Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs (A operand of layer 2)
-//   [ 64,192)  slot: FP32 accumulator of layer 1, then of each layer-2 quarter
-//              (128 hidden units); after the epilogue reads a quarter, its
-//              tanh'd BF16 pairs are written back into slot columns [0,32)
-//              (units 0-63, half 0) and [64,96) (units 64-127, half 1) -- each
-//              half writes only columns it read itself -- as layer 3's A operand
-//   [192,224)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
-//   [224,232)  A0: the split features (K = 16 BF16) of layer 1
+//   [ 64,192)  slot 0 and [192,320) slot 1: FP32 accumulators, used in turn by
+//              layer 1 and the four layer-2 quarters of each tile; after the
+//              epilogue reads its 32 columns of a quarter it writes their 16
+//              tanh'd BF16 pairs back into the first 16 of them, as layer 3's A
+//              operand
+//   [320,352)  and [352,384): layer-3 accumulators of even / odd tiles (hi part
+//              in columns 0-8, residual in 16-24)
+//   [384,392)  A0: the split features (K = 16 BF16) of layer 1
 // Shared memory: W2 (512 x 128), W3 (32 x 512) and W1 (128 x 16, in a 64-wide
 // slab) as BF16 in the canonical K-major 128-byte-swizzle layout, loaded once
-// per CTA; FP32 biases b2, b3; mbarriers.
-//
-// Per context and tile: features -> A0; MMA L1 -> slot; epilogue tanh -> A1;
-// then for each quarter q: MMA L2(q) -> slot, epilogue bias + tanh -> A2(q) in
-// the slot, MMA L3(q) -> D3. Every wait is bounded (about two seconds of
-// clock): on a timeout the CTA records an error, stops issuing work, drains
-// its MMAs and frees its tensor memory.
+// per CTA; FP32 biases b2, b3; mbarriers. Barriers that are signalled twice in a
+// row before their waiter looks (the two slots) exist per slot, so no waiter ever
+// falls two phases behind. Every wait is bounded (about two seconds of clock):
+// on a timeout the CTA records an error, stops issuing work, drains its MMAs
+// and frees its tensor memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -55,30 +58,23 @@ namespace tc {
 using hignn::TcWeights;
 
 constexpr int kTile = 128;
-constexpr int kGroupThreads = 256;
 constexpr int kEpiThreads = 512;
 constexpr int kThreads = 544;
 constexpr int kMmaWarp = 16;
-constexpr uint32_t kCtxCols = 256, kOffA1 = 0, kOffSlot = 64, kOffD3 = 192, kOffA0 = 224;
+constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffD3a = 320, kOffD3b = 352, kOffA0 = 384;
 constexpr int kW2Bytes = kH2 * kH1 * 2;      // 131072
 constexpr int kW3Rows = 32;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 32768
 constexpr int kW1Bytes = kH1 * 64 * 2;       // 16384: 128 rows x one 64-wide K slab (K 0-15 used)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
-struct CtxBars {
-  uint64_t a0_full, d1_full, a1_full, d2_full, a2_full, slot_free, d3_full, d3_free;
-  int exit_flag;
-  int pad;
-};
-
 struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
   uint8_t w3[kW3Bytes];
   uint8_t w1[kW1Bytes];
-  CtxBars ctx[2];
-  uint64_t drain;
+  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], slot_free[2], d3_full, d3_free[2], drain;
   uint32_t tmem_base;
+  int exit_flag;
   int abort_flag;
   alignas(16) float b2[kH2];  // FP32 layer-2 bias, added before rounding to BF16
   float b3[16];
@@ -102,20 +98,22 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Non-blocking test of a phase (never suspends the thread): the MMA lane polls two contexts.
-__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+// As mbar_try, but the thread may stay suspended in hardware for up to hint_ns while the phase is
+// incomplete (it resumes as soon as the phase completes): waiting warps then issue nothing, and
+// in particular do not fill the MIO queue that the MUFU instructions of the working warps share.
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t* b, uint32_t parity, uint32_t hint_ns) {
   uint32_t ok;
   asm volatile(
-      "{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\nselp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(saddr(b)), "r"(parity)
+      : "r"(saddr(b)), "r"(parity), "r"(hint_ns)
       : "memory");
   return ok != 0;
 }
 // Bounded wait: returns false (and raises the CTA abort flag) if the phase never completes.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* abort_flag, int* err, int code) {
   const long long t0 = clock64();
-  while (!mbar_try(b, parity)) {
+  while (!mbar_try_sleep(b, parity, 20000u)) {
     if (*(volatile int*)abort_flag) return false;
     if (clock64() - t0 > kWaitCycles) {
       atomicExch(abort_flag, 1);
@@ -173,6 +171,15 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
       : "memory");
 }
 
+// 16 consecutive 32-bit TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
 // 4 consecutive 32-bit TMEM columns of this thread's lane
 __device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3) {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};\n" ::"r"(taddr), "r"(v0), "r"(v1), "r"(v2),
@@ -226,19 +233,20 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t == 0) {
-    for (int c = 0; c < 2; c++) {
-      CtxBars& b = s.ctx[c];
-      mbar_init(&b.a0_full, kGroupThreads);
-      mbar_init(&b.d1_full, 1);
-      mbar_init(&b.a1_full, kGroupThreads);
-      mbar_init(&b.d2_full, 1);
-      mbar_init(&b.a2_full, kGroupThreads);
-      mbar_init(&b.slot_free, 1);
-      mbar_init(&b.d3_full, 1);
-      mbar_init(&b.d3_free, kGroupThreads);
-      b.exit_flag = 0;
-    }
+    mbar_init(&s.a0_full, kEpiThreads);
+    mbar_init(&s.d1_full, 1);
+    mbar_init(&s.a1_full, kEpiThreads);
+    mbar_init(&s.d2_full[0], 1);
+    mbar_init(&s.d2_full[1], 1);
+    mbar_init(&s.a2_full[0], kEpiThreads);
+    mbar_init(&s.a2_full[1], kEpiThreads);
+    mbar_init(&s.slot_free[0], 1);
+    mbar_init(&s.slot_free[1], 1);
+    mbar_init(&s.d3_full, 1);
+    mbar_init(&s.d3_free[0], kEpiThreads);
+    mbar_init(&s.d3_free[1], kEpiThreads);
     mbar_init(&s.drain, 1);
+    s.exit_flag = 0;
     s.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -258,107 +266,111 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
 }
 
 // ------------------------------------------------------------------ MMA lane
-// Non-blocking state machine per context; mma_loop returns when both epilogue groups
-// raised their exit flags (or the CTA aborted / nothing progressed for kWaitCycles).
-//   state 0: features of the next tile in A0 (and the slot free) -> layer 1
-//   state 1: A1 written -> layer 2 of quarter q
-//   state 2: A2(q) written (and, for q = 0, D3 read) -> layer 3 of quarter q
-//   state 3: layer 3 of quarter q released the slot -> layer 2 of quarter q + 1
-struct MmaCtx {
-  uint32_t tile = 0, q = 0, state = 0, l2s = 0, l3s = 0;
-  bool done = false;
+// One thread issues every MMA in a fixed order per tile t (slot of accumulation u = u & 1,
+// u = 5t + {0: L1, 1..4: quarters 0..3}):
+//   L2(t,0) L2(t,1) L3(t,0) L2(t,2) L3(t,1) L2(t,3) L3(t,2) L1(t+1) L3(t,3)
+// so that layer 1 of the next tile and layer 2 of the next quarter are computed while the
+// epilogue works on the current one. Before an accumulation into a slot the previous use of
+// that slot must be consumed: by the epilogue (a1_full) for a layer-1 use, by the layer-3 MMA
+// that read it (slot_free, committed after it) for a quarter.
+struct MmaLane {
+  Smem& s;
+  int* err;
+  uint32_t tb, w1, w2, w3;
+  // phase parities per slot, bit s for slot s (no arrays indexed at run time: they would live in
+  // local memory)
+  uint32_t par_a2 = 0, par_slotfree = 0;
+  bool ok = true;
+
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
+    if (!ok) return false;
+    ok = mbar_wait(b, parity, &s.abort_flag, err, code);
+    if (ok) fence_after();
+    return ok;
+  }
+  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tb + (u & 1 ? kOffS1 : kOffS0); }
+  __device__ __forceinline__ void l1(uint32_t u) {
+    mma_ts(slot(u), tb + kOffA0, sdesc(w1), idesc_bf16(128, 128), 0u);
+    mma_commit(&s.d1_full);
+  }
+  __device__ __forceinline__ void l2(uint32_t u, uint32_t q) {
+    const uint32_t id = idesc_bf16(128, 128);
+#pragma unroll
+    for (uint32_t kk = 0; kk < 8; kk++) {
+      const uint32_t bb = w2 + (kk >> 2) * (kH2 * 128) + q * (128 * 128) + (kk & 3) * 32;
+      mma_ts(slot(u), tb + kOffA1 + 8 * kk, sdesc(bb), id, kk > 0);
+    }
+    mma_commit(&s.d2_full[u & 1]);
+  }
+  // layer 3 of quarter q from the A2 pairs in slot(u) into D3 buffer d
+  __device__ __forceinline__ void l3(uint32_t u, uint32_t q, uint32_t d) {
+    const uint32_t id = idesc_bf16(128, kW3Rows);
+    const uint32_t dst = tb + (d ? kOffD3b : kOffD3a);
+#pragma unroll
+    for (uint32_t kk = 0; kk < 8; kk++) {
+      const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
+      const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
+      const uint32_t a_off = 32 * (kk >> 1) + 8 * (kk & 1);  // pairs of the thread owning units 32(kk/2)..
+      mma_ts(dst, slot(u) + a_off, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
+    }
+    mma_commit(&s.slot_free[u & 1]);
+  }
+  // the layer-3 MMA of the quarter accumulated in slot(u) two uses ago has read it
+  __device__ __forceinline__ bool slot_consumed(uint32_t u) {
+    const uint32_t b = u & 1;
+    const bool r = wait(&s.slot_free[b], (par_slotfree >> b) & 1, 12);
+    par_slotfree ^= 1u << b;
+    return r;
+  }
+  // the epilogue wrote the A2 pairs of the quarter accumulated in slot(u)
+  __device__ __forceinline__ bool a2(uint32_t u, int code) {
+    const uint32_t b = u & 1;
+    const bool r = wait(&s.a2_full[b], (par_a2 >> b) & 1, code);
+    par_a2 ^= 1u << b;
+    return r;
+  }
+
+  __device__ void run() {
+    // tile 0: layer 1 once its features are in A0
+    if (!wait(&s.a0_full, 0, 13)) return;
+    if (*(volatile int*)&s.exit_flag) return;
+    l1(0);
+    for (uint32_t t = 0;; t++) {
+      const uint32_t u = 5 * t;
+      const uint32_t d = t & 1;
+      if (!wait(&s.a1_full, t & 1, 14)) return;  // A1(t) written; slot of L1(t) consumed
+      if (t > 0 && !slot_consumed(u + 1)) return;  // previous use: quarter 3 of tile t-1
+      l2(u + 1, 0);
+      l2(u + 2, 1);
+      if (!a2(u + 1, 15)) return;
+      if (t >= 2 && !wait(&s.d3_free[d], ((t >> 1) - 1) & 1, 16)) return;
+      l3(u + 1, 0, d);
+      if (!slot_consumed(u + 3)) return;
+      l2(u + 3, 2);
+      if (!a2(u + 2, 17)) return;
+      l3(u + 2, 1, d);
+      if (!slot_consumed(u + 4)) return;
+      l2(u + 4, 3);
+      if (!a2(u + 3, 18)) return;
+      l3(u + 3, 2, d);
+      // layer 1 of the next tile (or the end of the stream)
+      if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;
+      const bool more = !*(volatile int*)&s.exit_flag;
+      if (more) {
+        if (!slot_consumed(u + 5)) return;
+        l1(u + 5);
+      }
+      if (!a2(u + 4, 20)) return;
+      l3(u + 4, 3, d);
+      mma_commit(&s.d3_full);
+      if (!more) return;
+    }
+  }
 };
 
-__device__ __forceinline__ void issue_l2(uint32_t base, uint32_t q, uint32_t w2) {
-  const uint32_t id_l2 = idesc_bf16(128, 128);
-#pragma unroll
-  for (uint32_t kk = 0; kk < 8; kk++) {
-    const uint32_t bb = w2 + (kk >> 2) * (kH2 * 128) + q * (128 * 128) + (kk & 3) * 32;
-    mma_ts(base + kOffSlot, base + kOffA1 + 8 * kk, sdesc(bb), id_l2, kk > 0);
-  }
-}
-
-__device__ __forceinline__ bool mma_step(Smem& s, MmaCtx& x, uint32_t c, uint32_t tbase, uint32_t w1, uint32_t w2,
-                                         uint32_t w3) {
-  CtxBars& b = s.ctx[c];
-  const uint32_t base = tbase + c * kCtxCols;
-  if (x.state == 0) {
-    if (!mbar_test(&b.a0_full, x.tile & 1)) return false;
-    if (x.l3s > 0 && !mbar_test(&b.slot_free, (x.l3s - 1) & 1)) return false;
-    fence_after();
-    if (*(volatile int*)&b.exit_flag) {
-      x.done = true;
-      return true;
-    }
-    mma_ts(base + kOffSlot, base + kOffA0, sdesc(w1), idesc_bf16(128, 128), 0u);
-    mma_commit(&b.d1_full);
-    x.q = 0;
-    x.state = 1;
-    return true;
-  }
-  if (x.state == 1) {
-    if (!mbar_test(&b.a1_full, x.tile & 1)) return false;
-    fence_after();
-    issue_l2(base, 0, w2);
-    mma_commit(&b.d2_full);
-    x.l2s++;
-    x.state = 2;
-    return true;
-  }
-  if (x.state == 3) {
-    if (!mbar_test(&b.slot_free, (x.l3s - 1) & 1)) return false;
-    fence_after();
-    issue_l2(base, x.q, w2);
-    mma_commit(&b.d2_full);
-    x.l2s++;
-    x.state = 2;
-    return true;
-  }
-  // state 2: layer 3 of quarter q
-  if (!mbar_test(&b.a2_full, (x.l2s - 1) & 1)) return false;
-  if (x.q == 0 && x.tile > 0 && !mbar_test(&b.d3_free, (x.tile - 1) & 1)) return false;
-  fence_after();
-  const uint32_t id_l3 = idesc_bf16(128, kW3Rows);
-#pragma unroll
-  for (uint32_t kk = 0; kk < 8; kk++) {
-    const uint32_t kg = x.q * 128 + kk * 16;  // global K of layer 3
-    const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-    const uint32_t a_off = kk < 4 ? 8 * kk : 64 + 8 * (kk - 4);  // A2 halves at slot columns 0 and 64
-    mma_ts(base + kOffD3, base + kOffSlot + a_off, sdesc(bb), id_l3, (x.q > 0 || kk > 0) ? 1u : 0u);
-  }
-  mma_commit(&b.slot_free);
-  x.l3s++;
-  if (x.q == 3) {
-    mma_commit(&b.d3_full);
-    x.tile++;
-    x.state = 0;
-  } else {
-    x.q++;
-    x.state = 3;
-  }
-  return true;
-}
-
 __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
-  const uint32_t tbase = s.tmem_base;
-  const uint32_t w1 = saddr(s.w1), w2 = saddr(s.w2), w3 = saddr(s.w3);
-  MmaCtx x[2];
-  long long last = clock64();
-  while (!(x[0].done && x[1].done)) {
-    bool prog = false;
-    if (!x[0].done) prog |= mma_step(s, x[0], 0, tbase, w1, w2, w3);
-    if (!x[1].done) prog |= mma_step(s, x[1], 1, tbase, w1, w2, w3);
-    if (prog) {
-      last = clock64();
-    } else {
-      if (*(volatile int*)&s.abort_flag) break;
-      if (clock64() - last > kWaitCycles) {
-        atomicExch(&s.abort_flag, 1);
-        atomicCAS(err, 0, 11);
-        break;
-      }
-    }
-  }
+  MmaLane lane{s, err, s.tmem_base, saddr(s.w1), saddr(s.w2), saddr(s.w3)};
+  lane.run();
   // drain: every MMA issued so far completes before tensor memory is released
   mma_commit(&s.drain);
   const long long t0 = clock64();
@@ -367,122 +379,135 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
 }
 
 // ------------------------------------------------------------------ epilogue side
-struct EpiState {
-  uint32_t tile = 0, quarters = 0;
-};
-
-__device__ __forceinline__ int epi_group() { return threadIdx.x >> 8; }                      // context 0 / 1
-__device__ __forceinline__ int epi_gthread() { return threadIdx.x & 255; }                   // 0..255 in group
+// Warp w (0-15) reaches TMEM lanes 32 (w % 4) ..; the evaluation (row) e = 32 (w % 4) + lane is
+// handled by four threads (warps w % 4 + 4 p, p = 0..3), thread p owning columns 32p..32p+31
+// of every 128-column accumulator.
 __device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
-__device__ __forceinline__ int epi_half() { return (threadIdx.x >> 7) & 1; }                 // column half
-__device__ __forceinline__ void epi_bar() {
-  if (epi_group() == 0)
-    asm volatile("bar.sync 1, 256;\n" ::: "memory");
-  else
-    asm volatile("bar.sync 2, 256;\n" ::: "memory");
+__device__ __forceinline__ int epi_part() { return (threadIdx.x >> 7) & 3; }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
+
+// All 512 epilogue threads agree on ok (false if any thread's bounded wait gave up).
+__device__ __forceinline__ bool epi_all(bool ok) {
+  uint32_t r;
+  asm volatile("{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, 512, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+               : "=r"(r)
+               : "r"((uint32_t)ok)
+               : "memory");
+  return r != 0;
 }
 
 __device__ __forceinline__ float bf16_round(float x) { return __uint_as_float(pack_bf16(x, 0.f) << 16); }
 
 // Layer-1 operand of one row: K = 16 BF16 values [r_hi(3), r_lo(3), r_hi(3), 1, 1, 0 x 5] packed in
-// pairs; half 0 writes columns 0-3, half 1 columns 4-7.
-__device__ __forceinline__ void write_features(uint32_t ta0, int h, float rx, float ry, float rz) {
+// pairs; part 0 writes columns 0-3, part 1 columns 4-7.
+__device__ __forceinline__ void write_features(uint32_t ta0, int p, float rx, float ry, float rz) {
   const float hx = bf16_round(rx), hy = bf16_round(ry), hz = bf16_round(rz);
-  if (h == 0) {
+  if (p == 0) {
     const float lx = rx - hx, ly = ry - hy, lz = rz - hz;  // exact in FP32
     tmem_st4(ta0, pack_bf16(hx, hy), pack_bf16(hz, lx), pack_bf16(ly, lz), pack_bf16(hx, hy));
-  } else {
+  } else if (p == 1) {
     tmem_st4(ta0 + 4, pack_bf16(hz, 1.f), pack_bf16(1.f, 0.f), 0u, 0u);
   }
 }
 
-// One tile for this thread's evaluation (row) with features r; writes M (row-major 3x3) into
-// both threads of the row. Returns false if the CTA aborted. All 256 threads of the group
-// call it together.
-__device__ __forceinline__ bool run_tile(Smem& s, EpiState& st, float rx, float ry, float rz, float (&M)[9],
-                                         int* err) {
-  const int c = epi_group(), h = epi_half();
-  CtxBars& b = s.ctx[c];
-  const uint32_t tb = s.tmem_base + c * kCtxCols + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16);
-  write_features(tb + kOffA0, h, rx, ry, rz);
-  tmem_wait_st();
-  fence_before();
-  mbar_arrive(&b.a0_full);
-  // layer 1 accumulator (bias included) -> tanh -> A1
-  if (!mbar_wait(&b.d1_full, st.tile & 1, &s.abort_flag, err, 21)) return false;
-  fence_after();
-  {
-    uint32_t out[32];
-#pragma unroll
-    for (int part = 0; part < 2; part++) {
-      uint32_t v[32];
-      tmem_ld32(tb + kOffSlot + 64 * h + 32 * part, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int k = 0; k < 16; k++)
-        out[16 * part + k] = tanh_bf16x2(pack_bf16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
-    }
-    tmem_st32(tb + kOffA1 + 32 * h, out);
+struct Epi {
+  Smem& s;
+  int* err;
+  uint32_t tl;  // TMEM base with this warp's lane field
+  int p;
+  uint32_t tile = 0, par_d2 = 0;  // phase parity of d2_full per slot (bit s)
+  bool ok = true;
+
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
+    if (!ok) return false;
+    ok = mbar_wait(b, parity, &s.abort_flag, err, code);
+    if (ok) fence_after();
+    return ok;
   }
-  tmem_wait_st();
-  fence_before();
-  mbar_arrive(&b.a1_full);
-  for (uint32_t q = 0; q < 4; q++) {
-    if (!mbar_wait(&b.d2_full, st.quarters & 1, &s.abort_flag, err, 22)) return false;
-    fence_after();
-    const uint32_t col = tb + kOffSlot + 64 * h;
-    uint32_t out[32];
-#pragma unroll
-    for (int part = 0; part < 2; part++) {
-      uint32_t v[32];
-      tmem_ld32(col + 32 * part, v);
+  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tl + (u & 1 ? kOffS1 : kOffS0); }
+  // features of the first tile (has = false: nothing to do at all)
+  __device__ __forceinline__ void start(bool has, float rx, float ry, float rz) {
+    if (has) {
+      write_features(tl + kOffA0, p, rx, ry, rz);
+      tmem_wait_st();
+    } else if (threadIdx.x == 0) {
+      *(volatile int*)&s.exit_flag = 1;  // released by this thread's arrival below
+    }
+    fence_before();
+    mbar_arrive(&s.a0_full);
+  }
+  // Current tile: layer-1 epilogue (and the next tile's features, or the end of the stream),
+  // the four layer-2 quarters and layer 3 -> M (row-major 3x3) in threads of parts 0 and 1.
+  // Returns false if the CTA aborted. All 512 epilogue threads call it together.
+  __device__ __forceinline__ bool step(bool has_next, float nx, float ny, float nz, float rx, float ry, float rz, float (&M)[9]) {
+    const uint32_t u = 5 * tile;
+    if (!wait(&s.d1_full, tile & 1, 21)) return false;
+    // A0 was consumed by L1(tile): the next tile's features (or the end of the stream)
+    if (has_next) {
+      write_features(tl + kOffA0, p, nx, ny, nz);
+      tmem_wait_st();
+    } else if (threadIdx.x == 0) {
+      *(volatile int*)&s.exit_flag = 1;  // released by this thread's arrival below
+    }
+    fence_before();
+    mbar_arrive(&s.a0_full);
+    {  // layer 1: tanh(W1 r + b1) -> A1
+      uint32_t v[32], out[16];
+      tmem_ld32(slot(u) + 32 * p, v);
       tmem_wait_ld();
-      const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 64 * h + 32 * part);
+#pragma unroll
+      for (int k = 0; k < 16; k++) out[k] = tanh_bf16x2(pack_bf16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
+      tmem_st16(tl + kOffA1 + 16 * p, out);
+      tmem_wait_st();
+    }
+    fence_before();
+    mbar_arrive(&s.a1_full);
+    for (uint32_t q = 0; q < 4; q++) {
+      const uint32_t sl = (u + 1 + q) & 1;
+      const bool got = wait(&s.d2_full[sl], (par_d2 >> sl) & 1, 22);
+      par_d2 ^= 1u << sl;
+      if (!got) return false;
+      const uint32_t col = slot(u + 1 + q) + 32 * p;
+      uint32_t v[32], out[16];
+      tmem_ld32(col, v);
+      tmem_wait_ld();
+      const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const float4 bv = bb[k];
-        uint32_t* o = out + 16 * part + 2 * k;
-        o[0] = tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
-        o[1] = tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
+        out[2 * k] = tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
+        out[2 * k + 1] =
+            tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
+      }
+      tmem_st16(col, out);  // inside the columns this thread read itself
+      tmem_wait_st();
+      fence_before();
+      mbar_arrive(&s.a2_full[sl]);
+    }
+    if (!wait(&s.d3_full, tile & 1, 23)) return false;
+    const uint32_t d3 = tl + (tile & 1 ? kOffD3b : kOffD3a);
+    if (p < 2) {
+      uint32_t v[32];
+      tmem_ld32(d3, v);
+      tmem_wait_ld();
+      const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
+      const float inv = __frcp_rn(nr);
+#pragma unroll
+      for (int o = 0; o < 9; o++) {
+        float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + s.b3[o];
+        const bool dg = (o == 0 || o == 4 || o == 8);
+        if (dg) y += 1.0f;
+        y = y * inv;
+        if (nr < 1e-5f) y = dg ? 1.0f : 0.0f;
+        M[o] = y;
       }
     }
-    tmem_st32(col, out);  // inside the columns this thread read itself
-    tmem_wait_st();
     fence_before();
-    mbar_arrive(&b.a2_full);
-    st.quarters++;
+    mbar_arrive(&s.d3_free[tile & 1]);
+    tile++;
+    return true;
   }
-  if (!mbar_wait(&b.d3_full, st.tile & 1, &s.abort_flag, err, 23)) return false;
-  fence_after();
-  {
-    uint32_t v[32];
-    tmem_ld32(tb + kOffD3, v);
-    tmem_wait_ld();
-    fence_before();
-    mbar_arrive(&b.d3_free);
-    const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
-    const float inv = __frcp_rn(nr);
-#pragma unroll
-    for (int o = 0; o < 9; o++) {
-      float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + s.b3[o];
-      const bool dg = (o == 0 || o == 4 || o == 8);
-      if (dg) y += 1.0f;
-      y = y * inv;
-      if (nr < 1e-5f) y = dg ? 1.0f : 0.0f;
-      M[o] = y;
-    }
-  }
-  st.tile++;
-  return true;
-}
-
-// Tells the MMA lane that this group has no more tiles (all 256 threads of the group call it).
-__device__ __forceinline__ void epi_finish(Smem& s) {
-  CtxBars& b = s.ctx[epi_group()];
-  if (epi_gthread() == 0) *(volatile int*)&b.exit_flag = 1;
-  epi_bar();
-  mbar_arrive(&b.a0_full);
-}
+};
 
 }  // namespace tc
 }  // namespace hignn
