@@ -96,6 +96,7 @@ struct hignn_model {
   int64_t far_batch_rows = int64_t(1) << 26;
   int64_t far_pool_bytes = int64_t(24) << 30;  // C + Q pool memory of one ACA batch
   int rank_hint_offset = 0;                      // added to recorded ranks when planning (tests)
+  int max_leaf = 0;                              // largest leaf of the close list
   // shard of the block lists this model computes (hignn_set_shard): close pairs [sh_c0, sh_c1),
   // far pairs [sh_f0, sh_f1) of the lists
   int shard_rank = 0, shard_world = 1;
@@ -242,6 +243,8 @@ void build_structures(hignn_model* m) {
     work[q] = w;
   }
   m->stats.close_evals = evals;
+  m->max_leaf = 0;
+  for (const auto& w : work) m->max_leaf = std::max(m->max_leaf, std::max(w.nI, w.nJ));
   m->close_work.ensure(sizeof(hignn::PairWork) * std::max<size_t>(1, work.size()));
   if (!work.empty())
     HIGNN_CUDA(cudaMemcpyAsync(m->close_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
@@ -698,8 +701,13 @@ void near_field(hignn_model* m) {
   a.xI = a.xJ = m->x4.as<float4>();
   a.fI = a.fJ = m->f4.as<float4>();
   a.uI = a.uJ = m->u.as<double>();
-  if (m->precision >= 1)
+  if (m->precision >= 1) {
+    if (m->max_leaf > hignn::kTcMaxLeaf)
+      throw Error(HIGNN_ERR_ARG, "the tensor-core forms (precision 1, 2) need leaves of at most " +
+                                     std::to_string(hignn::kTcMaxLeaf) + " particles (block_size <= " +
+                                     std::to_string(hignn::kTcMaxLeaf) + ")");
     hignn::launch_near_tc(a, m->wtc(), m->counter.as<int>(), m->err_flag(), m->num_sms, m->stream);
+  }
   else
     hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
 }

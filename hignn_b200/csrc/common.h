@@ -25,6 +25,7 @@ struct Error : std::runtime_error {
 #define HIGNN_CHECK_LAUNCH() HIGNN_CUDA(cudaGetLastError())
 
 constexpr int kMaxLeaf = 256;   // largest leaf the near-field kernels stage in shared memory
+constexpr int kTcMaxLeaf = 128; // largest leaf of the tensor-core near field (three staging buffers)
 constexpr int kH1 = 128;        // two-body network widths (python/convert.py:6-20 over nn/*.pkl)
 constexpr int kH2 = 512;
 constexpr int kOut = 9;

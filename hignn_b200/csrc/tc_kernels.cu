@@ -26,15 +26,21 @@ __device__ __forceinline__ uint8_t* align1k(uint8_t* p) {
   return p + ((1024u - (a & 1023u)) & 1023u);
 }
 
+// Leaves up to kTcLeaf particles (the tensor-core forms need block_size <= 128).
+constexpr int kTcLeaf = kTcMaxLeaf;
+
 struct NearStage {
-  float4 xI[kMaxLeaf], xJ[kMaxLeaf], fI[kMaxLeaf], fJ[kMaxLeaf];
-  float uI[kMaxLeaf][3], uJ[kMaxLeaf][3];
+  float4 xI[kTcLeaf], xJ[kTcLeaf], fI[kTcLeaf], fJ[kTcLeaf];
+  float uI[kTcLeaf][3], uJ[kTcLeaf][3];
 };
 
+// Three staging buffers: the pair of the tile being retired, of the tile in flight and of the
+// next tile can all differ (pairs of a single tile).
 struct NearTcSmem {
   tc::Smem tcs;
-  NearStage st[2];
-  int item[2];
+  NearStage st[3];
+  PairWork pw[3];
+  int item[3];
 };
 static_assert(sizeof(NearTcSmem) + 1024 <= 232448, "near-field shared memory exceeds 227 KB per CTA");
 
@@ -68,20 +74,23 @@ __device__ __forceinline__ void add_segmented(float (*uI)[3], int i, float v0, f
   }
 }
 
-// Position of one 128-evaluation tile in the near-field stream.
-struct NearCursor {
-  int buf, item, t0;
-  PairWork pw;
+// Position of one 128-evaluation tile in the near-field stream and this thread's row of it.
+struct NearTile {
+  int buf, t0;  // the pair itself is S.pw[buf]
+  int i, j;
+  bool valid, last;  // last: the final tile of its pair
+  float r[3];
 };
 
 // Next close pair from the global counter, staged into buffer b (all epilogue threads).
-__device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int* counter, int b, NearCursor& c) {
+__device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int* counter, int b, NearTile& c) {
   const int e = threadIdx.x;
   if (e == 0) S.item[b] = atomicAdd(counter, 1);
   tc::epi_bar();  // also: every thread is done with the pair last staged in buffer b
   const int item = S.item[b];
   if (item >= a.nwork) return false;
   const PairWork pw = a.work[item];
+  if (e == 0) S.pw[b] = pw;
   NearStage& G = S.st[b];
   for (int i = e; i < pw.nI; i += tc::kEpiThreads) {
     G.xI[i] = a.xI[pw.sI + i];
@@ -95,29 +104,66 @@ __device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int
   }
   tc::epi_bar();
   c.buf = b;
-  c.item = item;
   c.t0 = 0;
-  c.pw = pw;
   return true;
 }
 
 // This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
-__device__ __forceinline__ bool near_row(const NearTcSmem& S, const NearCursor& c, int row, int& i, int& j,
-                                         float (&r)[3]) {
-  const int total = c.pw.nI * c.pw.nJ;
+__device__ __forceinline__ void near_row(const NearTcSmem& S, NearTile& c, int row) {
+  const int nJ = S.pw[c.buf].nJ, total = S.pw[c.buf].nI * nJ;
   const int flat = c.t0 + row;
-  const bool valid = flat < total;
-  i = valid ? flat / c.pw.nJ : 0;
-  j = valid ? flat - i * c.pw.nJ : 0;
-  r[0] = 1.f;
-  r[1] = r[2] = 0.f;
-  if (valid) {
-    const float4 xi = S.st[c.buf].xI[i], xj = S.st[c.buf].xJ[j];
-    r[0] = xj.x - xi.x;
-    r[1] = xj.y - xi.y;
-    r[2] = xj.z - xi.z;
+  c.valid = flat < total;
+  c.last = c.t0 + tc::kTile >= total;
+  c.i = c.valid ? flat / nJ : 0;
+  c.j = c.valid ? flat - c.i * nJ : 0;
+  c.r[0] = 1.f;
+  c.r[1] = c.r[2] = 0.f;
+  if (c.valid) {
+    const float4 xi = S.st[c.buf].xI[c.i], xj = S.st[c.buf].xJ[c.j];
+    c.r[0] = xj.x - xi.x;
+    c.r[1] = xj.y - xi.y;
+    c.r[2] = xj.z - xi.z;
   }
-  return valid;
+}
+
+// Contraction of one retired tile: u_I += M f_J (part 0), u_J += M f_I for J > I (part 1)
+// (src/CloseDot.cpp:245-299), into the pair's shared-memory accumulators.
+__device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& c, int p, float (&M)[9]) {
+  if (!c.valid || p >= 2) return;
+  NearStage& G = S.st[c.buf];
+  const int flags = S.pw[c.buf].flags;
+  if (flags & kPairSymmetrize) {
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+      for (int k = q + 1; k < 3; k++) {
+        const float v = 0.5f * (M[3 * q + k] + M[3 * k + q]);
+        M[3 * q + k] = v;
+        M[3 * k + q] = v;
+      }
+  }
+  if (p == 0) {
+    const float4 fj = G.fJ[c.j];
+    add_segmented(G.uI, c.i, M[0] * fj.x + M[1] * fj.y + M[2] * fj.z, M[3] * fj.x + M[4] * fj.y + M[5] * fj.z,
+                  M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
+  } else if (flags & kPairTransposed) {  // same M, not transposed (src/CloseDot.cpp:281-298)
+    const float4 fi = G.fI[c.i];
+    atomicAdd(&G.uJ[c.j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
+    atomicAdd(&G.uJ[c.j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
+    atomicAdd(&G.uJ[c.j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
+  }
+}
+
+// The pair of a retired last tile is complete: flush its velocities (all epilogue threads).
+__device__ __forceinline__ void near_flush(NearTcSmem& S, const NearArgs& a, const NearTile& c) {
+  tc::epi_bar();
+  const NearStage& G = S.st[c.buf];
+  const PairWork pw = S.pw[c.buf];
+  for (int q = threadIdx.x; q < 3 * pw.nI; q += tc::kEpiThreads)
+    atomicAdd(&a.uI[3 * (size_t)pw.sI + q], (double)(&G.uI[0][0])[q]);
+  if (pw.flags & kPairTransposed)
+    for (int q = threadIdx.x; q < 3 * pw.nJ; q += tc::kEpiThreads)
+      atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&G.uJ[0][0])[q]);
 }
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
@@ -130,68 +176,37 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
-    const int e = threadIdx.x, row = tc::epi_row(), p = tc::epi_part();
+    const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
-    NearCursor cur;
-    bool have = near_fetch(S, a, work_counter, 0, cur);
-    int i = 0, j = 0;
-    float r[3];
-    bool valid = have && near_row(S, cur, row, i, j, r);
-    eng.start(have, r[0], r[1], r[2]);
+    NearTile prev{}, cur{};
+    int nbuf = 0;  // staging buffers are used in turn
+    const bool have = near_fetch(S, a, work_counter, nbuf, cur);
+    nbuf = (nbuf + 1) % 3;
+    if (have) near_row(S, cur, row);
+    eng.start(have, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true, has_prev = false;
     while (have) {
-      // the next tile: the rest of this pair, or the next pair staged into the other buffer
-      NearCursor nxt = cur;
+      // the next tile: the rest of this pair, or the next pair staged into the next buffer
+      NearTile nxt = cur;
       nxt.t0 += tc::kTile;
-      const bool last = nxt.t0 >= cur.pw.nI * cur.pw.nJ;
       bool has_next = true;
-      if (last) has_next = near_fetch(S, a, work_counter, cur.buf ^ 1, nxt);
-      int ni = 0, nj = 0;
-      float nr[3] = {1.f, 0.f, 0.f};
-      const bool nvalid = has_next && near_row(S, nxt, row, ni, nj, nr);
-      float M[9];
-      const bool ok = tc::epi_all(eng.step(has_next, nr[0], nr[1], nr[2], r[0], r[1], r[2], M));
+      if (cur.last) {
+        has_next = near_fetch(S, a, work_counter, nbuf, nxt);
+        nbuf = (nbuf + 1) % 3;
+      }
+      if (has_next) near_row(S, nxt, row);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { near_use(S, prev, p, M); }));
       if (!ok) break;
-      NearStage& G = S.st[cur.buf];
-      const bool trans = (cur.pw.flags & kPairTransposed) != 0;
-      if (valid && p < 2) {
-        if (cur.pw.flags & kPairSymmetrize) {
-#pragma unroll
-          for (int q = 0; q < 3; q++)
-#pragma unroll
-            for (int c = q + 1; c < 3; c++) {
-              const float v = 0.5f * (M[3 * q + c] + M[3 * c + q]);
-              M[3 * q + c] = v;
-              M[3 * c + q] = v;
-            }
-        }
-        if (p == 0) {  // u_I[i] += M f_J[j]
-          const float4 fj = G.fJ[j];
-          add_segmented(G.uI, i, M[0] * fj.x + M[1] * fj.y + M[2] * fj.z, M[3] * fj.x + M[4] * fj.y + M[5] * fj.z,
-                        M[6] * fj.x + M[7] * fj.y + M[8] * fj.z);
-        } else if (trans) {  // u_J[j] += M f_I[i] (same M, src/CloseDot.cpp:281-298)
-          const float4 fi = G.fI[i];
-          atomicAdd(&G.uJ[j][0], M[0] * fi.x + M[1] * fi.y + M[2] * fi.z);
-          atomicAdd(&G.uJ[j][1], M[3] * fi.x + M[4] * fi.y + M[5] * fi.z);
-          atomicAdd(&G.uJ[j][2], M[6] * fi.x + M[7] * fi.y + M[8] * fi.z);
-        }
-      }
-      if (last) {  // the pair is complete: flush its velocities
-        tc::epi_bar();
-        for (int q = e; q < 3 * cur.pw.nI; q += tc::kEpiThreads)
-          atomicAdd(&a.uI[3 * (size_t)cur.pw.sI + q], (double)(&G.uI[0][0])[q]);
-        if (trans)
-          for (int q = e; q < 3 * cur.pw.nJ; q += tc::kEpiThreads)
-            atomicAdd(&a.uJ[3 * (size_t)cur.pw.sJ + q], (double)(&G.uJ[0][0])[q]);
-      }
+      if (has_prev && prev.last) near_flush(S, a, prev);
+      prev = cur;
+      has_prev = true;
       if (!has_next) break;
       cur = nxt;
-      i = ni;
-      j = nj;
-      valid = nvalid;
-      r[0] = nr[0];
-      r[1] = nr[1];
-      r[2] = nr[2];
     }
+    if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
+                                                 [&](float (&M)[9]) { near_use(S, prev, p, M); })))
+      near_flush(S, a, prev);
   }
   tc::cta_teardown(S.tcs);
 }
@@ -201,12 +216,18 @@ struct FarTcSmem {
 };
 
 // This thread's row of far tile `tile`: block b, local index loc, term k, feature r.
-__device__ __forceinline__ bool far_row(const FarArgs& a, int which, int nact, int tot, int tile, int row, int& b,
-                                        int& loc, int& k, float (&r)[3]) {
+struct FarRow {
+  int b, loc, k;
+  bool valid;
+  float r[3];
+};
+
+__device__ __forceinline__ void far_row(const FarArgs& a, int which, int nact, int tot, int tile, int row, FarRow& f) {
   const int g = tile * tc::kTile + row;
-  r[0] = 1.f;
-  r[1] = r[2] = 0.f;
-  if (g >= tot) return false;
+  f.r[0] = 1.f;
+  f.r[1] = f.r[2] = 0.f;
+  f.valid = g < tot;
+  if (!f.valid) return;
   const int32_t* pre = which ? a.preJ : a.preI;
   int lo = 0, hi = nact;
   while (hi - lo > 1) {
@@ -216,22 +237,36 @@ __device__ __forceinline__ bool far_row(const FarArgs& a, int which, int nact, i
     else
       hi = mid;
   }
-  b = a.act[lo];
-  loc = g - pre[lo];
-  const FarBlock bk = a.blocks[b];
-  k = a.state[b].k;
+  f.b = a.act[lo];
+  f.loc = g - pre[lo];
+  const FarBlock bk = a.blocks[f.b];
+  f.k = a.state[f.b].k;
   float4 xi, xj;
   if (which == 0) {
-    xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
-    xi = a.x[bk.sI + loc];
+    xj = a.x[bk.sJ + a.cols[(size_t)f.b * a.ldr + f.k]];
+    xi = a.x[bk.sI + f.loc];
   } else {
-    xj = a.x[bk.sJ + loc];
-    xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
+    xj = a.x[bk.sJ + f.loc];
+    xi = a.x[bk.sI + a.rows[(size_t)f.b * a.ldr + f.k]];
   }
-  r[0] = xj.x - xi.x;
-  r[1] = xj.y - xi.y;
-  r[2] = xj.z - xi.z;
-  return true;
+  f.r[0] = xj.x - xi.x;
+  f.r[1] = xj.y - xi.y;
+  f.r[2] = xj.z - xi.z;
+}
+
+// symmetrised 3x3 of a retired far row into the C (which = 0) or Q pool; the two threads of a
+// row store alternate entries (src/FarDot.cpp:445-456: diagonal copied, off-diagonal halved sum)
+__device__ __forceinline__ void far_use(const FarArgs& a, int which, const FarRow& f, int p, const float (&M)[9]) {
+  if (!f.valid || p >= 2) return;
+  const FarBlock bk = a.blocks[f.b];
+  pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)f.k * bk.nI + f.loc)
+                           : a.Q + 9 * (bk.qOff + (int64_t)f.k * bk.nJ + f.loc);
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    if ((q & 1) != p) continue;
+    const int rr = q / 3, c = q % 3;
+    dst[q] = (rr == c) ? (double)M[q] : 0.5 * (double)(M[3 * rr + c] + M[3 * c + rr]);
+  }
 }
 
 __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
@@ -248,39 +283,26 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
   } else {
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
-    int tile = blockIdx.x, b = 0, loc = 0, k = 0;
-    float r[3];
-    bool valid = far_row(a, which, nact, tot, tile, row, b, loc, k, r);
-    eng.start(true, r[0], r[1], r[2]);
+    int tile = blockIdx.x;
+    FarRow prev{}, cur{};
+    far_row(a, which, nact, tot, tile, row, cur);
+    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true;
     for (;;) {
       const int nt = tile + gridDim.x;
       const bool has_next = nt * tc::kTile < tot;
-      int nb = 0, nloc = 0, nk = 0;
-      float nr[3] = {1.f, 0.f, 0.f};
-      const bool nvalid = has_next && far_row(a, which, nact, tot, nt, row, nb, nloc, nk, nr);
-      float M[9];
-      if (!tc::epi_all(eng.step(has_next, nr[0], nr[1], nr[2], r[0], r[1], r[2], M))) break;
-      if (valid && p < 2) {  // the two threads of a row store alternate entries
-        const FarBlock bk = a.blocks[b];
-        pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
-                                 : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-          if ((q & 1) != p) continue;
-          const int rr = q / 3, c = q % 3;
-          dst[q] = (rr == c) ? (double)M[q] : 0.5 * (double)(M[3 * rr + c] + M[3 * c + rr]);
-        }
-      }
+      FarRow nxt{};
+      nxt.r[0] = 1.f;
+      if (has_next) far_row(a, which, nact, tot, nt, row, nxt);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
+      if (!ok) break;
+      prev = cur;
       if (!has_next) break;
       tile = nt;
-      b = nb;
-      loc = nloc;
-      k = nk;
-      valid = nvalid;
-      r[0] = nr[0];
-      r[1] = nr[1];
-      r[2] = nr[2];
+      cur = nxt;
     }
+    if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
   }
   tc::cta_teardown(S.tcs);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(a.evals, (unsigned long long)tot);
@@ -290,16 +312,21 @@ struct EvalTcSmem {
   tc::Smem tcs;
 };
 
-__device__ __forceinline__ bool eval_row(const float* __restrict__ r, int64_t n, int64_t tile, int row,
-                                         float (&f)[3]) {
-  const int64_t g = tile * tc::kTile + row;
-  f[0] = 1.f;
-  f[1] = f[2] = 0.f;
-  if (g >= n) return false;
-  f[0] = r[3 * g];
-  f[1] = r[3 * g + 1];
-  f[2] = r[3 * g + 2];
-  return true;
+struct EvalRow {
+  int64_t g;
+  bool valid;
+  float r[3];
+};
+
+__device__ __forceinline__ void eval_row(const float* __restrict__ r, int64_t n, int64_t tile, int row, EvalRow& f) {
+  f.g = tile * tc::kTile + row;
+  f.valid = f.g < n;
+  f.r[0] = 1.f;
+  f.r[1] = f.r[2] = 0.f;
+  if (!f.valid) return;
+  f.r[0] = r[3 * f.g];
+  f.r[1] = r[3 * f.g + 1];
+  f.r[2] = r[3 * f.g + 2];
 }
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
@@ -314,30 +341,32 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   } else {
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
+    auto use = [&](const EvalRow& f, float(&M)[9]) {
+      if (f.valid && p < 2)  // the two threads of a row store alternate entries
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+          if ((q & 1) == p) y[9 * f.g + q] = M[q];
+    };
     int64_t tile = blockIdx.x;
-    float f[3];
-    bool valid = eval_row(r, n, tile, row, f);
-    eng.start(true, f[0], f[1], f[2]);
+    EvalRow prev{}, cur{};
+    eval_row(r, n, tile, row, cur);
+    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true;
     for (;;) {
       const int64_t nt = tile + gridDim.x;
       const bool has_next = nt * tc::kTile < n;
-      float nf[3] = {1.f, 0.f, 0.f};
-      const bool nvalid = has_next && eval_row(r, n, nt, row, nf);
-      float M[9];
-      if (!tc::epi_all(eng.step(has_next, nf[0], nf[1], nf[2], f[0], f[1], f[2], M))) break;
-      if (valid && p < 2) {
-        const int64_t g = tile * tc::kTile + row;
-#pragma unroll
-        for (int q = 0; q < 9; q++)
-          if ((q & 1) == p) y[9 * g + q] = M[q];
-      }
+      EvalRow nxt{};
+      nxt.r[0] = 1.f;
+      if (has_next) eval_row(r, n, nt, row, nxt);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { use(prev, M); }));
+      if (!ok) break;
+      prev = cur;
       if (!has_next) break;
       tile = nt;
-      valid = nvalid;
-      f[0] = nf[0];
-      f[1] = nf[1];
-      f[2] = nf[2];
+      cur = nxt;
     }
+    if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
   }
   tc::cta_teardown(S.tcs);
 }

@@ -18,8 +18,9 @@
 // saves issue slots, not MUFU time), i.e. 40 clocks per evaluation per SM,
 // twice the tensor-core time of the three layers. The pipeline is therefore
 // built to keep the MUFU busy: one tile stream per CTA, two FP32 accumulator
-// slots, and an MMA lane that runs one quarter ahead of the epilogue, so the
-// tanh of one quarter overlaps the layer-2 MMA of the next.
+// slots, separate buffers for layer 3's operand, and an MMA lane that runs a
+// quarter ahead of the epilogue without ever waiting for an MMA of its own (an
+// MMA's result reaches a waiting thread ~500 cycles after issue, measured).
 //
 // CTA = 17 warps:
 //   warps 0-15  epilogue; warp w reaches TMEM lanes 32 (w % 4) .. + 31, so the
@@ -30,20 +31,18 @@
 // Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed BF16 pairs (A operand of layer 2)
 //   [ 64,192)  slot 0 and [192,320) slot 1: FP32 accumulators, used in turn by
-//              layer 1 and the four layer-2 quarters of each tile; after the
-//              epilogue reads its 32 columns of a quarter it writes their 16
-//              tanh'd BF16 pairs back into the first 16 of them, as layer 3's A
-//              operand
-//   [320,352)  and [352,384): layer-3 accumulators of even / odd tiles (hi part
-//              in columns 0-8, residual in 16-24)
-//   [384,392)  A0: the split features (K = 16 BF16) of layer 1
+//              layer 1 and the four layer-2 quarters of each tile
+//   [320,384)  and [384,448): A2 of even / odd quarters, the tanh'd BF16 pairs
+//              of a quarter (A operand of layer 3)
+//   [448,480)  layer-3 accumulator (hi part in columns 0-8, residual in 16-24)
+//   [480,488)  A0: the split features (K = 16 BF16) of layer 1
 // Shared memory: W2 (512 x 128), W3 (32 x 512) and W1 (128 x 16, in a 64-wide
 // slab) as BF16 in the canonical K-major 128-byte-swizzle layout, loaded once
-// per CTA; FP32 biases b2, b3; mbarriers. Barriers that are signalled twice in a
-// row before their waiter looks (the two slots) exist per slot, so no waiter ever
-// falls two phases behind. Every wait is bounded (about two seconds of clock):
-// on a timeout the CTA records an error, stops issuing work, drains its MMAs
-// and frees its tensor memory.
+// per CTA; FP32 biases b2, b3; mbarriers. A barrier that completes twice per
+// tile (the per-slot and per-buffer ones) is waited with the parity of its
+// position in the tile, and no waiter can fall two phases behind. Every wait is
+// bounded (about two seconds of clock): on a timeout the CTA records an error,
+// stops issuing work, drains its MMAs and frees its tensor memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -61,7 +60,7 @@ constexpr int kTile = 128;
 constexpr int kEpiThreads = 512;
 constexpr int kThreads = 544;
 constexpr int kMmaWarp = 16;
-constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffD3a = 320, kOffD3b = 352, kOffA0 = 384;
+constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffA2a = 320, kOffA2b = 384, kOffD3 = 448, kOffA0 = 480;
 constexpr int kW2Bytes = kH2 * kH1 * 2;      // 131072
 constexpr int kW3Rows = 32;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 32768
@@ -72,7 +71,7 @@ struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
   uint8_t w3[kW3Bytes];
   uint8_t w1[kW1Bytes];
-  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], slot_free[2], d3_full, d3_free[2], drain;
+  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], a2_free[2], d3_full, d3_free, drain;
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
@@ -240,11 +239,10 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
     mbar_init(&s.d2_full[1], 1);
     mbar_init(&s.a2_full[0], kEpiThreads);
     mbar_init(&s.a2_full[1], kEpiThreads);
-    mbar_init(&s.slot_free[0], 1);
-    mbar_init(&s.slot_free[1], 1);
+    mbar_init(&s.a2_free[0], 1);
+    mbar_init(&s.a2_free[1], 1);
     mbar_init(&s.d3_full, 1);
-    mbar_init(&s.d3_free[0], kEpiThreads);
-    mbar_init(&s.d3_free[1], kEpiThreads);
+    mbar_init(&s.d3_free, kEpiThreads);
     mbar_init(&s.drain, 1);
     s.exit_flag = 0;
     s.abort_flag = 0;
@@ -266,20 +264,22 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
 }
 
 // ------------------------------------------------------------------ MMA lane
-// One thread issues every MMA in a fixed order per tile t (slot of accumulation u = u & 1,
-// u = 5t + {0: L1, 1..4: quarters 0..3}):
-//   L2(t,0) L2(t,1) L3(t,0) L2(t,2) L3(t,1) L2(t,3) L3(t,2) L1(t+1) L3(t,3)
-// so that layer 1 of the next tile and layer 2 of the next quarter are computed while the
-// epilogue works on the current one. Before an accumulation into a slot the previous use of
-// that slot must be consumed: by the epilogue (a1_full) for a layer-1 use, by the layer-3 MMA
-// that read it (slot_free, committed after it) for a quarter.
+// One thread issues every MMA, per tile t (u = 5t; accumulator slot of a use = u & 1; A2 buffer
+// of quarter q = q & 1), in this order:
+//   L2(t,0)->slot(u+1)  L2(t,1)->slot(u+2)          after a1_full(t): A1 written, L1 slot read
+//   L3(t,0)<-A2[0]  L2(t,2)->slot(u+3)               after a2(q0): slot(u+1) read, A2[0] written
+//   L3(t,1)<-A2[1]  L2(t,3)->slot(u+4)               after a2(q1)
+//   L3(t,2)<-A2[0]  L1(t+1)->slot(u+5)               after a2(q2) and a0_full(t+1)
+//   L3(t,3)<-A2[1]  commit d3_full                   after a2(q3)
+// An accumulator slot is reused as soon as the epilogue has read it (its tanh'd pairs go to a
+// separate A2 buffer), so the lane never waits for an MMA of its own: the ~500-cycle latency
+// from an MMA's issue to its commit reaching a waiting thread is paid only by threads that have
+// other work queued. L3(t,0) overwrites D3, so it also waits until the epilogue has read D3 of
+// tile t-1 (d3_free).
 struct MmaLane {
   Smem& s;
   int* err;
   uint32_t tb, w1, w2, w3;
-  // phase parities per slot, bit s for slot s (no arrays indexed at run time: they would live in
-  // local memory)
-  uint32_t par_a2 = 0, par_slotfree = 0;
   bool ok = true;
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
@@ -302,32 +302,22 @@ struct MmaLane {
     }
     mma_commit(&s.d2_full[u & 1]);
   }
-  // layer 3 of quarter q from the A2 pairs in slot(u) into D3 buffer d
-  __device__ __forceinline__ void l3(uint32_t u, uint32_t q, uint32_t d) {
+  // layer 3 of quarter q from its A2 buffer into D3
+  __device__ __forceinline__ void l3(uint32_t q) {
     const uint32_t id = idesc_bf16(128, kW3Rows);
-    const uint32_t dst = tb + (d ? kOffD3b : kOffD3a);
+    const uint32_t a2 = tb + (q & 1 ? kOffA2b : kOffA2a);
 #pragma unroll
     for (uint32_t kk = 0; kk < 8; kk++) {
       const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
       const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-      const uint32_t a_off = 32 * (kk >> 1) + 8 * (kk & 1);  // pairs of the thread owning units 32(kk/2)..
-      mma_ts(dst, slot(u) + a_off, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
+      mma_ts(tb + kOffD3, a2 + 8 * kk, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
     }
-    mma_commit(&s.slot_free[u & 1]);
+    mma_commit(&s.a2_free[q & 1]);
   }
-  // the layer-3 MMA of the quarter accumulated in slot(u) two uses ago has read it
-  __device__ __forceinline__ bool slot_consumed(uint32_t u) {
-    const uint32_t b = u & 1;
-    const bool r = wait(&s.slot_free[b], (par_slotfree >> b) & 1, 12);
-    par_slotfree ^= 1u << b;
-    return r;
-  }
-  // the epilogue wrote the A2 pairs of the quarter accumulated in slot(u)
-  __device__ __forceinline__ bool a2(uint32_t u, int code) {
-    const uint32_t b = u & 1;
-    const bool r = wait(&s.a2_full[b], (par_a2 >> b) & 1, code);
-    par_a2 ^= 1u << b;
-    return r;
+  // the epilogue wrote the A2 pairs of quarter q. Each of the two a2_full barriers completes
+  // twice per tile (quarters q and q + 2), so the phase parity is q / 2.
+  __device__ __forceinline__ bool a2(uint32_t u, uint32_t q, int code) {
+    return wait(&s.a2_full[(u + 1 + q) & 1], q >> 1, code);
   }
 
   __device__ void run() {
@@ -337,31 +327,23 @@ struct MmaLane {
     l1(0);
     for (uint32_t t = 0;; t++) {
       const uint32_t u = 5 * t;
-      const uint32_t d = t & 1;
-      if (!wait(&s.a1_full, t & 1, 14)) return;  // A1(t) written; slot of L1(t) consumed
-      if (t > 0 && !slot_consumed(u + 1)) return;  // previous use: quarter 3 of tile t-1
+      if (!wait(&s.a1_full, t & 1, 14)) return;
       l2(u + 1, 0);
       l2(u + 2, 1);
-      if (!a2(u + 1, 15)) return;
-      if (t >= 2 && !wait(&s.d3_free[d], ((t >> 1) - 1) & 1, 16)) return;
-      l3(u + 1, 0, d);
-      if (!slot_consumed(u + 3)) return;
+      if (!a2(u, 0, 15)) return;
+      if (t > 0 && !wait(&s.d3_free, (t - 1) & 1, 16)) return;
+      l3(0);
       l2(u + 3, 2);
-      if (!a2(u + 2, 17)) return;
-      l3(u + 2, 1, d);
-      if (!slot_consumed(u + 4)) return;
+      if (!a2(u, 1, 17)) return;
+      l3(1);
       l2(u + 4, 3);
-      if (!a2(u + 3, 18)) return;
-      l3(u + 3, 2, d);
-      // layer 1 of the next tile (or the end of the stream)
-      if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;
+      if (!a2(u, 2, 18)) return;
+      l3(2);
+      if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;  // the next tile's features, or the end
       const bool more = !*(volatile int*)&s.exit_flag;
-      if (more) {
-        if (!slot_consumed(u + 5)) return;
-        l1(u + 5);
-      }
-      if (!a2(u + 4, 20)) return;
-      l3(u + 4, 3, d);
+      if (more) l1(u + 5);
+      if (!a2(u, 3, 20)) return;
+      l3(3);
       mma_commit(&s.d3_full);
       if (!more) return;
     }
@@ -381,7 +363,7 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
 // ------------------------------------------------------------------ epilogue side
 // Warp w (0-15) reaches TMEM lanes 32 (w % 4) ..; the evaluation (row) e = 32 (w % 4) + lane is
 // handled by four threads (warps w % 4 + 4 p, p = 0..3), thread p owning columns 32p..32p+31
-// of every 128-column accumulator.
+// of every 128-column accumulator and packed columns 16p..16p+15 of A1 and of the A2 buffers.
 __device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
 __device__ __forceinline__ int epi_part() { return (threadIdx.x >> 7) & 3; }
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
@@ -410,12 +392,16 @@ __device__ __forceinline__ void write_features(uint32_t ta0, int p, float rx, fl
   }
 }
 
+// The tile engine seen from the epilogue threads. Tiles are retired one step late: step(t)
+// computes the network of tile t up to its layer-3 MMAs and hands the finished M of tile t-1 to
+// `use`, called between the layer-1 epilogue of tile t and its first quarter -- the time the
+// first layer-2 quarter of tile t spends on the tensor cores. finish() retires the last tile.
 struct Epi {
   Smem& s;
   int* err;
   uint32_t tl;  // TMEM base with this warp's lane field
   int p;
-  uint32_t tile = 0, par_d2 = 0;  // phase parity of d2_full per slot (bit s)
+  uint32_t tile = 0;
   bool ok = true;
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
@@ -424,7 +410,10 @@ struct Epi {
     if (ok) fence_after();
     return ok;
   }
+  // threads that receive M: parts 0 and 1 (both hold all nine entries)
+  __device__ __forceinline__ bool has_m() const { return p < 2; }
   __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tl + (u & 1 ? kOffS1 : kOffS0); }
+
   // features of the first tile (has = false: nothing to do at all)
   __device__ __forceinline__ void start(bool has, float rx, float ry, float rz) {
     if (has) {
@@ -436,10 +425,37 @@ struct Epi {
     fence_before();
     mbar_arrive(&s.a0_full);
   }
-  // Current tile: layer-1 epilogue (and the next tile's features, or the end of the stream),
-  // the four layer-2 quarters and layer 3 -> M (row-major 3x3) in threads of parts 0 and 1.
-  // Returns false if the CTA aborted. All 512 epilogue threads call it together.
-  __device__ __forceinline__ bool step(bool has_next, float nx, float ny, float nz, float rx, float ry, float rz, float (&M)[9]) {
+
+  // M (row-major 3x3) of the tile retired now, from D3 (parts 0 and 1 read it)
+  __device__ __forceinline__ bool read_d3(uint32_t t, float rx, float ry, float rz, float (&M)[9]) {
+    if (!wait(&s.d3_full, t & 1, 23)) return false;
+    if (p < 2) {
+      uint32_t v[32];
+      tmem_ld32(tl + kOffD3, v);
+      tmem_wait_ld();
+      const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
+      const float inv = __frcp_rn(nr);
+#pragma unroll
+      for (int o = 0; o < 9; o++) {
+        float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + s.b3[o];
+        const bool dg = (o == 0 || o == 4 || o == 8);
+        if (dg) y += 1.0f;
+        y = y * inv;
+        if (nr < 1e-5f) y = dg ? 1.0f : 0.0f;
+        M[o] = y;
+      }
+    }
+    fence_before();
+    mbar_arrive(&s.d3_free);
+    return true;
+  }
+
+  // Tile `tile`: layer-1 epilogue (and the next tile's features, or the end of the stream),
+  // retirement of the previous tile (use(M) with its features (px, py, pz)), then the four
+  // layer-2 quarters. Returns false if the CTA aborted. All 512 epilogue threads call it.
+  template <class Use>
+  __device__ __forceinline__ bool step(bool has_next, float nx, float ny, float nz, float px, float py, float pz,
+                                       Use&& use) {
     const uint32_t u = 5 * tile;
     if (!wait(&s.d1_full, tile & 1, 21)) return false;
     // A0 was consumed by L1(tile): the next tile's features (or the end of the stream)
@@ -456,20 +472,24 @@ struct Epi {
       tmem_ld32(slot(u) + 32 * p, v);
       tmem_wait_ld();
 #pragma unroll
-      for (int k = 0; k < 16; k++) out[k] = tanh_bf16x2(pack_bf16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
+      for (int k = 0; k < 16; k++)
+        out[k] = tanh_bf16x2(pack_bf16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
       tmem_st16(tl + kOffA1 + 16 * p, out);
       tmem_wait_st();
     }
     fence_before();
     mbar_arrive(&s.a1_full);
+    if (tile > 0) {  // retire the previous tile while L2(tile, 0) runs on the tensor cores
+      float M[9];
+      if (!read_d3(tile - 1, px, py, pz, M)) return false;
+      use(M);
+    }
     for (uint32_t q = 0; q < 4; q++) {
+      // each d2 / a2_full barrier completes twice per tile (quarters q and q + 2): parity q / 2
       const uint32_t sl = (u + 1 + q) & 1;
-      const bool got = wait(&s.d2_full[sl], (par_d2 >> sl) & 1, 22);
-      par_d2 ^= 1u << sl;
-      if (!got) return false;
-      const uint32_t col = slot(u + 1 + q) + 32 * p;
+      if (!wait(&s.d2_full[sl], q >> 1, 22)) return false;
       uint32_t v[32], out[16];
-      tmem_ld32(col, v);
+      tmem_ld32(slot(u + 1 + q) + 32 * p, v);
       tmem_wait_ld();
       const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
 #pragma unroll
@@ -479,32 +499,25 @@ struct Epi {
         out[2 * k + 1] =
             tanh_bf16x2(pack_bf16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
       }
-      tmem_st16(col, out);  // inside the columns this thread read itself
+      // A2 buffer q % 2 was last read by L3 of quarter q - 2 (this tile, first commit on its
+      // barrier: parity 0) or of quarter q + 2 of the previous tile (second commit: parity 1)
+      if ((tile > 0 || q >= 2) && !wait(&s.a2_free[q & 1], q >= 2 ? 0u : 1u, 24)) return false;
+      tmem_st16(tl + (q & 1 ? kOffA2b : kOffA2a) + 16 * p, out);
       tmem_wait_st();
       fence_before();
       mbar_arrive(&s.a2_full[sl]);
     }
-    if (!wait(&s.d3_full, tile & 1, 23)) return false;
-    const uint32_t d3 = tl + (tile & 1 ? kOffD3b : kOffD3a);
-    if (p < 2) {
-      uint32_t v[32];
-      tmem_ld32(d3, v);
-      tmem_wait_ld();
-      const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
-      const float inv = __frcp_rn(nr);
-#pragma unroll
-      for (int o = 0; o < 9; o++) {
-        float y = __uint_as_float(v[o]) + __uint_as_float(v[16 + o]) + s.b3[o];
-        const bool dg = (o == 0 || o == 4 || o == 8);
-        if (dg) y += 1.0f;
-        y = y * inv;
-        if (nr < 1e-5f) y = dg ? 1.0f : 0.0f;
-        M[o] = y;
-      }
-    }
-    fence_before();
-    mbar_arrive(&s.d3_free[tile & 1]);
     tile++;
+    return true;
+  }
+
+  // Retires the last tile (features px, py, pz) after its final step.
+  template <class Use>
+  __device__ __forceinline__ bool finish(float px, float py, float pz, Use&& use) {
+    if (tile == 0) return true;
+    float M[9];
+    if (!read_d3(tile - 1, px, py, pz, M)) return false;
+    use(M);
     return true;
   }
 };

@@ -44,7 +44,8 @@ enum hignn_param {
   HIGNN_P_USE_SYMMETRY = 7,               /* J >= I lists + transposed update, default 1 */
   HIGNN_P_MAX_FAR_FIELD_DISTANCE = 8,     /* stored, unused (as in the reference)       */
   /* keys of this implementation */
-  HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field */
+  HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field;
+                                    1 and 2 need block_size <= 128                               */
   HIGNN_P_FAR_BATCH_ROWS = 101,  /* max rows (sum of |I|+|J|) per ACA batch, default 1<<26   */
   HIGNN_P_TIMING = 102,          /* 1 = record per-phase CUDA-event times in hignn_stats     */
   HIGNN_P_STUDENT_TOL = 103,     /* student fallback: a far block whose 64 sampled entries differ from
