@@ -267,10 +267,13 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
 // One thread issues every MMA, per tile t (u = 5t; accumulator slot of a use = u & 1; A2 buffer
 // of quarter q = q & 1), in this order:
 //   L2(t,0)->slot(u+1)  L2(t,1)->slot(u+2)          after a1_full(t): A1 written, L1 slot read
-//   L3(t,0)<-A2[0]  L2(t,2)->slot(u+3)               after a2(q0): slot(u+1) read, A2[0] written
-//   L3(t,1)<-A2[1]  L2(t,3)->slot(u+4)               after a2(q1)
-//   L3(t,2)<-A2[0]  L1(t+1)->slot(u+5)               after a2(q2) and a0_full(t+1)
+//   L2(t,2)->slot(u+3)  L3(t,0)<-A2[0]               after a2(q0): slot(u+1) read, A2[0] written
+//   L2(t,3)->slot(u+4)  L3(t,1)<-A2[1]               after a2(q1)
+//   L1(t+1)->slot(u+5)  L3(t,2)<-A2[0]               after a2(q2) and a0_full(t+1)
 //   L3(t,3)<-A2[1]  commit d3_full                   after a2(q3)
+// Every MMA holds the tensor pipe >= ~64 cycles whatever its N, so the eight layer-3 MMAs of a
+// quarter cost as much as its eight layer-2 MMAs; the accumulator the epilogue waits for next
+// is therefore queued ahead of the layer-3 MMAs, whose result is needed only at retirement.
 // An accumulator slot is reused as soon as the epilogue has read it (its tanh'd pairs go to a
 // separate A2 buffer), so the lane never waits for an MMA of its own: the ~500-cycle latency
 // from an MMA's issue to its commit reaching a waiting thread is paid only by threads that have
@@ -331,17 +334,17 @@ struct MmaLane {
       l2(u + 1, 0);
       l2(u + 2, 1);
       if (!a2(u, 0, 15)) return;
+      l2(u + 3, 2);  // the next accumulator first: the epilogue waits for it, D3 only at retirement
       if (t > 0 && !wait(&s.d3_free, (t - 1) & 1, 16)) return;
       l3(0);
-      l2(u + 3, 2);
       if (!a2(u, 1, 17)) return;
-      l3(1);
       l2(u + 4, 3);
+      l3(1);
       if (!a2(u, 2, 18)) return;
-      l3(2);
       if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;  // the next tile's features, or the end
       const bool more = !*(volatile int*)&s.exit_flag;
       if (more) l1(u + 5);
+      l3(2);
       if (!a2(u, 3, 20)) return;
       l3(3);
       mma_commit(&s.d3_full);

@@ -2,7 +2,7 @@
 // f32, f16x2 and bf16x2 forms, conversions, integer and FP adds), eight independent chains per
 // thread, 2 CTAs x 1024 threads per SM, clock64 per CTA. Build and run on a B200:
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -o instruction_rates \
-//        hignn_b200/probes/instruction_rates.cu && ./instruction_rates
+//        hignn_b200/probes/instruction_rates.cu && ./instruction_rates [occupancy]
 #include <cstdio>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -59,7 +59,16 @@ void run(const char* name, int blocks_per_sm, int threads) {
   printf("%-28s err=%d  cycles=%lld  lane-ops/clk/SM=%.2f\n", name, (int)e, mx, ops_per_sm / mx);
   cudaFree(out); cudaFree(cyc); delete[] h;
 }
-int main() {
+int main(int argc, char** argv) {
+  if (argc > 1) {  // occupancy sweep of the packed tanh: lanes/clk/SM with fewer resident warps
+    run<1>("tanh.approx.bf16x2 1x128", 1, 128);
+    run<1>("tanh.approx.bf16x2 1x256", 1, 256);
+    run<1>("tanh.approx.bf16x2 1x512", 1, 512);
+    run<1>("tanh.approx.bf16x2 1x1024", 1, 1024);
+    run<8>("cvt+tanh 1x512", 1, 512);
+    run<2>("tanh.approx.f32 1x512", 1, 512);
+    return 0;
+  }
   run<5>("fadd.f32", 2, 1024);
   run<0>("cvt.rn.bf16x2.f32", 2, 1024);
   run<14>("cvt.rn.satfinite.bf16x2", 2, 1024);
