@@ -316,6 +316,14 @@ def main():
     st = m.stats()
     ms = max_over_ranks(float(np.mean(times)))
     value = n / (ms / 1e3)
+    # one more (untimed) matvec with CUDA events around every far-field launch: the far breakdown
+    m.set(capi.P_TIMING, 2)
+    step_device(u_d)
+    sb = m.stats()
+    m.set(capi.P_TIMING, 1)
+    far_breakdown = {"queries": sb["t_far_query_ms"], "pivots_and_apply": sb["t_far_pivot_ms"],
+                     "active_lists": sb["t_far_active_ms"], "student_check": sb["t_far_check_ms"],
+                     "total": sb["t_far_ms"], "note": "one untimed matvec with an event around every launch"}
 
     # end to end through the public C ABI from pinned host memory (H2D + matvec + D2H per step)
     if args.no_e2e:
@@ -388,7 +396,7 @@ def main():
         "plain_fp32": plain,
         "student": student,
         "breakdown_ms": {"near": float(np.mean(near_ms)), "far": float(np.mean(far_ms)),
-                         "build_host": st0["t_build_ms"]},
+                         "build_host": st0["t_build_ms"], "far_by_kernel": far_breakdown},
         "work": {"close_pairs": st["num_close"], "far_pairs": st["num_far"], "close_evals": st["close_evals"],
                  "far_evals": st["far_evals"], "far_rank_mean": st["far_rank_sum"] / max(1, st["num_far"]),
                  "far_rank_max": st["far_rank_max"], "far_iterations": st["far_iterations"],

@@ -35,6 +35,7 @@ CU_SOURCES = {
     "tc_kernels.cu": [],
     "noalloc.cu": [],
     "student.cu": [],
+    "step.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

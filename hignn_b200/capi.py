@@ -49,7 +49,8 @@ class HignnStats(C.Structure):
         ("num_far", C.c_int64), ("close_evals", C.c_int64), ("far_evals", C.c_int64), ("far_rank_sum", C.c_int64),
         ("far_rank_max", C.c_int32), ("far_iterations", C.c_int32), ("student_fallback_blocks", C.c_int64),
         ("t_build_ms", C.c_double), ("t_close_ms", C.c_double), ("t_far_ms", C.c_double), ("t_dot_ms", C.c_double),
-        ("gpu_launches", C.c_int64),
+        ("gpu_launches", C.c_int64), ("t_far_query_ms", C.c_double), ("t_far_pivot_ms", C.c_double),
+        ("t_far_active_ms", C.c_double), ("t_far_check_ms", C.c_double),
     ]
 
     def as_dict(self):
@@ -86,6 +87,10 @@ SIGNATURES = {
     "hignn_student_eval": ([_P, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "hignn_student_grad": ([_P, C.c_void_p, C.c_void_p, C.c_int64, _fp, _dp], C.c_int),
     "hignn_set_shard": ([_P, C.c_int, C.c_int], C.c_int),
+    "hignn_update_coord_keep_tree": ([_P, _fp, C.c_int64], C.c_int),
+    "hignn_pair_forces": ([_P, _fp, _fp, C.c_int64, _fp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
+    "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, _fp, C.c_double, C.c_double, C.c_double,
+                         C.c_double], C.c_int),
     "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
@@ -230,6 +235,28 @@ class Model:
         check(lib.hignn_get_lists(self._h, ci.ctypes.data_as(_i64p), cj.ctypes.data_as(_i64p),
                                   fi.ctypes.data_as(_i64p), fj.ctypes.data_as(_i64p)))
         return ci, cj, fi, fj
+
+    def update_coord_keep_tree(self, x):
+        """New positions on the existing cluster tree (lists and ACA plan kept)."""
+        x = np.ascontiguousarray(x, np.float32)
+        check(lib.hignn_update_coord_keep_tree(self._h, fptr(x), len(x)))
+
+    def pair_forces(self, x, gravity=(0.0, 0.0, 0.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
+        """gravity + Morse pair forces of positions x (n, 3) on the device."""
+        x = np.ascontiguousarray(x, np.float32)
+        f = np.empty_like(x)
+        g = np.ascontiguousarray(gravity, np.float32)
+        check(lib.hignn_pair_forces(self._h, fptr(x), fptr(f), len(x), fptr(g), float(De), float(a), float(re),
+                                    float(cutoff)))
+        return f
+
+    def run_euler(self, x, steps, dt, rebuild_every=1, gravity=(0.0, 0.0, -1.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
+        """Explicit Euler on the device; returns the final positions."""
+        x = np.array(x, np.float32, copy=True)
+        g = np.ascontiguousarray(gravity, np.float32)
+        check(lib.hignn_run_euler(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every), fptr(g),
+                                  float(De), float(a), float(re), float(cutoff)))
+        return x
 
     def set_shard(self, rank, world):
         """Compute only shard `rank` of `world` of the block lists; dot then returns partial velocities."""

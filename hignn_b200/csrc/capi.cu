@@ -51,26 +51,7 @@ int guard(F&& f) {
   }
 }
 
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  void ensure(size_t b) {
-    if (b <= bytes && p) return;
-    release();
-    if (b == 0) return;
-    HIGNN_CUDA(cudaMalloc(&p, b));
-    bytes = b;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  template <class T>
-  T* as() const {
-    return reinterpret_cast<T*>(p);
-  }
-};
+using hignn::DevBuf;
 
 int host_threads() {
   int n = 8;
@@ -102,7 +83,8 @@ struct hignn_model {
   int shard_rank = 0, shard_world = 1;
   int64_t sh_c0 = 0, sh_c1 = 0, sh_f0 = 0, sh_f1 = 0;
   bool shard_ready = false;
-  bool timing = false;
+  int timing = 0;
+  hignn::FarTimer far_timer;
   double student_tol = 1e-3;
   int fields = 3;
   bool record_pivots = false;
@@ -127,6 +109,7 @@ struct hignn_model {
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
+  hignn::CellList cells;  // neighbour search of the pair forces
   int32_t* host_ctr = nullptr;
 
   // far-field plan: blocks in batch order; iters > 0 when every block's rank is known
@@ -574,8 +557,9 @@ FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& p
     const auto& last = plan[bt.b1 - 1];
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
+    hignn::FarTimer* tm = m->timing >= 2 ? &m->far_timer : nullptr;
     const int nd = hignn::far_batch_plain(a, w, m->precision >= 1 ? &tcw : nullptr, student, m->err_flag(),
-                                          m->num_sms, m->host_ctr, m->stream, bt.iters, iterations);
+                                          m->num_sms, m->host_ctr, m->stream, bt.iters, iterations, tm);
     m->stats.far_rank_max = std::max(m->stats.far_rank_max, m->host_ctr[hignn::kCtrRankMax]);
     m->stats.gpu_launches += 1;
     const int nb = bt.b1 - bt.b0, ld = a.ldr;
@@ -589,8 +573,16 @@ FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& p
       // block is sent back to the teacher when the student's sampled error exceeds the accuracy
       // the ACA block is held to anyway: the larger of student_tol and epsilon.
       const float tol = (float)std::max(m->student_tol, m->epsilon);
+      if (tm) HIGNN_CUDA(cudaEventRecord(m->ev[3], m->stream));
       nfail = hignn::far_student_check(a, tcw, student, tol, feat, feat + 3 * ns, feat + 12 * ns,
                                        reinterpret_cast<int*>(feat + 21 * ns), m->err_flag(), m->num_sms, m->stream);
+      if (tm) {  // far_student_check synchronised the stream
+        HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
+        HIGNN_CUDA(cudaEventSynchronize(m->ev[2]));
+        float ms = 0;
+        HIGNN_CUDA(cudaEventElapsedTime(&ms, m->ev[3], m->ev[2]));
+        m->stats.t_far_check_ms += ms;
+      }
       m->stats.student_fallback_blocks += nfail;
       m->stats.gpu_launches += 5;
     }
@@ -656,6 +648,8 @@ void far_field(hignn_model* m) {
   }
   HIGNN_CUDA(cudaMemsetAsync(m->far_stats.p, 0, sizeof(unsigned long long) * 4, m->stream));
   m->stats.student_fallback_blocks = 0;
+  m->stats.t_far_query_ms = m->stats.t_far_pivot_ms = m->stats.t_far_active_ms = m->stats.t_far_check_ms = 0;
+  m->far_timer.active_ms = m->far_timer.query_ms = m->far_timer.pivot_ms = 0;
   int iterations = 0;
   const bool student_pass = m->precision == 2 && m->has_student;
   FarOutcome res =
@@ -679,6 +673,9 @@ void far_field(hignn_model* m) {
   m->stats.far_rank_sum = (int64_t)st[0];
   m->stats.far_evals = (int64_t)st[1];
   m->stats.far_iterations = iterations;
+  m->stats.t_far_query_ms = m->far_timer.query_ms;
+  m->stats.t_far_pivot_ms = m->far_timer.pivot_ms;
+  m->stats.t_far_active_ms = m->far_timer.active_ms;
   // per ACA iteration: active list, column eval, column pivot, row eval, row pivot
   m->stats.gpu_launches += 5 * (int64_t)iterations;
   if (!m->plan_hinted || had_deferred) {  // record the ranks for the next far field on this tree
@@ -734,6 +731,37 @@ void matvec_tree_order(hignn_model* m) {
 }
 
 void post_check(hignn_model* m);
+
+// New positions (m->xyz, caller order) on the existing tree: x4 and the tree-order host copy are
+// refreshed, the tree, the lists and the ACA plan are kept.
+void refit_positions(hignn_model* m) {
+  const int64_t n = m->n;
+  std::vector<float4> x4(n);
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t p = m->tree.perm[i];
+    m->xt[3 * i] = m->xyz[3 * p];
+    m->xt[3 * i + 1] = m->xyz[3 * p + 1];
+    m->xt[3 * i + 2] = m->xyz[3 * p + 2];
+    x4[i] = make_float4(m->xt[3 * i], m->xt[3 * i + 1], m->xt[3 * i + 2], 0.f);
+  }
+  if (m->device < 0) return;
+  HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+}
+
+// Current device positions (tree order) back into m->xyz (caller order) and m->xt.
+void download_positions(hignn_model* m) {
+  const int64_t n = m->n;
+  std::vector<float4> x4(n);
+  HIGNN_CUDA(cudaMemcpyAsync(x4.data(), m->x4.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t p = m->tree.perm[i];
+    m->xyz[3 * p] = m->xt[3 * i] = x4[i].x;
+    m->xyz[3 * p + 1] = m->xt[3 * i + 1] = x4[i].y;
+    m->xyz[3 * p + 2] = m->xt[3 * i + 2] = x4[i].z;
+  }
+}
 
 void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
   m->stats.gpu_launches = 2;  // gather + scatter
@@ -985,7 +1013,7 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         m->far_pool_bytes = (int64_t)(v * 1048576.0);
         break;
       case HIGNN_P_RANK_HINT_OFFSET: m->rank_hint_offset = (int)v; break;
-      case HIGNN_P_TIMING: m->timing = v != 0; break;
+      case HIGNN_P_TIMING: m->timing = (int)v; break;
       case HIGNN_P_STUDENT_TOL: m->student_tol = v; break;
       case HIGNN_P_FIELDS:
         if (v < 0 || v > 3) throw Error(HIGNN_ERR_ARG, "fields must be in [0, 3]");
@@ -1033,6 +1061,79 @@ int hignn_update_coord(hignn_model* m, const float* xyz, int64_t n) {
       if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
     m->xyz.assign(xyz, xyz + 3 * n);
     build_structures(m);
+  });
+}
+
+int hignn_update_coord_keep_tree(hignn_model* m, const float* xyz, int64_t n) {
+  return guard([&] {
+    if (!m || !xyz) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n)
+      throw Error(HIGNN_ERR_ARG, "update_coord_keep_tree: expected " + std::to_string(m->n) + " particles, got " +
+                                     std::to_string(n));
+    for (int64_t i = 0; i < 3 * n; i++)
+      if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+    ensure_tree(m);
+    m->xyz.assign(xyz, xyz + 3 * n);
+    refit_positions(m);
+  });
+}
+
+int hignn_pair_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const float* gravity, double De,
+                      double a, double re, double cutoff) {
+  return guard([&] {
+    if (!m || !xyz || !f) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n <= 0) throw Error(HIGNN_ERR_ARG, "pair_forces: n must be positive");
+    if (cutoff < 0) throw Error(HIGNN_ERR_ARG, "pair_forces: cutoff must be >= 0");
+    require_device(m);
+    m->tmp_x.ensure(sizeof(float4) * n);
+    m->io_f.ensure(sizeof(float) * 3 * n);
+    m->io_u.ensure(sizeof(float) * 3 * n);
+    HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, m->stream));
+    hignn::launch_pack_positions(m->io_f.as<float>(), n, m->tmp_x.as<float4>(), m->stream);
+    const hignn::MorseParams mp{(float)De, (float)a, (float)re, cutoff};
+    if (cutoff > 0) m->cells.build(m->tmp_x.as<float4>(), n, cutoff, m->stream);
+    const float3 g = gravity ? make_float3(gravity[0], gravity[1], gravity[2]) : make_float3(0.f, 0.f, 0.f);
+    hignn::launch_morse(m->tmp_x.as<float4>(), n, m->cells, mp, g, nullptr, m->io_u.as<float>(), m->stream);
+    HIGNN_CUDA(cudaMemcpyAsync(f, m->io_u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+                    const float* gravity, double De, double a, double re, double cutoff) {
+  return guard([&] {
+    if (!m || !xyz) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n) throw Error(HIGNN_ERR_ARG, "run_euler: particle count differs from the model's");
+    if (steps < 0 || !(dt > 0) || rebuild_every < 0 || cutoff < 0)
+      throw Error(HIGNN_ERR_ARG, "run_euler: need steps >= 0, dt > 0, rebuild_every >= 0, cutoff >= 0");
+    require_device(m);
+    require_weights(m);
+    require_student_if_needed(m);
+    if (m->shard_world != 1)
+      throw Error(HIGNN_ERR_STATE, "run_euler needs the whole product (shard world 1): a sharded step would "
+                                   "need the all-reduce of u between the matvec and the update");
+    for (int64_t i = 0; i < 3 * n; i++)
+      if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+    // start from xyz with a tree built for it
+    m->xyz.assign(xyz, xyz + 3 * n);
+    build_structures(m);
+    const hignn::MorseParams mp{(float)De, (float)a, (float)re, cutoff};
+    const float3 g = gravity ? make_float3(gravity[0], gravity[1], gravity[2]) : make_float3(0.f, 0.f, 0.f);
+    for (int s = 0; s < steps; s++) {
+      if (s > 0 && rebuild_every > 0 && s % rebuild_every == 0) {
+        download_positions(m);  // m->xyz <- current positions
+        build_structures(m);
+      }
+      // forces at the current positions, in tree order, straight into the matvec's input
+      if (cutoff > 0) m->cells.build(m->x4.as<float4>(), n, cutoff, m->stream);
+      hignn::launch_morse(m->x4.as<float4>(), n, m->cells, mp, g, m->f4.as<float4>(), nullptr, m->stream);
+      HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
+      matvec_tree_order(m);
+      hignn::launch_advance(m->x4.as<float4>(), m->u.as<double>(), n, (float)dt, m->stream);
+      if (m->precision >= 1) check_device_error(m);
+    }
+    download_positions(m);
+    std::copy(m->xyz.begin(), m->xyz.end(), xyz);
   });
 }
 

@@ -24,6 +24,28 @@ struct Error : std::runtime_error {
 
 #define HIGNN_CHECK_LAUNCH() HIGNN_CUDA(cudaGetLastError())
 
+// Device allocation owned by the model (grown on demand, never shrunk; contents not kept).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t b) {
+    if (b <= bytes && p) return;
+    release();
+    if (b == 0) return;
+    HIGNN_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
 constexpr int kMaxLeaf = 256;   // largest leaf the near-field kernels stage in shared memory
 constexpr int kTcMaxLeaf = 128; // largest leaf of the tensor-core near field (three staging buffers)
 constexpr int kH1 = 128;        // two-body network widths (python/convert.py:6-20 over nn/*.pkl)

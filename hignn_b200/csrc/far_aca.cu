@@ -637,8 +637,38 @@ __global__ void k_far_check(FarArgs a, const float* __restrict__ yt, const float
 
 }  // namespace
 
+cudaEvent_t FarTimer::next() {
+  if (used == ev.size()) {
+    cudaEvent_t e;
+    HIGNN_CUDA(cudaEventCreate(&e));
+    ev.push_back(e);
+  }
+  return ev[used++];
+}
+
+// events are recorded in groups of six per iteration: before the active list, after it, after
+// the column query, after the column pivot, after the row query, after the row pivot
+void FarTimer::collect() {
+  for (size_t g = 0; g + 6 <= used; g += 6) {
+    float t[5];
+    for (int q = 0; q < 5; q++) HIGNN_CUDA(cudaEventElapsedTime(&t[q], ev[g + q], ev[g + q + 1]));
+    active_ms += t[0];
+    query_ms += t[1] + t[3];
+    pivot_ms += t[2] + t[4];
+  }
+  used = 0;
+}
+
+FarTimer::~FarTimer() {
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
 int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
-                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations) {
+                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations,
+                    FarTimer* timer) {
+  auto mark = [&]() {
+    if (timer) HIGNN_CUDA(cudaEventRecord(timer->next(), s));
+  };
   if (a.nb <= 0) return 0;
   const size_t eval_smem = sizeof(EvalSmem);
   const size_t row_smem = sizeof(double) * (9 + 3 + 3) * a.ldr;
@@ -658,25 +688,32 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
   while (it < limit && !finished) {
     const int span = known_iters > 0 ? limit : (it + kCheck < limit ? kCheck : limit - it);
     for (int q = 0; q < span; q++, it++) {
+      mark();
       k_far_active<<<1, 1024, 0, s>>>(a);
+      mark();
       if (student)
         launch_far_student(a, student, 0, num_sms, s);
       else if (tcw)
         launch_far_tc(a, *tcw, 0, err, num_sms, s);
       else
         k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
+      mark();
       k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
+      mark();
       if (student)
         launch_far_student(a, student, 1, num_sms, s);
       else if (tcw)
         launch_far_tc(a, *tcw, 1, err, num_sms, s);
       else
         k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
+      mark();
       k_far_row_pivot<<<piv_grid, kPivThreads, row_smem, s>>>(a);
+      mark();
       HIGNN_CHECK_LAUNCH();
     }
     HIGNN_CUDA(cudaMemcpyAsync(host_ctr, a.ctr, sizeof(int32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
     HIGNN_CUDA(cudaStreamSynchronize(s));
+    if (timer) timer->collect();
     if (host_ctr[kCtrError] != 0)
       throw Error(-5, "ACA: pivot search found no unused row/column (non-finite block entries?)");
     finished = host_ctr[kCtrRemaining] == 0;

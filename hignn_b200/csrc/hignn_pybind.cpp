@@ -87,6 +87,14 @@ class HignnModel {
     py::gil_scoped_release nogil;
     check(hignn_update_coord(m_, p, n_));
   }
+  // addition: new positions on the kept tree (a simulation that rebuilds every k steps)
+  void update_coord_keep_tree(py::array coord) {
+    farr x = as_n3(coord, "coord");
+    if (x.shape(0) != n_) throw std::invalid_argument("update_coord_keep_tree: particle count changed");
+    const float* p = x.data();
+    py::gil_scoped_release nogil;
+    check(hignn_update_coord_keep_tree(m_, p, n_));
+  }
   void dot(py::array uArray, py::array fArray) { run(uArray, fArray, false); }
   void dense_dot(py::array uArray, py::array fArray) { run(uArray, fArray, true); }
   py::dict stats() {
@@ -328,6 +336,51 @@ class ExplicitRk4 : public TimeIntegrator {
   double thr_ = 1e-3;
 };
 
+// PotentialForce (include/PotentialForce.hpp, bound at interface/HignnInterface.cpp:66-71):
+// Morse pair forces of every particle from its neighbours within the two-body epsilon, here on
+// the device (cell list) through hignn_pair_forces. The reference hard-codes De = 1, a = 1,
+// re = 2.5; set_parameters changes them (an addition). Periodic images are not implemented:
+// set_periodic(True) / set_domain raise.
+class PotentialForce {
+ public:
+  PotentialForce() {
+    const float origin[3] = {0.f, 0.f, 0.f};
+    check(hignn_create(origin, 1, 128, default_device(), &m_));  // device context and buffers only
+  }
+  ~PotentialForce() {
+    if (m_) hignn_destroy(m_);
+  }
+  void set_periodic(bool periodic) {
+    if (periodic) throw std::runtime_error("hignn: periodic pair forces are not supported by hignn_b200");
+  }
+  void set_domain(py::array) {
+    throw std::runtime_error("hignn: periodic pair forces are not supported by hignn_b200");
+  }
+  void set_two_body_epsilon(float eps) { eps_ = eps; }
+  void set_parameters(double De, double a, double re) {
+    De_ = De;
+    a_ = a;
+    re_ = re;
+  }
+  py::array_t<float> get_potential_force(py::array coord) {
+    farr x = as_n3(coord, "coord");
+    const int64_t n = x.shape(0);
+    py::array_t<float> f({(py::ssize_t)n, (py::ssize_t)3});
+    float* fp = f.mutable_data();
+    const float* xp = x.data();
+    {
+      py::gil_scoped_release nogil;
+      check(hignn_pair_forces(m_, xp, fp, n, nullptr, De_, a_, re_, eps_));
+    }
+    return f;
+  }
+
+ private:
+  hignn_model* m_ = nullptr;
+  double De_ = 1.0, a_ = 1.0, re_ = 2.5;
+  float eps_ = 0.f;
+};
+
 }  // namespace
 
 PYBIND11_MODULE(hignn, m) {
@@ -353,9 +406,18 @@ PYBIND11_MODULE(hignn, m) {
       .def("set_param", &HignnModel::set)
       .def("get_param", &HignnModel::get)
       .def("update_coord", &HignnModel::update_coord)
+      .def("update_coord_keep_tree", &HignnModel::update_coord_keep_tree)
       .def("dot", &HignnModel::dot)
       .def("dense_dot", &HignnModel::dense_dot)
       .def("stats", &HignnModel::stats);
+
+  py::class_<PotentialForce>(m, "PotentialForce")
+      .def(py::init())
+      .def("set_periodic", &PotentialForce::set_periodic, py::arg("isPeriodicBoundary") = false)
+      .def("set_domain", &PotentialForce::set_domain)
+      .def("set_two_body_epsilon", &PotentialForce::set_two_body_epsilon)
+      .def("set_parameters", &PotentialForce::set_parameters)
+      .def("get_potential_force", &PotentialForce::get_potential_force);
 
   py::class_<ExplicitEuler>(m, "ExplicitEuler")
       .def(py::init())

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "common.h"
 
@@ -86,8 +87,20 @@ constexpr int kFarSamples = 64;  // sampled entries per block in the student res
 // every block stops (converges or is deferred) within that many iterations, so they are
 // launched without reading the counters back in between; 0: counters are read every
 // few iterations. Returns the number of deferred blocks.
+// Optional per-category timing of a batch: CUDA events around every launch, summed after the
+// batch (milliseconds added to the four totals).
+struct FarTimer {
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  double active_ms = 0, query_ms = 0, pivot_ms = 0;
+  cudaEvent_t next();  // records nothing; returns a fresh event from the pool
+  void collect();      // sums the recorded batch (after the stream has synchronised)
+  ~FarTimer();
+};
+
 int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
-                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations);
+                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations,
+                    FarTimer* timer = nullptr);
 
 // Student residual check of a finished batch run with defer_apply = 1: kFarSamples entries per
 // converged block are evaluated by the student and by the teacher (tensor cores); blocks whose
@@ -113,6 +126,40 @@ void launch_far_student(const FarArgs& a, const float* params, int which, int nu
 void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, int* err, int num_sms, cudaStream_t s);
 void launch_far_tc(const FarArgs& a, const TcWeights& w, int which, int* err, int num_sms, cudaStream_t s);
 void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int* err, int num_sms, cudaStream_t s);
+
+// ---------------------------------------------------------------- time step (step.cu)
+struct CellGrid {
+  float3 lo;
+  float inv;  // 1 / cell size
+  int nx, ny, nz, ncell;
+};
+
+// Morse pair force parameters (include/PotentialForce.hpp:115-140 hard-codes De = 1, a = 1,
+// re = 2.5); cutoff = radius of the neighbour search (0: no pair forces).
+struct MorseParams {
+  float De, a, re;
+  double cutoff;
+};
+
+constexpr int kMaxCells = 16 * 1024 * 1024;
+
+// Uniform grid of cells no smaller than the cutoff over the positions' bounding box; items lists
+// the positions cell by cell (start[c] .. start[c + 1]).
+struct CellList {
+  CellGrid grid{};
+  DevBuf box, cell, items, count, start, sums;
+  void build(const float4* x, int64_t n, double cutoff, cudaStream_t s);
+};
+
+// f = gravity + Morse forces of every position (f4 and / or f3 (n, 3); either may be null).
+void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorseParams& mp, float3 grav, float4* f4,
+                  float* f3, cudaStream_t s);
+// Neighbours j != i within the cutoff (the reference's radius-search test): per-particle counts
+// (out null) or the sorted lists at out[off[i] ..].
+void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int* count, const int64_t* off,
+                       int* out, cudaStream_t s);
+void launch_advance(float4* x, const double* u, int64_t n, float dt, cudaStream_t s);
+void launch_pack_positions(const float* xyz, int64_t n, float4* x4, cudaStream_t s);
 
 // ---------------------------------------------------------------- reorder / misc
 void launch_gather_forces(const float* f, const int32_t* perm, float4* f4, double* u, int64_t n, cudaStream_t s);

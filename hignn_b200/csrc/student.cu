@@ -70,18 +70,34 @@ __device__ __forceinline__ void student_forward(const float* __restrict__ p, flo
     const float z = fmaf(p[kOffW1 + 3 * k + 2], x2, fmaf(p[kOffW1 + 3 * k + 1], x1, fmaf(p[kOffW1 + 3 * k], x0, p[kOffB1 + k])));
     h1[k] = silu_fast(z);
   }
+  // rows of W2, W3, W4 start on 16-byte boundaries (offsets 128, 1184, 2240 floats): one
+  // 128-bit shared-memory broadcast feeds four FMAs
 #pragma unroll
   for (int k = 0; k < kS; k++) {
     float z = p[kOffB2 + k];
+    const float4* w = reinterpret_cast<const float4*>(p + kOffW2 + kS * k);
 #pragma unroll
-    for (int m = 0; m < kS; m++) z = fmaf(p[kOffW2 + kS * k + m], h1[m], z);
+    for (int m = 0; m < kS / 4; m++) {
+      const float4 wv = w[m];
+      z = fmaf(wv.x, h1[4 * m], z);
+      z = fmaf(wv.y, h1[4 * m + 1], z);
+      z = fmaf(wv.z, h1[4 * m + 2], z);
+      z = fmaf(wv.w, h1[4 * m + 3], z);
+    }
     h2[k] = silu_fast(z);
   }
 #pragma unroll
   for (int k = 0; k < kS; k++) {
     float z = p[kOffB3 + k];
+    const float4* w = reinterpret_cast<const float4*>(p + kOffW3 + kS * k);
 #pragma unroll
-    for (int m = 0; m < kS; m++) z = fmaf(p[kOffW3 + kS * k + m], h2[m], z);
+    for (int m = 0; m < kS / 4; m++) {
+      const float4 wv = w[m];
+      z = fmaf(wv.x, h2[4 * m], z);
+      z = fmaf(wv.y, h2[4 * m + 1], z);
+      z = fmaf(wv.z, h2[4 * m + 2], z);
+      z = fmaf(wv.w, h2[4 * m + 3], z);
+    }
     h1[k] = silu_fast(z);  // h3
   }
   float y[9];
@@ -89,8 +105,15 @@ __device__ __forceinline__ void student_forward(const float* __restrict__ p, flo
 #pragma unroll
   for (int o = 0; o < 9; o++) {
     float z = p[kOffB4 + o];
+    const float4* w = reinterpret_cast<const float4*>(p + kOffW4 + kS * o);
 #pragma unroll
-    for (int m = 0; m < kS; m++) z = fmaf(p[kOffW4 + kS * o + m], h1[m], z);
+    for (int m = 0; m < kS / 4; m++) {
+      const float4 wv = w[m];
+      z = fmaf(wv.x, h1[4 * m], z);
+      z = fmaf(wv.y, h1[4 * m + 1], z);
+      z = fmaf(wv.z, h1[4 * m + 2], z);
+      z = fmaf(wv.w, h1[4 * m + 3], z);
+    }
     y[o] += z;
   }
 #pragma unroll
@@ -298,7 +321,7 @@ __global__ void k_student_adam(float* __restrict__ p, const float* __restrict__ 
 
 __global__ void k_student_eval(const float* __restrict__ params, const float* __restrict__ r, float* __restrict__ y,
                                int64_t n) {
-  __shared__ float p[kStudentParams];
+  __shared__ __align__(16) float p[kStudentParams];
   for (int i = threadIdx.x; i < kStudentParams; i += blockDim.x) p[i] = params[i];
   __syncthreads();
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
@@ -311,22 +334,34 @@ __global__ void k_student_eval(const float* __restrict__ params, const float* __
 
 // ACA column (which = 0) / row (which = 1) queries of all active blocks with the student.
 __global__ void __launch_bounds__(256, 2) k_far_student(FarArgs a, const float* __restrict__ params, int which) {
-  __shared__ float p[kStudentParams];
+  __shared__ __align__(16) float p[kStudentParams];
   const int nact = a.ctr[kCtrActive];
   const int tot = which ? a.ctr[kCtrTotJ] : a.ctr[kCtrTotI];
   if ((int)(blockIdx.x * blockDim.x) >= tot) return;
   for (int i = threadIdx.x; i < kStudentParams; i += blockDim.x) p[i] = params[i];
   __syncthreads();
   const int32_t* pre = which ? a.preJ : a.preI;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
-    int lo = 0, hi = nact;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (pre[mid] <= g)
-        lo = mid;
-      else
-        hi = mid;
+  __shared__ int s_first;
+  // chunks of blockDim.x consecutive rows: one binary search per chunk for the active block of its
+  // first row, then each thread steps forward to its own row's block (a chunk spans few blocks)
+  for (int g0 = blockIdx.x * blockDim.x; g0 < tot; g0 += gridDim.x * blockDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nact;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= g0)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      s_first = lo;
     }
+    __syncthreads();
+    const int g = g0 + threadIdx.x;
+    int lo = s_first;
+    __syncthreads();
+    if (g >= tot) continue;
+    while (pre[lo + 1] <= g) lo++;
     const int b = a.act[lo];
     const int loc = g - pre[lo];
     const FarBlock bk = a.blocks[b];

@@ -29,6 +29,7 @@ def main():
     ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
+    ap.add_argument("--timing", type=int, default=2, help="2 = far-field breakdown by kernel category")
     ap.add_argument("--student-steps", type=int, default=4000, help="training steps when --precision 2")
     ap.add_argument("--student-batch", type=int, default=16384)
     ap.add_argument("--student-samples", type=int, default=2_000_000)
@@ -75,7 +76,7 @@ def main():
         m.set(capi.P_PRECISION, a.precision)
         m.set(capi.P_FIELDS, a.fields)
         m.set(capi.P_EPSILON, a.epsilon)
-        m.set(capi.P_TIMING, 1)
+        m.set(capi.P_TIMING, a.timing)
         if a.precision == 2:
             import time
 
@@ -110,7 +111,8 @@ def main():
                    far_evals_per_s=st["far_evals"] / max(1e-9, np.min(far)) * 1e3 if st["far_evals"] else None,
                    far_iterations=st["far_iterations"], far_rank_max=st["far_rank_max"],
                    student_fallback_blocks=st["student_fallback_blocks"], gpu_launches=st["gpu_launches"],
-                   num_far=st["num_far"])
+                   num_far=st["num_far"], far_query_ms=st["t_far_query_ms"], far_pivot_ms=st["t_far_pivot_ms"],
+                   far_active_ms=st["t_far_active_ms"], far_check_ms=st["t_far_check_ms"])
     print(json.dumps(out), flush=True)
 
 

@@ -47,7 +47,8 @@ enum hignn_param {
   HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field;
                                     1 and 2 need block_size <= 128                               */
   HIGNN_P_FAR_BATCH_ROWS = 101,  /* max rows (sum of |I|+|J|) per ACA batch, default 1<<26   */
-  HIGNN_P_TIMING = 102,          /* 1 = record per-phase CUDA-event times in hignn_stats     */
+  HIGNN_P_TIMING = 102,          /* 1 = per-phase CUDA-event times in hignn_stats, 2 = also the
+                                    far-field breakdown (events around every far launch)        */
   HIGNN_P_STUDENT_TOL = 103,     /* student fallback: a far block whose 64 sampled entries differ from
                                     the teacher by more than max(this, epsilon) relative (Frobenius)
                                     is recomputed with the teacher; default 1e-3                   */
@@ -75,6 +76,11 @@ typedef struct hignn_stats {
   double t_far_ms;         /* device time of the last far field (TIMING = 1)    */
   double t_dot_ms;         /* device time of the last dot (TIMING = 1)          */
   int64_t gpu_launches;    /* kernels launched by the last dot                    */
+  /* far-field breakdown of the last dot (TIMING = 2; CUDA events around each launch) */
+  double t_far_query_ms;   /* column / row queries (network evaluations)         */
+  double t_far_pivot_ms;   /* orthogonalisation, pivots, stopping norms, apply    */
+  double t_far_active_ms;  /* active lists                                       */
+  double t_far_check_ms;   /* student residual check and deferred apply          */
 } hignn_stats;
 
 /* Message of the calling thread's last error (empty string if none). */
@@ -107,6 +113,28 @@ int hignn_get_param(hignn_model* m, int key, double* value);
 /* UpdateCoord -- src/HignnModel.cpp:744-762: copy coordinates, rebuild the tree
  * (src/Build.cpp:17-265) and the close/far lists (src/CloseFarCheck.cpp:11-465). */
 int hignn_update_coord(hignn_model* m, const float* xyz, int64_t n);
+
+/* New coordinates on the existing tree: the positions are replaced, the cluster tree, the
+ * close/far lists and the ACA plan are kept (the reference always rebuilds,
+ * src/HignnModel.cpp:744-762; a simulation that rebuilds every k steps moves the particles in
+ * between with this call). */
+int hignn_update_coord_keep_tree(hignn_model* m, const float* xyz, int64_t n);
+
+/* Pair forces of PotentialForce::GetPotentialForce (include/PotentialForce.hpp:468-593) plus a
+ * uniform body force: f_i = gravity + sum over j != i with |x_i - x_j| < cutoff and
+ * |r| > 1e-3 of r fMag / |r|, r = x_i - x_j, fMag = -2 a De (exp(-a(|r| - re)) - exp(-2a(|r| - re)))
+ * (the reference hard-codes De = 1, a = 1, re = 2.5). Neighbours from a device cell list.
+ * Host pointers, (n, 3) float32; gravity may be null; cutoff = 0 gives gravity only. */
+int hignn_pair_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const float* gravity, double De,
+                      double a, double re, double cutoff);
+
+/* ExplicitEuler::Run (include/TimeIntegrator.hpp:431-488) with the velocity callback's work on
+ * the device: per step f = gravity + pair forces (as hignn_pair_forces), u = M(x) f (as
+ * hignn_dot, current settings), x += u dt (float). The tree and lists are built for xyz and
+ * rebuilt every `rebuild_every` steps (0: never); in between positions move on the kept tree.
+ * xyz (n, 3) is read as the start and overwritten with the final positions. */
+int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+                    const float* gravity, double De, double a, double re, double cutoff);
 
 /* Dot -- src/HignnModel.cpp:545-634: u = M(x) f through the H-matrix (close
  * field + ACA far field). Host pointers; u is written, its input ignored. */

@@ -846,3 +846,42 @@ def dp45_run(x0, velocity, dt, tf, threshold=1e-3, output=None, output_step=1):
         k[1] = k[7].copy()
         count += 1
     return x, count
+
+
+# ----------------------------------------------------------------------------------------------
+# Pair forces: PotentialForce::GetPotentialForce (include/PotentialForce.hpp:468-593) with the
+# Morse force of CalculatePotentialForce (:115-140), parameters instead of De = 1, a = 1, re = 2.5
+# ----------------------------------------------------------------------------------------------
+def pair_forces(x, gravity=(0.0, 0.0, 0.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
+    """f_i = gravity + sum over neighbours j != i of r fMag / |r|, r = x_i - x_j (float32).
+
+    Neighbours: sqrt(sum (double)(x_j - x_i)^2) squared < cutoff^2 (the kd-tree radius search's
+    metric, include/PointCloudSearch.hpp:231-240, strict <), and |r| > 1e-3 (float).
+    fMag = -2 a De (exp(-a (|r| - re)) - exp(-2 a (|r| - re))): the exponentials in float, the
+    product with -2 a De in double, stored as float (include/PotentialForce.hpp:125-131).
+    """
+    from scipy.spatial import cKDTree
+
+    x = np.asarray(x, np.float32)
+    n = len(x)
+    f = np.zeros((n, 3), np.float32)
+    if cutoff > 0:
+        pairs = cKDTree(x.astype(np.float64)).query_pairs(cutoff * (1 + 1e-6), output_type="ndarray")
+        if len(pairs):
+            ii = np.concatenate([pairs[:, 0], pairs[:, 1]])
+            jj = np.concatenate([pairs[:, 1], pairs[:, 0]])
+            d = x[jj].astype(np.float64) - x[ii].astype(np.float64)
+            dist = np.sqrt(np.sum(d * d, axis=1))
+            keep = dist * dist < float(cutoff) * float(cutoff)
+            ii, jj = ii[keep], jj[keep]
+            r = (x[ii] - x[jj]).astype(np.float32)
+            rn = np.sqrt(np.sum(r * r, axis=1, dtype=np.float32)).astype(np.float32)
+            keep = rn > np.float32(1e-3)
+            ii, r, rn = ii[keep], r[keep], rn[keep]
+            a32, re32, de32 = np.float32(a), np.float32(re), np.float32(De)
+            e1 = np.exp((-a32 * (rn - re32)).astype(np.float32)).astype(np.float32)
+            e2 = np.exp((np.float32(-2.0) * a32 * (rn - re32)).astype(np.float32)).astype(np.float32)
+            fmag = (-2.0 * float(a32) * float(de32) * (e1 - e2).astype(np.float64)).astype(np.float32)
+            ratio = (fmag / rn).astype(np.float32)
+            np.add.at(f, ii, (r * ratio[:, None]).astype(np.float32))
+    return (f + np.asarray(gravity, np.float32)[None, :]).astype(np.float32)

@@ -1,0 +1,113 @@
+"""Device time step: pair forces on the cell list and the explicit Euler loop (C ABI).
+
+Pair forces are compared with the oracle's restatement of PotentialForce::GetPotentialForce
+(include/PotentialForce.hpp:468-593) to 1e-4 relative per particle (float sums of up to a few
+dozen terms of both signs, in another order).
+The device Euler loop must equal the same loop driven from the host through the C ABI
+(hignn_pair_forces, hignn_dot / hignn_update_coord_keep_tree, x += u dt in float32): to 1e-5 of
+the displacement with the FP32 network, 1e-4 with the BF16 one. The two loops sum the Morse terms
+in different orders (tree order on the device, input order on the host), so after the first step
+the positions differ in the last bits; the BF16 network rounds its hidden activations to 8 bits,
+which turns those last-bit differences into differences at the BF16 level in some evaluations.
+"""
+import numpy as np
+import pytest
+
+from conftest import WEIGHTS
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from hignn_b200 import capi  # noqa: E402
+from hignn_b200 import synthetic as S  # noqa: E402
+from oracle import hignn_oracle as O  # noqa: E402
+
+MORSE = dict(De=1.0, a=5.0, re=2.1, cutoff=3.0)  # a Morse repulsion of the clustered suspension
+G = (0.0, 0.0, -1.0)
+
+
+def make_model(x, **params):
+    m = capi.Model(x, 128, device=0)
+    m.load_two_body(WEIGHTS)
+    for k, v in params.items():
+        m.set(getattr(capi, "P_" + k.upper()), v)
+    return m
+
+
+def rel_rows(a, b):
+    return float(np.max(np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-6)))
+
+
+def test_pair_forces_match_oracle():
+    x = S.uniform_min_dist(6000, 0.15, 5)  # separations >= 2.05: finite Morse forces
+    m = make_model(x)
+    f = m.pair_forces(x, G, **MORSE)
+    ref = O.pair_forces(x, G, **MORSE)
+    assert rel_rows(f, ref) < 1e-4
+    # gravity only, and the reference's hard-coded parameters (De = 1, a = 1, re = 2.5)
+    assert np.array_equal(m.pair_forces(x, G), np.tile(np.float32(G), (len(x), 1)))
+    f2 = m.pair_forces(x, (0, 0, 0), 1.0, 1.0, 2.5, 4.0)
+    assert rel_rows(f2, O.pair_forces(x, (0, 0, 0), 1.0, 1.0, 2.5, 4.0)) < 1e-4
+
+
+def test_pair_forces_clustered_and_coincident():
+    x = np.concatenate([S.uniform_min_dist(3000, 0.1, 6), np.zeros((2, 3), np.float32) + 5.0])
+    m = make_model(x)
+    f = m.pair_forces(x, G, **MORSE)
+    ref = O.pair_forces(x, G, **MORSE)
+    assert np.all(np.isfinite(f))
+    assert rel_rows(f, ref) < 1e-4  # the coincident pair (|r| < 1e-3) contributes nothing
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_device_euler_matches_host_loop(precision):
+    x0 = S.uniform_min_dist(8000, 0.1, 7)
+    steps, dt, k = 4, 1e-3, 2
+    m = make_model(x0, epsilon=1e-2, precision=precision)
+    xd = m.run_euler(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE)
+    h = make_model(x0, epsilon=1e-2, precision=precision)
+    x = x0.copy()
+    for s in range(steps):
+        if s > 0 and s % k == 0:
+            h.update_coord(x)
+        elif s > 0:
+            h.update_coord_keep_tree(x)
+        f = h.pair_forces(x, G, **MORSE)
+        u = h.dot(f)
+        x = (x + u * np.float32(dt)).astype(np.float32)
+    disp = np.linalg.norm(x - x0)
+    assert disp > 0
+    assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 1e-4)
+
+
+def test_keep_tree_is_close_to_rebuild():
+    x0 = S.uniform_min_dist(8000, 0.1, 8)
+    f = S.sedimenting_forces(8000, 8)
+    x1 = x0 + np.float32(0.05) * np.random.default_rng(1).standard_normal(x0.shape).astype(np.float32)
+    a = make_model(x0, epsilon=1e-2)
+    a.dot(f)
+    a.update_coord_keep_tree(x1)
+    ua = a.dot(f)
+    b = make_model(x1, epsilon=1e-2)
+    ub = b.dot(f)
+    assert np.linalg.norm(ua - ub) / np.linalg.norm(ub) < 2e-3  # two H-matrix approximations at eps 1e-2
+    dense = b.dense_rows(f, np.arange(0, 8000, 40), 0)
+    assert np.linalg.norm(ua[::40] - dense) / np.linalg.norm(dense) < 2e-3
+
+
+def test_pybind_potential_force():
+    from hignn_b200 import hignn
+
+    x = S.uniform_min_dist(3000, 0.15, 9)
+    pf = hignn.PotentialForce()
+    pf.set_two_body_epsilon(4.0)
+    f = pf.get_potential_force(x)  # the reference's constants De = 1, a = 1, re = 2.5
+    assert rel_rows(f, O.pair_forces(x, (0, 0, 0), 1.0, 1.0, 2.5, 4.0)) < 1e-4
+    pf.set_parameters(1.0, 5.0, 2.1)
+    f = pf.get_potential_force(x)
+    assert rel_rows(f, O.pair_forces(x, (0, 0, 0), 1.0, 5.0, 2.1, 4.0)) < 1e-4
+    with pytest.raises(RuntimeError):
+        pf.set_periodic(True)
