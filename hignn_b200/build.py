@@ -36,6 +36,7 @@ CU_SOURCES = {
     "noalloc.cu": [],
     "student.cu": [],
     "step.cu": [],
+    "neighbors.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

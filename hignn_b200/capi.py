@@ -61,6 +61,12 @@ _P = C.c_void_p
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)
+_u64p = C.POINTER(C.c_uint64)
+
+# edge list kinds (HIGNN_EDGES_*)
+EDGES_TWO_BODY = 0
+EDGES_THREE_BODY = 1
+EDGES_THREE_BODY_SELF = 2
 
 SIGNATURES = {
     "hignn_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
@@ -95,6 +101,17 @@ SIGNATURES = {
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
     "hignn_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
+    "hignn_nbl_create": ([C.c_int, C.POINTER(_P)], C.c_int),
+    "hignn_nbl_destroy": ([_P], None),
+    "hignn_nbl_update_coord": ([_P, _fp, C.c_int64], C.c_int),
+    "hignn_nbl_set_two_body_epsilon": ([_P, C.c_float], C.c_int),
+    "hignn_nbl_set_three_body_epsilon": ([_P, C.c_float], C.c_int),
+    "hignn_nbl_build_two_body_info": ([_P], C.c_int),
+    "hignn_nbl_build_three_body_info": ([_P], C.c_int),
+    "hignn_nbl_get_edge_info": ([_P, C.c_int, C.c_int, _u64p, C.c_int64, _u64p, C.c_int64, _i64p], C.c_int),
+    "hignn_nbl_edge_info_device": ([_P, C.c_int, C.POINTER(C.c_void_p), _i64p], C.c_int),
+    "hignn_nbl_last_build_ms": ([_P, _dp], C.c_int),
+    "hignn_nbl_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
 }
 
 for _name, (_args, _res) in SIGNATURES.items():
@@ -313,3 +330,65 @@ class Model:
         s = C.c_void_p()
         check(lib.hignn_get_stream(self._h, C.byref(s)))
         return s.value
+
+
+class NeighborLists:
+    """Owner of a ``hignn_nbl*``: the reference's NeighborLists (include/NeighborLists.hpp) on one device.
+
+    Getters return uint64 arrays of shape (rows, E), as the reference's do.
+    """
+
+    def __init__(self, device=0):
+        h = _P()
+        check(lib.hignn_nbl_create(int(device), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hignn_nbl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def update_coord(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        if x.ndim != 2 or x.shape[1] != 3:
+            raise ValueError("coordinates must be (n, 3)")
+        check(lib.hignn_nbl_update_coord(self._h, fptr(x), len(x)))
+
+    def set_two_body_epsilon(self, eps):
+        check(lib.hignn_nbl_set_two_body_epsilon(self._h, float(eps)))
+
+    def set_three_body_epsilon(self, eps):
+        check(lib.hignn_nbl_set_three_body_epsilon(self._h, float(eps)))
+
+    def build_two_body_info(self):
+        check(lib.hignn_nbl_build_two_body_info(self._h))
+
+    def build_three_body_info(self):
+        check(lib.hignn_nbl_build_three_body_info(self._h))
+
+    def last_build_ms(self):
+        v = C.c_double()
+        check(lib.hignn_nbl_last_build_ms(self._h, C.byref(v)))
+        return v.value
+
+    def edges(self, kind, index=None):
+        """(rows, E) uint64 edge list of `kind` (EDGES_*), or its ByIndex variant for `index`."""
+        rows = 3 if kind == EDGES_THREE_BODY else 2
+        by = index is not None
+        idx = np.ascontiguousarray(index if by else np.zeros(0), np.uint64)
+        ip = idx.ctypes.data_as(_u64p)
+        e = C.c_int64()
+        check(lib.hignn_nbl_get_edge_info(self._h, kind, int(by), ip, len(idx), None, 0, C.byref(e)))
+        out = np.empty((rows, e.value), np.uint64)
+        check(lib.hignn_nbl_get_edge_info(self._h, kind, int(by), ip, len(idx), out.ctypes.data_as(_u64p), out.size,
+                                          C.byref(e)))
+        return out
+
+    def device_edges(self, kind):
+        """(device pointer, E) of a whole list; the pointer is owned by this object."""
+        p, e = C.c_void_p(), C.c_int64()
+        check(lib.hignn_nbl_edge_info_device(self._h, kind, C.byref(p), C.byref(e)))
+        return p.value, e.value

@@ -24,6 +24,7 @@
 #include "common.h"
 #include "kernels.h"
 #include "model_view.h"
+#include "neighbors.h"
 #include "tree.h"
 
 using hignn::Error;
@@ -1471,3 +1472,97 @@ int hignn_get_stream(hignn_model* m, void** stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- neighbour lists
+
+struct hignn_nbl {
+  hignn::NeighbourLists lists;
+  explicit hignn_nbl(int device) : lists(device) {}
+};
+
+int hignn_nbl_create(int device, hignn_nbl** out) {
+  return guard([&] {
+    if (!out) throw Error(HIGNN_ERR_ARG, "null argument");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      throw Error(HIGNN_ERR_NODEV, "neighbour lists: no CUDA device");
+    }
+    if (device < 0 || device >= count) throw Error(HIGNN_ERR_ARG, "neighbour lists: bad device");
+    *out = new hignn_nbl(device);
+  });
+}
+
+void hignn_nbl_destroy(hignn_nbl* l) { delete l; }
+
+int hignn_nbl_update_coord(hignn_nbl* l, const float* xyz, int64_t n) {
+  return guard([&] {
+    if (!l) throw Error(HIGNN_ERR_ARG, "null argument");
+    l->lists.update_coord(xyz, n);
+  });
+}
+
+int hignn_nbl_set_two_body_epsilon(hignn_nbl* l, float eps) {
+  return guard([&] {
+    if (!l) throw Error(HIGNN_ERR_ARG, "null argument");
+    l->lists.set_two_body_epsilon(eps);
+  });
+}
+
+int hignn_nbl_set_three_body_epsilon(hignn_nbl* l, float eps) {
+  return guard([&] {
+    if (!l) throw Error(HIGNN_ERR_ARG, "null argument");
+    l->lists.set_three_body_epsilon(eps);
+  });
+}
+
+int hignn_nbl_build_two_body_info(hignn_nbl* l) {
+  return guard([&] {
+    if (!l) throw Error(HIGNN_ERR_ARG, "null argument");
+    l->lists.build_two_body();
+  });
+}
+
+int hignn_nbl_build_three_body_info(hignn_nbl* l) {
+  return guard([&] {
+    if (!l) throw Error(HIGNN_ERR_ARG, "null argument");
+    l->lists.build_three_body();
+  });
+}
+
+int hignn_nbl_get_edge_info(hignn_nbl* l, int kind, int by_index, const uint64_t* index, int64_t nindex,
+                            uint64_t* out, int64_t cap, int64_t* num_edges) {
+  return guard([&] {
+    if (!l || !num_edges) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (kind < HIGNN_EDGES_TWO_BODY || kind > HIGNN_EDGES_THREE_BODY_SELF)
+      throw Error(HIGNN_ERR_ARG, "neighbour lists: unknown edge kind");
+    const int64_t e = l->lists.count(kind, by_index != 0, index, nindex);
+    *num_edges = e;
+    if (!out) return;
+    const int rows = kind == HIGNN_EDGES_THREE_BODY ? 3 : 2;
+    if (cap < rows * e) throw Error(HIGNN_ERR_ARG, "neighbour lists: output holds fewer than rows * edges entries");
+    l->lists.copy_out(kind, by_index != 0, index, nindex, out);
+  });
+}
+
+int hignn_nbl_edge_info_device(hignn_nbl* l, int kind, const uint64_t** d_info, int64_t* num_edges) {
+  return guard([&] {
+    if (!l || !d_info || !num_edges) throw Error(HIGNN_ERR_ARG, "null argument");
+    *d_info = l->lists.device_list(kind, num_edges);
+  });
+}
+
+int hignn_nbl_last_build_ms(hignn_nbl* l, double* ms) {
+  return guard([&] {
+    if (!l || !ms) throw Error(HIGNN_ERR_ARG, "null argument");
+    *ms = l->lists.last_build_ms();
+  });
+}
+
+int hignn_nbl_get_stream(hignn_nbl* l, void** stream) {
+  return guard([&] {
+    if (!l || !stream) throw Error(HIGNN_ERR_ARG, "null argument");
+    *stream = (void*)l->lists.stream();
+  });
+}

@@ -381,6 +381,63 @@ class PotentialForce {
   float eps_ = 0.f;
 };
 
+// NeighborLists (include/NeighborLists.hpp, bound at interface/HignnInterface.cpp:73-91): the
+// two-body, three-body and three-body self edge lists, built on the device. Getters return
+// uint64 (rows, E) arrays as the reference's size_t arrays; each particle's neighbours are in
+// ascending order (the reference's follow its kd-tree). Periodic images are not implemented in
+// the reference either (its periodic branch builds no source sites): set_periodic(True) and
+// set_domain raise.
+class NeighborLists {
+ public:
+  NeighborLists() { check(hignn_nbl_create(default_device(), &l_)); }
+  ~NeighborLists() {
+    if (l_) hignn_nbl_destroy(l_);
+  }
+  void set_periodic(bool periodic) {
+    if (periodic) throw std::runtime_error("hignn: periodic neighbour lists are not supported");
+  }
+  void set_domain(py::array) { throw std::runtime_error("hignn: periodic neighbour lists are not supported"); }
+  void update_coord(py::array coord) {
+    farr x = as_n3(coord, "coord");
+    const float* p = x.data();
+    const int64_t n = x.shape(0);
+    py::gil_scoped_release nogil;
+    check(hignn_nbl_update_coord(l_, p, n));
+  }
+  void set_two_body_epsilon(float e) { check(hignn_nbl_set_two_body_epsilon(l_, e)); }
+  void set_three_body_epsilon(float e) { check(hignn_nbl_set_three_body_epsilon(l_, e)); }
+  void build_two_body_info() {
+    py::gil_scoped_release nogil;
+    check(hignn_nbl_build_two_body_info(l_));
+  }
+  void build_three_body_info() {
+    py::gil_scoped_release nogil;
+    check(hignn_nbl_build_three_body_info(l_));
+  }
+  py::array_t<uint64_t> get(int kind) { return fetch(kind, false, nullptr, 0); }
+  py::array_t<uint64_t> get_by_index(int kind, py::array index) {
+    using uarr = py::array_t<uint64_t, py::array::c_style | py::array::forcecast>;
+    uarr idx = uarr::ensure(index);
+    if (!idx || idx.ndim() != 1) throw std::invalid_argument("target index must be a 1-D integer array");
+    return fetch(kind, true, idx.data(), idx.shape(0));
+  }
+
+ private:
+  py::array_t<uint64_t> fetch(int kind, bool by_index, const uint64_t* idx, int64_t m) {
+    const py::ssize_t rows = kind == HIGNN_EDGES_THREE_BODY ? 3 : 2;
+    int64_t e = 0;
+    check(hignn_nbl_get_edge_info(l_, kind, by_index, idx, m, nullptr, 0, &e));
+    py::array_t<uint64_t> out({rows, (py::ssize_t)e});
+    uint64_t* o = out.mutable_data();
+    {
+      py::gil_scoped_release nogil;
+      check(hignn_nbl_get_edge_info(l_, kind, by_index, idx, m, o, rows * e, &e));
+    }
+    return out;
+  }
+  hignn_nbl* l_ = nullptr;
+};
+
 }  // namespace
 
 PYBIND11_MODULE(hignn, m) {
@@ -418,6 +475,25 @@ PYBIND11_MODULE(hignn, m) {
       .def("set_two_body_epsilon", &PotentialForce::set_two_body_epsilon)
       .def("set_parameters", &PotentialForce::set_parameters)
       .def("get_potential_force", &PotentialForce::get_potential_force);
+
+  py::class_<NeighborLists>(m, "NeighborLists")
+      .def(py::init())
+      .def("set_periodic", &NeighborLists::set_periodic, py::arg("isPeriodicBoundary") = false)
+      .def("set_domain", &NeighborLists::set_domain)
+      .def("update_coord", &NeighborLists::update_coord)
+      .def("set_two_body_epsilon", &NeighborLists::set_two_body_epsilon)
+      .def("set_three_body_epsilon", &NeighborLists::set_three_body_epsilon)
+      .def("get_two_body_edge_info", [](NeighborLists& l) { return l.get(HIGNN_EDGES_TWO_BODY); })
+      .def("get_two_body_edge_info_by_index",
+           [](NeighborLists& l, py::array i) { return l.get_by_index(HIGNN_EDGES_TWO_BODY, i); })
+      .def("get_three_body_edge_info", [](NeighborLists& l) { return l.get(HIGNN_EDGES_THREE_BODY); })
+      .def("get_three_body_edge_info_by_index",
+           [](NeighborLists& l, py::array i) { return l.get_by_index(HIGNN_EDGES_THREE_BODY, i); })
+      .def("get_three_body_edge_self_info", [](NeighborLists& l) { return l.get(HIGNN_EDGES_THREE_BODY_SELF); })
+      .def("get_three_body_edge_self_info_by_index",
+           [](NeighborLists& l, py::array i) { return l.get_by_index(HIGNN_EDGES_THREE_BODY_SELF, i); })
+      .def("build_two_body_info", &NeighborLists::build_two_body_info)
+      .def("build_three_body_info", &NeighborLists::build_three_body_info);
 
   py::class_<ExplicitEuler>(m, "ExplicitEuler")
       .def(py::init())

@@ -128,9 +128,20 @@ void launch_far_tc(const FarArgs& a, const TcWeights& w, int which, int* err, in
 void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int* err, int num_sms, cudaStream_t s);
 
 // ---------------------------------------------------------------- time step (step.cu)
+// The reference's squared search radius: epsilon is a float and is squared in float
+// (include/PointCloudSearch.hpp:395-397, epsilons(i) * epsilons(i) of a float view), then widened.
+__host__ __device__ inline double radius_sq(double eps) {
+  const float e = (float)eps;
+#ifdef __CUDA_ARCH__
+  return (double)__fmul_rn(e, e);
+#else
+  return (double)(e * e);
+#endif
+}
+
 struct CellGrid {
-  float3 lo;
-  float inv;  // 1 / cell size
+  double3 lo;
+  double inv;  // 1 / cell size (cell coordinates in double: exact to far below the cell margin)
   int nx, ny, nz, ncell;
 };
 
@@ -156,8 +167,8 @@ void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorsePar
                   float* f3, cudaStream_t s);
 // Neighbours j != i within the cutoff (the reference's radius-search test): per-particle counts
 // (out null) or the sorted lists at out[off[i] ..].
-void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int* count, const int64_t* off,
-                       int* out, cudaStream_t s);
+void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int64_t* count,
+                       const int64_t* off, int* out, cudaStream_t s);
 void launch_advance(float4* x, const double* u, int64_t n, float dt, cudaStream_t s);
 void launch_pack_positions(const float* xyz, int64_t n, float4* x4, cudaStream_t s);
 

@@ -55,8 +55,8 @@ __global__ void k_bbox(const float4* __restrict__ x, int64_t n, unsigned* __rest
 }
 
 __device__ __forceinline__ int3 cell_of(const float4 p, const CellGrid& g) {
-  int cx = (int)floorf((p.x - g.lo.x) * g.inv), cy = (int)floorf((p.y - g.lo.y) * g.inv),
-      cz = (int)floorf((p.z - g.lo.z) * g.inv);
+  int cx = (int)floor(((double)p.x - g.lo.x) * g.inv), cy = (int)floor(((double)p.y - g.lo.y) * g.inv),
+      cz = (int)floor(((double)p.z - g.lo.z) * g.inv);
   cx = min(max(cx, 0), g.nx - 1);
   cy = min(max(cy, 0), g.ny - 1);
   cz = min(max(cz, 0), g.nz - 1);
@@ -165,7 +165,7 @@ __global__ void k_morse(const float4* __restrict__ x, int64_t n, CellGrid g, con
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (mp.cutoff > 0.0) {
     const int3 c = cell_of(xi, g);
-    const double c2 = mp.cutoff * mp.cutoff;
+    const double c2 = radius_sq(mp.cutoff);
     for (int dz = -1; dz <= 1; dz++) {
       const int z = c.z + dz;
       if (z < 0 || z >= g.nz) continue;
@@ -221,12 +221,12 @@ __device__ __forceinline__ bool is_neighbour(const float4 xi, const float4 xj, d
 // Neighbours j != i of every i within the cutoff: count (out == nullptr) or write them, ascending,
 // at out[off[i] ..] (insertion into the sorted run as they are found).
 __global__ void k_neighbours(const float4* __restrict__ x, int64_t n, CellGrid g, const int* __restrict__ start,
-                             const int* __restrict__ items, double cutoff, int* __restrict__ count,
+                             const int* __restrict__ items, double cutoff, int64_t* __restrict__ count,
                              const int64_t* __restrict__ off, int* __restrict__ out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 xi = x[i];
-  const double c2 = cutoff * cutoff;
+  const double c2 = radius_sq(cutoff);
   const int3 c = cell_of(xi, g);
   int cnt = 0;
   int* dst = out ? out + off[i] : nullptr;
@@ -316,8 +316,8 @@ void CellList::build(const float4* x, int64_t n, double cutoff, cudaStream_t s) 
   };
   int nd[3];
   while (dims(size, nd) > kMaxCells) size *= 1.26;
-  grid.lo = make_float3(lo[0], lo[1], lo[2]);
-  grid.inv = (float)(1.0 / size);
+  grid.lo = make_double3(lo[0], lo[1], lo[2]);
+  grid.inv = 1.0 / size;
   grid.nx = nd[0];
   grid.ny = nd[1];
   grid.nz = nd[2];
@@ -346,8 +346,8 @@ void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorsePar
   HIGNN_CHECK_LAUNCH();
 }
 
-void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int* count, const int64_t* off,
-                       int* out, cudaStream_t s) {
+void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int64_t* count,
+                       const int64_t* off, int* out, cudaStream_t s) {
   if (n <= 0) return;
   k_neighbours<<<nblk(n, 128), 128, 0, s>>>(x, n, cl.grid, cl.start.as<int>(), cl.items.as<int>(), cutoff, count, off,
                                             out);

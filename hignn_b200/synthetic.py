@@ -66,6 +66,19 @@ def uniform(n: int, phi: float, seed: int) -> np.ndarray:
     return rng.uniform(0.0, cube_side(n, phi), size=(n, 3)).astype(np.float32)
 
 
+def filaments(n_filament: int, n_chain: int, bond: float, phi: float, seed: int) -> np.ndarray:
+    """Straight chains of ``n_chain`` beads ``bond`` apart, random starts and directions in a cube
+    sized for ``phi`` (filament f holds rows f * n_chain .. (f + 1) * n_chain - 1)."""
+    rng = np.random.default_rng(seed)
+    n = n_filament * n_chain
+    side = cube_side(n, phi)
+    start = rng.uniform(0.0, side, size=(n_filament, 1, 3))
+    d = rng.normal(size=(n_filament, 1, 3))
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    k = np.arange(n_chain, dtype=np.float64)[None, :, None]
+    return (start + bond * k * d).reshape(n, 3).astype(np.float32)
+
+
 def sedimenting_forces(n: int, seed: int) -> np.ndarray:
     """F_i = (0, 0, -1) + N(0, 0.1^2) per component, FP32."""
     rng = np.random.default_rng(seed + 1000)

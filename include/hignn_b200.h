@@ -234,6 +234,53 @@ int hignn_synchronize(hignn_model* m);
 /* The model's CUDA stream (cudaStream_t), for callers that order their own work. */
 int hignn_get_stream(hignn_model* m, void** stream);
 
+/* ---------------------------------------------------------------- neighbour lists
+ * The reference's NeighborLists class (include/NeighborLists.hpp, bound at
+ * interface/HignnInterface.cpp:73-91), built on the device. A neighbour of i is any j with
+ * sqrt(sum (double)(x_j - x_i)^2)^2 < (float)eps * (float)eps (the kd-tree radius search of
+ * include/PointCloudSearch.hpp:274-450). Each particle's neighbours come out in ascending
+ * index order (the reference's follow its kd-tree traversal; the sets are the same). */
+typedef struct hignn_nbl hignn_nbl;
+
+#define HIGNN_EDGES_TWO_BODY 0        /* (2, E): (i, j), j in N(i) \ {i} at the two-body eps   */
+#define HIGNN_EDGES_THREE_BODY 1      /* (3, E): (i, j, k), j in N(i) \ {i}, k in N(j) \ {j, i} */
+#define HIGNN_EDGES_THREE_BODY_SELF 2 /* (2, E): (i, j), j in N(i) \ {i} at the three-body eps */
+
+/* NeighborLists::NeighborLists: an empty set of lists on `device`. */
+int hignn_nbl_create(int device, hignn_nbl** out);
+void hignn_nbl_destroy(hignn_nbl* l);
+
+/* NeighborLists::UpdateCoord (include/NeighborLists.hpp:252-279): copy n float32 (x, y, z)
+ * rows (host). Lists built before stay until the next build. */
+int hignn_nbl_update_coord(hignn_nbl* l, const float* xyz, int64_t n);
+
+/* SetTwoBodyEpsilon / SetThreeBodyEpsilon (include/NeighborLists.hpp:281-287). */
+int hignn_nbl_set_two_body_epsilon(hignn_nbl* l, float eps);
+int hignn_nbl_set_three_body_epsilon(hignn_nbl* l, float eps);
+
+/* BuildTwoBodyInfo (include/NeighborLists.hpp:466-510) and BuildThreeBodyInfo (:512-585; the
+ * triplets and the self edges). The epsilon must be positive (the reference's lists underflow
+ * at 0). */
+int hignn_nbl_build_two_body_info(hignn_nbl* l);
+int hignn_nbl_build_three_body_info(hignn_nbl* l);
+
+/* The getters of include/NeighborLists.hpp:289-464, two calls: with out = NULL only
+ * *num_edges is set; then out (host, uint64 (rows, *num_edges) row-major, cap entries) is
+ * filled. by_index = 0: Get{TwoBody,ThreeBody,ThreeBodySelf}EdgeInfo; by_index = 1: the
+ * ByIndex variant for the nindex targets index[] (< n): two-body lists all j != p for each
+ * target p, rows (j, p); three-body the target's triplets with rows (k, j, i); self rows
+ * (j, i). A list that was never built has 0 edges. */
+int hignn_nbl_get_edge_info(hignn_nbl* l, int kind, int by_index, const uint64_t* index, int64_t nindex,
+                            uint64_t* out, int64_t cap, int64_t* num_edges);
+
+/* A whole list on the device (uint64 (rows, *num_edges) row-major, owned by l, valid until
+ * the next build or hignn_nbl_destroy); NULL when not built. */
+int hignn_nbl_edge_info_device(hignn_nbl* l, int kind, const uint64_t** d_info, int64_t* num_edges);
+
+/* Wall time of the last build (ms), and the lists' CUDA stream. */
+int hignn_nbl_last_build_ms(hignn_nbl* l, double* ms);
+int hignn_nbl_get_stream(hignn_nbl* l, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -872,7 +872,7 @@ def pair_forces(x, gravity=(0.0, 0.0, 0.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
             jj = np.concatenate([pairs[:, 1], pairs[:, 0]])
             d = x[jj].astype(np.float64) - x[ii].astype(np.float64)
             dist = np.sqrt(np.sum(d * d, axis=1))
-            keep = dist * dist < float(cutoff) * float(cutoff)
+            keep = dist * dist < float(np.float32(cutoff) * np.float32(cutoff))  # float radius, squared in float
             ii, jj = ii[keep], jj[keep]
             r = (x[ii] - x[jj]).astype(np.float32)
             rn = np.sqrt(np.sum(r * r, axis=1, dtype=np.float32)).astype(np.float32)
@@ -885,3 +885,127 @@ def pair_forces(x, gravity=(0.0, 0.0, 0.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
             ratio = (fmag / rn).astype(np.float32)
             np.add.at(f, ii, (r * ratio[:, None]).astype(np.float32))
     return (f + np.asarray(gravity, np.float32)[None, :]).astype(np.float32)
+
+
+# ---------------------------------------------------------------- neighbour lists
+def radius_sq(eps):
+    """The reference's squared search radius: eps squared in float, then widened
+    (include/PointCloudSearch.hpp:395-397: epsilons(i) * epsilons(i) of a float view)."""
+    e = np.float32(eps)
+    return float(np.float32(e * e))
+
+
+def neighbour_csr(x, eps):
+    """Per particle i the neighbours j != i, ascending: (off int64[n + 1], nbr int64[E]).
+
+    A neighbour is any j with sqrt(sum((double)x_j - (double)x_i)^2)^2 < radius_sq(eps): the vendored
+    nanoflann metric (include/nanoflann.hpp:387-399 squares PointCloudSearch::kdtree_distance,
+    include/PointCloudSearch.hpp:231-240) and RadiusResultSet::addPoint's strict test
+    (include/PointCloudSearch.hpp:56-72). The particle itself (distance 0) is the entry the reference
+    swaps to the front and skips (include/NeighborLists.hpp:207-224, 496-506).
+    """
+    from scipy.spatial import cKDTree
+
+    x = np.asarray(x, np.float32)
+    n = len(x)
+    if n == 0:
+        return np.zeros(1, np.int64), np.zeros(0, np.int64)
+    x64 = x.astype(np.float64)
+    c2 = radius_sq(eps)
+    pairs = cKDTree(x64).query_pairs(math.sqrt(c2) * (1 + 1e-6), output_type="ndarray")
+    if len(pairs) == 0:
+        return np.zeros(n + 1, np.int64), np.zeros(0, np.int64)
+    ii = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    jj = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    d = x64[jj] - x64[ii]
+    dist = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    keep = dist * dist < c2
+    ii, jj = ii[keep], jj[keep]
+    order = np.lexsort((jj, ii))
+    ii, jj = ii[order], jj[order]
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(ii, minlength=n), out=off[1:])
+    return off, jj.astype(np.int64)
+
+
+def neighbour_csr_brute(x, eps):
+    """neighbour_csr by an all-pairs loop over rows (checks the kd-tree candidate search)."""
+    x = np.asarray(x, np.float32)
+    x64 = x.astype(np.float64)
+    c2 = radius_sq(eps)
+    off, nbr = [0], []
+    for i in range(len(x)):
+        d = x64 - x64[i]
+        dist = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+        js = np.nonzero(dist * dist < c2)[0]
+        js = js[js != i]
+        nbr.extend(js.tolist())
+        off.append(len(nbr))
+    return np.asarray(off, np.int64), np.asarray(nbr, np.int64)
+
+
+def two_body_edge_info(off, nbr):
+    """BuildTwoBodyInfo + GetTwoBodyEdgeInfo (include/NeighborLists.hpp:466-510, 289-307):
+    uint64 (2, E), rows (i, j) for j in N(i) \\ {i}."""
+    n = len(off) - 1
+    i = np.repeat(np.arange(n, dtype=np.uint64), np.diff(off))
+    return np.stack([i, nbr.astype(np.uint64)]) if len(nbr) else np.zeros((2, 0), np.uint64)
+
+
+def three_body_edge_info(off, nbr):
+    """BuildThreeBodyInfo + GetThreeBodyEdgeInfo (include/NeighborLists.hpp:512-585, 342-360):
+    uint64 (3, E), rows (i, j, k) for j in N(i) \\ {i}, k in N(j) \\ {j}, k != i; and the
+    triplet offsets per particle (int64[n + 1]). Vectorised form of the loops over i, j, k."""
+    n = len(off) - 1
+    deg = np.diff(off)
+    ei = np.repeat(np.arange(n, dtype=np.int64), deg)  # the (i, j) edges in order
+    ej = nbr
+    dj = deg[ej] if len(ej) else np.zeros(0, np.int64)
+    tot = int(dj.sum())
+    ti = np.repeat(ei, dj)
+    tj = np.repeat(ej, dj)
+    first = np.repeat(off[ej] - np.concatenate([[0], np.cumsum(dj)[:-1]]) if len(ej) else np.zeros(0, np.int64), dj)
+    tk = nbr[first + np.arange(tot, dtype=np.int64)] if tot else np.zeros(0, np.int64)
+    keep = tk != ti
+    ti, tj, tk = ti[keep], tj[keep], tk[keep]
+    off3 = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(ti, minlength=n), out=off3[1:])
+    info = np.stack([ti, tj, tk]).astype(np.uint64) if len(ti) else np.zeros((3, 0), np.uint64)
+    return info, off3
+
+
+def three_body_edge_info_loops(off, nbr):
+    """three_body_edge_info by the reference's own loops (small inputs)."""
+    rows = []
+    n = len(off) - 1
+    for i in range(n):
+        for t in range(off[i], off[i + 1]):
+            j = int(nbr[t])
+            for q in range(off[j], off[j + 1]):
+                k = int(nbr[q])
+                if k != i:
+                    rows.append((i, j, k))
+    return np.asarray(rows, np.uint64).T.reshape(3, -1)
+
+
+def two_body_edge_info_by_index(n, index):
+    """GetTwoBodyEdgeInfoByIndex (include/NeighborLists.hpp:309-340): for each target p all
+    j != p in order, rows (j, p)."""
+    rows0, rows1 = [], []
+    for p in np.asarray(index, np.uint64):
+        j = np.arange(n, dtype=np.uint64)
+        j = j[j != p]
+        rows0.append(j)
+        rows1.append(np.full(len(j), p, np.uint64))
+    if not rows0:
+        return np.zeros((2, 0), np.uint64)
+    return np.stack([np.concatenate(rows0), np.concatenate(rows1)])
+
+
+def edge_info_by_index(info, off, index):
+    """GetThreeBodyEdgeInfoByIndex / GetThreeBodyEdgeSelfInfoByIndex (include/NeighborLists.hpp:
+    362-403, 424-464): each target's edges in turn, rows reversed."""
+    parts = [info[::-1, off[p]:off[p + 1]] for p in np.asarray(index, np.int64)]
+    if not parts:
+        return np.zeros((info.shape[0], 0), np.uint64)
+    return np.concatenate(parts, axis=1)
