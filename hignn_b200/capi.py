@@ -95,8 +95,8 @@ SIGNATURES = {
     "hignn_set_shard": ([_P, C.c_int, C.c_int], C.c_int),
     "hignn_update_coord_keep_tree": ([_P, _fp, C.c_int64], C.c_int),
     "hignn_pair_forces": ([_P, _fp, _fp, C.c_int64, _fp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
-    "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, _fp, C.c_double, C.c_double, C.c_double,
-                         C.c_double], C.c_int),
+    "hignn_forces": ([_P, _fp, _fp, C.c_int64, C.c_void_p], C.c_int),
+    "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
     "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
@@ -118,6 +118,33 @@ for _name, (_args, _res) in SIGNATURES.items():
     _f = getattr(lib, _name)
     _f.argtypes = _args
     _f.restype = _res
+
+
+class ForceModel(C.Structure):
+    """hignn_force_model: body force, Morse pair forces, filament bending and tension."""
+
+    _fields_ = [
+        ("gravity", C.c_float * 3),
+        ("morse_De", C.c_double),
+        ("morse_a", C.c_double),
+        ("morse_re", C.c_double),
+        ("morse_cutoff", C.c_double),
+        ("n_filament", C.c_int64),
+        ("n_chain", C.c_int32),
+        ("rest_length", C.c_double),
+        ("k_t", C.c_double),
+        ("k_b", C.c_double),
+    ]
+
+
+def force_model(gravity=(0.0, 0.0, 0.0), De=1.0, a=1.0, re=2.5, cutoff=0.0, n_filament=0, n_chain=0,
+                rest_length=0.0, k_t=0.0, k_b=0.0):
+    fm = ForceModel()
+    fm.gravity[:] = [float(v) for v in gravity]
+    fm.morse_De, fm.morse_a, fm.morse_re, fm.morse_cutoff = float(De), float(a), float(re), float(cutoff)
+    fm.n_filament, fm.n_chain = int(n_filament), int(n_chain)
+    fm.rest_length, fm.k_t, fm.k_b = float(rest_length), float(k_t), float(k_b)
+    return fm
 
 
 class HignnError(RuntimeError):
@@ -267,12 +294,20 @@ class Model:
                                     float(cutoff)))
         return f
 
-    def run_euler(self, x, steps, dt, rebuild_every=1, gravity=(0.0, 0.0, -1.0), De=1.0, a=1.0, re=2.5, cutoff=0.0):
-        """Explicit Euler on the device; returns the final positions."""
+    def forces(self, x, **model):
+        """Forces of force_model(**model) at positions x (n, 3), on the device."""
+        x = np.ascontiguousarray(x, np.float32)
+        f = np.empty_like(x)
+        fm = force_model(**model)
+        check(lib.hignn_forces(self._h, fptr(x), fptr(f), len(x), C.addressof(fm)))
+        return f
+
+    def run_euler(self, x, steps, dt, rebuild_every=1, gravity=(0.0, 0.0, -1.0), **model):
+        """Explicit Euler on the device with the forces of force_model(gravity, **model); returns the final positions."""
         x = np.array(x, np.float32, copy=True)
-        g = np.ascontiguousarray(gravity, np.float32)
-        check(lib.hignn_run_euler(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every), fptr(g),
-                                  float(De), float(a), float(re), float(cutoff)))
+        fm = force_model(gravity=gravity, **model)
+        check(lib.hignn_run_euler(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every),
+                                  C.addressof(fm)))
         return x
 
     def set_shard(self, rank, world):

@@ -106,7 +106,7 @@ struct hignn_model {
   bool has_student = false;
   DevBuf student;         // 2537 FP32 parameters of the far-field student network
 
-  DevBuf x4, perm, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
+  DevBuf x4, perm, slot, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
@@ -195,13 +195,16 @@ void build_structures(hignn_model* m) {
   HIGNN_CUDA(cudaSetDevice(m->device));
   const int64_t n = m->n;
   std::vector<float4> x4(n);
-  std::vector<int32_t> perm(n);
+  std::vector<int32_t> perm(n), slot(n);
   for (int64_t i = 0; i < n; i++) {
     x4[i] = make_float4(m->xt[3 * i], m->xt[3 * i + 1], m->xt[3 * i + 2], 0.f);
     perm[i] = (int32_t)m->tree.perm[i];
+    slot[i] = (int32_t)m->inv_perm[i];
   }
   m->x4.ensure(sizeof(float4) * n);
   m->perm.ensure(sizeof(int32_t) * n);
+  m->slot.ensure(sizeof(int32_t) * n);
+  HIGNN_CUDA(cudaMemcpyAsync(m->slot.p, slot.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
   m->f4.ensure(sizeof(float4) * n);
   m->u.ensure(sizeof(double) * 3 * n);
   m->io_f.ensure(sizeof(float) * 3 * n);
@@ -900,12 +903,13 @@ int hignn_destroy(hignn_model* m) {
   if (m->device >= 0) {
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
-    for (DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
+    for (DevBuf* b : {&m->x4, &m->perm, &m->slot, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
                       &m->weights_tc, &m->counter, &m->student,
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
-                      &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
+                      &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
       b->release();
+    m->cells.release();
     for (auto& e : m->ev)
       if (e) cudaEventDestroy(e);
     if (m->host_ctr) cudaFreeHost(m->host_ctr);
@@ -1100,13 +1104,55 @@ int hignn_pair_forces(hignn_model* m, const float* xyz, float* f, int64_t n, con
   });
 }
 
-int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
-                    const float* gravity, double De, double a, double re, double cutoff) {
+namespace {
+
+void check_force_model(const hignn_force_model& fm, int64_t n) {
+  if (!(fm.morse_cutoff >= 0)) throw Error(HIGNN_ERR_ARG, "forces: the Morse cutoff must be >= 0");
+  if (fm.n_filament < 0 || fm.n_chain < 0 || (fm.n_filament > 0 && fm.n_chain < 1))
+    throw Error(HIGNN_ERR_ARG, "forces: bad filament counts");
+  if (fm.n_filament > 0 && fm.n_filament * (int64_t)fm.n_chain > n)
+    throw Error(HIGNN_ERR_ARG, "forces: the filaments hold more rows than there are particles");
+}
+
+// Forces of fm at positions x (slot[row] = position of caller row `row` in x, or null: x in
+// caller order) into f4 or f3 (same order as x).
+void apply_forces(hignn_model* m, const float4* x, int64_t n, const int32_t* slot, const hignn_force_model& fm,
+                  float4* f4, float* f3) {
+  const hignn::MorseParams mp{(float)fm.morse_De, (float)fm.morse_a, (float)fm.morse_re, fm.morse_cutoff};
+  if (fm.morse_cutoff > 0) m->cells.build(x, n, fm.morse_cutoff, m->stream);
+  const float3 g = make_float3(fm.gravity[0], fm.gravity[1], fm.gravity[2]);
+  hignn::launch_morse(x, n, m->cells, mp, g, f4, f3, m->stream);
+  const hignn::FilamentParams fp{fm.n_filament, fm.n_chain, (float)fm.rest_length, (float)fm.k_t, fm.k_b};
+  hignn::launch_filaments(x, slot, fp, f4, f3, m->stream);
+}
+
+}  // namespace
+
+int hignn_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const hignn_force_model* fm) {
   return guard([&] {
-    if (!m || !xyz) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (!m || !xyz || !f || !fm) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n <= 0) throw Error(HIGNN_ERR_ARG, "forces: n must be positive");
+    check_force_model(*fm, n);
+    require_device(m);
+    m->tmp_x.ensure(sizeof(float4) * n);
+    m->io_f.ensure(sizeof(float) * 3 * n);
+    m->io_u.ensure(sizeof(float) * 3 * n);
+    HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, m->stream));
+    hignn::launch_pack_positions(m->io_f.as<float>(), n, m->tmp_x.as<float4>(), m->stream);
+    apply_forces(m, m->tmp_x.as<float4>(), n, nullptr, *fm, nullptr, m->io_u.as<float>());
+    HIGNN_CUDA(cudaMemcpyAsync(f, m->io_u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+                    const hignn_force_model* fm) {
+  return guard([&] {
+    if (!m || !xyz || !fm) throw Error(HIGNN_ERR_ARG, "null argument");
     if (n != m->n) throw Error(HIGNN_ERR_ARG, "run_euler: particle count differs from the model's");
-    if (steps < 0 || !(dt > 0) || rebuild_every < 0 || cutoff < 0)
-      throw Error(HIGNN_ERR_ARG, "run_euler: need steps >= 0, dt > 0, rebuild_every >= 0, cutoff >= 0");
+    if (steps < 0 || !(dt > 0) || rebuild_every < 0)
+      throw Error(HIGNN_ERR_ARG, "run_euler: need steps >= 0, dt > 0, rebuild_every >= 0");
+    check_force_model(*fm, n);
     require_device(m);
     require_weights(m);
     require_student_if_needed(m);
@@ -1118,16 +1164,13 @@ int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt,
     // start from xyz with a tree built for it
     m->xyz.assign(xyz, xyz + 3 * n);
     build_structures(m);
-    const hignn::MorseParams mp{(float)De, (float)a, (float)re, cutoff};
-    const float3 g = gravity ? make_float3(gravity[0], gravity[1], gravity[2]) : make_float3(0.f, 0.f, 0.f);
     for (int s = 0; s < steps; s++) {
       if (s > 0 && rebuild_every > 0 && s % rebuild_every == 0) {
         download_positions(m);  // m->xyz <- current positions
         build_structures(m);
       }
       // forces at the current positions, in tree order, straight into the matvec's input
-      if (cutoff > 0) m->cells.build(m->x4.as<float4>(), n, cutoff, m->stream);
-      hignn::launch_morse(m->x4.as<float4>(), n, m->cells, mp, g, m->f4.as<float4>(), nullptr, m->stream);
+      apply_forces(m, m->x4.as<float4>(), n, m->slot.as<int32_t>(), *fm, m->f4.as<float4>(), nullptr);
       HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
       matvec_tree_order(m);
       hignn::launch_advance(m->x4.as<float4>(), m->u.as<double>(), n, (float)dt, m->stream);

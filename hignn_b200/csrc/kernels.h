@@ -154,12 +154,24 @@ struct MorseParams {
 
 constexpr int kMaxCells = 16 * 1024 * 1024;
 
+// Filament forces of python/simulate.py:14-88. rest_length and k_t meet float32 arrays there and
+// act as float32; k_b scales the float64 bending sum.
+struct FilamentParams {
+  int64_t n_filament;
+  int n_chain;
+  float rest_length, k_t;
+  double k_b;
+};
+
 // Uniform grid of cells no smaller than the cutoff over the positions' bounding box; items lists
 // the positions cell by cell (start[c] .. start[c + 1]).
 struct CellList {
   CellGrid grid{};
-  DevBuf box, cell, items, count, start, sums;
+  DevBuf box, cell, items, count, start, sums, iota, sorted_cell, sort_tmp;
   void build(const float4* x, int64_t n, double cutoff, cudaStream_t s);
+  void release() {
+    for (DevBuf* b : {&box, &cell, &items, &count, &start, &sums, &iota, &sorted_cell, &sort_tmp}) b->release();
+  }
 };
 
 // f = gravity + Morse forces of every position (f4 and / or f3 (n, 3); either may be null).
@@ -170,6 +182,10 @@ void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorsePar
 void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int64_t* count,
                        const int64_t* off, int* out, cudaStream_t s);
 void launch_advance(float4* x, const double* u, int64_t n, float dt, cudaStream_t s);
+// f += bending, then f += tension, for the filament rows (row -> slot of x and f: slot[row], or
+// the row itself when slot is null); f4 or f3 (n, 3) as in launch_morse.
+void launch_filaments(const float4* x, const int32_t* slot, const FilamentParams& fp, float4* f4, float* f3,
+                      cudaStream_t s);
 void launch_pack_positions(const float* xyz, int64_t n, float4* x4, cudaStream_t s);
 
 // ---------------------------------------------------------------- reorder / misc

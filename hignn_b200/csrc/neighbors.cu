@@ -151,9 +151,8 @@ NeighbourLists::NeighbourLists(int device) : device_(device) {
 NeighbourLists::~NeighbourLists() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
-  for (DevBuf* b : {&x4_, &scan_tmp_, &index_, &loc_off_, &out_, &info2_, &self3_, &info3_, &cells_.box, &cells_.cell,
-                    &cells_.items, &cells_.count, &cells_.start, &cells_.sums})
-    b->release();
+  for (DevBuf* b : {&x4_, &scan_tmp_, &index_, &loc_off_, &out_, &info2_, &self3_, &info3_}) b->release();
+  cells_.release();
   for (NeighbourCsr* c : {&two_, &three_, &trip_}) {
     c->deg.release();
     c->off.release();

@@ -12,6 +12,8 @@
 // device: a uniform grid of cells no smaller than the cutoff replaces the kd-tree (the same
 // neighbour set: every pair within the cutoff lies in adjacent cells), positions stay in tree
 // order, and only the cluster tree is rebuilt on the host, every `rebuild_every` steps.
+#include <cub/device/device_radix_sort.cuh>
+
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -146,12 +148,9 @@ __global__ void k_scan_add(int* __restrict__ start, int m, const int* __restrict
   if (k < m) start[k] += sums[k / kScanChunk];
 }
 
-__global__ void k_cell_fill(const int* __restrict__ cell, int64_t n, const int* __restrict__ start,
-                            int* __restrict__ cursor, int* __restrict__ items) {
+__global__ void k_iota(int* __restrict__ v, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int c = cell[i];
-  items[start[c] + atomicAdd(&cursor[c], 1)] = (int)i;
+  if (i < n) v[i] = (int)i;
 }
 
 // f_i = g + sum of Morse forces of the neighbours of i within the cutoff (order of the reference's
@@ -259,6 +258,116 @@ __global__ void k_neighbours(const float4* __restrict__ x, int64_t n, CellGrid g
   if (count) count[i] = cnt;
 }
 
+// ---- filaments (python/simulate.py:14-88), numpy's arithmetic: every float32 operation rounded on
+// its own (no contraction), the bending and tension sums in float64.
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) {
+  return make_float3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z));
+}
+// np.linalg.norm(v, axis=1): sqrt((x^2 + y^2) + z^2) in float32
+__device__ __forceinline__ float norm3(float3 a) {
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
+}
+__device__ __forceinline__ float3 div3(float3 a, float d) {
+  return make_float3(__fdiv_rn(a.x, d), __fdiv_rn(a.y, d), __fdiv_rn(a.z, d));
+}
+// np.cross: (a1 b2 - a2 b1, a2 b0 - a0 b2, a0 b1 - a1 b0), products rounded before the difference
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+                     __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+                     __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
+// chain_bending's f21 and f23 of the angle at beads (p0, p1, p2) (python/simulate.py:33-50)
+__device__ void bend_terms(float3 p0, float3 p1, float3 p2, float3& f21, float3& f23) {
+  float3 a1 = sub3(p1, p0), a2 = sub3(p2, p1);
+  a1 = div3(a1, norm3(a1));
+  a2 = div3(a2, norm3(a2));
+  const float c = __fadd_rn(__fadd_rn(__fmul_rn(a1.x, a2.x), __fmul_rn(a1.y, a2.y)), __fmul_rn(a1.z, a2.z));
+  float t = __fsub_rn(1.0f, __fmul_rn(c, c));
+  if (t < 0.f) t = 0.f;
+  const float sn = __fsqrt_rn(t);
+  const float3 uv = cross3(a1, a2);
+  const float3 tq = make_float3(__fmul_rn(-uv.x, sn), __fmul_rn(-uv.y, sn), __fmul_rn(-uv.z, sn));
+  f21 = cross3(tq, a1);
+  f23 = cross3(tq, a2);
+}
+
+// chain_tension's nodal force of the bond (p0, p1) (python/simulate.py:77-86)
+__device__ float3 tension_term(float3 p0, float3 p1, float rest, float kt) {
+  const float3 r = sub3(p0, p1);
+  const float rn = norm3(r);
+  const float fm = __fmul_rn(kt, __fsub_rn(rn, rest));
+  const float3 e = div3(r, rn);
+  return make_float3(__fmul_rn(e.x, fm), __fmul_rn(e.y, fm), __fmul_rn(e.z, fm));
+}
+
+__global__ void k_filaments(const float4* __restrict__ x, const int32_t* __restrict__ slot, FilamentParams fp,
+                            float4* __restrict__ f4, float* __restrict__ f3) {
+  const int64_t rows = fp.n_filament * fp.n_chain;
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int N = fp.n_chain;
+  const int s = (int)(r % N);
+  const int64_t base = r - s;
+  auto pos = [&](int q) {
+    const int64_t row = base + q;
+    const float4 v = x[slot ? slot[row] : row];
+    return make_float3(v.x, v.y, v.z);
+  };
+  // F[0:N-2] += f21; F[1:N-1] -= f21 + f23; F[2:N] += f23; F *= k_b
+  double b[3] = {0.0, 0.0, 0.0};
+  float3 f21, f23;
+  if (s <= N - 3) {
+    bend_terms(pos(s), pos(s + 1), pos(s + 2), f21, f23);
+    b[0] = __dadd_rn(b[0], (double)f21.x);
+    b[1] = __dadd_rn(b[1], (double)f21.y);
+    b[2] = __dadd_rn(b[2], (double)f21.z);
+  }
+  if (s >= 1 && s <= N - 2) {
+    bend_terms(pos(s - 1), pos(s), pos(s + 1), f21, f23);
+    b[0] = __dsub_rn(b[0], (double)__fadd_rn(f21.x, f23.x));
+    b[1] = __dsub_rn(b[1], (double)__fadd_rn(f21.y, f23.y));
+    b[2] = __dsub_rn(b[2], (double)__fadd_rn(f21.z, f23.z));
+  }
+  if (s >= 2) {
+    bend_terms(pos(s - 2), pos(s - 1), pos(s), f21, f23);
+    b[0] = __dadd_rn(b[0], (double)f23.x);
+    b[1] = __dadd_rn(b[1], (double)f23.y);
+    b[2] = __dadd_rn(b[2], (double)f23.z);
+  }
+  // F[0:N-1] -= nodal; F[1:N] += nodal
+  double t[3] = {0.0, 0.0, 0.0};
+  if (s <= N - 2) {
+    const float3 q = tension_term(pos(s), pos(s + 1), fp.rest_length, fp.k_t);
+    t[0] = __dsub_rn(t[0], (double)q.x);
+    t[1] = __dsub_rn(t[1], (double)q.y);
+    t[2] = __dsub_rn(t[2], (double)q.z);
+  }
+  if (s >= 1) {
+    const float3 q = tension_term(pos(s - 1), pos(s), fp.rest_length, fp.k_t);
+    t[0] = __dadd_rn(t[0], (double)q.x);
+    t[1] = __dadd_rn(t[1], (double)q.y);
+    t[2] = __dadd_rn(t[2], (double)q.z);
+  }
+  const int64_t o = slot ? slot[r] : r;
+  float v[3];
+  if (f4) {
+    const float4 w = f4[o];
+    v[0] = w.x, v[1] = w.y, v[2] = w.z;
+  } else {
+    v[0] = f3[3 * o], v[1] = f3[3 * o + 1], v[2] = f3[3 * o + 2];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    v[d] = __double2float_rn(__dadd_rn((double)v[d], __dmul_rn(fp.k_b, b[d])));
+    v[d] = __double2float_rn(__dadd_rn((double)v[d], t[d]));
+  }
+  if (f4)
+    f4[o] = make_float4(v[0], v[1], v[2], 0.f);
+  else
+    f3[3 * o] = v[0], f3[3 * o + 1] = v[1], f3[3 * o + 2] = v[2];
+}
+
 // x += (float) u dt (include/TimeIntegrator.hpp:452: mPosition + mVelocity * dt, float velocity)
 __global__ void k_advance(float4* __restrict__ x, const double* __restrict__ u, int64_t n, float dt) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -334,9 +443,20 @@ void CellList::build(const float4* x, int64_t n, double cutoff, cudaStream_t s) 
   k_scan_blocks<<<nb, kScanThreads, 0, s>>>(count.as<int>(), m, start.as<int>(), sums.as<int>());
   k_scan_sums<<<1, kScanThreads, 0, s>>>(sums.as<int>(), nb, start.as<int>() + m);
   k_scan_add<<<nblk(m, 256), 256, 0, s>>>(start.as<int>(), m, sums.as<int>());
-  HIGNN_CUDA(cudaMemsetAsync(count.p, 0, sizeof(int) * (m + 1), s));  // reused as fill cursors
-  k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(cell.as<int>(), n, start.as<int>(), count.as<int>(), items.as<int>());
+  // items: particle indices ordered by (cell, index), by a stable radix sort of the cell ids, so
+  // every sum over a cell's items runs in the same order on every build
+  iota.ensure(sizeof(int) * n);
+  sorted_cell.ensure(sizeof(int) * n);
+  k_iota<<<nblk(n, 256), 256, 0, s>>>(iota.as<int>(), n);
   HIGNN_CHECK_LAUNCH();
+  int bits = 1;
+  while (bits < 31 && (1 << bits) < m) bits++;
+  size_t tmp_bytes = 0;
+  HIGNN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cell.as<int>(), sorted_cell.as<int>(),
+                                             iota.as<int>(), items.as<int>(), (int)n, 0, bits, s));
+  sort_tmp.ensure(tmp_bytes > 0 ? tmp_bytes : 1);
+  HIGNN_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp.p, tmp_bytes, cell.as<int>(), sorted_cell.as<int>(),
+                                             iota.as<int>(), items.as<int>(), (int)n, 0, bits, s));
 }
 
 void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorseParams& mp, float3 grav, float4* f4,
@@ -357,6 +477,14 @@ void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cu
 void launch_advance(float4* x, const double* u, int64_t n, float dt, cudaStream_t s) {
   if (n <= 0) return;
   k_advance<<<nblk(n, 256), 256, 0, s>>>(x, u, n, dt);
+  HIGNN_CHECK_LAUNCH();
+}
+
+void launch_filaments(const float4* x, const int32_t* slot, const FilamentParams& fp, float4* f4, float* f3,
+                      cudaStream_t s) {
+  const int64_t rows = fp.n_filament * (int64_t)fp.n_chain;
+  if (rows <= 0) return;
+  k_filaments<<<nblk(rows, 128), 128, 0, s>>>(x, slot, fp, f4, f3);
   HIGNN_CHECK_LAUNCH();
 }
 

@@ -128,13 +128,29 @@ int hignn_update_coord_keep_tree(hignn_model* m, const float* xyz, int64_t n);
 int hignn_pair_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const float* gravity, double De,
                       double a, double re, double cutoff);
 
+/* The forces of a step: a body force, Morse pair forces (as hignn_pair_forces; cutoff 0: none)
+ * and the filament forces of python/simulate.py:14-88 (chain_bending, then chain_tension, each
+ * added to the float32 force as velocity_update does at :130-142). Filament f holds rows
+ * f * n_chain .. (f + 1) * n_chain - 1 for f < n_filament; the rest are free particles. The
+ * filament arithmetic follows numpy's: float32 arms, norms, crosses and tension, float64 sums. */
+typedef struct hignn_force_model {
+  float gravity[3];
+  double morse_De, morse_a, morse_re, morse_cutoff;
+  int64_t n_filament;
+  int32_t n_chain;
+  double rest_length, k_t, k_b;
+} hignn_force_model;
+
+/* f (n, 3) = the forces of fm at positions xyz (n, 3); host pointers. */
+int hignn_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const hignn_force_model* fm);
+
 /* ExplicitEuler::Run (include/TimeIntegrator.hpp:431-488) with the velocity callback's work on
- * the device: per step f = gravity + pair forces (as hignn_pair_forces), u = M(x) f (as
- * hignn_dot, current settings), x += u dt (float). The tree and lists are built for xyz and
- * rebuilt every `rebuild_every` steps (0: never); in between positions move on the kept tree.
+ * the device: per step f = the forces of fm (as hignn_forces), u = M(x) f (as hignn_dot,
+ * current settings), x += u dt (float). The tree and lists are built for xyz and rebuilt
+ * every `rebuild_every` steps (0: never); in between positions move on the kept tree.
  * xyz (n, 3) is read as the start and overwritten with the final positions. */
 int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
-                    const float* gravity, double De, double a, double re, double cutoff);
+                    const hignn_force_model* fm);
 
 /* Dot -- src/HignnModel.cpp:545-634: u = M(x) f through the H-matrix (close
  * field + ACA far field). Host pointers; u is written, its input ignored. */

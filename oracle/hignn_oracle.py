@@ -1009,3 +1009,74 @@ def edge_info_by_index(info, off, index):
     if not parts:
         return np.zeros((info.shape[0], 0), np.uint64)
     return np.concatenate(parts, axis=1)
+
+
+# ---------------------------------------------------------------- filament forces
+def _cross32(a, b):
+    """np.cross of float32 3-vectors: each product rounded, then the difference."""
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                     a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+
+def _norm32(v):
+    """np.linalg.norm(v, axis=-1) of float32 3-vectors: sqrt((x^2 + y^2) + z^2) in float32."""
+    s = v * v
+    return np.sqrt((s[..., 0] + s[..., 1]) + s[..., 2])
+
+
+def chain_bending(X, k_b):
+    """python/simulate.py:14-54 for chains X (..., N, 3) float32 -> float64 (..., N, 3)."""
+    N = X.shape[-2]
+    F = np.zeros(X.shape, np.float64)
+    if N < 3:
+        return F
+    arm1 = X[..., 1:N - 1, :] - X[..., 0:N - 2, :]
+    arm2 = X[..., 2:N, :] - X[..., 1:N - 1, :]
+    arm1 = arm1 / _norm32(arm1)[..., None]
+    arm2 = arm2 / _norm32(arm2)[..., None]
+    p = arm1 * arm2
+    cos = (p[..., 0] + p[..., 1]) + p[..., 2]
+    tmp = np.float32(1) - cos * cos
+    tmp[tmp < 0] = np.float32(0)
+    sin = np.sqrt(tmp)[..., None]
+    torque = -_cross32(arm1, arm2) * sin
+    f21 = _cross32(torque, arm1)
+    f23 = _cross32(torque, arm2)
+    F[..., 0:N - 2, :] += f21
+    F[..., 1:N - 1, :] -= f21 + f23
+    F[..., 2:N, :] += f23
+    return k_b * F
+
+
+def chain_tension(X, k_t, rest_length):
+    """python/simulate.py:56-88 for chains X (..., N, 3) float32 -> float64 (..., N, 3); rest_length
+    and k_t meet float32 arrays there and act as float32."""
+    N = X.shape[-2]
+    F = np.zeros(X.shape, np.float64)
+    if N < 2:
+        return F
+    r = X[..., 0:N - 1, :] - X[..., 1:N, :]
+    rn = _norm32(r)[..., None]
+    r = r / rn
+    fm = np.float32(k_t) * (rn - np.float32(rest_length))
+    nodal = r * fm
+    F[..., 0:N - 1, :] -= nodal
+    F[..., 1:N, :] += nodal
+    return F
+
+
+def filament_forces(x, f0, n_filament, n_chain, rest_length, k_t, k_b):
+    """velocity_update's force assembly (python/simulate.py:130-142): f0 (float32) += bending, then
+    += tension, per filament of n_chain consecutive rows; all filaments at once (elementwise the same)."""
+    f = np.array(f0, np.float32, copy=True)
+    rows = n_filament * n_chain
+    if rows == 0:
+        return f
+    X = np.asarray(x, np.float32)[:rows].reshape(n_filament, n_chain, 3)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fb = chain_bending(X, float(k_b)).reshape(rows, 3)
+        ft = chain_tension(X, k_t, rest_length).reshape(rows, 3)
+    f[:rows] = (f[:rows].astype(np.float64) + fb).astype(np.float32)
+    f[:rows] = (f[:rows].astype(np.float64) + ft).astype(np.float32)
+    return f

@@ -10,6 +10,8 @@ in different orders (tree order on the device, input order on the host), so afte
 the positions differ in the last bits; the BF16 network rounds its hidden activations to 8 bits,
 which turns those last-bit differences into differences at the BF16 level in some evaluations.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -62,12 +64,41 @@ def test_pair_forces_clustered_and_coincident():
     assert rel_rows(f, ref) < 1e-4  # the coincident pair (|r| < 1e-3) contributes nothing
 
 
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "filament_forces.npz")
+FIL = dict(n_filament=100, n_chain=32, rest_length=2.2, k_t=100.0, k_b=10.0)
+
+
+@pytest.mark.parametrize("case", ["chains", "short", "pairs", "single"])
+def test_filament_forces_match_reference_golden(case):
+    # bit-exact with the reference's own chain_bending / chain_tension (numpy arithmetic)
+    g = np.load(GOLD)
+    nf, nc, L, kt, kb = g[f"{case}_params"]
+    x = g[f"{case}_x"]
+    m = make_model(x)
+    f = m.forces(x, gravity=(0.0, 0.0, -1.0), n_filament=int(nf), n_chain=int(nc), rest_length=L, k_t=kt, k_b=kb)
+    assert np.array_equal(f, g[f"{case}_f"])
+
+
+def test_filaments_compose_with_pair_forces():
+    x = S.filaments(100, 32, 2.2, 0.05, 21)
+    x = (x + np.random.default_rng(2).normal(0, 0.2, x.shape)).astype(np.float32)
+    m = make_model(x)
+    both = m.forces(x, gravity=G, **MORSE, **FIL)
+    pair = m.forces(x, gravity=G, **MORSE)
+    assert np.array_equal(both, O.filament_forces(x, pair, 100, 32, 2.2, 100.0, 10.0))
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_device_euler_matches_host_loop(precision):
     x0 = S.uniform_min_dist(8000, 0.1, 7)
+    # 100 slightly bent filaments along x on a 10 x 10 grid 6 apart, beside the free particles
+    yz = np.stack(np.meshgrid(np.arange(10), np.arange(10)), -1).reshape(100, 1, 2) * 6.0
+    fil = np.concatenate([np.broadcast_to(200.0 + 2.2 * np.arange(32)[None, :, None], (100, 32, 1)),
+                          np.broadcast_to(yz, (100, 32, 2))], axis=2).reshape(3200, 3)
+    x0[:3200] = fil + np.random.default_rng(3).normal(0, 0.05, fil.shape)
     steps, dt, k = 4, 1e-3, 2
     m = make_model(x0, epsilon=1e-2, precision=precision)
-    xd = m.run_euler(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE)
+    xd = m.run_euler(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE, **FIL)
     h = make_model(x0, epsilon=1e-2, precision=precision)
     x = x0.copy()
     for s in range(steps):
@@ -75,7 +106,7 @@ def test_device_euler_matches_host_loop(precision):
             h.update_coord(x)
         elif s > 0:
             h.update_coord_keep_tree(x)
-        f = h.pair_forces(x, G, **MORSE)
+        f = h.forces(x, gravity=G, **MORSE, **FIL)
         u = h.dot(f)
         x = (x + u * np.float32(dt)).astype(np.float32)
     disp = np.linalg.norm(x - x0)
