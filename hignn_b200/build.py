@@ -37,6 +37,7 @@ CU_SOURCES = {
     "student.cu": [],
     "step.cu": [],
     "neighbors.cu": [],
+    "three_body.cu": [],
     "capi.cu": [],
 }
 CXX_SOURCES = {

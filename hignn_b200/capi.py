@@ -112,6 +112,13 @@ SIGNATURES = {
     "hignn_nbl_edge_info_device": ([_P, C.c_int, C.POINTER(C.c_void_p), _i64p], C.c_int),
     "hignn_nbl_last_build_ms": ([_P, _dp], C.c_int),
     "hignn_nbl_get_stream": ([_P, C.POINTER(C.c_void_p)], C.c_int),
+    "hignn_tb_create": ([C.c_int, C.POINTER(_P)], C.c_int),
+    "hignn_tb_destroy": ([_P], None),
+    "hignn_tb_load": ([_P, C.c_int, C.c_char_p], C.c_int),
+    "hignn_tb_load_mem": ([_P, C.c_int, C.c_int, C.POINTER(C.c_int32), _fp], C.c_int),
+    "hignn_tb_set_epsilon": ([_P, C.c_float], C.c_int),
+    "hignn_tb_velocity": ([_P, _fp, _fp, _fp, C.c_int64], C.c_int),
+    "hignn_tb_stats": ([_P, _dp, _dp, _dp, _i64p, _i64p], C.c_int),
 }
 
 for _name, (_args, _res) in SIGNATURES.items():
@@ -427,3 +434,47 @@ class NeighborLists:
         p, e = C.c_void_p(), C.c_int64()
         check(lib.hignn_nbl_edge_info_device(self._h, kind, C.byref(p), C.byref(e)))
         return p.value, e.value
+
+
+TB_THREE_BODY = 0
+TB_SELF = 1
+
+
+class ThreeBody:
+    """Owner of a ``hignn_tb*``: the three-body and self terms of the reference's HIGNN model
+    (python/HIGNN/model_structure.py:76-139) on one device."""
+
+    def __init__(self, device=0, three_body_path=None, self_path=None, epsilon=5.0):
+        from .weights import default_three_body_paths
+
+        h = _P()
+        check(lib.hignn_tb_create(int(device), C.byref(h)))
+        self._h = h
+        d3, ds = default_three_body_paths()
+        check(lib.hignn_tb_load(self._h, TB_THREE_BODY, (three_body_path or d3).encode()))
+        check(lib.hignn_tb_load(self._h, TB_SELF, (self_path or ds).encode()))
+        self.set_epsilon(epsilon)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hignn_tb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_epsilon(self, eps):
+        check(lib.hignn_tb_set_epsilon(self._h, float(eps)))
+
+    def velocity(self, x, f):
+        x = _f32(x)
+        f = _f32(f, x.shape)
+        u = np.empty_like(x)
+        check(lib.hignn_tb_velocity(self._h, fptr(x), fptr(f), fptr(u), len(x)))
+        return u
+
+    def stats(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        t, p = C.c_int64(), C.c_int64()
+        check(lib.hignn_tb_stats(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(t), C.byref(p)))
+        return dict(ms_lists=a.value, ms_three=b.value, ms_self=c.value, triplets=t.value, pairs=p.value)

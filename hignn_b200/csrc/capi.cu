@@ -25,6 +25,7 @@
 #include "kernels.h"
 #include "model_view.h"
 #include "neighbors.h"
+#include "three_body.h"
 #include "tree.h"
 
 using hignn::Error;
@@ -919,46 +920,59 @@ int hignn_destroy(hignn_model* m) {
   return HIGNN_OK;
 }
 
+namespace {
+
+// An HGNW weight file (hignn_b200/weights.py): dense layers W (out x in, row-major) and b.
+void read_hgnw(const char* path, uint32_t want_wrap, std::vector<std::vector<float>>& W,
+               std::vector<std::vector<float>>& B, std::vector<int>& dims) {
+  std::ifstream fh(path, std::ios::binary);
+  if (!fh) throw Error(HIGNN_ERR_IO, std::string("cannot open weight file ") + path);
+  std::vector<char> data((std::istreambuf_iterator<char>(fh)), std::istreambuf_iterator<char>());
+  auto rd32 = [&](size_t off) {
+    if (off + 4 > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
+    uint32_t v;
+    std::memcpy(&v, data.data() + off, 4);
+    return v;
+  };
+  if (data.size() < 20 || std::memcmp(data.data(), "HGNW", 4) != 0)
+    throw Error(HIGNN_ERR_IO, std::string(path) + " is not an HGNW weight file");
+  if (rd32(4) != 1) throw Error(HIGNN_ERR_IO, "unsupported HGNW version");
+  const uint32_t L = rd32(8), act = rd32(12), wrap = rd32(16);
+  if (act != 1 || wrap != want_wrap) throw Error(HIGNN_ERR_IO, std::string(path) + ": not the expected tanh network");
+  if (L < 1 || L > 16) throw Error(HIGNN_ERR_IO, "bad layer count in weight file");
+  size_t off = 20;
+  std::vector<std::pair<uint32_t, uint32_t>> shp;
+  for (uint32_t l = 0; l < L; l++) {
+    shp.push_back({rd32(off), rd32(off + 4)});
+    off += 8;
+  }
+  dims.assign(1, (int)shp[0].second);
+  for (auto& sh : shp) dims.push_back((int)sh.first);
+  W.clear();
+  B.clear();
+  for (auto& sh : shp) {
+    const size_t nw = (size_t)sh.first * sh.second;
+    if (off + 4 * (nw + sh.first) > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
+    std::vector<float> w(nw), b(sh.first);
+    std::memcpy(w.data(), data.data() + off, 4 * nw);
+    off += 4 * nw;
+    std::memcpy(b.data(), data.data() + off, 4 * sh.first);
+    off += 4 * sh.first;
+    W.push_back(std::move(w));
+    B.push_back(std::move(b));
+  }
+  if (off != data.size()) throw Error(HIGNN_ERR_IO, "trailing bytes in weight file");
+}
+
+}  // namespace
+
 int hignn_load_two_body(hignn_model* m, const char* path) {
   return guard([&] {
     if (!m || !path) throw Error(HIGNN_ERR_ARG, "null argument");
-    std::ifstream fh(path, std::ios::binary);
-    if (!fh) throw Error(HIGNN_ERR_IO, std::string("cannot open weight file ") + path);
-    std::vector<char> data((std::istreambuf_iterator<char>(fh)), std::istreambuf_iterator<char>());
-    auto rd32 = [&](size_t off) {
-      if (off + 4 > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
-      uint32_t v;
-      std::memcpy(&v, data.data() + off, 4);
-      return v;
-    };
-    if (data.size() < 20 || std::memcmp(data.data(), "HGNW", 4) != 0)
-      throw Error(HIGNN_ERR_IO, std::string(path) + " is not an HGNW weight file");
-    if (rd32(4) != 1) throw Error(HIGNN_ERR_IO, "unsupported HGNW version");
-    const uint32_t L = rd32(8), act = rd32(12), wrap = rd32(16);
-    if (act != 1 || wrap != 1) throw Error(HIGNN_ERR_IO, "weight file is not a tanh mobility network");
-    if (L != 3) throw Error(HIGNN_ERR_ARG, "two-body network must have 3 dense layers");
-    std::vector<int> dims;
-    size_t off = 20;
-    std::vector<std::pair<uint32_t, uint32_t>> shp;
-    for (uint32_t l = 0; l < L; l++) {
-      shp.push_back({rd32(off), rd32(off + 4)});
-      off += 8;
-    }
-    dims.push_back((int)shp[0].second);
-    for (auto& s : shp) dims.push_back((int)s.first);
     std::vector<std::vector<float>> W, B;
-    for (auto& s : shp) {
-      const size_t nw = (size_t)s.first * s.second;
-      if (off + 4 * (nw + s.first) > data.size()) throw Error(HIGNN_ERR_IO, "truncated weight file");
-      std::vector<float> w(nw), b(s.first);
-      std::memcpy(w.data(), data.data() + off, 4 * nw);
-      off += 4 * nw;
-      std::memcpy(b.data(), data.data() + off, 4 * s.first);
-      off += 4 * s.first;
-      W.push_back(std::move(w));
-      B.push_back(std::move(b));
-    }
-    if (off != data.size()) throw Error(HIGNN_ERR_IO, "trailing bytes in weight file");
+    std::vector<int> dims;
+    read_hgnw(path, 1, W, B, dims);
+    if (W.size() != 3) throw Error(HIGNN_ERR_ARG, "two-body network must have 3 dense layers");
     upload_weights(m, W, B, dims);
   });
 }
@@ -1607,5 +1621,158 @@ int hignn_nbl_get_stream(hignn_nbl* l, void** stream) {
   return guard([&] {
     if (!l || !stream) throw Error(HIGNN_ERR_ARG, "null argument");
     *stream = (void*)l->lists.stream();
+  });
+}
+
+// ---------------------------------------------------------------- three-body near field
+
+struct hignn_tb {
+  hignn::NeighbourLists lists;
+  hignn::TbNet nets[2];
+  int num_sms = 0;
+  float eps = 5.0f;
+  DevBuf f4, fin, u, err;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double ms_lists = 0, ms_three = 0, ms_self = 0;
+  int64_t triplets = 0, pairs = 0;
+  explicit hignn_tb(int device) : lists(device) {
+    HIGNN_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    for (auto& e : ev) HIGNN_CUDA(cudaEventCreate(&e));
+  }
+  ~hignn_tb() {
+    cudaSetDevice(lists.device());
+    cudaStreamSynchronize(lists.stream());
+    for (DevBuf* b : {&f4, &fin, &u, &err}) b->release();
+    for (auto& n : nets)
+      for (DevBuf* b : {&n.d_img, &n.d_w1, &n.d_b2, &n.d_b3, &n.d_w4, &n.d_b4}) b->release();
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+namespace {
+
+void tb_set(hignn_tb* t, int which, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,
+            const std::vector<int>& dims) {
+  if (which != HIGNN_TB_THREE_BODY && which != HIGNN_TB_SELF) throw Error(HIGNN_ERR_ARG, "unknown network kind");
+  const int kin = which == HIGNN_TB_THREE_BODY ? 6 : 3;
+  if (dims.size() != 5 || dims[0] != kin || dims[1] != hignn::kTbH1 || dims[2] != hignn::kTbH2 ||
+      dims[3] != hignn::kTbH3 || dims[4] != 9)
+    throw Error(HIGNN_ERR_ARG, which == HIGNN_TB_THREE_BODY ? "three-body network must be 6 -> 256 -> 1024 -> 512 -> 9"
+                                                            : "self network must be 3 -> 256 -> 1024 -> 512 -> 9");
+  HIGNN_CUDA(cudaSetDevice(t->lists.device()));
+  hignn::tb_upload(t->nets[which], kin, W, B, t->lists.stream());
+}
+
+}  // namespace
+
+int hignn_tb_create(int device, hignn_tb** out) {
+  return guard([&] {
+    if (!out) throw Error(HIGNN_ERR_ARG, "null argument");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      throw Error(HIGNN_ERR_NODEV, "three-body: no CUDA device");
+    }
+    if (device < 0 || device >= count) throw Error(HIGNN_ERR_ARG, "three-body: bad device");
+    *out = new hignn_tb(device);
+  });
+}
+
+void hignn_tb_destroy(hignn_tb* t) { delete t; }
+
+int hignn_tb_load(hignn_tb* t, int which, const char* path) {
+  return guard([&] {
+    if (!t || !path) throw Error(HIGNN_ERR_ARG, "null argument");
+    std::vector<std::vector<float>> W, B;
+    std::vector<int> dims;
+    read_hgnw(path, which == HIGNN_TB_SELF ? 3u : 2u, W, B, dims);
+    tb_set(t, which, W, B, dims);
+  });
+}
+
+int hignn_tb_load_mem(hignn_tb* t, int which, int num_layers, const int32_t* dims, const float* params) {
+  return guard([&] {
+    if (!t || !dims || !params) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (num_layers != 4) throw Error(HIGNN_ERR_ARG, "three-body networks have 4 dense layers");
+    std::vector<int> d(dims, dims + num_layers + 1);
+    std::vector<std::vector<float>> W, B;
+    const float* p = params;
+    for (int l = 0; l < num_layers; l++) {
+      const size_t o = d[l + 1], i = d[l];
+      W.emplace_back(p, p + o * i);
+      p += o * i;
+      B.emplace_back(p, p + o);
+      p += o;
+    }
+    tb_set(t, which, W, B, d);
+  });
+}
+
+int hignn_tb_set_epsilon(hignn_tb* t, float eps) {
+  return guard([&] {
+    if (!t) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (!(eps > 0.f)) throw Error(HIGNN_ERR_ARG, "three-body: epsilon must be positive");
+    t->eps = eps;
+  });
+}
+
+int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n) {
+  return guard([&] {
+    if (!t || !xyz || !f || !u) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n <= 0) throw Error(HIGNN_ERR_ARG, "three-body: n must be positive");
+    if (!t->nets[0].loaded || !t->nets[1].loaded)
+      throw Error(HIGNN_ERR_STATE, "three-body: load both the three-body and the self network");
+    HIGNN_CUDA(cudaSetDevice(t->lists.device()));
+    cudaStream_t s = t->lists.stream();
+    const auto t0 = std::chrono::steady_clock::now();
+    t->lists.update_coord(xyz, n);
+    t->lists.set_three_body_epsilon(t->eps);
+    t->lists.build_three_body();
+    t->ms_lists = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    int64_t e3 = 0, es = 0;
+    const uint64_t* tri = t->lists.device_list(hignn::kEdgesThreeBody, &e3);
+    const uint64_t* self = t->lists.device_list(hignn::kEdgesThreeBodySelf, &es);
+    t->triplets = e3;
+    t->pairs = es;
+    t->fin.ensure(sizeof(float) * 3 * n);
+    t->f4.ensure(sizeof(float4) * n);
+    t->u.ensure(sizeof(float) * 3 * n);
+    t->err.ensure(sizeof(int));
+    HIGNN_CUDA(cudaMemcpyAsync(t->fin.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+    hignn::launch_pack_positions(t->fin.as<float>(), n, t->f4.as<float4>(), s);
+    HIGNN_CUDA(cudaMemsetAsync(t->u.p, 0, sizeof(float) * 3 * n, s));
+    HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), s));
+    HIGNN_CUDA(cudaEventRecord(t->ev[0], s));
+    hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), tri, e3, t->lists.positions(), t->f4.as<float4>(),
+                             t->u.as<float>(), t->err.as<int>(), t->num_sms, s);
+    HIGNN_CUDA(cudaEventRecord(t->ev[1], s));
+    hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), self, es, t->lists.positions(), t->f4.as<float4>(),
+                             t->u.as<float>(), t->err.as<int>(), t->num_sms, s);
+    HIGNN_CUDA(cudaEventRecord(t->ev[2], s));
+    int e = 0;
+    HIGNN_CUDA(cudaMemcpyAsync(u, t->u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+    HIGNN_CUDA(cudaMemcpyAsync(&e, t->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HIGNN_CUDA(cudaStreamSynchronize(s));
+    float a = 0, b = 0;
+    HIGNN_CUDA(cudaEventElapsedTime(&a, t->ev[0], t->ev[1]));
+    HIGNN_CUDA(cudaEventElapsedTime(&b, t->ev[1], t->ev[2]));
+    t->ms_three = a;
+    t->ms_self = b;
+    if (e != 0)
+      throw Error(HIGNN_ERR_LIMIT, "three-body kernel: a wait timed out (code " + std::to_string(e) + ")");
+  });
+}
+
+int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
+                   int64_t* pairs) {
+  return guard([&] {
+    if (!t) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (ms_lists) *ms_lists = t->ms_lists;
+    if (ms_three) *ms_three = t->ms_three;
+    if (ms_self) *ms_self = t->ms_self;
+    if (triplets) *triplets = t->triplets;
+    if (pairs) *pairs = t->pairs;
   });
 }

@@ -49,6 +49,8 @@ class NeighbourLists {
   // The whole list on the device, (rows, edges) row-major, owned by this object.
   const uint64_t* device_list(int kind, int64_t* edges) const;
   cudaStream_t stream() const { return stream_; }
+  const float4* positions() const { return x4_.as<float4>(); }
+  int device() const { return device_; }
   double last_build_ms() const { return build_ms_; }
 
  private:

@@ -1,0 +1,569 @@
+// Three-body and self near field on the tensor cores (python/HIGNN/model_structure.py:41-139).
+//
+// The reference evaluates, for every triplet (a, b, c) of the three-body edge list
+// (include/NeighborLists.hpp:512-585; the model reads its rows as (j, k, i)),
+//     M = Three_body_net(x_b - x_a, x_c - x_b) = net(.) / |x_b - x_a| / |x_c - x_b|   (3 x 3)
+//     u_c += M f_a                                                              (:94-101)
+// and for every self pair (a, b) of the self edge list,
+//     M = Two_body_self_net(x_a - x_b) = net(.) / |x_a - x_b| / |x_a - x_b|,   u_b += M f_b
+// (:57-67, 120-125), with torch FP32 Linear layers kin -> 256 -> 1024 -> 512 -> 9 and tanh.
+//
+// Here one persistent kernel per list does gather -> network -> bmm -> scatter for 128 edges per
+// tile. Layer 1 (kin <= 6 inputs) runs on the CUDA cores in FP32 and writes tanh'd FP16 pairs as
+// the A operand of layer 2. Layers 2 and 3 are tcgen05 MMAs (FP16 in, FP32 accumulated in tensor
+// memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP32 tanh of layer 3.
+// Tensor memory holds 512 FP32 columns per lane: two 128-column layer-2 accumulators and a
+// 256-column layer-3 accumulator. The 512 layer-3 outputs therefore take two passes per tile,
+// each recomputing layer 2 (1.33x the network's FLOPs) -- the layer-2 activations of a tile
+// (128 x 1024 FP16 = 256 KB) fit neither shared nor tensor memory.
+// Layer 2 is cut into eight chunks of 128 outputs; each chunk's accumulator is tanh'd by the
+// epilogue into an FP16 buffer (two of them, in turn) that is at once the K-slice of layer 3.
+// The weights (1.6 MB of FP16) stream through a six-deep ring of 16 KB shared-memory stages,
+// filled by bulk copies from a host-built image laid out in the order the MMAs consume it.
+//
+// CTA = 18 warps: 0-15 epilogue (warp w reaches TMEM lanes 32 (w % 4) + 0..31, so row
+// e = 32 (w % 4) + lane has four threads, part p = w / 4), 16 MMA lane, 17 producer.
+// Every wait is bounded (about two seconds of clock); on a timeout the CTA records an error,
+// stops, lets its copies and MMAs drain and frees its tensor memory.
+#include <cuda_fp16.h>
+
+#include <cstring>
+
+#include "three_body.h"
+#include "tc_mlp.cuh"
+
+namespace hignn {
+
+namespace {
+
+using tc::fence_after;
+using tc::fence_before;
+using tc::mbar_arrive;
+using tc::mbar_init;
+using tc::mbar_try_sleep;
+using tc::mma_commit;
+using tc::saddr;
+using tc::sdesc;
+using tc::tmem_ld32;
+using tc::tmem_wait_ld;
+
+constexpr int kEpiThreads = 512;
+constexpr int kMmaWarp = 16, kProdWarp = 17, kThreads = 576;
+constexpr int kRing = 6;
+constexpr uint32_t kOffD2 = 0, kOffD3 = 256;  // D2 buffers at 0 and 128
+constexpr long long kWait = 4000000000LL;      // ~2 s at 1.9 GHz
+
+struct TbSmem {
+  uint8_t act1[4][16384];     // A of layer 2: 128 rows x 256 K (FP16), four 64-wide K blocks
+  uint8_t act2[2][2][16384];  // A of layer 3, two buffers of 128 rows x 128 K
+  uint8_t ring[kRing][kTbStageBytes];
+  uint64_t act1_full, d2_full[2], e2_done[2], d3_full, d3_free, ring_full[kRing], ring_empty[kRing], drain;
+  uint32_t tmem_base;
+  int abort_flag;
+};
+constexpr size_t kSmemBytes = sizeof(TbSmem) + 1024;  // + alignment slack
+static_assert(kSmemBytes <= 232448, "three-body shared memory exceeds the per-CTA limit");
+
+__device__ __forceinline__ bool wait_bar(uint64_t* b, uint32_t parity, int* abort_flag, int* err, int code,
+                                         bool honour_abort = true) {
+  const long long t0 = clock64();
+  while (!mbar_try_sleep(b, parity, 20000u)) {
+    if (honour_abort && *(volatile int*)abort_flag) return false;
+    if (clock64() - t0 > kWait) {
+      atomicExch(abort_flag, 1);
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(saddr(dst)),
+      "l"(src), "r"(bytes), "r"(saddr(bar))
+      : "memory");
+}
+
+// FP16 operands: layer inputs are tanh outputs in [-1, 1] and the weights stay below 1 in
+// magnitude, so FP16's 11-bit significand (BF16 has 8) costs no range and cuts the rounding
+// error of the tensor-core layers about eightfold at the same MMA rate.
+__device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ uint32_t tanh_f16x2(uint32_t x) {
+  uint32_t y;
+  asm("tanh.approx.f16x2 %0, %1;\n" : "=r"(y) : "r"(x));
+  return y;
+}
+// Instruction descriptor: F16 x F16 -> FP32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, const uint32_t* v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3])
+               : "memory");
+}
+
+__device__ __forceinline__ bool epi_all(bool ok) {
+  uint32_t r;
+  asm volatile("{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, 512, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+               : "=r"(r)
+               : "r"((uint32_t)ok)
+               : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
+
+// Byte offset of (row, k) in a 128-row, 64-wide K block (K-major, 128-byte swizzle) for the
+// 16-byte chunk kc8 = k / 8.
+__device__ __forceinline__ uint32_t swz_chunk(int row, int kc8) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((kc8 ^ (row & 7)) << 4));
+}
+
+// The network input of edge q (6 features; the self net uses the first 3) and its endpoints.
+template <int KIND>
+__device__ __forceinline__ void edge_input(const uint64_t* __restrict__ edges, int64_t E, int64_t q,
+                                           const float4* __restrict__ x, float (&in)[6], int64_t& src, int64_t& dst) {
+  if (KIND == kTbThreeBody) {
+    const int64_t a = (int64_t)edges[q], b = (int64_t)edges[E + q], c = (int64_t)edges[2 * E + q];
+    const float4 xa = x[a], xb = x[b], xc = x[c];
+    in[0] = xb.x - xa.x, in[1] = xb.y - xa.y, in[2] = xb.z - xa.z;
+    in[3] = xc.x - xb.x, in[4] = xc.y - xb.y, in[5] = xc.z - xb.z;
+    src = a, dst = c;
+  } else {
+    const int64_t a = (int64_t)edges[q], b = (int64_t)edges[E + q];
+    const float4 xa = x[a], xb = x[b];
+    in[0] = xa.x - xb.x, in[1] = xa.y - xb.y, in[2] = xa.z - xb.z;
+    in[3] = in[4] = in[5] = 0.f;
+    src = b, dst = b;
+  }
+}
+
+__device__ __forceinline__ float norm3f(float a, float b, float c) { return sqrtf(a * a + b * b + c * c); }
+
+// ------------------------------------------------------------------ epilogue warps
+template <int KIND>
+struct Epi {
+  TbSmem& s;
+  TbWeightsDev w;
+  const uint64_t* edges;
+  int64_t E;
+  const float4* x;
+  const float4* f;
+  float* u;
+  int* err;
+  int e, part;     // row of the tile, column part
+  uint32_t tlane;  // TMEM address of this warp's lane quarter
+  bool ok = true;
+
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
+    if (!ok) return false;
+    ok = wait_bar(b, parity, &s.abort_flag, err, code);
+    if (ok) fence_after();
+    return ok;
+  }
+
+  // features and layer 1 of tile t into act1 (this thread: outputs 64 part .. + 63 of row e)
+  __device__ void layer1(int64_t t) {
+    const int64_t q = t * 128 + e;
+    float in[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int64_t src, dst;
+    if (q < E) edge_input<KIND>(edges, E, q, x, in, src, dst);
+    const float4* w1 = reinterpret_cast<const float4*>(w.w1);
+    const uint32_t base = saddr(s.act1[part]);
+#pragma unroll 1
+    for (int jj = 0; jj < 8; jj++) {
+      uint32_t v[4];
+#pragma unroll
+      for (int pr = 0; pr < 4; pr++) {
+        float acc[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int n = 64 * part + 8 * jj + 2 * pr + h;
+          const float4 wa = __ldg(&w1[2 * n]), wb = __ldg(&w1[2 * n + 1]);
+          float a = wb.z;  // b1
+          a = fmaf(wa.x, in[0], a);
+          a = fmaf(wa.y, in[1], a);
+          a = fmaf(wa.z, in[2], a);
+          a = fmaf(wa.w, in[3], a);
+          a = fmaf(wb.x, in[4], a);
+          a = fmaf(wb.y, in[5], a);
+          acc[h] = a;
+        }
+        v[pr] = tanh_f16x2(pack_f16(acc[0], acc[1]));
+      }
+      st_shared_v4(base + swz_chunk(e, jj), v);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    mbar_arrive(&s.act1_full);
+  }
+
+  // layer-2 chunk g: accumulator buffer g & 1 -> tanh'd FP16 into act2[g & 1]
+  __device__ void layer2(uint32_t g) {
+    const uint32_t b = g & 1;
+    if (wait(&s.d2_full[b], (g >> 1) & 1, 41)) {
+      uint32_t v[32];
+      tmem_ld32(tlane + kOffD2 + 128 * b + 32 * part, v);
+      tmem_wait_ld();
+      const float* b2 = w.b2 + (g & 7) * 128 + 32 * part;
+      uint32_t pk[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const float lo = __uint_as_float(v[2 * j]) + __ldg(&b2[2 * j]);
+        const float hi = __uint_as_float(v[2 * j + 1]) + __ldg(&b2[2 * j + 1]);
+        pk[j] = tanh_f16x2(pack_f16(lo, hi));
+      }
+      const uint32_t base = saddr(s.act2[b][part >> 1]);
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) st_shared_v4(base + swz_chunk(e, 4 * (part & 1) + jj), pk + 4 * jj);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    fence_before();
+    mbar_arrive(&s.e2_done[b]);
+  }
+
+  // layer 3 of pass h (D3 columns 64 part .. + 63) and its share of layer 4
+  __device__ void layer3(uint32_t P, int h, float (&y)[9]) {
+    if (wait(&s.d3_full, P & 1, 42)) {
+#pragma unroll 1
+      for (int half = 0; half < 2; half++) {
+        uint32_t v[32];
+        tmem_ld32(tlane + kOffD3 + 64 * part + 32 * half, v);
+        tmem_wait_ld();
+        const int n0 = h * 256 + 64 * part + 32 * half;
+#pragma unroll 4
+        for (int j = 0; j < 32; j++) {
+          const int n = n0 + j;
+          float a;
+          asm("tanh.approx.f32 %0, %1;\n" : "=f"(a) : "f"(__uint_as_float(v[j]) + __ldg(&w.b3[n])));
+#pragma unroll
+          for (int o = 0; o < 9; o++) y[o] = fmaf(a, __ldg(&w.w4[o * kTbH3 + n]), y[o]);
+        }
+      }
+    }
+    fence_before();
+    mbar_arrive(&s.d3_free);
+  }
+
+  // sum of the four parts' layer-4 shares, wrapper, 3x3 times the force, scatter (part 0)
+  __device__ void output(int64_t t) {
+    const int64_t q = t * 128 + e;
+    if (q >= E) return;
+    const float* scratch = reinterpret_cast<const float*>(&s.act2[0][0][0]);
+    float yy[9];
+#pragma unroll
+    for (int o = 0; o < 9; o++) {
+      float v = scratch[(0 * 128 + e) * 9 + o];
+      v += scratch[(1 * 128 + e) * 9 + o];
+      v += scratch[(2 * 128 + e) * 9 + o];
+      v += scratch[(3 * 128 + e) * 9 + o];
+      yy[o] = v + __ldg(&w.b4[o]);
+    }
+    float in[6];
+    int64_t src, dst;
+    edge_input<KIND>(edges, E, q, x, in, src, dst);
+    if (KIND == kTbThreeBody) {
+      const float r1 = norm3f(in[0], in[1], in[2]), r2 = norm3f(in[3], in[4], in[5]);
+#pragma unroll
+      for (int o = 0; o < 9; o++) yy[o] = yy[o] / r1 / r2;
+    } else {
+      const float r = norm3f(in[0], in[1], in[2]);
+#pragma unroll
+      for (int o = 0; o < 9; o++) yy[o] = yy[o] / r / r;
+    }
+    const float4 fs = f[src];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      atomicAdd(&u[3 * dst + i], yy[3 * i] * fs.x + yy[3 * i + 1] * fs.y + yy[3 * i + 2] * fs.z);
+  }
+
+  __device__ void run(int64_t ntiles) {
+    uint32_t g = 0, P = 0;
+    if ((int64_t)blockIdx.x < ntiles) layer1(blockIdx.x);
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      float y[9];
+#pragma unroll
+      for (int o = 0; o < 9; o++) y[o] = 0.f;
+      bool go = true;
+      for (int h = 0; h < 2 && go; h++) {
+#pragma unroll 1
+        for (int c = 0; c < 8; c++, g++) {
+          layer2(g);
+          // all layer-2 MMAs of tile t are complete (the last chunk's accumulator was waited
+          // for): act1 may take the next tile
+          if (h == 1 && c == 7 && ok && t + gridDim.x < ntiles) layer1(t + gridDim.x);
+        }
+        layer3(P++, h, y);
+        if (h == 1) {
+          float* scratch = reinterpret_cast<float*>(&s.act2[0][0][0]);
+#pragma unroll
+          for (int o = 0; o < 9; o++) scratch[(part * 128 + e) * 9 + o] = y[o];
+        }
+        go = epi_all(ok);
+        if (go && h == 1) {
+          if (part == 0) output(t);
+          epi_bar();  // the scratch is act2, which the next tile's first chunk overwrites
+        }
+      }
+      if (!go) break;
+    }
+  }
+};
+
+// ------------------------------------------------------------------ MMA lane
+struct MmaLaneTb {
+  TbSmem& s;
+  int* err;
+  uint32_t tb;
+  uint32_t S = 0;  // weight stages consumed
+  bool ok = true;
+
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
+    if (!ok) return false;
+    ok = wait_bar(b, parity, &s.abort_flag, err, code);
+    if (ok) fence_after();
+    return ok;
+  }
+  __device__ __forceinline__ bool stage_ready() { return wait(&s.ring_full[S % kRing], (S / kRing) & 1, 51); }
+  __device__ __forceinline__ void stage_done() {
+    mma_commit(&s.ring_empty[S % kRing]);
+    S++;
+  }
+  // layer-2 chunk g (of a 16-chunk tile) into D2[g & 1]
+  __device__ bool l2(uint32_t g) {
+    if (g >= 2 && !wait(&s.e2_done[g & 1], ((g - 2) >> 1) & 1, 52)) return false;
+    const uint32_t d = tb + kOffD2 + 128 * (g & 1);
+    const uint32_t id = idesc_f16(128, 128);
+    for (uint32_t kb = 0; kb < 4; kb++) {
+      if (!stage_ready()) return false;
+      const uint32_t a = saddr(s.act1[kb]), b = saddr(s.ring[S % kRing]);
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++) mma_ss(d, sdesc(a + 32 * kk), sdesc(b + 32 * kk), id, (kb | kk) != 0);
+      stage_done();
+    }
+    mma_commit(&s.d2_full[g & 1]);
+    return true;
+  }
+  // layer-3 K-slice of chunk g (local chunk c) into D3
+  __device__ bool l3(uint32_t g, uint32_t c, uint32_t P) {
+    if (!wait(&s.e2_done[g & 1], (g >> 1) & 1, 53)) return false;
+    if (c == 0 && P > 0 && !wait(&s.d3_free, (P - 1) & 1, 54)) return false;
+    const uint32_t id = idesc_f16(128, 128);
+    for (uint32_t nh = 0; nh < 2; nh++)
+      for (uint32_t kb = 0; kb < 2; kb++) {
+        if (!stage_ready()) return false;
+        const uint32_t a = saddr(s.act2[g & 1][kb]), b = saddr(s.ring[S % kRing]);
+#pragma unroll
+        for (uint32_t kk = 0; kk < 4; kk++)
+          mma_ss(tb + kOffD3 + 128 * nh, sdesc(a + 32 * kk), sdesc(b + 32 * kk), id, (c | kb | kk) != 0);
+        stage_done();
+      }
+    if (c == 7) mma_commit(&s.d3_full);
+    return true;
+  }
+
+  __device__ void run(int64_t ntiles) {
+    uint32_t g = 0, P = 0, k = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, k++) {
+      if (!wait(&s.act1_full, k & 1, 50)) break;
+      for (int h = 0; h < 2 && ok; h++, g += 8, P++) {
+        // per pass: L2(0) L2(1) L3(0) L2(2) L3(1) ... L2(7) L3(6) L3(7)
+        for (int step = 0; step < 16 && ok; step++) {
+          if (step < 2)
+            l2(g + step);
+          else if (step == 15)
+            l3(g + 7, 7, P);
+          else if ((step & 1) == 0)
+            l3(g + (step - 2) / 2, (step - 2) / 2, P);
+          else
+            l2(g + (step + 1) / 2);
+        }
+      }
+    }
+    // let every issued MMA finish before the tensor memory is freed
+    mma_commit(&s.drain);
+    wait_bar(&s.drain, 0, &s.abort_flag, err, 55, false);
+  }
+};
+
+// ------------------------------------------------------------------ producer
+__device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err) {
+  uint32_t S = 0;
+  bool ok = true;
+  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x)
+    for (int st = 0; st < kTbStagesPerTile; st++, S++) {
+      const uint32_t slot = S % kRing;
+      if (S >= kRing && !wait_bar(&s.ring_empty[slot], ((S / kRing) - 1) & 1, &s.abort_flag, err, 56)) {
+        ok = false;
+        break;
+      }
+      bulk_load(s.ring[slot], img + (size_t)st * kTbStageBytes, kTbStageBytes, &s.ring_full[slot]);
+    }
+  // every issued copy must land before the CTA exits
+  const uint32_t first = S > (uint32_t)kRing ? S - kRing : 0;
+  for (uint32_t q = first; q < S; q++) wait_bar(&s.ring_full[q % kRing], (q / kRing) & 1, &s.abort_flag, err, 57, false);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_three_body(TbWeightsDev w, const uint64_t* __restrict__ edges, int64_t E, int64_t ntiles,
+                 const float4* __restrict__ x, const float4* __restrict__ f, float* __restrict__ u, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = saddr(smem_raw);
+  TbSmem& s = *reinterpret_cast<TbSmem*>(smem_raw + (((raw + 1023u) & ~1023u) - raw));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&s.act1_full, kEpiThreads);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&s.d2_full[b], 1);
+      mbar_init(&s.e2_done[b], kEpiThreads);
+    }
+    mbar_init(&s.d3_full, 1);
+    mbar_init(&s.d3_free, kEpiThreads);
+    for (int r = 0; r < kRing; r++) {
+      mbar_init(&s.ring_full[r], 1);
+      mbar_init(&s.ring_empty[r], 1);
+    }
+    mbar_init(&s.drain, 1);
+    s.abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == kMmaWarp) tc::tmem_alloc(&s.tmem_base, 512);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp < kMmaWarp) {
+    Epi<KIND> ep{s, w, edges, E, x, f, u, err};
+    ep.e = 32 * (warp & 3) + lane;
+    ep.part = warp >> 2;
+    ep.tlane = s.tmem_base + ((uint32_t)(32 * (warp & 3)) << 16);
+    ep.run(ntiles);
+  } else if (warp == kMmaWarp) {
+    if (lane == 0) {
+      MmaLaneTb ml{s, err, s.tmem_base};
+      ml.run(ntiles);
+    }
+  } else if (warp == kProdWarp && lane == 0) {
+    producer(s, w.img, ntiles, err);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == kMmaWarp) {
+    __syncwarp();
+    tc::tmem_dealloc(s.tmem_base, 512);
+  }
+}
+
+template <int KIND>
+void launch_kind(const TbWeightsDev& w, const uint64_t* edges, int64_t E, int64_t ntiles, const float4* x,
+                 const float4* f, float* u, int* err, int num_sms, cudaStream_t s) {
+  HIGNN_CUDA(cudaFuncSetAttribute(k_three_body<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  const int grid = (int)(ntiles < num_sms ? ntiles : num_sms);
+  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(w, edges, E, ntiles, x, f, u, err);
+  HIGNN_CHECK_LAUNCH();
+}
+
+uint16_t f16_of(float v) {
+  const __half h = __float2half_rn(v);
+  uint16_t b;
+  std::memcpy(&b, &h, 2);
+  return b;
+}
+
+}  // namespace
+
+int64_t launch_three_body(int kind, const TbWeightsDev& w, const uint64_t* edges, int64_t num_edges, const float4* x,
+                          const float4* f, float* u, int* err, int num_sms, cudaStream_t s) {
+  const int64_t ntiles = (num_edges + 127) / 128;
+  if (ntiles == 0) return 0;
+  if (kind == kTbThreeBody)
+    launch_kind<kTbThreeBody>(w, edges, num_edges, ntiles, x, f, u, err, num_sms, s);
+  else
+    launch_kind<kTbSelf>(w, edges, num_edges, ntiles, x, f, u, err, num_sms, s);
+  return ntiles;
+}
+
+void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,
+               cudaStream_t s) {
+  if (W.size() != 4 || B.size() != 4) throw Error(-1, "three-body network: need 4 dense layers");
+  const size_t want[4][2] = {{kTbH1, (size_t)kin}, {kTbH2, kTbH1}, {kTbH3, kTbH2}, {9, kTbH3}};
+  for (int l = 0; l < 4; l++)
+    if (W[l].size() != want[l][0] * want[l][1] || B[l].size() != want[l][0])
+      throw Error(-1, "three-body network: layer sizes must be kin -> 256 -> 1024 -> 512 -> 9");
+  net.kin = kin;
+  net.w1.assign(kTbH1 * 8, 0.f);
+  for (int n = 0; n < kTbH1; n++) {
+    for (int k = 0; k < kin; k++) net.w1[n * 8 + k] = W[0][(size_t)n * kin + k];
+    net.w1[n * 8 + 6] = B[0][n];
+  }
+  net.b2 = B[1];
+  net.b3 = B[2];
+  net.w4 = W[3];
+  net.b4 = B[3];
+  // layers 2 and 3 as 16 KB FP16 stages (128 rows x 64 K, K-major, 128-byte swizzle) in the MMA
+  // lane's order: per pass h, L2(0) L2(1) L3(0) L2(2) L3(1) ... L2(7) L3(6) L3(7); an L2 chunk c is
+  // four K blocks of W2 rows c*128..; an L3 slice (h, c) is (N half, K block) pairs of W3 rows
+  // h*256 + nh*128.. and columns c*128 + kb*64..
+  std::vector<uint8_t> img(kTbImageBytes, 0);
+  auto swz = [](int row, int kc) -> size_t {
+    return (size_t)(row >> 3) * 1024 + (row & 7) * 128 + (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
+  };
+  size_t st = 0;
+  auto put_stage = [&](const std::vector<float>& M, int ld, int row0, int col0) {
+    uint8_t* dst = img.data() + st * kTbStageBytes;
+    for (int n = 0; n < 128; n++)
+      for (int kc = 0; kc < 64; kc++) {
+        const uint16_t v = f16_of(M[(size_t)(row0 + n) * ld + col0 + kc]);
+        std::memcpy(dst + swz(n, kc), &v, 2);
+      }
+    st++;
+  };
+  for (int h = 0; h < 2; h++)
+    for (int step = 0; step < 16; step++) {
+      int c;
+      bool isl2;
+      if (step < 2)
+        c = step, isl2 = true;
+      else if (step == 15)
+        c = 7, isl2 = false;
+      else if ((step & 1) == 0)
+        c = (step - 2) / 2, isl2 = false;
+      else
+        c = (step + 1) / 2, isl2 = true;
+      if (isl2)
+        for (int kb = 0; kb < 4; kb++) put_stage(W[1], kTbH1, c * 128, kb * 64);
+      else
+        for (int nh = 0; nh < 2; nh++)
+          for (int kb = 0; kb < 2; kb++) put_stage(W[2], kTbH2, h * 256 + nh * 128, c * 128 + kb * 64);
+    }
+  if (st != (size_t)kTbStagesPerTile) throw Error(-1, "three-body image: stage count mismatch");
+  net.d_img.ensure(img.size());
+  net.d_w1.ensure(sizeof(float) * net.w1.size());
+  net.d_b2.ensure(sizeof(float) * net.b2.size());
+  net.d_b3.ensure(sizeof(float) * net.b3.size());
+  net.d_w4.ensure(sizeof(float) * net.w4.size());
+  net.d_b4.ensure(sizeof(float) * net.b4.size());
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_img.p, img.data(), img.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_w1.p, net.w1.data(), sizeof(float) * net.w1.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_b2.p, net.b2.data(), sizeof(float) * net.b2.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_b3.p, net.b3.data(), sizeof(float) * net.b3.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_w4.p, net.w4.data(), sizeof(float) * net.w4.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaMemcpyAsync(net.d_b4.p, net.b4.data(), sizeof(float) * net.b4.size(), cudaMemcpyHostToDevice, s));
+  HIGNN_CUDA(cudaStreamSynchronize(s));
+  net.loaded = true;
+}
+
+}  // namespace hignn

@@ -12,7 +12,8 @@ little-endian blob instead (extension ``.hgnw``):
     4       u32         format version (1)
     8       u32         number of dense layers L
     12      u32         hidden activation (1 = tanh, 2 = SiLU)
-    16      u32         output wrapper (1 = mobility: (y + I) / |r|, I for |r| < 1e-5)
+    16      u32         output wrapper (1 = mobility: (y + I) / |r|, I for |r| < 1e-5;
+                        2 = three-body: y / |r1| / |r2|; 3 = self: y / |r| / |r|)
     20      u32[2L]     (out_features, in_features) per layer
     ...     f32[]       per layer: weight (out x in, row-major), then bias (out)
 
@@ -32,6 +33,8 @@ VERSION = 1
 ACT_TANH = 1
 ACT_SILU = 2
 WRAP_MOBILITY = 1
+WRAP_THREE_BODY = 2
+WRAP_SELF = 3
 
 
 @dataclass
@@ -86,11 +89,39 @@ def load_hgnw(path: str) -> MlpWeights:
     return MlpWeights(ws, bs, act, wrap)
 
 
-def export_pkl(pkl_path: str, out_path: str) -> MlpWeights:
-    """Convert a reference ``nn.Sequential`` pickle into an ``.hgnw`` blob."""
+def _load_reference_pickle(pkl_path: str, module_dir: str | None):
+    """Unpickle a reference network. The three-body and self networks are pickled inside the
+    wrappers of python/HIGNN/model_structure.py, which import torch_scatter at module level; a
+    stand-in module is enough to unpickle them (scatter is not called)."""
+    import sys
+    import types
+
+    import torch
+
+    added = False
+    if module_dir and module_dir not in sys.path:
+        sys.path.insert(0, module_dir)
+        added = True
+    stub = "torch_scatter" not in sys.modules
+    if stub:
+        sys.modules["torch_scatter"] = types.SimpleNamespace(scatter=None)
+    try:
+        return torch.load(pkl_path, weights_only=False, map_location="cpu")
+    finally:
+        if stub:
+            del sys.modules["torch_scatter"]
+        if added:
+            sys.path.remove(module_dir)
+
+
+def export_pkl(pkl_path: str, out_path: str, wrapper: int = WRAP_MOBILITY, module_dir: str | None = None) -> MlpWeights:
+    """Convert a reference ``nn.Sequential`` pickle (or a model_structure wrapper holding one as
+    ``.net``) into an ``.hgnw`` blob."""
     import torch  # only needed to unpickle the reference file
 
-    net = torch.load(pkl_path, weights_only=False, map_location="cpu")
+    net = _load_reference_pickle(pkl_path, module_dir)
+    if hasattr(net, "net") and isinstance(net.net, torch.nn.Module):
+        net = net.net
     mods = list(net.children()) if hasattr(net, "children") else list(net)
     ws, bs, act = [], [], None
     for m in mods:
@@ -105,9 +136,16 @@ def export_pkl(pkl_path: str, out_path: str) -> MlpWeights:
             raise ValueError(f"unsupported module in {pkl_path}: {m}")
     if act is None:
         raise ValueError(f"{pkl_path}: mixed or missing activations")
-    mlp = MlpWeights(ws, bs, act, WRAP_MOBILITY)
+    mlp = MlpWeights(ws, bs, act, wrapper)
     save_hgnw(out_path, mlp)
     return mlp
+
+
+def default_three_body_paths():
+    """The shipped three-body and self networks (exported from the reference's
+    python/Saved_Model/Unbounded/HIGNN_nn_{3body,self}.pkl)."""
+    d = os.path.join(os.path.dirname(__file__), "data")
+    return os.path.join(d, "three_body_unbounded.hgnw"), os.path.join(d, "self_unbounded.hgnw")
 
 
 def default_two_body_path() -> str:
@@ -139,6 +177,10 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="export a reference .pkl network to .hgnw")
     ap.add_argument("pkl")
     ap.add_argument("out")
+    ap.add_argument("--wrapper", type=int, default=WRAP_MOBILITY,
+                    help="1 two-body mobility, 2 three-body, 3 self")
+    ap.add_argument("--module-dir", default=None,
+                    help="directory holding the HIGNN package the pickle refers to (reference python/)")
     a = ap.parse_args()
-    m = export_pkl(a.pkl, a.out)
+    m = export_pkl(a.pkl, a.out, a.wrapper, a.module_dir)
     print("exported", a.out, "dims", m.dims)

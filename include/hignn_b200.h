@@ -297,6 +297,40 @@ int hignn_nbl_edge_info_device(hignn_nbl* l, int kind, const uint64_t** d_info, 
 int hignn_nbl_last_build_ms(hignn_nbl* l, double* ms);
 int hignn_nbl_get_stream(hignn_nbl* l, void** stream);
 
+/* ---------------------------------------------------------------- three-body near field
+ * The three-body and self terms of HIGNN_model.forward (python/HIGNN/model_structure.py:76-139)
+ * with Three_body_net (:41-55) and Two_body_self_net (:58-70): for every triplet (a, b, c) of
+ * the three-body edge list at epsilon (NeighborLists::BuildThreeBodyInfo, read as (j, k, i)),
+ *     u_c += (net3(x_b - x_a, x_c - x_b) / |x_b - x_a| / |x_c - x_b|) f_a
+ * and for every self edge (a, b),  u_b += (net_self(x_a - x_b) / |x_a - x_b|^2) f_b
+ * (the two-body term is the H-matrix product, hignn_dot). Networks kin -> 256 -> 1024 -> 512
+ * -> 9 with tanh (kin 6 and 3); layers 2 and 3 on the tensor cores (BF16 operands, FP32
+ * accumulation), layers 1 and 4 in FP32. */
+typedef struct hignn_tb hignn_tb;
+
+#define HIGNN_TB_THREE_BODY 0
+#define HIGNN_TB_SELF 1
+
+int hignn_tb_create(int device, hignn_tb** out);
+void hignn_tb_destroy(hignn_tb* t);
+
+/* Load the three-body (which = HIGNN_TB_THREE_BODY, HGNW wrapper 2) or self (HIGNN_TB_SELF,
+ * wrapper 3) network from an HGNW file, or from memory: dims[num_layers + 1], params = per layer
+ * W (out x in, row-major) then b, float32. */
+int hignn_tb_load(hignn_tb* t, int which, const char* path);
+int hignn_tb_load_mem(hignn_tb* t, int which, int num_layers, const int32_t* dims, const float* params);
+
+/* Three-body cutoff (the NeighborLists three-body epsilon; default 5). */
+int hignn_tb_set_epsilon(hignn_tb* t, float eps);
+
+/* u (n, 3) = three-body + self velocities for positions xyz and forces f (host, float32 (n, 3)).
+ * Builds the edge lists on the device, then runs both networks. */
+int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n);
+
+/* Last call: ms of the list build, the three-body and the self kernels, and the edge counts. */
+int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
+                   int64_t* pairs);
+
 #ifdef __cplusplus
 }
 #endif

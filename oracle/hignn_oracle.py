@@ -1080,3 +1080,67 @@ def filament_forces(x, f0, n_filament, n_chain, rest_length, k_t, k_b):
     f[:rows] = (f[:rows].astype(np.float64) + fb).astype(np.float32)
     f[:rows] = (f[:rows].astype(np.float64) + ft).astype(np.float32)
     return f
+
+
+# ---------------------------------------------------------------- three-body near field
+class DenseTanh:
+    """A tanh MLP (W: out x in, row-major) as python/HIGNN/model_structure.py's nn.Sequential."""
+
+    def __init__(self, weights, biases):
+        self.w64 = [np.asarray(w, np.float64) for w in weights]
+        self.b64 = [np.asarray(b, np.float64) for b in biases]
+
+    @classmethod
+    def from_hgnw(cls, path):
+        import sys
+
+        sys.path.insert(0, os.path.dirname(_HERE))
+        from hignn_b200.weights import load_hgnw  # file-format reader only
+
+        m = load_hgnw(path)
+        return cls(m.weights, m.biases)
+
+    def __call__(self, z, chunk=8192):
+        z = np.asarray(z, np.float64)
+        out = np.empty((len(z), self.w64[-1].shape[0]), np.float64)
+        for s in range(0, len(z), chunk):
+            h = z[s:s + chunk]
+            for li, (w, b) in enumerate(zip(self.w64, self.b64)):
+                h = h @ w.T + b
+                if li + 1 < len(self.w64):
+                    h = np.tanh(h)
+            out[s:s + chunk] = h
+        return out
+
+
+def three_body_velocity(x, f, eps, net3, net_self):
+    """The three-body and self terms of HIGNN_model.forward (python/HIGNN/model_structure.py:94-139)
+    on the edge lists of NeighborLists at the three-body epsilon, in FP64 from float32 positions:
+      triplet rows (a, b, c) (read as (j, k, i)): x_in = (x_b - x_a, x_c - x_b) in float32,
+        M = net3(x_in) / |x_b - x_a| / |x_c - x_b|  (Three_body_net, :41-55),  u_c += M f_a;
+      self rows (a, b) (read as (j, i)): x_in = x_a - x_b,
+        M = net_self(x_in) / |x_in| / |x_in|  (Two_body_self_net, :58-70),  u_b += M f_b."""
+    x = np.asarray(x, np.float32)
+    f = np.asarray(f, np.float32).astype(np.float64)
+    n = len(x)
+    off, nbr = neighbour_csr(x, eps)
+    info, _ = three_body_edge_info(off, nbr)
+    pairs = two_body_edge_info(off, nbr)
+    u = np.zeros((n, 3), np.float64)
+    if info.shape[1]:
+        a, b, c = (info[k].astype(np.int64) for k in range(3))
+        d1 = x[b] - x[a]
+        d2 = x[c] - x[b]
+        y = net3(np.concatenate([d1, d2], axis=1))
+        r1 = np.linalg.norm(d1.astype(np.float64), axis=1)
+        r2 = np.linalg.norm(d2.astype(np.float64), axis=1)
+        M = (y / r1[:, None] / r2[:, None]).reshape(-1, 3, 3)
+        np.add.at(u, c, np.einsum("eij,ej->ei", M, f[a]))
+    if pairs.shape[1]:
+        a, b = (pairs[k].astype(np.int64) for k in range(2))
+        d = x[a] - x[b]
+        y = net_self(d)
+        r = np.linalg.norm(d.astype(np.float64), axis=1)
+        M = (y / r[:, None] / r[:, None]).reshape(-1, 3, 3)
+        np.add.at(u, b, np.einsum("eij,ej->ei", M, f[b]))
+    return u
