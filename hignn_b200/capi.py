@@ -119,6 +119,7 @@ SIGNATURES = {
     "hignn_tb_set_epsilon": ([_P, C.c_float], C.c_int),
     "hignn_tb_velocity": ([_P, _fp, _fp, _fp, C.c_int64], C.c_int),
     "hignn_tb_stats": ([_P, _dp, _dp, _dp, _i64p, _i64p], C.c_int),
+    "hignn_tb_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
 }
 
 for _name, (_args, _res) in SIGNATURES.items():
@@ -478,3 +479,11 @@ class ThreeBody:
         t, p = C.c_int64(), C.c_int64()
         check(lib.hignn_tb_stats(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(t), C.byref(p)))
         return dict(ms_lists=a.value, ms_three=b.value, ms_self=c.value, triplets=t.value, pairs=p.value)
+
+    def wait_profile(self):
+        """Clocks the three-body (then self) kernel's MMA lane waited for act1, weight stages, layer-2
+        epilogues, the layer-3 accumulator; its total; the producer's waits for free slots."""
+        c = (C.c_uint64 * 12)()
+        check(lib.hignn_tb_wait_profile(self._h, c))
+        keys = ["wait_act1", "wait_stage", "wait_epilogue", "wait_d3", "total", "producer_wait"]
+        return {"three_body": dict(zip(keys, c[:6])), "self": dict(zip(keys, c[6:]))}

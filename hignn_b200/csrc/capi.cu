@@ -1631,7 +1631,7 @@ struct hignn_tb {
   hignn::TbNet nets[2];
   int num_sms = 0;
   float eps = 5.0f;
-  DevBuf f4, fin, u, err;
+  DevBuf f4, fin, u, err, prof;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double ms_lists = 0, ms_three = 0, ms_self = 0;
   int64_t triplets = 0, pairs = 0;
@@ -1642,7 +1642,7 @@ struct hignn_tb {
   ~hignn_tb() {
     cudaSetDevice(lists.device());
     cudaStreamSynchronize(lists.stream());
-    for (DevBuf* b : {&f4, &fin, &u, &err}) b->release();
+    for (DevBuf* b : {&f4, &fin, &u, &err, &prof}) b->release();
     for (auto& n : nets)
       for (DevBuf* b : {&n.d_img, &n.d_w1, &n.d_b2, &n.d_b3, &n.d_w4, &n.d_b4}) b->release();
     for (auto& e : ev)
@@ -1740,16 +1740,18 @@ int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, i
     t->f4.ensure(sizeof(float4) * n);
     t->u.ensure(sizeof(float) * 3 * n);
     t->err.ensure(sizeof(int));
+    t->prof.ensure(sizeof(unsigned long long) * 12);
+    HIGNN_CUDA(cudaMemsetAsync(t->prof.p, 0, sizeof(unsigned long long) * 12, s));
     HIGNN_CUDA(cudaMemcpyAsync(t->fin.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
     hignn::launch_pack_positions(t->fin.as<float>(), n, t->f4.as<float4>(), s);
     HIGNN_CUDA(cudaMemsetAsync(t->u.p, 0, sizeof(float) * 3 * n, s));
     HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), s));
     HIGNN_CUDA(cudaEventRecord(t->ev[0], s));
     hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), tri, e3, t->lists.positions(), t->f4.as<float4>(),
-                             t->u.as<float>(), t->err.as<int>(), t->num_sms, s);
+                             t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>(), t->num_sms, s);
     HIGNN_CUDA(cudaEventRecord(t->ev[1], s));
     hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), self, es, t->lists.positions(), t->f4.as<float4>(),
-                             t->u.as<float>(), t->err.as<int>(), t->num_sms, s);
+                             t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>() + 6, t->num_sms, s);
     HIGNN_CUDA(cudaEventRecord(t->ev[2], s));
     int e = 0;
     HIGNN_CUDA(cudaMemcpyAsync(u, t->u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
@@ -1762,6 +1764,16 @@ int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, i
     t->ms_self = b;
     if (e != 0)
       throw Error(HIGNN_ERR_LIMIT, "three-body kernel: a wait timed out (code " + std::to_string(e) + ")");
+  });
+}
+
+int hignn_tb_wait_profile(hignn_tb* t, uint64_t* counters) {
+  return guard([&] {
+    if (!t || !counters) throw Error(HIGNN_ERR_ARG, "null argument");
+    HIGNN_CUDA(cudaSetDevice(t->lists.device()));
+    std::memset(counters, 0, sizeof(uint64_t) * 12);
+    if (!t->prof.p) return;
+    HIGNN_CUDA(cudaMemcpy(counters, t->prof.p, sizeof(uint64_t) * 12, cudaMemcpyDeviceToHost));
   });
 }
 

@@ -217,13 +217,13 @@ struct Epi {
       uint32_t v[32];
       tmem_ld32(tlane + kOffD2 + 128 * b + 32 * part, v);
       tmem_wait_ld();
-      const float* b2 = w.b2 + (g & 7) * 128 + 32 * part;
+      const float4* b2 = reinterpret_cast<const float4*>(w.b2 + (g & 7) * 128 + 32 * part);
       uint32_t pk[16];
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const float lo = __uint_as_float(v[2 * j]) + __ldg(&b2[2 * j]);
-        const float hi = __uint_as_float(v[2 * j + 1]) + __ldg(&b2[2 * j + 1]);
-        pk[j] = tanh_f16x2(pack_f16(lo, hi));
+      for (int j = 0; j < 8; j++) {
+        const float4 bb = __ldg(&b2[j]);
+        pk[2 * j] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * j]) + bb.x, __uint_as_float(v[4 * j + 1]) + bb.y));
+        pk[2 * j + 1] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * j + 2]) + bb.z, __uint_as_float(v[4 * j + 3]) + bb.w));
       }
       const uint32_t base = saddr(s.act2[b][part >> 1]);
 #pragma unroll
@@ -243,13 +243,28 @@ struct Epi {
         tmem_ld32(tlane + kOffD3 + 64 * part + 32 * half, v);
         tmem_wait_ld();
         const int n0 = h * 256 + 64 * part + 32 * half;
-#pragma unroll 4
-        for (int j = 0; j < 32; j++) {
-          const int n = n0 + j;
-          float a;
-          asm("tanh.approx.f32 %0, %1;\n" : "=f"(a) : "f"(__uint_as_float(v[j]) + __ldg(&w.b3[n])));
+        const float4* b3 = reinterpret_cast<const float4*>(w.b3 + n0);
+        const float4* w4 = reinterpret_cast<const float4*>(w.w4) + 3 * n0;  // [n][12]: W4[0..8][n], 0, 0, 0
+#pragma unroll 2
+        for (int j4 = 0; j4 < 8; j4++) {
+          const float4 bb = __ldg(&b3[j4]);
+          const float bv[4] = {bb.x, bb.y, bb.z, bb.w};
 #pragma unroll
-          for (int o = 0; o < 9; o++) y[o] = fmaf(a, __ldg(&w.w4[o * kTbH3 + n]), y[o]);
+          for (int i = 0; i < 4; i++) {
+            const int j = 4 * j4 + i;
+            float a;
+            asm("tanh.approx.f32 %0, %1;\n" : "=f"(a) : "f"(__uint_as_float(v[j]) + bv[i]));
+            const float4 wa = __ldg(&w4[3 * j]), wb = __ldg(&w4[3 * j + 1]), wc = __ldg(&w4[3 * j + 2]);
+            y[0] = fmaf(a, wa.x, y[0]);
+            y[1] = fmaf(a, wa.y, y[1]);
+            y[2] = fmaf(a, wa.z, y[2]);
+            y[3] = fmaf(a, wa.w, y[3]);
+            y[4] = fmaf(a, wb.x, y[4]);
+            y[5] = fmaf(a, wb.y, y[5]);
+            y[6] = fmaf(a, wb.z, y[6]);
+            y[7] = fmaf(a, wb.w, y[7]);
+            y[8] = fmaf(a, wc.x, y[8]);
+          }
         }
       }
     }
@@ -329,10 +344,13 @@ struct MmaLaneTb {
   uint32_t tb;
   uint32_t S = 0;  // weight stages consumed
   bool ok = true;
+  long long waited[4] = {0, 0, 0, 0};  // clocks spent waiting for act1, weight stages, epilogues, D3
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
     if (!ok) return false;
+    const long long t0 = clock64();
     ok = wait_bar(b, parity, &s.abort_flag, err, code);
+    waited[code == 50 ? 0 : code == 51 ? 1 : code == 54 ? 3 : 2] += clock64() - t0;
     if (ok) fence_after();
     return ok;
   }
@@ -374,7 +392,8 @@ struct MmaLaneTb {
     return true;
   }
 
-  __device__ void run(int64_t ntiles) {
+  __device__ void run(int64_t ntiles, unsigned long long* prof) {
+    const long long start = clock64();
     uint32_t g = 0, P = 0, k = 0;
     for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, k++) {
       if (!wait(&s.act1_full, k & 1, 50)) break;
@@ -395,17 +414,25 @@ struct MmaLaneTb {
     // let every issued MMA finish before the tensor memory is freed
     mma_commit(&s.drain);
     wait_bar(&s.drain, 0, &s.abort_flag, err, 55, false);
+    if (prof) {
+      for (int i = 0; i < 4; i++) atomicAdd(&prof[i], (unsigned long long)waited[i]);
+      atomicAdd(&prof[4], (unsigned long long)(clock64() - start));
+    }
   }
 };
 
 // ------------------------------------------------------------------ producer
-__device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err) {
+__device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err, unsigned long long* prof) {
   uint32_t S = 0;
   bool ok = true;
+  long long waited = 0;
   for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x)
     for (int st = 0; st < kTbStagesPerTile; st++, S++) {
       const uint32_t slot = S % kRing;
-      if (S >= kRing && !wait_bar(&s.ring_empty[slot], ((S / kRing) - 1) & 1, &s.abort_flag, err, 56)) {
+      const long long t0 = clock64();
+      const bool got = S < kRing || wait_bar(&s.ring_empty[slot], ((S / kRing) - 1) & 1, &s.abort_flag, err, 56);
+      waited += clock64() - t0;
+      if (!got) {
         ok = false;
         break;
       }
@@ -414,12 +441,14 @@ __device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err
   // every issued copy must land before the CTA exits
   const uint32_t first = S > (uint32_t)kRing ? S - kRing : 0;
   for (uint32_t q = first; q < S; q++) wait_bar(&s.ring_full[q % kRing], (q / kRing) & 1, &s.abort_flag, err, 57, false);
+  if (prof) atomicAdd(&prof[5], (unsigned long long)waited);
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1)
     k_three_body(TbWeightsDev w, const uint64_t* __restrict__ edges, int64_t E, int64_t ntiles,
-                 const float4* __restrict__ x, const float4* __restrict__ f, float* __restrict__ u, int* err) {
+                 const float4* __restrict__ x, const float4* __restrict__ f, float* __restrict__ u, int* err,
+                 unsigned long long* prof) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = saddr(smem_raw);
   TbSmem& s = *reinterpret_cast<TbSmem*>(smem_raw + (((raw + 1023u) & ~1023u) - raw));
@@ -453,10 +482,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == kMmaWarp) {
     if (lane == 0) {
       MmaLaneTb ml{s, err, s.tmem_base};
-      ml.run(ntiles);
+      ml.run(ntiles, prof);
     }
   } else if (warp == kProdWarp && lane == 0) {
-    producer(s, w.img, ntiles, err);
+    producer(s, w.img, ntiles, err, prof);
   }
   fence_before();
   __syncthreads();
@@ -469,10 +498,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 template <int KIND>
 void launch_kind(const TbWeightsDev& w, const uint64_t* edges, int64_t E, int64_t ntiles, const float4* x,
-                 const float4* f, float* u, int* err, int num_sms, cudaStream_t s) {
+                 const float4* f, float* u, int* err, unsigned long long* prof, int num_sms, cudaStream_t s) {
   HIGNN_CUDA(cudaFuncSetAttribute(k_three_body<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   const int grid = (int)(ntiles < num_sms ? ntiles : num_sms);
-  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(w, edges, E, ntiles, x, f, u, err);
+  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(w, edges, E, ntiles, x, f, u, err, prof);
   HIGNN_CHECK_LAUNCH();
 }
 
@@ -486,13 +515,14 @@ uint16_t f16_of(float v) {
 }  // namespace
 
 int64_t launch_three_body(int kind, const TbWeightsDev& w, const uint64_t* edges, int64_t num_edges, const float4* x,
-                          const float4* f, float* u, int* err, int num_sms, cudaStream_t s) {
+                          const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
+                          cudaStream_t s) {
   const int64_t ntiles = (num_edges + 127) / 128;
   if (ntiles == 0) return 0;
   if (kind == kTbThreeBody)
-    launch_kind<kTbThreeBody>(w, edges, num_edges, ntiles, x, f, u, err, num_sms, s);
+    launch_kind<kTbThreeBody>(w, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
   else
-    launch_kind<kTbSelf>(w, edges, num_edges, ntiles, x, f, u, err, num_sms, s);
+    launch_kind<kTbSelf>(w, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
   return ntiles;
 }
 
@@ -511,7 +541,9 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   }
   net.b2 = B[1];
   net.b3 = B[2];
-  net.w4 = W[3];
+  net.w4.assign((size_t)kTbH3 * 12, 0.f);  // transposed, 12 per row (three float4 loads)
+  for (int n = 0; n < kTbH3; n++)
+    for (int o = 0; o < 9; o++) net.w4[(size_t)n * 12 + o] = W[3][(size_t)o * kTbH3 + n];
   net.b4 = B[3];
   // layers 2 and 3 as 16 KB FP16 stages (128 rows x 64 K, K-major, 128-byte swizzle) in the MMA
   // lane's order: per pass h, L2(0) L2(1) L3(0) L2(2) L3(1) ... L2(7) L3(6) L3(7); an L2 chunk c is

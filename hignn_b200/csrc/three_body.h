@@ -22,7 +22,7 @@ struct TbWeightsDev {
   const float* w1;     // [256][8]: W1 row (kin entries, zero padded to 6), b1, 0
   const float* b2;     // [1024]
   const float* b3;     // [512]
-  const float* w4;     // [9][512]
+  const float* w4;     // [512][12]: column n of W4 (9 entries), zero padded
   const float* b4;     // [9]
 };
 
@@ -43,9 +43,12 @@ struct TbNet {
 // u[c] += ((net(x_b - x_a, x_c - x_b) / |x_b - x_a| / |x_c - x_b|) as 3x3) f[a] for every triplet
 // (a, b, c) of the list (rows of the (3, E) uint64 edge list), kind kTbThreeBody; or
 // u[b] += ((net(x_a - x_b) / |x_a - x_b|^2) as 3x3) f[b] for every pair (a, b), kind kTbSelf.
-// x, f as float4 (w unused), u float (n, 3). Returns the number of 128-edge tiles launched.
+// x, f as float4 (w unused), u float (n, 3). prof (optional, 6 counters, summed over CTAs):
+// clocks the MMA lane waited for layer-1 operands, weight stages, layer-2 epilogues and the
+// layer-3 accumulator, its total clocks, and clocks the producer waited for free ring slots.
+// Returns the number of 128-edge tiles launched.
 int64_t launch_three_body(int kind, const TbWeightsDev& w, const uint64_t* edges, int64_t num_edges, const float4* x,
-                          const float4* f, float* u, int* err, int num_sms, cudaStream_t s);
+                          const float4* f, float* u, int* err, unsigned long long* prof, int num_sms, cudaStream_t s);
 
 // Builds the device image of a network from its dense layers (W row-major out x in, b).
 void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,

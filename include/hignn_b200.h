@@ -331,6 +331,11 @@ int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, i
 int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
                    int64_t* pairs);
 
+/* Where the last call's kernels waited, summed over CTAs (12 counters: three-body, then self):
+ * clocks the MMA lane waited for layer-1 operands, weight stages, layer-2 epilogues and the
+ * layer-3 accumulator; its total clocks; clocks the producer waited for free weight slots. */
+int hignn_tb_wait_profile(hignn_tb* t, uint64_t* counters);
+
 #ifdef __cplusplus
 }
 #endif
