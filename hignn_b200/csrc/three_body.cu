@@ -9,16 +9,20 @@
 // (:57-67, 120-125), with torch FP32 Linear layers kin -> 256 -> 1024 -> 512 -> 9 and tanh.
 //
 // Here one persistent kernel per list does gather -> network -> bmm -> scatter for 128 edges per
-// tile. Layer 1 (kin <= 6 inputs) runs on the CUDA cores in FP32 and writes tanh'd FP16 pairs as
-// the A operand of layer 2. Layers 2 and 3 are tcgen05 MMAs (FP16 in, FP32 accumulated in tensor
-// memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP32 tanh of layer 3.
-// Tensor memory holds 512 FP32 columns per lane: two 128-column layer-2 accumulators and a
-// 256-column layer-3 accumulator. The 512 layer-3 outputs therefore take two passes per tile,
-// each recomputing layer 2 (1.33x the network's FLOPs) -- the layer-2 activations of a tile
-// (128 x 1024 FP16 = 256 KB) fit neither shared nor tensor memory.
-// Layer 2 is cut into eight chunks of 128 outputs; each chunk's accumulator is tanh'd by the
-// epilogue into an FP16 buffer (two of them, in turn) that is at once the K-slice of layer 3.
-// The weights (1.6 MB of FP16) stream through a six-deep ring of 16 KB shared-memory stages,
+// tile. Layer 1 (kin <= 6 inputs) runs on the CUDA cores in FP32 and writes tanh'd FP16 pairs
+// into tensor memory as the A operand of layer 2. Layers 2 and 3 are tcgen05 MMAs (FP16 in, FP32
+// accumulated in tensor memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP32
+// tanh of layer 3. Tensor memory (512 columns) holds the layer-1 activations (128 columns of FP16
+// pairs), one 128-column layer-2 accumulator and a 256-column layer-3 accumulator. The 512
+// layer-3 outputs therefore take two passes per tile, each recomputing layer 2 (1.33x the
+// network's FLOPs) -- the layer-2 activations of a tile (128 x 1024 FP16 = 256 KB) fit neither
+// shared nor tensor memory.
+// Layer 2 is cut into sixteen chunks of 128 outputs (eight per pass); the epilogue releases the
+// layer-2 accumulator as soon as it has read it, then writes the chunk's tanh'd FP16 values to a
+// shared-memory buffer (two, in turn) that is the K-slice of layer 3 (N = 256). The MMA lane
+// interleaves the chunks, L2(g + 1) before L3(g), so the tensor pipe has a layer-3 slice to run
+// while the epilogue turns an accumulator around.
+// The weights (1.6 MB of FP16) stream through a five-deep ring of 32 KB shared-memory stages,
 // filled by bulk copies from a host-built image laid out in the order the MMAs consume it.
 //
 // CTA = 18 warps: 0-15 epilogue (warp w reaches TMEM lanes 32 (w % 4) + 0..31, so row
@@ -49,15 +53,14 @@ using tc::tmem_wait_ld;
 
 constexpr int kEpiThreads = 512;
 constexpr int kMmaWarp = 16, kProdWarp = 17, kThreads = 576;
-constexpr int kRing = 6;
-constexpr uint32_t kOffD2 = 0, kOffD3 = 256;  // D2 buffers at 0 and 128
+constexpr int kRing = 5;
+constexpr uint32_t kOffA1 = 0, kOffD2 = 128, kOffD3 = 256;  // tensor-memory columns
 constexpr long long kWait = 4000000000LL;      // ~2 s at 1.9 GHz
 
 struct TbSmem {
-  uint8_t act1[4][16384];     // A of layer 2: 128 rows x 256 K (FP16), four 64-wide K blocks
-  uint8_t act2[2][2][16384];  // A of layer 3, two buffers of 128 rows x 128 K
+  uint8_t act2[2][2][16384];  // A of layer 3, two buffers of 128 rows x 128 K (FP16)
   uint8_t ring[kRing][kTbStageBytes];
-  uint64_t act1_full, d2_full[2], e2_done[2], d3_full, d3_free, ring_full[kRing], ring_empty[kRing], drain;
+  uint64_t act1_full, d2_full, d2_free, act2_full[2], d3_full, d3_free, ring_full[kRing], ring_empty[kRing], drain;
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -175,23 +178,23 @@ struct Epi {
     return ok;
   }
 
-  // features and layer 1 of tile t into act1 (this thread: outputs 64 part .. + 63 of row e)
+  // features and layer 1 of tile t into the tensor-memory A operand of layer 2 (this thread:
+  // outputs 64 part .. + 63 of row e, as FP16 pairs in columns 32 part .. + 31)
   __device__ void layer1(int64_t t) {
     const int64_t q = t * 128 + e;
     float in[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int64_t src, dst;
     if (q < E) edge_input<KIND>(edges, E, q, x, in, src, dst);
     const float4* w1 = reinterpret_cast<const float4*>(w.w1);
-    const uint32_t base = saddr(s.act1[part]);
 #pragma unroll 1
-    for (int jj = 0; jj < 8; jj++) {
-      uint32_t v[4];
+    for (int half = 0; half < 2; half++) {
+      uint32_t pk[16];
 #pragma unroll
-      for (int pr = 0; pr < 4; pr++) {
+      for (int pr = 0; pr < 16; pr++) {
         float acc[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const int n = 64 * part + 8 * jj + 2 * pr + h;
+          const int n = 64 * part + 32 * half + 2 * pr + h;
           const float4 wa = __ldg(&w1[2 * n]), wb = __ldg(&w1[2 * n + 1]);
           float a = wb.z;  // b1
           a = fmaf(wa.x, in[0], a);
@@ -202,21 +205,24 @@ struct Epi {
           a = fmaf(wb.y, in[5], a);
           acc[h] = a;
         }
-        v[pr] = tanh_f16x2(pack_f16(acc[0], acc[1]));
+        pk[pr] = tanh_f16x2(pack_f16(acc[0], acc[1]));
       }
-      st_shared_v4(base + swz_chunk(e, jj), v);
+      tc::tmem_st16(tlane + kOffA1 + 32 * part + 16 * half, pk);
     }
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    tc::tmem_wait_st();
+    fence_before();
     mbar_arrive(&s.act1_full);
   }
 
-  // layer-2 chunk g: accumulator buffer g & 1 -> tanh'd FP16 into act2[g & 1]
+  // layer-2 chunk g: the accumulator (released once read) -> tanh'd FP16 into act2[g & 1]
   __device__ void layer2(uint32_t g) {
     const uint32_t b = g & 1;
-    if (wait(&s.d2_full[b], (g >> 1) & 1, 41)) {
+    if (wait(&s.d2_full, g & 1, 41)) {
       uint32_t v[32];
-      tmem_ld32(tlane + kOffD2 + 128 * b + 32 * part, v);
+      tmem_ld32(tlane + kOffD2 + 32 * part, v);
       tmem_wait_ld();
+      fence_before();
+      mbar_arrive(&s.d2_free);
       const float4* b2 = reinterpret_cast<const float4*>(w.b2 + (g & 7) * 128 + 32 * part);
       uint32_t pk[16];
 #pragma unroll
@@ -229,9 +235,10 @@ struct Epi {
 #pragma unroll
       for (int jj = 0; jj < 4; jj++) st_shared_v4(base + swz_chunk(e, 4 * (part & 1) + jj), pk + 4 * jj);
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    } else {
+      mbar_arrive(&s.d2_free);
     }
-    fence_before();
-    mbar_arrive(&s.e2_done[b]);
+    mbar_arrive(&s.act2_full[b]);
   }
 
   // layer 3 of pass h (D3 columns 64 part .. + 63) and its share of layer 4
@@ -304,6 +311,9 @@ struct Epi {
       atomicAdd(&u[3 * dst + i], yy[3 * i] * fs.x + yy[3 * i + 1] * fs.y + yy[3 * i + 2] * fs.z);
   }
 
+  // Per tile: E2 of chunks 0..15, with layer 3 of pass 0 read after chunk 8 (its accumulator is
+  // complete once L3(7) is, which the MMA lane issues after L2(8)), the next tile's layer 1 after
+  // chunk 15 (every layer-2 MMA of this tile is then complete), then layer 3 of pass 1.
   __device__ void run(int64_t ntiles) {
     uint32_t g = 0, P = 0;
     if ((int64_t)blockIdx.x < ntiles) layer1(blockIdx.x);
@@ -311,28 +321,19 @@ struct Epi {
       float y[9];
 #pragma unroll
       for (int o = 0; o < 9; o++) y[o] = 0.f;
-      bool go = true;
-      for (int h = 0; h < 2 && go; h++) {
 #pragma unroll 1
-        for (int c = 0; c < 8; c++, g++) {
-          layer2(g);
-          // all layer-2 MMAs of tile t are complete (the last chunk's accumulator was waited
-          // for): act1 may take the next tile
-          if (h == 1 && c == 7 && ok && t + gridDim.x < ntiles) layer1(t + gridDim.x);
-        }
-        layer3(P++, h, y);
-        if (h == 1) {
-          float* scratch = reinterpret_cast<float*>(&s.act2[0][0][0]);
-#pragma unroll
-          for (int o = 0; o < 9; o++) scratch[(part * 128 + e) * 9 + o] = y[o];
-        }
-        go = epi_all(ok);
-        if (go && h == 1) {
-          if (part == 0) output(t);
-          epi_bar();  // the scratch is act2, which the next tile's first chunk overwrites
-        }
+      for (int c = 0; c < 16; c++, g++) {
+        layer2(g);
+        if (c == 8) layer3(P++, 0, y);
       }
-      if (!go) break;
+      if (ok && t + gridDim.x < ntiles) layer1(t + gridDim.x);
+      layer3(P++, 1, y);
+      float* scratch = reinterpret_cast<float*>(&s.act2[0][0][0]);
+#pragma unroll
+      for (int o = 0; o < 9; o++) scratch[(part * 128 + e) * 9 + o] = y[o];
+      if (!epi_all(ok)) break;
+      if (part == 0) output(t);
+      epi_bar();  // the scratch is act2, which the next tile's first chunk overwrites
     }
   }
 };
@@ -359,56 +360,53 @@ struct MmaLaneTb {
     mma_commit(&s.ring_empty[S % kRing]);
     S++;
   }
-  // layer-2 chunk g (of a 16-chunk tile) into D2[g & 1]
+  // layer-2 chunk g (global chunk index; the accumulator is free once the epilogue has read
+  // chunk g - 1): A = layer 1 in tensor memory, two 32 KB stages of W2 (K 0-127, 128-255)
   __device__ bool l2(uint32_t g) {
-    if (g >= 2 && !wait(&s.e2_done[g & 1], ((g - 2) >> 1) & 1, 52)) return false;
-    const uint32_t d = tb + kOffD2 + 128 * (g & 1);
+    if (g > 0 && !wait(&s.d2_free, (g - 1) & 1, 52)) return false;
     const uint32_t id = idesc_f16(128, 128);
-    for (uint32_t kb = 0; kb < 4; kb++) {
+    for (uint32_t st = 0; st < 2; st++) {
       if (!stage_ready()) return false;
-      const uint32_t a = saddr(s.act1[kb]), b = saddr(s.ring[S % kRing]);
+      const uint64_t b0 = sdesc(saddr(s.ring[S % kRing]));
 #pragma unroll
-      for (uint32_t kk = 0; kk < 4; kk++) mma_ss(d, sdesc(a + 32 * kk), sdesc(b + 32 * kk), id, (kb | kk) != 0);
+      for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t k16 = 8 * st + i;  // K = 16 k16 .. + 15
+        const uint64_t bd = b0 + (i >> 2) * (16384 >> 4) + (i & 3) * 2;
+        tc::mma_ts(tb + kOffD2, tb + kOffA1 + 8 * k16, bd, id, k16 != 0);
+      }
       stage_done();
     }
-    mma_commit(&s.d2_full[g & 1]);
+    mma_commit(&s.d2_full);
     return true;
   }
-  // layer-3 K-slice of chunk g (local chunk c) into D3
+  // layer-3 K-slice of chunk g (local chunk c, pass P) into D3: N = 256, two 32 KB stages of W3
+  // (256 rows x 64 K each)
   __device__ bool l3(uint32_t g, uint32_t c, uint32_t P) {
-    if (!wait(&s.e2_done[g & 1], (g >> 1) & 1, 53)) return false;
+    if (!wait(&s.act2_full[g & 1], (g >> 1) & 1, 53)) return false;
     if (c == 0 && P > 0 && !wait(&s.d3_free, (P - 1) & 1, 54)) return false;
-    const uint32_t id = idesc_f16(128, 128);
-    for (uint32_t nh = 0; nh < 2; nh++)
-      for (uint32_t kb = 0; kb < 2; kb++) {
-        if (!stage_ready()) return false;
-        const uint32_t a = saddr(s.act2[g & 1][kb]), b = saddr(s.ring[S % kRing]);
+    const uint32_t id = idesc_f16(128, 256);
+    for (uint32_t kb = 0; kb < 2; kb++) {
+      if (!stage_ready()) return false;
+      const uint64_t a0 = sdesc(saddr(s.act2[g & 1][kb])), b0 = sdesc(saddr(s.ring[S % kRing]));
 #pragma unroll
-        for (uint32_t kk = 0; kk < 4; kk++)
-          mma_ss(tb + kOffD3 + 128 * nh, sdesc(a + 32 * kk), sdesc(b + 32 * kk), id, (c | kb | kk) != 0);
-        stage_done();
-      }
+      for (uint32_t kk = 0; kk < 4; kk++) mma_ss(tb + kOffD3, a0 + 2 * kk, b0 + 2 * kk, id, (c | kb | kk) != 0);
+      stage_done();
+    }
     if (c == 7) mma_commit(&s.d3_full);
     return true;
   }
 
   __device__ void run(int64_t ntiles, unsigned long long* prof) {
     const long long start = clock64();
-    uint32_t g = 0, P = 0, k = 0;
-    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, k++) {
+    uint32_t g = 0, k = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, k++, g += 16) {
+      // per tile: L2(0), then L2(c + 1) L3(c) for c = 0..15 (L2 only up to chunk 15); chunks
+      // 0-7 are pass 0, 8-15 pass 1
       if (!wait(&s.act1_full, k & 1, 50)) break;
-      for (int h = 0; h < 2 && ok; h++, g += 8, P++) {
-        // per pass: L2(0) L2(1) L3(0) L2(2) L3(1) ... L2(7) L3(6) L3(7)
-        for (int step = 0; step < 16 && ok; step++) {
-          if (step < 2)
-            l2(g + step);
-          else if (step == 15)
-            l3(g + 7, 7, P);
-          else if ((step & 1) == 0)
-            l3(g + (step - 2) / 2, (step - 2) / 2, P);
-          else
-            l2(g + (step + 1) / 2);
-        }
+      l2(g);
+      for (uint32_t c = 0; c < 16 && ok; c++) {
+        if (c < 15) l2(g + c + 1);
+        if (ok) l3(g + c, c & 7, 2 * k + (c >> 3));
       }
     }
     // let every issued MMA finish before the tensor memory is freed
@@ -455,10 +453,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(&s.act1_full, kEpiThreads);
-    for (int b = 0; b < 2; b++) {
-      mbar_init(&s.d2_full[b], 1);
-      mbar_init(&s.e2_done[b], kEpiThreads);
-    }
+    mbar_init(&s.d2_full, 1);
+    mbar_init(&s.d2_free, kEpiThreads);
+    for (int b = 0; b < 2; b++) mbar_init(&s.act2_full[b], kEpiThreads);
     mbar_init(&s.d3_full, 1);
     mbar_init(&s.d3_free, kEpiThreads);
     for (int r = 0; r < kRing; r++) {
@@ -545,42 +542,37 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   for (int n = 0; n < kTbH3; n++)
     for (int o = 0; o < 9; o++) net.w4[(size_t)n * 12 + o] = W[3][(size_t)o * kTbH3 + n];
   net.b4 = B[3];
-  // layers 2 and 3 as 16 KB FP16 stages (128 rows x 64 K, K-major, 128-byte swizzle) in the MMA
-  // lane's order: per pass h, L2(0) L2(1) L3(0) L2(2) L3(1) ... L2(7) L3(6) L3(7); an L2 chunk c is
-  // four K blocks of W2 rows c*128..; an L3 slice (h, c) is (N half, K block) pairs of W3 rows
-  // h*256 + nh*128.. and columns c*128 + kb*64..
+  // layers 2 and 3 as 32 KB FP16 stages (K-major, 128-byte swizzle; a 64-wide K block of R rows
+  // is R x 128 B, 8-row groups 1024 B apart) in the MMA lane's order per tile: L2(0), then
+  // L2(c + 1) L3(c) for c = 0..15 (no L2(16)). An L2 chunk c (pass c / 8, W2 rows (c % 8) 128 ..)
+  // is two stages of two 128-row K blocks (K 0-127, 128-255); an L3 slice c is two stages of one
+  // 256-row K block: W3 rows (c / 8) 256 .., columns (c % 8) 128 + 64 kb ...
   std::vector<uint8_t> img(kTbImageBytes, 0);
   auto swz = [](int row, int kc) -> size_t {
     return (size_t)(row >> 3) * 1024 + (row & 7) * 128 + (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
   };
   size_t st = 0;
-  auto put_stage = [&](const std::vector<float>& M, int ld, int row0, int col0) {
-    uint8_t* dst = img.data() + st * kTbStageBytes;
-    for (int n = 0; n < 128; n++)
+  auto put_block = [&](uint8_t* dst, const std::vector<float>& M, int ld, int rows, int row0, int col0) {
+    for (int n = 0; n < rows; n++)
       for (int kc = 0; kc < 64; kc++) {
         const uint16_t v = f16_of(M[(size_t)(row0 + n) * ld + col0 + kc]);
         std::memcpy(dst + swz(n, kc), &v, 2);
       }
-    st++;
   };
-  for (int h = 0; h < 2; h++)
-    for (int step = 0; step < 16; step++) {
-      int c;
-      bool isl2;
-      if (step < 2)
-        c = step, isl2 = true;
-      else if (step == 15)
-        c = 7, isl2 = false;
-      else if ((step & 1) == 0)
-        c = (step - 2) / 2, isl2 = false;
-      else
-        c = (step + 1) / 2, isl2 = true;
-      if (isl2)
-        for (int kb = 0; kb < 4; kb++) put_stage(W[1], kTbH1, c * 128, kb * 64);
-      else
-        for (int nh = 0; nh < 2; nh++)
-          for (int kb = 0; kb < 2; kb++) put_stage(W[2], kTbH2, h * 256 + nh * 128, c * 128 + kb * 64);
-    }
+  auto put_l2 = [&](int c) {
+    for (int half = 0; half < 2; half++, st++)
+      for (int i = 0; i < 2; i++)
+        put_block(img.data() + st * kTbStageBytes + i * 16384, W[1], kTbH1, 128, (c % 8) * 128, (2 * half + i) * 64);
+  };
+  auto put_l3 = [&](int c) {
+    for (int kb = 0; kb < 2; kb++, st++)
+      put_block(img.data() + st * kTbStageBytes, W[2], kTbH2, 256, (c / 8) * 256, (c % 8) * 128 + kb * 64);
+  };
+  put_l2(0);
+  for (int c = 0; c < 16; c++) {
+    if (c < 15) put_l2(c + 1);
+    put_l3(c);
+  }
   if (st != (size_t)kTbStagesPerTile) throw Error(-1, "three-body image: stage count mismatch");
   net.d_img.ensure(img.size());
   net.d_w1.ensure(sizeof(float) * net.w1.size());

@@ -12,8 +12,8 @@
 namespace hignn {
 
 constexpr int kTbH1 = 256, kTbH2 = 1024, kTbH3 = 512;
-constexpr int kTbStageBytes = 128 * 64 * 2;         // one 16 KB weight stage: 128 rows x 64 K (FP16)
-constexpr int kTbStagesPerTile = 128;                // 2 passes x 16 MMA groups x 4 stages
+constexpr int kTbStageBytes = 32768;                // one weight stage: 256 rows x 64 K or 128 x 128 K (FP16)
+constexpr int kTbStagesPerTile = 64;                 // 16 layer-2 chunks and 16 layer-3 slices, 2 stages each
 constexpr int kTbImageBytes = kTbStagesPerTile * kTbStageBytes;  // 2 MB
 
 // Device weights of one three-body-shaped network (kin -> 256 -> 1024 -> 512 -> 9, tanh).
