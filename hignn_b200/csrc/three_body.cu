@@ -11,7 +11,7 @@
 // Here one persistent kernel per list does gather -> network -> bmm -> scatter for 128 edges per
 // tile. Layer 1 (kin <= 6 inputs) runs on the CUDA cores in FP32 and writes tanh'd FP16 pairs
 // into tensor memory as the A operand of layer 2. Layers 2 and 3 are tcgen05 MMAs (FP16 in, FP32
-// accumulated in tensor memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP32
+// accumulated in tensor memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP16
 // tanh of layer 3. Tensor memory (512 columns) holds the layer-1 activations (128 columns of FP16
 // pairs), one 128-column layer-2 accumulator and a 256-column layer-3 accumulator. The 512
 // layer-3 outputs therefore take two passes per tile, each recomputing layer 2 (1.33x the
@@ -241,42 +241,52 @@ struct Epi {
     mbar_arrive(&s.act2_full[b]);
   }
 
-  // layer 3 of pass h (D3 columns 64 part .. + 63) and its share of layer 4
+  // layer 3 of pass h (D3 columns 64 part .. + 63) and its share of layer 4. The accumulator is
+  // read, tanh'd into FP16 pairs (as layer 2's activations are) and released before layer 4 runs
+  // from the pairs, so the MMA lane's next layer-3 slice does not wait for layer 4.
   __device__ void layer3(uint32_t P, int h, float (&y)[9]) {
-    if (wait(&s.d3_full, P & 1, 42)) {
-#pragma unroll 1
+    uint32_t a3[32];
+    const bool got = wait(&s.d3_full, P & 1, 42);
+    if (got) {
+#pragma unroll
       for (int half = 0; half < 2; half++) {
         uint32_t v[32];
         tmem_ld32(tlane + kOffD3 + 64 * part + 32 * half, v);
         tmem_wait_ld();
-        const int n0 = h * 256 + 64 * part + 32 * half;
-        const float4* b3 = reinterpret_cast<const float4*>(w.b3 + n0);
-        const float4* w4 = reinterpret_cast<const float4*>(w.w4) + 3 * n0;  // [n][12]: W4[0..8][n], 0, 0, 0
-#pragma unroll 2
-        for (int j4 = 0; j4 < 8; j4++) {
-          const float4 bb = __ldg(&b3[j4]);
-          const float bv[4] = {bb.x, bb.y, bb.z, bb.w};
+        const float4* b3 = reinterpret_cast<const float4*>(w.b3 + h * 256 + 64 * part + 32 * half);
 #pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int j = 4 * j4 + i;
-            float a;
-            asm("tanh.approx.f32 %0, %1;\n" : "=f"(a) : "f"(__uint_as_float(v[j]) + bv[i]));
-            const float4 wa = __ldg(&w4[3 * j]), wb = __ldg(&w4[3 * j + 1]), wc = __ldg(&w4[3 * j + 2]);
-            y[0] = fmaf(a, wa.x, y[0]);
-            y[1] = fmaf(a, wa.y, y[1]);
-            y[2] = fmaf(a, wa.z, y[2]);
-            y[3] = fmaf(a, wa.w, y[3]);
-            y[4] = fmaf(a, wb.x, y[4]);
-            y[5] = fmaf(a, wb.y, y[5]);
-            y[6] = fmaf(a, wb.z, y[6]);
-            y[7] = fmaf(a, wb.w, y[7]);
-            y[8] = fmaf(a, wc.x, y[8]);
-          }
+        for (int j = 0; j < 8; j++) {
+          const float4 bb = __ldg(&b3[j]);
+          a3[16 * half + 2 * j] =
+              tanh_f16x2(pack_f16(__uint_as_float(v[4 * j]) + bb.x, __uint_as_float(v[4 * j + 1]) + bb.y));
+          a3[16 * half + 2 * j + 1] =
+              tanh_f16x2(pack_f16(__uint_as_float(v[4 * j + 2]) + bb.z, __uint_as_float(v[4 * j + 3]) + bb.w));
         }
       }
     }
     fence_before();
     mbar_arrive(&s.d3_free);
+    if (!got) return;
+    const float4* w4 = reinterpret_cast<const float4*>(w.w4) + 3 * (h * 256 + 64 * part);  // [n][12]
+#pragma unroll 4
+    for (int j2 = 0; j2 < 32; j2++) {
+      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&a3[j2]));
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int j = 2 * j2 + i;
+        const float av = i ? a.y : a.x;
+        const float4 wa = __ldg(&w4[3 * j]), wb = __ldg(&w4[3 * j + 1]), wc = __ldg(&w4[3 * j + 2]);
+        y[0] = fmaf(av, wa.x, y[0]);
+        y[1] = fmaf(av, wa.y, y[1]);
+        y[2] = fmaf(av, wa.z, y[2]);
+        y[3] = fmaf(av, wa.w, y[3]);
+        y[4] = fmaf(av, wb.x, y[4]);
+        y[5] = fmaf(av, wb.y, y[5]);
+        y[6] = fmaf(av, wb.z, y[6]);
+        y[7] = fmaf(av, wb.w, y[7]);
+        y[8] = fmaf(av, wc.x, y[8]);
+      }
+    }
   }
 
   // sum of the four parts' layer-4 shares, wrapper, 3x3 times the force, scatter (part 0)
