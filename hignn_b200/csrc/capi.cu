@@ -1644,7 +1644,7 @@ struct hignn_tb {
     cudaStreamSynchronize(lists.stream());
     for (DevBuf* b : {&f4, &fin, &u, &err, &prof}) b->release();
     for (auto& n : nets)
-      for (DevBuf* b : {&n.d_img, &n.d_w1, &n.d_b2, &n.d_b3, &n.d_w4, &n.d_b4}) b->release();
+      for (DevBuf* b : {&n.d_img, &n.d_w4}) b->release();
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
   }
@@ -1747,10 +1747,10 @@ int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, i
     HIGNN_CUDA(cudaMemsetAsync(t->u.p, 0, sizeof(float) * 3 * n, s));
     HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), s));
     HIGNN_CUDA(cudaEventRecord(t->ev[0], s));
-    hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), tri, e3, t->lists.positions(), t->f4.as<float4>(),
+    hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), t->nets[0].cst, tri, e3, t->lists.positions(), t->f4.as<float4>(),
                              t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>(), t->num_sms, s);
     HIGNN_CUDA(cudaEventRecord(t->ev[1], s));
-    hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), self, es, t->lists.positions(), t->f4.as<float4>(),
+    hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), t->nets[1].cst, self, es, t->lists.positions(), t->f4.as<float4>(),
                              t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>() + 6, t->num_sms, s);
     HIGNN_CUDA(cudaEventRecord(t->ev[2], s));
     int e = 0;

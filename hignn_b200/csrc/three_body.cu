@@ -31,6 +31,7 @@
 // stops, lets its copies and MMAs drain and frees its tensor memory.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "three_body.h"
@@ -66,6 +67,7 @@ struct TbSmem {
 };
 constexpr size_t kSmemBytes = sizeof(TbSmem) + 1024;  // + alignment slack
 static_assert(kSmemBytes <= 232448, "three-body shared memory exceeds the per-CTA limit");
+static_assert(sizeof(TbConst) + 256 <= 32764, "three-body kernel parameters exceed the launch limit");
 
 __device__ __forceinline__ bool wait_bar(uint64_t* b, uint32_t parity, int* abort_flag, int* err, int code,
                                          bool honour_abort = true) {
@@ -160,6 +162,7 @@ __device__ __forceinline__ float norm3f(float a, float b, float c) { return sqrt
 template <int KIND>
 struct Epi {
   TbSmem& s;
+  const TbConst& c;
   TbWeightsDev w;
   const uint64_t* edges;
   int64_t E;
@@ -185,7 +188,6 @@ struct Epi {
     float in[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int64_t src, dst;
     if (q < E) edge_input<KIND>(edges, E, q, x, in, src, dst);
-    const float4* w1 = reinterpret_cast<const float4*>(w.w1);
 #pragma unroll 1
     for (int half = 0; half < 2; half++) {
       uint32_t pk[16];
@@ -195,14 +197,10 @@ struct Epi {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int n = 64 * part + 32 * half + 2 * pr + h;
-          const float4 wa = __ldg(&w1[2 * n]), wb = __ldg(&w1[2 * n + 1]);
-          float a = wb.z;  // b1
-          a = fmaf(wa.x, in[0], a);
-          a = fmaf(wa.y, in[1], a);
-          a = fmaf(wa.z, in[2], a);
-          a = fmaf(wa.w, in[3], a);
-          a = fmaf(wb.x, in[4], a);
-          a = fmaf(wb.y, in[5], a);
+          const float* wr = c.w1 + 8 * n;
+          float a = wr[6];  // b1
+#pragma unroll
+          for (int k = 0; k < 6; k++) a = fmaf(wr[k], in[k], a);
           acc[h] = a;
         }
         pk[pr] = tanh_f16x2(pack_f16(acc[0], acc[1]));
@@ -223,14 +221,11 @@ struct Epi {
       tmem_wait_ld();
       fence_before();
       mbar_arrive(&s.d2_free);
-      const float4* b2 = reinterpret_cast<const float4*>(w.b2 + (g & 7) * 128 + 32 * part);
+      const float* b2 = c.b2 + (g & 7) * 128 + 32 * part;
       uint32_t pk[16];
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const float4 bb = __ldg(&b2[j]);
-        pk[2 * j] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * j]) + bb.x, __uint_as_float(v[4 * j + 1]) + bb.y));
-        pk[2 * j + 1] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * j + 2]) + bb.z, __uint_as_float(v[4 * j + 3]) + bb.w));
-      }
+      for (int j = 0; j < 16; j++)
+        pk[j] = tanh_f16x2(pack_f16(__uint_as_float(v[2 * j]) + b2[2 * j], __uint_as_float(v[2 * j + 1]) + b2[2 * j + 1]));
       const uint32_t base = saddr(s.act2[b][part >> 1]);
 #pragma unroll
       for (int jj = 0; jj < 4; jj++) st_shared_v4(base + swz_chunk(e, 4 * (part & 1) + jj), pk + 4 * jj);
@@ -253,15 +248,11 @@ struct Epi {
         uint32_t v[32];
         tmem_ld32(tlane + kOffD3 + 64 * part + 32 * half, v);
         tmem_wait_ld();
-        const float4* b3 = reinterpret_cast<const float4*>(w.b3 + h * 256 + 64 * part + 32 * half);
+        const float* b3 = c.b3 + h * 256 + 64 * part + 32 * half;
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const float4 bb = __ldg(&b3[j]);
-          a3[16 * half + 2 * j] =
-              tanh_f16x2(pack_f16(__uint_as_float(v[4 * j]) + bb.x, __uint_as_float(v[4 * j + 1]) + bb.y));
-          a3[16 * half + 2 * j + 1] =
-              tanh_f16x2(pack_f16(__uint_as_float(v[4 * j + 2]) + bb.z, __uint_as_float(v[4 * j + 3]) + bb.w));
-        }
+        for (int j = 0; j < 16; j++)
+          a3[16 * half + j] =
+              tanh_f16x2(pack_f16(__uint_as_float(v[2 * j]) + b3[2 * j], __uint_as_float(v[2 * j + 1]) + b3[2 * j + 1]));
       }
     }
     fence_before();
@@ -301,7 +292,7 @@ struct Epi {
       v += scratch[(1 * 128 + e) * 9 + o];
       v += scratch[(2 * 128 + e) * 9 + o];
       v += scratch[(3 * 128 + e) * 9 + o];
-      yy[o] = v + __ldg(&w.b4[o]);
+      yy[o] = v + c.b4[o];
     }
     float in[6];
     int64_t src, dst;
@@ -454,7 +445,8 @@ __device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err
 
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_three_body(TbWeightsDev w, const uint64_t* __restrict__ edges, int64_t E, int64_t ntiles,
+    k_three_body(const __grid_constant__ TbConst cst, TbWeightsDev w, const uint64_t* __restrict__ edges, int64_t E,
+                 int64_t ntiles,
                  const float4* __restrict__ x, const float4* __restrict__ f, float* __restrict__ u, int* err,
                  unsigned long long* prof) {
   extern __shared__ uint8_t smem_raw[];
@@ -481,7 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   fence_after();
   if (warp < kMmaWarp) {
-    Epi<KIND> ep{s, w, edges, E, x, f, u, err};
+    Epi<KIND> ep{s, cst, w, edges, E, x, f, u, err};
     ep.e = 32 * (warp & 3) + lane;
     ep.part = warp >> 2;
     ep.tlane = s.tmem_base + ((uint32_t)(32 * (warp & 3)) << 16);
@@ -504,11 +496,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 template <int KIND>
-void launch_kind(const TbWeightsDev& w, const uint64_t* edges, int64_t E, int64_t ntiles, const float4* x,
-                 const float4* f, float* u, int* err, unsigned long long* prof, int num_sms, cudaStream_t s) {
+void launch_kind(const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t E, int64_t ntiles,
+                 const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
+                 cudaStream_t s) {
   HIGNN_CUDA(cudaFuncSetAttribute(k_three_body<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   const int grid = (int)(ntiles < num_sms ? ntiles : num_sms);
-  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(w, edges, E, ntiles, x, f, u, err, prof);
+  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(c, w, edges, E, ntiles, x, f, u, err, prof);
   HIGNN_CHECK_LAUNCH();
 }
 
@@ -521,15 +514,15 @@ uint16_t f16_of(float v) {
 
 }  // namespace
 
-int64_t launch_three_body(int kind, const TbWeightsDev& w, const uint64_t* edges, int64_t num_edges, const float4* x,
-                          const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
+int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
+                          const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
                           cudaStream_t s) {
   const int64_t ntiles = (num_edges + 127) / 128;
   if (ntiles == 0) return 0;
   if (kind == kTbThreeBody)
-    launch_kind<kTbThreeBody>(w, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
+    launch_kind<kTbThreeBody>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
   else
-    launch_kind<kTbSelf>(w, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
+    launch_kind<kTbSelf>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
   return ntiles;
 }
 
@@ -541,17 +534,17 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
     if (W[l].size() != want[l][0] * want[l][1] || B[l].size() != want[l][0])
       throw Error(-1, "three-body network: layer sizes must be kin -> 256 -> 1024 -> 512 -> 9");
   net.kin = kin;
-  net.w1.assign(kTbH1 * 8, 0.f);
+  net.cst = TbConst{};
   for (int n = 0; n < kTbH1; n++) {
-    for (int k = 0; k < kin; k++) net.w1[n * 8 + k] = W[0][(size_t)n * kin + k];
-    net.w1[n * 8 + 6] = B[0][n];
+    for (int k = 0; k < kin; k++) net.cst.w1[n * 8 + k] = W[0][(size_t)n * kin + k];
+    net.cst.w1[n * 8 + 6] = B[0][n];
   }
-  net.b2 = B[1];
-  net.b3 = B[2];
+  std::copy(B[1].begin(), B[1].end(), net.cst.b2);
+  std::copy(B[2].begin(), B[2].end(), net.cst.b3);
+  std::copy(B[3].begin(), B[3].end(), net.cst.b4);
   net.w4.assign((size_t)kTbH3 * 12, 0.f);  // transposed, 12 per row (three float4 loads)
   for (int n = 0; n < kTbH3; n++)
     for (int o = 0; o < 9; o++) net.w4[(size_t)n * 12 + o] = W[3][(size_t)o * kTbH3 + n];
-  net.b4 = B[3];
   // layers 2 and 3 as 32 KB FP16 stages (K-major, 128-byte swizzle; a 64-wide K block of R rows
   // is R x 128 B, 8-row groups 1024 B apart) in the MMA lane's order per tile: L2(0), then
   // L2(c + 1) L3(c) for c = 0..15 (no L2(16)). An L2 chunk c (pass c / 8, W2 rows (c % 8) 128 ..)
@@ -585,17 +578,9 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   }
   if (st != (size_t)kTbStagesPerTile) throw Error(-1, "three-body image: stage count mismatch");
   net.d_img.ensure(img.size());
-  net.d_w1.ensure(sizeof(float) * net.w1.size());
-  net.d_b2.ensure(sizeof(float) * net.b2.size());
-  net.d_b3.ensure(sizeof(float) * net.b3.size());
   net.d_w4.ensure(sizeof(float) * net.w4.size());
-  net.d_b4.ensure(sizeof(float) * net.b4.size());
   HIGNN_CUDA(cudaMemcpyAsync(net.d_img.p, img.data(), img.size(), cudaMemcpyHostToDevice, s));
-  HIGNN_CUDA(cudaMemcpyAsync(net.d_w1.p, net.w1.data(), sizeof(float) * net.w1.size(), cudaMemcpyHostToDevice, s));
-  HIGNN_CUDA(cudaMemcpyAsync(net.d_b2.p, net.b2.data(), sizeof(float) * net.b2.size(), cudaMemcpyHostToDevice, s));
-  HIGNN_CUDA(cudaMemcpyAsync(net.d_b3.p, net.b3.data(), sizeof(float) * net.b3.size(), cudaMemcpyHostToDevice, s));
   HIGNN_CUDA(cudaMemcpyAsync(net.d_w4.p, net.w4.data(), sizeof(float) * net.w4.size(), cudaMemcpyHostToDevice, s));
-  HIGNN_CUDA(cudaMemcpyAsync(net.d_b4.p, net.b4.data(), sizeof(float) * net.b4.size(), cudaMemcpyHostToDevice, s));
   HIGNN_CUDA(cudaStreamSynchronize(s));
   net.loaded = true;
 }

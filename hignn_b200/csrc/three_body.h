@@ -16,14 +16,19 @@ constexpr int kTbStageBytes = 32768;                // one weight stage: 256 row
 constexpr int kTbStagesPerTile = 64;                 // 16 layer-2 chunks and 16 layer-3 slices, 2 stages each
 constexpr int kTbImageBytes = kTbStagesPerTile * kTbStageBytes;  // 2 MB
 
+// Small per-network constants, passed to the kernel as a parameter: the epilogue reads them
+// with warp-uniform indices, which the constant bank serves without a memory round trip.
+struct TbConst {
+  float w1[kTbH1 * 8];  // row n: W1[n][0..kin) zero padded to 6, b1[n], 0
+  float b2[kTbH2];
+  float b3[kTbH3];
+  float b4[16];  // 9 used
+};
+
 // Device weights of one three-body-shaped network (kin -> 256 -> 1024 -> 512 -> 9, tanh).
 struct TbWeightsDev {
   const uint8_t* img;  // layers 2 and 3 as FP16 stages in the order the MMA lane consumes them
-  const float* w1;     // [256][8]: W1 row (kin entries, zero padded to 6), b1, 0
-  const float* b2;     // [1024]
-  const float* b3;     // [512]
   const float* w4;     // [512][12]: column n of W4 (9 entries), zero padded
-  const float* b4;     // [9]
 };
 
 enum TbKind : int { kTbThreeBody = 0, kTbSelf = 1 };
@@ -32,12 +37,10 @@ enum TbKind : int { kTbThreeBody = 0, kTbSelf = 1 };
 struct TbNet {
   bool loaded = false;
   int kin = 0;
-  std::vector<float> w1, b2, b3, w4, b4;
-  DevBuf d_img, d_w1, d_b2, d_b3, d_w4, d_b4;
-  TbWeightsDev dev() const {
-    return {d_img.as<uint8_t>(), d_w1.as<float>(), d_b2.as<float>(), d_b3.as<float>(), d_w4.as<float>(),
-            d_b4.as<float>()};
-  }
+  TbConst cst{};
+  std::vector<float> w4;
+  DevBuf d_img, d_w4;
+  TbWeightsDev dev() const { return {d_img.as<uint8_t>(), d_w4.as<float>()}; }
 };
 
 // u[c] += ((net(x_b - x_a, x_c - x_b) / |x_b - x_a| / |x_c - x_b|) as 3x3) f[a] for every triplet
@@ -47,8 +50,9 @@ struct TbNet {
 // clocks the MMA lane waited for layer-1 operands, weight stages, layer-2 epilogues and the
 // layer-3 accumulator, its total clocks, and clocks the producer waited for free ring slots.
 // Returns the number of 128-edge tiles launched.
-int64_t launch_three_body(int kind, const TbWeightsDev& w, const uint64_t* edges, int64_t num_edges, const float4* x,
-                          const float4* f, float* u, int* err, unsigned long long* prof, int num_sms, cudaStream_t s);
+int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
+                          const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
+                          cudaStream_t s);
 
 // Builds the device image of a network from its dense layers (W row-major out x in, b).
 void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,
