@@ -1644,7 +1644,7 @@ struct hignn_tb {
     cudaStreamSynchronize(lists.stream());
     for (DevBuf* b : {&f4, &fin, &u, &err, &prof}) b->release();
     for (auto& n : nets)
-      for (DevBuf* b : {&n.d_img, &n.d_w4}) b->release();
+      n.d_img.release();
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
   }

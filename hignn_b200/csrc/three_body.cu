@@ -67,7 +67,7 @@ struct TbSmem {
 };
 constexpr size_t kSmemBytes = sizeof(TbSmem) + 1024;  // + alignment slack
 static_assert(kSmemBytes <= 232448, "three-body shared memory exceeds the per-CTA limit");
-static_assert(sizeof(TbConst) + 256 <= 32764, "three-body kernel parameters exceed the launch limit");
+static_assert(sizeof(TbConst) + 128 <= 32764, "three-body kernel parameters exceed the launch limit");
 
 __device__ __forceinline__ bool wait_bar(uint64_t* b, uint32_t parity, int* abort_flag, int* err, int code,
                                          bool honour_abort = true) {
@@ -197,7 +197,7 @@ struct Epi {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int n = 64 * part + 32 * half + 2 * pr + h;
-          const float* wr = c.w1 + 8 * n;
+          const float* wr = c.w1 + 7 * n;
           float a = wr[6];  // b1
 #pragma unroll
           for (int k = 0; k < 6; k++) a = fmaf(wr[k], in[k], a);
@@ -258,24 +258,16 @@ struct Epi {
     fence_before();
     mbar_arrive(&s.d3_free);
     if (!got) return;
-    const float4* w4 = reinterpret_cast<const float4*>(w.w4) + 3 * (h * 256 + 64 * part);  // [n][12]
+    const float* w4 = c.w4 + 9 * (h * 256 + 64 * part);
 #pragma unroll 4
     for (int j2 = 0; j2 < 32; j2++) {
       const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&a3[j2]));
 #pragma unroll
       for (int i = 0; i < 2; i++) {
-        const int j = 2 * j2 + i;
         const float av = i ? a.y : a.x;
-        const float4 wa = __ldg(&w4[3 * j]), wb = __ldg(&w4[3 * j + 1]), wc = __ldg(&w4[3 * j + 2]);
-        y[0] = fmaf(av, wa.x, y[0]);
-        y[1] = fmaf(av, wa.y, y[1]);
-        y[2] = fmaf(av, wa.z, y[2]);
-        y[3] = fmaf(av, wa.w, y[3]);
-        y[4] = fmaf(av, wb.x, y[4]);
-        y[5] = fmaf(av, wb.y, y[5]);
-        y[6] = fmaf(av, wb.z, y[6]);
-        y[7] = fmaf(av, wb.w, y[7]);
-        y[8] = fmaf(av, wc.x, y[8]);
+        const float* wj = w4 + 9 * (2 * j2 + i);
+#pragma unroll
+        for (int o = 0; o < 9; o++) y[o] = fmaf(av, wj[o], y[o]);
       }
     }
   }
@@ -536,15 +528,14 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   net.kin = kin;
   net.cst = TbConst{};
   for (int n = 0; n < kTbH1; n++) {
-    for (int k = 0; k < kin; k++) net.cst.w1[n * 8 + k] = W[0][(size_t)n * kin + k];
-    net.cst.w1[n * 8 + 6] = B[0][n];
+    for (int k = 0; k < kin; k++) net.cst.w1[n * 7 + k] = W[0][(size_t)n * kin + k];
+    net.cst.w1[n * 7 + 6] = B[0][n];
   }
   std::copy(B[1].begin(), B[1].end(), net.cst.b2);
   std::copy(B[2].begin(), B[2].end(), net.cst.b3);
   std::copy(B[3].begin(), B[3].end(), net.cst.b4);
-  net.w4.assign((size_t)kTbH3 * 12, 0.f);  // transposed, 12 per row (three float4 loads)
   for (int n = 0; n < kTbH3; n++)
-    for (int o = 0; o < 9; o++) net.w4[(size_t)n * 12 + o] = W[3][(size_t)o * kTbH3 + n];
+    for (int o = 0; o < 9; o++) net.cst.w4[n * 9 + o] = W[3][(size_t)o * kTbH3 + n];
   // layers 2 and 3 as 32 KB FP16 stages (K-major, 128-byte swizzle; a 64-wide K block of R rows
   // is R x 128 B, 8-row groups 1024 B apart) in the MMA lane's order per tile: L2(0), then
   // L2(c + 1) L3(c) for c = 0..15 (no L2(16)). An L2 chunk c (pass c / 8, W2 rows (c % 8) 128 ..)
@@ -578,9 +569,7 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   }
   if (st != (size_t)kTbStagesPerTile) throw Error(-1, "three-body image: stage count mismatch");
   net.d_img.ensure(img.size());
-  net.d_w4.ensure(sizeof(float) * net.w4.size());
   HIGNN_CUDA(cudaMemcpyAsync(net.d_img.p, img.data(), img.size(), cudaMemcpyHostToDevice, s));
-  HIGNN_CUDA(cudaMemcpyAsync(net.d_w4.p, net.w4.data(), sizeof(float) * net.w4.size(), cudaMemcpyHostToDevice, s));
   HIGNN_CUDA(cudaStreamSynchronize(s));
   net.loaded = true;
 }

@@ -19,16 +19,16 @@ constexpr int kTbImageBytes = kTbStagesPerTile * kTbStageBytes;  // 2 MB
 // Small per-network constants, passed to the kernel as a parameter: the epilogue reads them
 // with warp-uniform indices, which the constant bank serves without a memory round trip.
 struct TbConst {
-  float w1[kTbH1 * 8];  // row n: W1[n][0..kin) zero padded to 6, b1[n], 0
+  float w1[kTbH1 * 7];  // row n: W1[n][0..kin) zero padded to 6, then b1[n]
   float b2[kTbH2];
   float b3[kTbH3];
-  float b4[16];  // 9 used
+  float w4[kTbH3 * 9];  // column n of W4: w4[9 n + o] = W4[o][n]
+  float b4[9];
 };
 
 // Device weights of one three-body-shaped network (kin -> 256 -> 1024 -> 512 -> 9, tanh).
 struct TbWeightsDev {
   const uint8_t* img;  // layers 2 and 3 as FP16 stages in the order the MMA lane consumes them
-  const float* w4;     // [512][12]: column n of W4 (9 entries), zero padded
 };
 
 enum TbKind : int { kTbThreeBody = 0, kTbSelf = 1 };
@@ -38,9 +38,8 @@ struct TbNet {
   bool loaded = false;
   int kin = 0;
   TbConst cst{};
-  std::vector<float> w4;
-  DevBuf d_img, d_w4;
-  TbWeightsDev dev() const { return {d_img.as<uint8_t>(), d_w4.as<float>()}; }
+  DevBuf d_img;
+  TbWeightsDev dev() const { return {d_img.as<uint8_t>()}; }
 };
 
 // u[c] += ((net(x_b - x_a, x_c - x_b) / |x_b - x_a| / |x_c - x_b|) as 3x3) f[a] for every triplet
