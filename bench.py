@@ -62,7 +62,32 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the three-body near-field measurement added to the line")
     return ap.parse_args()
+
+
+def three_body_row(args):
+    """The three-body + self near field (131,072 filament beads, cutoff 5) on this GPU, with the
+    oracle's FP64 network on a bounded sample of triplets as its CPU baseline."""
+    import time
+    from types import SimpleNamespace
+
+    from hignn_b200.microbench import three_body
+    from hignn_b200.weights import default_three_body_paths
+    from oracle import hignn_oracle as O
+
+    row = three_body(SimpleNamespace(filaments=4096, reps=3))
+    net = O.DenseTanh.from_hgnw(default_three_body_paths()[0])
+    sample = 20000
+    z = np.random.default_rng(0).normal(0, 3, (sample, 6))
+    t0 = time.perf_counter()
+    net(z)
+    dt = time.perf_counter() - t0
+    row["workload"] = "4,096 filaments x 32 beads, bond 2.2, phi 0.05, seed 3, three-body cutoff 5"
+    row["cpu_baseline"] = {"value": sample / dt, "unit": "triplets/s", "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"{sample} triplets through the oracle's FP64 numpy network"}
+    return row
 
 
 def workload(n):
@@ -405,9 +430,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds, st["close_evals"],
                                             st["far_evals"])
+    m.close()
+    if rank == 0 and world == 1 and not args.no_next_rows:
+        line["next_rows"] = {"three_body": three_body_row(args)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    m.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -2,6 +2,10 @@
 
     python -m hignn_b200.microbench eval --n 378880 --precision 1
     python -m hignn_b200.microbench dot --workload medium --precision 1 --fields 1
+    python -m hignn_b200.microbench three_body --filaments 4096
+
+`three_body` times the three-body + self near field on filaments of 32 beads 2.2 apart at volume
+fraction 0.05 (seed 3) with three-body cutoff 5, against the measured bf16 tensor peak.
 
 Prints one JSON line: milliseconds per call and evaluations per second.
 """
@@ -22,7 +26,8 @@ FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["eval", "dot"])
+    ap.add_argument("what", choices=["eval", "dot", "three_body"])
+    ap.add_argument("--filaments", type=int, default=4096)
     ap.add_argument("--n", type=int, default=148 * 128 * 20)
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
@@ -43,7 +48,9 @@ def main():
     from hignn_b200 import synthetic as S
 
     out = {"what": a.what, "precision": a.precision}
-    if a.what == "eval":
+    if a.what == "three_body":
+        out.update(three_body(a))
+    elif a.what == "eval":
         rng = np.random.default_rng(1)
         v = rng.normal(size=(a.n, 3))
         v /= np.linalg.norm(v, axis=1, keepdims=True)
@@ -114,6 +121,48 @@ def main():
                    num_far=st["num_far"], far_query_ms=st["t_far_query_ms"], far_pivot_ms=st["t_far_pivot_ms"],
                    far_active_ms=st["t_far_active_ms"], far_check_ms=st["t_far_check_ms"])
     print(json.dumps(out), flush=True)
+
+
+TB_FLOP = 2 * (6 * 256 + 256 * 1024 + 1024 * 512 + 512 * 9)    # per triplet
+TB_SELF_FLOP = 2 * (3 * 256 + 256 * 1024 + 1024 * 512 + 512 * 9)
+
+
+def three_body(a, reps=None):
+    import time
+
+    from hignn_b200 import capi
+    from hignn_b200 import synthetic as S
+    x = S.filaments(a.filaments, 32, 2.2, 0.05, 3)
+    f = S.sedimenting_forces(len(x), 3)
+    tb = capi.ThreeBody(0)
+    tb.set_epsilon(5.0)
+    for _ in range(3):
+        tb.velocity(x, f)
+    runs = []
+    for _ in range(max(1, reps or a.reps)):
+        t0 = time.perf_counter()
+        tb.velocity(x, f)
+        st = tb.stats()
+        st["wall_ms"] = (time.perf_counter() - t0) * 1e3
+        runs.append(st)
+    best = min(runs, key=lambda r: r["ms_three"] + r["ms_self"])
+    flop = best["triplets"] * TB_FLOP + best["pairs"] * TB_SELF_FLOP
+    kernel_ms = best["ms_three"] + best["ms_self"]
+    peaks = {}
+    pk = os.path.join(os.path.dirname(HERE), "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = peaks.get("bf16_tflops", 1590.0)
+    tflops = best["triplets"] * TB_FLOP / best["ms_three"] / 1e9
+    out = dict(n=len(x), triplets=best["triplets"], pairs=best["pairs"], ms_lists=best["ms_lists"],
+               ms_three=best["ms_three"], ms_self=best["ms_self"], e2e_ms=best["wall_ms"],
+               edges_per_s=(best["triplets"] + best["pairs"]) / kernel_ms * 1e3,
+               roofline={"bound": "tensor", "kernel": "k_three_body<0>", "achieved": tflops, "peak": peak,
+                         "unit": "TFLOP/s", "frac": tflops / peak,
+                         "peak_source": "measured" if peaks else "fallback"},
+               total_tflops=flop / kernel_ms / 1e9, wait_profile=tb.wait_profile())
+    out["triplets_per_s"] = best["triplets"] / best["ms_three"] * 1e3
+    return out
 
 
 if __name__ == "__main__":
