@@ -692,7 +692,7 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
       k_far_active<<<1, 1024, 0, s>>>(a);
       mark();
       if (student)
-        launch_far_student(a, student, 0, num_sms, s);
+        launch_far_student(a, student, 0, err, num_sms, s);
       else if (tcw)
         launch_far_tc(a, *tcw, 0, err, num_sms, s);
       else
@@ -701,7 +701,7 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
       k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
       mark();
       if (student)
-        launch_far_student(a, student, 1, num_sms, s);
+        launch_far_student(a, student, 1, err, num_sms, s);
       else if (tcw)
         launch_far_tc(a, *tcw, 1, err, num_sms, s);
       else

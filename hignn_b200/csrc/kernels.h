@@ -120,7 +120,7 @@ void launch_student_grad(const float* params, const float* r, const float* t, in
 void launch_student_adam(float* p, const float* g, float* m1, float* m2, float lr, float b1t, float b2t,
                          cudaStream_t s);
 void launch_student_eval(const float* params, const float* r, float* y, int64_t n, int num_sms, cudaStream_t s);
-void launch_far_student(const FarArgs& a, const float* params, int which, int num_sms, cudaStream_t s);
+void launch_far_student(const FarArgs& a, const float* params, int which, int* err, int num_sms, cudaStream_t s);
 
 // tensor-core kernels (tc_kernels.cu); err receives a nonzero code if a bounded wait timed out
 void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, int* err, int num_sms, cudaStream_t s);

@@ -19,8 +19,11 @@
 #include <cmath>
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "common.h"
 #include "kernels.h"
+#include "tc_mlp.cuh"
 
 namespace hignn {
 
@@ -332,20 +335,119 @@ __global__ void k_student_eval(const float* __restrict__ params, const float* __
   }
 }
 
-// ACA column (which = 0) / row (which = 1) queries of all active blocks with the student.
-__global__ void __launch_bounds__(256, 2) k_far_student(FarArgs a, const float* __restrict__ params, int which) {
-  __shared__ __align__(16) float p[kStudentParams];
+// ---------------------------------------------------------------- student queries on tcgen05
+// ACA column (which = 0) / row (which = 1) queries of all active blocks with the student, 128
+// entries per tile and one tile at a time per CTA:
+// every thread owns one entry (row) and one tensor-memory lane. Layer 1 (3 -> 32) runs in FP32 on
+// the CUDA cores; layers 2, 3 (32 -> 32) and 4 (32 -> 9, padded to 16) are tcgen05 MMAs, M = 128,
+// with FP16 operands (the A operand in tensor memory, the weights in shared memory as 128-byte
+// swizzled K-major tiles padded to K = 64) and FP32 accumulation. SiLU between layers is
+// z / 2 (1 + tanh(z / 2)) on FP16 pairs (one tanh.approx.f16x2 per pair), written back as the
+// next A operand. A tile's three MMA rounds wait on one another, so several CTAs share an SM
+// (64 tensor-memory columns each: A [0, 16), layer 2/3 accumulator [16, 48), layer 4 [48, 64)).
+// Waits are bounded; a timeout records an error code and the CTA stops after draining its MMAs.
+constexpr int kStcThreads = 128;
+constexpr uint32_t kStcA = 0, kStcD = 16, kStcD4 = 48, kStcCols = 64;
+constexpr long long kStcWait = 4000000000LL;
+
+struct StcSmem {
+  uint8_t w2[32 * 128];  // 32 rows (outputs) x 64 K (32 used), FP16, swizzled
+  uint8_t w3[32 * 128];
+  uint8_t w4[16 * 128];  // 9 rows used
+  float w1b1[32 * 4];    // W1 row k (3), b1[k]
+  float b2[32], b3[32], b4[16];
+  uint64_t bar;
+  uint32_t tmem;
+  int s_first;
+};
+constexpr size_t kStcSmemBytes = 28 * 1024;  // at most eight CTAs per SM: 8 x 64 tensor-memory columns
+static_assert(sizeof(StcSmem) + 1024 <= kStcSmemBytes, "student tile shared memory");
+
+__device__ __forceinline__ uint32_t stc_swz(int row, int k) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + (((k >> 3) ^ (row & 7)) << 4) + (k & 7) * 2);
+}
+
+// SiLU of two FP32 pre-activations as one FP16 pair: (z / 2)(1 + tanh(z / 2))
+__device__ __forceinline__ uint32_t silu_f16x2(float z0, float z1) {
+  const __half2 hz = __floats2half2_rn(0.5f * z0, 0.5f * z1);
+  uint32_t t;
+  asm("tanh.approx.f16x2 %0, %1;\n" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t*>(&hz)));
+  const __half2 r = __hfma2(hz, *reinterpret_cast<const __half2*>(&t), hz);
+  return *reinterpret_cast<const uint32_t*>(&r);
+}
+
+__global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const float* __restrict__ params, int which,
+                                                                int* err) {
+  extern __shared__ uint8_t raw[];
+  const uint32_t rb = tc::saddr(raw);
+  StcSmem& S = *reinterpret_cast<StcSmem*>(raw + (((rb + 1023u) & ~1023u) - rb));
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int nact = a.ctr[kCtrActive];
   const int tot = which ? a.ctr[kCtrTotJ] : a.ctr[kCtrTotI];
-  if ((int)(blockIdx.x * blockDim.x) >= tot) return;
-  for (int i = threadIdx.x; i < kStudentParams; i += blockDim.x) p[i] = params[i];
+  const int ntiles = (tot + kStcThreads - 1) / kStcThreads;
+  if ((int)blockIdx.x >= ntiles) return;
+  // weights: FP16 swizzled tiles of W2, W3, W4 (rows = outputs, K = inputs), FP32 W1/b1 and biases
+  for (int i = tid; i < 32 * 128 / 4; i += kStcThreads) {
+    reinterpret_cast<uint32_t*>(S.w2)[i] = 0u;
+    reinterpret_cast<uint32_t*>(S.w3)[i] = 0u;
+    if (i < 16 * 128 / 4) reinterpret_cast<uint32_t*>(S.w4)[i] = 0u;
+  }
   __syncthreads();
+  for (int i = tid; i < 32 * 32; i += kStcThreads) {
+    const int n = i >> 5, k = i & 31;
+    *reinterpret_cast<__half*>(S.w2 + stc_swz(n, k)) = __float2half_rn(params[kOffW2 + i]);
+    *reinterpret_cast<__half*>(S.w3 + stc_swz(n, k)) = __float2half_rn(params[kOffW3 + i]);
+    if (n < 9) *reinterpret_cast<__half*>(S.w4 + stc_swz(n, k)) = __float2half_rn(params[kOffW4 + i]);
+  }
+  if (tid < 32) {
+    S.w1b1[4 * tid] = params[kOffW1 + 3 * tid];
+    S.w1b1[4 * tid + 1] = params[kOffW1 + 3 * tid + 1];
+    S.w1b1[4 * tid + 2] = params[kOffW1 + 3 * tid + 2];
+    S.w1b1[4 * tid + 3] = params[kOffB1 + tid];
+    S.b2[tid] = params[kOffB2 + tid];
+    S.b3[tid] = params[kOffB3 + tid];
+    S.b4[tid & 15] = (tid & 15) < 9 ? params[kOffB4 + (tid & 15)] : 0.f;
+  }
+  if (tid == 0) {
+    tc::mbar_init(&S.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (warp == 0) tc::tmem_alloc(&S.tmem, kStcCols);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tb = S.tmem, tl = tb + ((uint32_t)(32 * warp) << 16);
+  const uint64_t d2 = tc::sdesc(tc::saddr(S.w2)), d3 = tc::sdesc(tc::saddr(S.w3)), d4 = tc::sdesc(tc::saddr(S.w4));
   const int32_t* pre = which ? a.preJ : a.preI;
-  __shared__ int s_first;
-  // chunks of blockDim.x consecutive rows: one binary search per chunk for the active block of its
-  // first row, then each thread steps forward to its own row's block (a chunk spans few blocks)
-  for (int g0 = blockIdx.x * blockDim.x; g0 < tot; g0 += gridDim.x * blockDim.x) {
-    if (threadIdx.x == 0) {
+  uint32_t phase = 0;
+  bool ok = true;
+  // one MMA round: everyone's A is in tensor memory; thread 0 issues, all wait for the commit
+  auto round = [&](uint64_t bdesc, uint32_t d, uint32_t idesc) {
+    tc::tmem_wait_st();
+    tc::fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after();
+      tc::mma_ts(tb + d, tb + kStcA, bdesc, idesc, 0u);
+      tc::mma_ts(tb + d, tb + kStcA + 8, bdesc + 2, idesc, 1u);
+      tc::mma_commit(&S.bar);
+    }
+    const long long t0 = clock64();
+    while (!tc::mbar_try_sleep(&S.bar, phase & 1, 2000u)) {
+      if (clock64() - t0 > kStcWait) {
+        atomicCAS(err, 0, 71);
+        ok = false;
+        break;
+      }
+    }
+    phase++;
+    tc::fence_after();
+    ok = __syncthreads_and(ok);
+  };
+  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const int g0 = t * kStcThreads, g = g0 + tid;
+    if (tid == 0) {
       int lo = 0, hi = nact;
       while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
@@ -354,36 +456,97 @@ __global__ void __launch_bounds__(256, 2) k_far_student(FarArgs a, const float* 
         else
           hi = mid;
       }
-      s_first = lo;
+      S.s_first = lo;
     }
     __syncthreads();
-    const int g = g0 + threadIdx.x;
-    int lo = s_first;
-    __syncthreads();
-    if (g >= tot) continue;
-    while (pre[lo + 1] <= g) lo++;
-    const int b = a.act[lo];
-    const int loc = g - pre[lo];
-    const FarBlock bk = a.blocks[b];
-    const int k = a.state[b].k;
-    float4 xi, xj;
-    if (which == 0) {
-      xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
-      xi = a.x[bk.sI + loc];
-    } else {
-      xj = a.x[bk.sJ + loc];
-      xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
+    float rx = 0.f, ry = 0.f, rz = 0.f;
+    pool_t* dst = nullptr;
+    if (g < tot) {
+      int lo = S.s_first;
+      while (pre[lo + 1] <= g) lo++;
+      const int b = a.act[lo];
+      const int loc = g - pre[lo];
+      const FarBlock bk = a.blocks[b];
+      const int k = a.state[b].k;
+      float4 xi, xj;
+      if (which == 0) {
+        xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
+        xi = a.x[bk.sI + loc];
+        dst = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc);
+      } else {
+        xj = a.x[bk.sJ + loc];
+        xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
+        dst = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
+      }
+      rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
     }
-    float M[9];
-    student_forward(p, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, M);
-    pool_t* dst = which == 0 ? a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc)
-                             : a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
+    const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
+    const float sc = nr >= 1e-5f ? __logf(nr * 0.5f) / nr : 0.f;
+    const float x0 = rx * sc, x1 = ry * sc, x2 = rz * sc;
+    {  // layer 1 -> A
+      uint32_t pk[16];
 #pragma unroll
-    for (int r = 0; r < 3; r++)
+      for (int j = 0; j < 16; j++) {
+        const float4 w0 = *reinterpret_cast<const float4*>(&S.w1b1[8 * j]);
+        const float4 w1 = *reinterpret_cast<const float4*>(&S.w1b1[8 * j + 4]);
+        pk[j] = silu_f16x2(fmaf(w0.z, x2, fmaf(w0.y, x1, fmaf(w0.x, x0, w0.w))),
+                           fmaf(w1.z, x2, fmaf(w1.y, x1, fmaf(w1.x, x0, w1.w))));
+      }
+      tc::tmem_st16(tl + kStcA, pk);
+    }
+    // layers 2 and 3
+    for (int l = 0; l < 2 && ok; l++) {
+      round(l == 0 ? d2 : d3, kStcD, tc::idesc_f16x(128, 32));
+      if (!ok) break;
+      uint32_t v[32];
+      tc::tmem_ld32(tl + kStcD, v);
+      tc::tmem_wait_ld();
+      const float* bb = l == 0 ? S.b2 : S.b3;
+      uint32_t pk[16];
 #pragma unroll
-      for (int c = 0; c < 3; c++)
-        dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+      for (int j = 0; j < 16; j++)
+        pk[j] = silu_f16x2(__uint_as_float(v[2 * j]) + bb[2 * j], __uint_as_float(v[2 * j + 1]) + bb[2 * j + 1]);
+      tc::tmem_st16(tl + kStcA, pk);
+    }
+    if (!ok) break;
+    round(d4, kStcD4, tc::idesc_f16x(128, 16));
+    if (!ok) break;
+    uint32_t v[16];
+    tc::tmem_ld16(tl + kStcD4, v);
+    tc::tmem_wait_ld();
+    if (dst) {
+      float M[9];
+      if (nr < 1e-5f) {
+#pragma unroll
+        for (int o = 0; o < 9; o++) M[o] = (o == 0 || o == 4 || o == 8) ? 1.0f : 0.0f;
+      } else {
+        float y[9];
+        rpy_inner(rx, ry, rz, y);
+#pragma unroll
+        for (int o = 0; o < 9; o++) {
+          float z = y[o] + __uint_as_float(v[o]) + S.b4[o];
+          if (o == 0 || o == 4 || o == 8) z += 1.0f;
+          M[o] = z / nr;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+    }
   }
+  // no MMA of this CTA may be in flight when its tensor memory is freed
+  if (tid == 0) {
+    tc::mma_commit(&S.bar);
+    const long long t0 = clock64();
+    while (!tc::mbar_try(&S.bar, phase & 1) && clock64() - t0 < kStcWait) {
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (warp == 0) tc::tmem_dealloc(tb, kStcCols);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(a.evals, (unsigned long long)tot);
 }
 
@@ -432,8 +595,9 @@ void launch_student_eval(const float* params, const float* r, float* y, int64_t 
   HIGNN_CHECK_LAUNCH();
 }
 
-void launch_far_student(const FarArgs& a, const float* params, int which, int num_sms, cudaStream_t s) {
-  k_far_student<<<8 * num_sms, 256, 0, s>>>(a, params, which);
+void launch_far_student(const FarArgs& a, const float* params, int which, int* err, int num_sms, cudaStream_t s) {
+  HIGNN_CUDA(cudaFuncSetAttribute(k_far_student_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStcSmemBytes));
+  k_far_student_tc<<<8 * num_sms, kStcThreads, kStcSmemBytes, s>>>(a, params, which, err);
   HIGNN_CHECK_LAUNCH();
 }
 
