@@ -483,9 +483,10 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
                      2.0 * v[11] * v[5];
   double mu2 = a.state[b].mu2 + nu2;  // every thread tracks the same value; thread 0 stores it
   // cross terms for l < k - 1 (src/FarDot.cpp:1041-1077), eight l per pass, one warp per l
-  for (int lb = 0; lb < k - 1; lb += 8) {
+  const int nw = blockDim.x >> 5;  // at most 8 (cross)
+  for (int lb = 0; lb < k - 1; lb += nw) {
     const int l = lb + wid;
-    if (wid < 8 && l < k - 1) {
+    if (l < k - 1) {
       double acc[18];
 #pragma unroll
       for (int q = 0; q < 18; q++) acc[q] = 0.0;
@@ -526,7 +527,7 @@ __global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
         for (int q = 0; q < 18; q++) cross[wid][q] = acc[q];
     }
     __syncthreads();
-    for (int ww = 0; ww < 8 && lb + ww < k - 1; ww++)
+    for (int ww = 0; ww < nw && lb + ww < k - 1; ww++)
       for (int q = 0; q < 9; q++) mu2 += 2.0 * fabs(cross[ww][q]) * fabs(cross[ww][9 + q]);
     __syncthreads();
   }
