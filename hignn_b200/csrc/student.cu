@@ -358,7 +358,6 @@ struct StcSmem {
   float b2[32], b3[32], b4[16];
   uint64_t bar;
   uint32_t tmem;
-  int s_first;
 };
 constexpr size_t kStcSmemBytes = 28 * 1024;  // at most eight CTAs per SM: 8 x 64 tensor-memory columns
 static_assert(sizeof(StcSmem) + 1024 <= kStcSmemBytes, "student tile shared memory");
@@ -423,7 +422,9 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
   uint32_t phase = 0;
   bool ok = true;
   // one MMA round: everyone's A is in tensor memory; thread 0 issues, all wait for the commit
-  auto round = [&](uint64_t bdesc, uint32_t d, uint32_t idesc) {
+  // one MMA round: everyone's A is in tensor memory; thread 0 issues (issue), all wait for the
+  // commit (await); work that does not touch tensor memory may run in between
+  auto issue = [&](uint64_t bdesc, uint32_t d, uint32_t idesc) {
     tc::tmem_wait_st();
     tc::fence_before();
     __syncthreads();
@@ -433,6 +434,8 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
       tc::mma_ts(tb + d, tb + kStcA + 8, bdesc + 2, idesc, 1u);
       tc::mma_commit(&S.bar);
     }
+  };
+  auto await = [&]() {
     const long long t0 = clock64();
     while (!tc::mbar_try_sleep(&S.bar, phase & 1, 2000u)) {
       if (clock64() - t0 > kStcWait) {
@@ -445,24 +448,24 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
     tc::fence_after();
     ok = __syncthreads_and(ok);
   };
-  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+  // The entry of this thread in tile t: its block through a 128-way search of the active blocks'
+  // row prefix (all threads probe, three rounds for up to 2M blocks), then the positions.
+  struct Entry {
+    float rx, ry, rz;
+    pool_t* dst;
+  };
+  auto lookup = [&](int t) {
+    Entry en{0.f, 0.f, 0.f, nullptr};
     const int g0 = t * kStcThreads, g = g0 + tid;
-    if (tid == 0) {
-      int lo = 0, hi = nact;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (pre[mid] <= g0)
-          lo = mid;
-        else
-          hi = mid;
-      }
-      S.s_first = lo;
+    int lo = 0, hi = nact;  // pre[lo] <= g0 < pre[hi]
+    while (hi - lo > 1) {
+      const int step = (hi - lo + kStcThreads - 1) / kStcThreads;
+      const int p = lo + tid * step;
+      const int cnt = __syncthreads_count(tid > 0 && p < hi && pre[p] <= g0);
+      lo += cnt * step;
+      hi = min(hi, lo + step);
     }
-    __syncthreads();
-    float rx = 0.f, ry = 0.f, rz = 0.f;
-    pool_t* dst = nullptr;
     if (g < tot) {
-      int lo = S.s_first;
       while (pre[lo + 1] <= g) lo++;
       const int b = a.act[lo];
       const int loc = g - pre[lo];
@@ -472,14 +475,19 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
       if (which == 0) {
         xj = a.x[bk.sJ + a.cols[(size_t)b * a.ldr + k]];
         xi = a.x[bk.sI + loc];
-        dst = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc);
+        en.dst = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI + loc);
       } else {
         xj = a.x[bk.sJ + loc];
         xi = a.x[bk.sI + a.rows[(size_t)b * a.ldr + k]];
-        dst = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
+        en.dst = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ + loc);
       }
-      rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
+      en.rx = xj.x - xi.x, en.ry = xj.y - xi.y, en.rz = xj.z - xi.z;
     }
+    return en;
+  };
+  Entry cur = lookup(blockIdx.x);
+  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const float rx = cur.rx, ry = cur.ry, rz = cur.rz;
     const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
     const float sc = nr >= 1e-5f ? __logf(nr * 0.5f) / nr : 0.f;
     const float x0 = rx * sc, x1 = ry * sc, x2 = rz * sc;
@@ -494,9 +502,12 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
       }
       tc::tmem_st16(tl + kStcA, pk);
     }
-    // layers 2 and 3
-    for (int l = 0; l < 2 && ok; l++) {
-      round(l == 0 ? d2 : d3, kStcD, tc::idesc_f16x(128, 32));
+    // layers 2 and 3; the next tile's entries are fetched while layer 2 runs
+    Entry nxt{0.f, 0.f, 0.f, nullptr};
+    for (int l = 0; l < 2; l++) {
+      issue(l == 0 ? d2 : d3, kStcD, tc::idesc_f16x(128, 32));
+      if (l == 0 && t + (int)gridDim.x < ntiles) nxt = lookup(t + gridDim.x);
+      await();
       if (!ok) break;
       uint32_t v[32];
       tc::tmem_ld32(tl + kStcD, v);
@@ -509,12 +520,13 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
       tc::tmem_st16(tl + kStcA, pk);
     }
     if (!ok) break;
-    round(d4, kStcD4, tc::idesc_f16x(128, 16));
+    issue(d4, kStcD4, tc::idesc_f16x(128, 16));
+    await();
     if (!ok) break;
     uint32_t v[16];
     tc::tmem_ld16(tl + kStcD4, v);
     tc::tmem_wait_ld();
-    if (dst) {
+    if (cur.dst) {
       float M[9];
       if (nr < 1e-5f) {
 #pragma unroll
@@ -533,8 +545,9 @@ __global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const
       for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++)
-          dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+          cur.dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
     }
+    cur = nxt;
   }
   // no MMA of this CTA may be in flight when its tensor memory is freed
   if (tid == 0) {
