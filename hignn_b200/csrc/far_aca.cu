@@ -25,6 +25,10 @@ namespace hignn {
 
 namespace {
 
+// Pivot CTAs work on one block at a time through a chain of dependent phases (orthogonalisation,
+// argmax, norms, cross terms), so their rate is set by how many blocks are in flight per SM: the
+// pivot kernels are capped at 64 registers per thread (four CTAs per SM instead of two; 381 ms
+// against 527 ms of pivots at N = 1M; a cap of 40 spills too much and is slower).
 constexpr int kPivThreads = 256;
 
 __device__ __forceinline__ double det3(const double* m) {
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF3
 }
 
 // Orthogonalise the new column, pick the pivot row, normalise (one CTA per active block).
-__global__ void __launch_bounds__(kPivThreads) k_far_col_pivot(FarArgs a) {
+__global__ void __launch_bounds__(kPivThreads, 4) k_far_col_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* qj = dsm;  // [k][9]
   __shared__ double sv[32], inv[9];
@@ -400,7 +404,7 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
 }
 
 // Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
-__global__ void __launch_bounds__(kPivThreads) k_far_row_pivot(FarArgs a) {
+__global__ void __launch_bounds__(kPivThreads, 4) k_far_row_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* ci = dsm;                          // [k][9]
   double* mid = dsm + 9 * a.ldr;            // [rank][3]
