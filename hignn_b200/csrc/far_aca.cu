@@ -27,9 +27,11 @@ namespace {
 
 // Pivot CTAs work on one block at a time through a chain of dependent phases (orthogonalisation,
 // argmax, norms, cross terms), so their rate is set by how many blocks are in flight per SM: the
-// pivot kernels are capped at 64 registers per thread (four CTAs per SM instead of two; 381 ms
-// against 527 ms of pivots at N = 1M; a cap of 40 spills too much and is slower).
-constexpr int kPivThreads = 256;
+// pivot kernels run 128-thread CTAs capped at 64 registers per thread, eight per SM (357 ms of
+// pivots at N = 1M, against 527 ms for 256-thread CTAs at ~126 registers, two per SM; a cap of
+// 40 registers spills too much and is slower).
+constexpr int kPivThreads = 128;
+constexpr int kApplyThreads = 256;  // the deferred apply: few phases, wider CTAs
 
 __device__ __forceinline__ double det3(const double* m) {
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF3
 }
 
 // Orthogonalise the new column, pick the pivot row, normalise (one CTA per active block).
-__global__ void __launch_bounds__(kPivThreads, 4) k_far_col_pivot(FarArgs a) {
+__global__ void __launch_bounds__(kPivThreads, 8) k_far_col_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* qj = dsm;  // [k][9]
   __shared__ double sv[32], inv[9];
@@ -404,7 +406,7 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
 }
 
 // Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
-__global__ void __launch_bounds__(kPivThreads, 4) k_far_row_pivot(FarArgs a) {
+__global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* ci = dsm;                          // [k][9]
   double* mid = dsm + 9 * a.ldr;            // [rank][3]
@@ -573,7 +575,7 @@ __global__ void __launch_bounds__(kPivThreads, 4) k_far_row_pivot(FarArgs a) {
 
 // Applies every converged block of the batch (state done == 1): the student path defers the
 // apply until the sampled residual check has accepted the block.
-__global__ void __launch_bounds__(kPivThreads) k_far_apply(FarArgs a) {
+__global__ void __launch_bounds__(kApplyThreads) k_far_apply(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
   double* mid = dsm;
   double* mid2 = dsm + 3 * a.ldr;
@@ -681,7 +683,7 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem));
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_row_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
   HIGNN_CUDA(cudaFuncSetAttribute(k_far_col_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-  const int piv_grid = a.nb < 8 * num_sms ? a.nb : 8 * num_sms;  // grid-stride over active blocks
+  const int piv_grid = a.nb < 16 * num_sms ? a.nb : 16 * num_sms;  // grid-stride over active blocks
   k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   HIGNN_CHECK_LAUNCH();
   // Without a known bound the counters are read back every kCheck iterations; the kernels of
@@ -741,7 +743,7 @@ int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* stude
   HIGNN_CHECK_LAUNCH();
   const size_t smem = sizeof(double) * 6 * a.ldr;
   const int grid = a.nb < 8 * num_sms ? a.nb : 8 * num_sms;
-  k_far_apply<<<grid, kPivThreads, smem, s>>>(a);
+  k_far_apply<<<grid, kApplyThreads, smem, s>>>(a);
   HIGNN_CHECK_LAUNCH();
   int nfail = 0;
   HIGNN_CUDA(cudaMemcpyAsync(&nfail, nfail_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
