@@ -359,7 +359,9 @@ struct StcSmem {
   uint64_t bar;
   uint32_t tmem;
 };
-constexpr size_t kStcSmemBytes = 28 * 1024;  // at most eight CTAs per SM: 8 x 64 tensor-memory columns
+// Eight CTAs per SM (8 x 64 tensor-memory columns): 26 KB of shared memory and at most 64
+// registers per thread let eight fit.
+constexpr size_t kStcSmemBytes = 26 * 1024;
 static_assert(sizeof(StcSmem) + 1024 <= kStcSmemBytes, "student tile shared memory");
 
 __device__ __forceinline__ uint32_t stc_swz(int row, int k) {
@@ -375,7 +377,7 @@ __device__ __forceinline__ uint32_t silu_f16x2(float z0, float z1) {
   return *reinterpret_cast<const uint32_t*>(&r);
 }
 
-__global__ void __launch_bounds__(kStcThreads) k_far_student_tc(FarArgs a, const float* __restrict__ params, int which,
+__global__ void __launch_bounds__(kStcThreads, 8) k_far_student_tc(FarArgs a, const float* __restrict__ params, int which,
                                                                 int* err) {
   extern __shared__ uint8_t raw[];
   const uint32_t rb = tc::saddr(raw);
