@@ -10,9 +10,10 @@
 //
 // Here one persistent kernel per list does gather -> network -> bmm -> scatter for 128 edges per
 // tile. Layer 1 (kin <= 6 inputs) runs on the CUDA cores in FP32 and writes tanh'd FP16 pairs
-// into tensor memory as the A operand of layer 2. Layers 2 and 3 are tcgen05 MMAs (FP16 in, FP32
-// accumulated in tensor memory); layer 4 (512 -> 9) runs on the CUDA cores in FP32 from the FP16
-// tanh of layer 3. Tensor memory (512 columns) holds the layer-1 activations (128 columns of FP16
+// into tensor memory as the A operand of layer 2. Layers 2, 3 and 4 are tcgen05 MMAs (FP16 in,
+// FP32 accumulated in tensor memory); layer 4 (512 -> 9, N = 16) takes each pass's tanh'd layer-3
+// values from tensor memory, where they replace the read accumulator. Tensor memory (512
+// columns) holds the layer-1 activations (128 columns of FP16
 // pairs), one 128-column layer-2 accumulator and a 256-column layer-3 accumulator. The 512
 // layer-3 outputs therefore take two passes per tile, each recomputing layer 2 (1.33x the
 // network's FLOPs) -- the layer-2 activations of a tile (128 x 1024 FP16 = 256 KB) fit neither
@@ -55,13 +56,17 @@ using tc::tmem_wait_ld;
 constexpr int kEpiThreads = 512;
 constexpr int kMmaWarp = 16, kProdWarp = 17, kThreads = 576;
 constexpr int kRing = 5;
-constexpr uint32_t kOffA1 = 0, kOffD2 = 128, kOffD3 = 256;  // tensor-memory columns
+// tensor-memory columns: layer 1 (A of layer 2), layer-2 accumulator, layer-3 accumulator; once
+// the layer-3 accumulator of a pass is read, its first 128 columns take that pass's tanh'd
+// layer-3 values (A of layer 4) and columns 384-399 the layer-4 accumulator
+constexpr uint32_t kOffA1 = 0, kOffD2 = 128, kOffD3 = 256, kOffA3 = 256, kOffD4 = 384;
 constexpr long long kWait = 4000000000LL;      // ~2 s at 1.9 GHz
 
 struct TbSmem {
   uint8_t act2[2][2][16384];  // A of layer 3, two buffers of 128 rows x 128 K (FP16)
   uint8_t ring[kRing][kTbStageBytes];
-  uint64_t act1_full, d2_full, d2_free, act2_full[2], d3_full, d3_free, ring_full[kRing], ring_empty[kRing], drain;
+  uint64_t act1_full, d2_full, d2_free, act2_full[2], d3_full, act3_full, d4_full, d3_free, ring_full[kRing],
+      ring_empty[kRing], drain;
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -236,56 +241,56 @@ struct Epi {
     mbar_arrive(&s.act2_full[b]);
   }
 
-  // layer 3 of pass h (D3 columns 64 part .. + 63) and its share of layer 4. The accumulator is
-  // read, tanh'd into FP16 pairs (as layer 2's activations are) and released before layer 4 runs
-  // from the pairs, so the MMA lane's next layer-3 slice does not wait for layer 4.
-  __device__ void layer3(uint32_t P, int h, float (&y)[9]) {
+  // Layer 3 of pass h: read the accumulator (D3 columns 64 part .. + 63), add b3, tanh into FP16
+  // pairs, and once every thread has read its columns, write the pairs back as the A operand of
+  // layer 4 (columns 256 + 32 part ..). Every epilogue thread runs this (it holds a barrier).
+  __device__ void layer3(uint32_t P, int h) {
     uint32_t a3[32];
     const bool got = wait(&s.d3_full, P & 1, 42);
     if (got) {
 #pragma unroll
-      for (int half = 0; half < 2; half++) {
-        uint32_t v[32];
-        tmem_ld32(tlane + kOffD3 + 64 * part + 32 * half, v);
+      for (int q = 0; q < 4; q++) {
+        uint32_t v[16];
+        tc::tmem_ld16(tlane + kOffD3 + 64 * part + 16 * q, v);
         tmem_wait_ld();
-        const float* b3 = c.b3 + h * 256 + 64 * part + 32 * half;
+        const float* b3 = c.b3 + h * 256 + 64 * part + 16 * q;
 #pragma unroll
-        for (int j = 0; j < 16; j++)
-          a3[16 * half + j] =
+        for (int j = 0; j < 8; j++)
+          a3[8 * q + j] =
               tanh_f16x2(pack_f16(__uint_as_float(v[2 * j]) + b3[2 * j], __uint_as_float(v[2 * j + 1]) + b3[2 * j + 1]));
       }
     }
     fence_before();
-    mbar_arrive(&s.d3_free);
-    if (!got) return;
-    const float* w4 = c.w4 + 9 * (h * 256 + 64 * part);
-#pragma unroll 4
-    for (int j2 = 0; j2 < 32; j2++) {
-      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&a3[j2]));
-#pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const float av = i ? a.y : a.x;
-        const float* wj = w4 + 9 * (2 * j2 + i);
-#pragma unroll
-        for (int o = 0; o < 9; o++) y[o] = fmaf(av, wj[o], y[o]);
-      }
+    epi_bar();  // every column of D3 has been read before any is overwritten
+    fence_after();
+    if (got) {
+      tc::tmem_st32(tlane + kOffA3 + 32 * part, a3);
+      tc::tmem_wait_st();
     }
+    fence_before();
+    mbar_arrive(&s.act3_full);
   }
 
-  // sum of the four parts' layer-4 shares, wrapper, 3x3 times the force, scatter (part 0)
-  __device__ void output(int64_t t) {
+  // Layer 4 of pass P (part 0): add the accumulator's nine columns to y and release D3 / D4.
+  __device__ void layer4(uint32_t P, float (&y)[9]) {
+    if (wait(&s.d4_full, P & 1, 43)) {
+      uint32_t v[16];
+      tc::tmem_ld16(tlane + kOffD4, v);
+      tmem_wait_ld();
+#pragma unroll
+      for (int o = 0; o < 9; o++) y[o] += __uint_as_float(v[o]);
+    }
+    fence_before();
+    mbar_arrive(&s.d3_free);
+  }
+
+  // layer 4's two passes plus b4, the wrapper, 3x3 times the force, scatter (part 0)
+  __device__ void output(int64_t t, const float (&y)[9]) {
     const int64_t q = t * 128 + e;
     if (q >= E) return;
-    const float* scratch = reinterpret_cast<const float*>(&s.act2[0][0][0]);
     float yy[9];
 #pragma unroll
-    for (int o = 0; o < 9; o++) {
-      float v = scratch[(0 * 128 + e) * 9 + o];
-      v += scratch[(1 * 128 + e) * 9 + o];
-      v += scratch[(2 * 128 + e) * 9 + o];
-      v += scratch[(3 * 128 + e) * 9 + o];
-      yy[o] = v + c.b4[o];
-    }
+    for (int o = 0; o < 9; o++) yy[o] = y[o] + c.b4[o];
     float in[6];
     int64_t src, dst;
     edge_input<KIND>(edges, E, q, x, in, src, dst);
@@ -304,29 +309,46 @@ struct Epi {
       atomicAdd(&u[3 * dst + i], yy[3 * i] * fs.x + yy[3 * i + 1] * fs.y + yy[3 * i + 2] * fs.z);
   }
 
-  // Per tile: E2 of chunks 0..15, with layer 3 of pass 0 read after chunk 8 (its accumulator is
-  // complete once L3(7) is, which the MMA lane issues after L2(8)), the next tile's layer 1 after
-  // chunk 15 (every layer-2 MMA of this tile is then complete), then layer 3 of pass 1.
+  // The epilogue follows the MMA lane's order: per tile E2 of chunks 0..15, layer 3 of pass 0
+  // after chunk 8 and its layer 4 (part 0) after chunk 9, the next tile's layer 1 after chunk 15,
+  // then layer 3 of pass 1; layer 4 of pass 1 and the output come after the next tile's first
+  // chunk (the MMA lane issues that chunk's layer 2 before layer 4 of pass 1).
   __device__ void run(int64_t ntiles) {
     uint32_t g = 0, P = 0;
+    float y[9];
+#pragma unroll
+    for (int o = 0; o < 9; o++) y[o] = 0.f;
     if ((int64_t)blockIdx.x < ntiles) layer1(blockIdx.x);
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      float y[9];
-#pragma unroll
-      for (int o = 0; o < 9; o++) y[o] = 0.f;
+    bool go = true;
+    int64_t prev = -1;
+    for (int64_t t = blockIdx.x; t < ntiles && go; t += gridDim.x) {
 #pragma unroll 1
-      for (int c = 0; c < 16; c++, g++) {
+      for (int cc = 0; cc < 16; cc++, g++) {
         layer2(g);
-        if (c == 8) layer3(P++, 0, y);
-      }
-      if (ok && t + gridDim.x < ntiles) layer1(t + gridDim.x);
-      layer3(P++, 1, y);
-      float* scratch = reinterpret_cast<float*>(&s.act2[0][0][0]);
+        if (cc == 0 && prev >= 0) {  // finish the previous tile
+          if (part == 0) {
+            layer4(P - 1, y);
+            output(prev, y);
+          }
+          go = epi_all(ok);
+          if (!go) break;
 #pragma unroll
-      for (int o = 0; o < 9; o++) scratch[(part * 128 + e) * 9 + o] = y[o];
-      if (!epi_all(ok)) break;
-      if (part == 0) output(t);
-      epi_bar();  // the scratch is act2, which the next tile's first chunk overwrites
+          for (int o = 0; o < 9; o++) y[o] = 0.f;
+        }
+        if (cc == 8) layer3(P++, 0);
+        if (cc == 9 && part == 0) layer4(P - 1, y);
+      }
+      if (!go) break;
+      if (ok && t + gridDim.x < ntiles) layer1(t + gridDim.x);
+      layer3(P++, 1);
+      prev = t;
+    }
+    if (go && prev >= 0) {
+      if (part == 0) {
+        layer4(P - 1, y);
+        output(prev, y);
+      }
+      epi_all(ok);
     }
   }
 };
@@ -389,18 +411,36 @@ struct MmaLaneTb {
     return true;
   }
 
+  // layer 4 of pass P: A = the tanh'd layer 3 in tensor memory, one stage with W4's rows for
+  // this pass (16 rows, 9 used, x 256 K, four 2 KB K blocks)
+  __device__ bool l4(uint32_t P) {
+    if (!wait(&s.act3_full, P & 1, 58)) return false;
+    if (!stage_ready()) return false;
+    const uint64_t b0 = sdesc(saddr(s.ring[S % kRing]));
+    const uint32_t id = idesc_f16(128, 16);
+#pragma unroll
+    for (uint32_t k16 = 0; k16 < 16; k16++)
+      tc::mma_ts(tb + kOffD4, tb + kOffA3 + 8 * k16, b0 + (k16 >> 2) * (2048 >> 4) + (k16 & 3) * 2, id, k16 != 0);
+    stage_done();
+    mma_commit(&s.d4_full);
+    return true;
+  }
+
   __device__ void run(int64_t ntiles, unsigned long long* prof) {
     const long long start = clock64();
     uint32_t g = 0, k = 0;
+    // per tile: [L2(0) for the first tile], then L2(c + 1) L3(c) for c = 0..15 (no L2(16)) with
+    // L4 of pass 0 before L3(8); then the next tile's L2(0) and L4 of pass 1. Chunks 0-7 are
+    // pass 0, 8-15 pass 1.
+    if ((int64_t)blockIdx.x < ntiles && wait(&s.act1_full, 0, 50)) l2(0);
     for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, k++, g += 16) {
-      // per tile: L2(0), then L2(c + 1) L3(c) for c = 0..15 (L2 only up to chunk 15); chunks
-      // 0-7 are pass 0, 8-15 pass 1
-      if (!wait(&s.act1_full, k & 1, 50)) break;
-      l2(g);
       for (uint32_t c = 0; c < 16 && ok; c++) {
         if (c < 15) l2(g + c + 1);
+        if (c == 8 && ok) l4(2 * k);
         if (ok) l3(g + c, c & 7, 2 * k + (c >> 3));
       }
+      if (ok && t + gridDim.x < ntiles && wait(&s.act1_full, (k + 1) & 1, 50)) l2(g + 16);
+      if (ok) l4(2 * k + 1);
     }
     // let every issued MMA finish before the tensor memory is freed
     mma_commit(&s.drain);
@@ -417,8 +457,18 @@ __device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err
   uint32_t S = 0;
   bool ok = true;
   long long waited = 0;
-  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x)
-    for (int st = 0; st < kTbStagesPerTile; st++, S++) {
+  // per tile: [segment A for the first tile], segment B, [segment A if a tile follows], W4 of
+  // pass 1 -- the MMA lane's order (the image holds A | B | W4 of pass 1)
+  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const bool first = t == (int64_t)blockIdx.x, next = t + gridDim.x < ntiles;
+    const int count = (first ? kTbSegA : 0) + kTbSegB + (next ? kTbSegA : 0) + 1;
+    for (int i = 0; i < count; i++, S++) {
+      int st = i;
+      if (!first) st += kTbSegA;                          // skip the leading segment A
+      if (st >= kTbSegA + kTbSegB) {                      // past segment B
+        const int r = st - kTbSegA - kTbSegB;
+        st = (next && r < kTbSegA) ? r : kTbSegA + kTbSegB;  // segment A again, then W4
+      }
       const uint32_t slot = S % kRing;
       const long long t0 = clock64();
       const bool got = S < kRing || wait_bar(&s.ring_empty[slot], ((S / kRing) - 1) & 1, &s.abort_flag, err, 56);
@@ -429,6 +479,7 @@ __device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err
       }
       bulk_load(s.ring[slot], img + (size_t)st * kTbStageBytes, kTbStageBytes, &s.ring_full[slot]);
     }
+  }
   // every issued copy must land before the CTA exits
   const uint32_t first = S > (uint32_t)kRing ? S - kRing : 0;
   for (uint32_t q = first; q < S; q++) wait_bar(&s.ring_full[q % kRing], (q / kRing) & 1, &s.abort_flag, err, 57, false);
@@ -451,7 +502,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(&s.d2_free, kEpiThreads);
     for (int b = 0; b < 2; b++) mbar_init(&s.act2_full[b], kEpiThreads);
     mbar_init(&s.d3_full, 1);
-    mbar_init(&s.d3_free, kEpiThreads);
+    mbar_init(&s.act3_full, kEpiThreads);
+    mbar_init(&s.d4_full, 1);
+    mbar_init(&s.d3_free, kEpiThreads / 4);  // part 0 reads layer 4
     for (int r = 0; r < kRing; r++) {
       mbar_init(&s.ring_full[r], 1);
       mbar_init(&s.ring_empty[r], 1);
@@ -534,8 +587,6 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
   std::copy(B[1].begin(), B[1].end(), net.cst.b2);
   std::copy(B[2].begin(), B[2].end(), net.cst.b3);
   std::copy(B[3].begin(), B[3].end(), net.cst.b4);
-  for (int n = 0; n < kTbH3; n++)
-    for (int o = 0; o < 9; o++) net.cst.w4[n * 9 + o] = W[3][(size_t)o * kTbH3 + n];
   // layers 2 and 3 as 32 KB FP16 stages (K-major, 128-byte swizzle; a 64-wide K block of R rows
   // is R x 128 B, 8-row groups 1024 B apart) in the MMA lane's order per tile: L2(0), then
   // L2(c + 1) L3(c) for c = 0..15 (no L2(16)). An L2 chunk c (pass c / 8, W2 rows (c % 8) 128 ..)
@@ -562,11 +613,25 @@ void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, co
     for (int kb = 0; kb < 2; kb++, st++)
       put_block(img.data() + st * kTbStageBytes, W[2], kTbH2, 256, (c / 8) * 256, (c % 8) * 128 + kb * 64);
   };
-  put_l2(0);
-  for (int c = 0; c < 16; c++) {
+  // W4 rows of pass h: 16 rows (outputs, 9 used) x 256 K (layer-3 outputs h 256 ..), four
+  // 64-wide K blocks of 2 KB at the start of a stage
+  auto put_l4 = [&](int h) {
+    uint8_t* dst = img.data() + st * kTbStageBytes;
+    for (int kb = 0; kb < 4; kb++)
+      for (int o = 0; o < 9; o++)
+        for (int kc = 0; kc < 64; kc++) {
+          const uint16_t v = f16_of(W[3][(size_t)o * kTbH3 + h * 256 + kb * 64 + kc]);
+          std::memcpy(dst + kb * 2048 + swz(o, kc), &v, 2);
+        }
+    st++;
+  };
+  put_l2(0);  // segment A
+  for (int c = 0; c < 16; c++) {  // segment B
     if (c < 15) put_l2(c + 1);
+    if (c == 8) put_l4(0);
     put_l3(c);
   }
+  put_l4(1);
   if (st != (size_t)kTbStagesPerTile) throw Error(-1, "three-body image: stage count mismatch");
   net.d_img.ensure(img.size());
   HIGNN_CUDA(cudaMemcpyAsync(net.d_img.p, img.data(), img.size(), cudaMemcpyHostToDevice, s));

@@ -12,9 +12,12 @@
 namespace hignn {
 
 constexpr int kTbH1 = 256, kTbH2 = 1024, kTbH3 = 512;
-constexpr int kTbStageBytes = 32768;                // one weight stage: 256 rows x 64 K or 128 x 128 K (FP16)
-constexpr int kTbStagesPerTile = 64;                 // 16 layer-2 chunks and 16 layer-3 slices, 2 stages each
-constexpr int kTbImageBytes = kTbStagesPerTile * kTbStageBytes;  // 2 MB
+constexpr int kTbStageBytes = 32768;  // one weight stage: 256 rows x 64 K or 128 x 128 K (FP16)
+// Image segments in the MMA lane's order: A = layer 2 chunk 0 (2 stages), B = the rest of a tile
+// (15 layer-2 chunks and 16 layer-3 slices of 2 stages, layer 4 of pass 0), then layer 4 of pass 1
+constexpr int kTbSegA = 2, kTbSegB = 15 * 2 + 16 * 2 + 1;
+constexpr int kTbStagesPerTile = kTbSegA + kTbSegB + 1;
+constexpr int kTbImageBytes = kTbStagesPerTile * kTbStageBytes;  // 2.06 MB
 
 // Small per-network constants, passed to the kernel as a parameter: the epilogue reads them
 // with warp-uniform indices, which the constant bank serves without a memory round trip.
@@ -22,7 +25,6 @@ struct TbConst {
   float w1[kTbH1 * 7];  // row n: W1[n][0..kin) zero padded to 6, then b1[n]
   float b2[kTbH2];
   float b3[kTbH3];
-  float w4[kTbH3 * 9];  // column n of W4: w4[9 n + o] = W4[o][n]
   float b4[9];
 };
 
