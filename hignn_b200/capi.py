@@ -118,6 +118,7 @@ SIGNATURES = {
     "hignn_tb_load_mem": ([_P, C.c_int, C.c_int, C.POINTER(C.c_int32), _fp], C.c_int),
     "hignn_tb_set_epsilon": ([_P, C.c_float], C.c_int),
     "hignn_tb_velocity": ([_P, _fp, _fp, _fp, C.c_int64], C.c_int),
+    "hignn_tb_velocity_edges": ([_P, _fp, _fp, _fp, C.c_int64, _u64p, C.c_int64, _u64p, C.c_int64], C.c_int),
     "hignn_tb_stats": ([_P, _dp, _dp, _dp, _i64p, _i64p], C.c_int),
     "hignn_tb_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
 }
@@ -472,6 +473,18 @@ class ThreeBody:
         f = _f32(f, x.shape)
         u = np.empty_like(x)
         check(lib.hignn_tb_velocity(self._h, fptr(x), fptr(f), fptr(u), len(x)))
+        return u
+
+    def velocity_edges(self, x, f, tri, self_edges):
+        """The same two terms on caller-given edge lists: tri (3, E3) and self_edges (2, Es), the
+        rows of NeighborLists.get_three_body_edge_info / get_three_body_edge_self_info."""
+        x = _f32(x)
+        f = _f32(f, x.shape)
+        tri = np.ascontiguousarray(tri, np.uint64).reshape(3, -1)
+        se = np.ascontiguousarray(self_edges, np.uint64).reshape(2, -1)
+        u = np.empty_like(x)
+        check(lib.hignn_tb_velocity_edges(self._h, fptr(x), fptr(f), fptr(u), len(x), tri.ctypes.data_as(_u64p),
+                                          tri.shape[1], se.ctypes.data_as(_u64p), se.shape[1]))
         return u
 
     def stats(self):

@@ -1631,7 +1631,7 @@ struct hignn_tb {
   hignn::TbNet nets[2];
   int num_sms = 0;
   float eps = 5.0f;
-  DevBuf f4, fin, u, err, prof;
+  DevBuf f4, fin, u, err, prof, etri, eself;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double ms_lists = 0, ms_three = 0, ms_self = 0;
   int64_t triplets = 0, pairs = 0;
@@ -1642,7 +1642,7 @@ struct hignn_tb {
   ~hignn_tb() {
     cudaSetDevice(lists.device());
     cudaStreamSynchronize(lists.stream());
-    for (DevBuf* b : {&f4, &fin, &u, &err, &prof}) b->release();
+    for (DevBuf* b : {&f4, &fin, &u, &err, &prof, &etri, &eself}) b->release();
     for (auto& n : nets)
       n.d_img.release();
     for (auto& e : ev)
@@ -1718,14 +1718,59 @@ int hignn_tb_set_epsilon(hignn_tb* t, float eps) {
   });
 }
 
+namespace {
+
+// The two kernels on the device edge lists tri (3, e3) and self (2, es) at the positions already
+// in t->lists; f and u are host arrays.
+void tb_run(hignn_tb* t, const float* f, float* u, int64_t n, const uint64_t* tri, int64_t e3, const uint64_t* self,
+            int64_t es) {
+  cudaStream_t s = t->lists.stream();
+  t->triplets = e3;
+  t->pairs = es;
+  t->fin.ensure(sizeof(float) * 3 * n);
+  t->f4.ensure(sizeof(float4) * n);
+  t->u.ensure(sizeof(float) * 3 * n);
+  t->err.ensure(sizeof(int));
+  t->prof.ensure(sizeof(unsigned long long) * 12);
+  HIGNN_CUDA(cudaMemsetAsync(t->prof.p, 0, sizeof(unsigned long long) * 12, s));
+  HIGNN_CUDA(cudaMemcpyAsync(t->fin.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+  hignn::launch_pack_positions(t->fin.as<float>(), n, t->f4.as<float4>(), s);
+  HIGNN_CUDA(cudaMemsetAsync(t->u.p, 0, sizeof(float) * 3 * n, s));
+  HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), s));
+  HIGNN_CUDA(cudaEventRecord(t->ev[0], s));
+  hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), t->nets[0].cst, tri, e3, t->lists.positions(),
+                           t->f4.as<float4>(), t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>(),
+                           t->num_sms, s);
+  HIGNN_CUDA(cudaEventRecord(t->ev[1], s));
+  hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), t->nets[1].cst, self, es, t->lists.positions(),
+                           t->f4.as<float4>(), t->u.as<float>(), t->err.as<int>(),
+                           t->prof.as<unsigned long long>() + 6, t->num_sms, s);
+  HIGNN_CUDA(cudaEventRecord(t->ev[2], s));
+  int e = 0;
+  HIGNN_CUDA(cudaMemcpyAsync(u, t->u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+  HIGNN_CUDA(cudaMemcpyAsync(&e, t->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HIGNN_CUDA(cudaStreamSynchronize(s));
+  float a = 0, b = 0;
+  HIGNN_CUDA(cudaEventElapsedTime(&a, t->ev[0], t->ev[1]));
+  HIGNN_CUDA(cudaEventElapsedTime(&b, t->ev[1], t->ev[2]));
+  t->ms_three = a;
+  t->ms_self = b;
+  if (e != 0) throw Error(HIGNN_ERR_LIMIT, "three-body kernel: a wait timed out (code " + std::to_string(e) + ")");
+}
+
+void tb_check(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n) {
+  if (!t || !xyz || !f || !u) throw Error(HIGNN_ERR_ARG, "null argument");
+  if (n <= 0) throw Error(HIGNN_ERR_ARG, "three-body: n must be positive");
+  if (!t->nets[0].loaded || !t->nets[1].loaded)
+    throw Error(HIGNN_ERR_STATE, "three-body: load both the three-body and the self network");
+}
+
+}  // namespace
+
 int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n) {
   return guard([&] {
-    if (!t || !xyz || !f || !u) throw Error(HIGNN_ERR_ARG, "null argument");
-    if (n <= 0) throw Error(HIGNN_ERR_ARG, "three-body: n must be positive");
-    if (!t->nets[0].loaded || !t->nets[1].loaded)
-      throw Error(HIGNN_ERR_STATE, "three-body: load both the three-body and the self network");
+    tb_check(t, xyz, f, u, n);
     HIGNN_CUDA(cudaSetDevice(t->lists.device()));
-    cudaStream_t s = t->lists.stream();
     const auto t0 = std::chrono::steady_clock::now();
     t->lists.update_coord(xyz, n);
     t->lists.set_three_body_epsilon(t->eps);
@@ -1734,36 +1779,30 @@ int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, i
     int64_t e3 = 0, es = 0;
     const uint64_t* tri = t->lists.device_list(hignn::kEdgesThreeBody, &e3);
     const uint64_t* self = t->lists.device_list(hignn::kEdgesThreeBodySelf, &es);
-    t->triplets = e3;
-    t->pairs = es;
-    t->fin.ensure(sizeof(float) * 3 * n);
-    t->f4.ensure(sizeof(float4) * n);
-    t->u.ensure(sizeof(float) * 3 * n);
-    t->err.ensure(sizeof(int));
-    t->prof.ensure(sizeof(unsigned long long) * 12);
-    HIGNN_CUDA(cudaMemsetAsync(t->prof.p, 0, sizeof(unsigned long long) * 12, s));
-    HIGNN_CUDA(cudaMemcpyAsync(t->fin.p, f, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
-    hignn::launch_pack_positions(t->fin.as<float>(), n, t->f4.as<float4>(), s);
-    HIGNN_CUDA(cudaMemsetAsync(t->u.p, 0, sizeof(float) * 3 * n, s));
-    HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), s));
-    HIGNN_CUDA(cudaEventRecord(t->ev[0], s));
-    hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), t->nets[0].cst, tri, e3, t->lists.positions(), t->f4.as<float4>(),
-                             t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>(), t->num_sms, s);
-    HIGNN_CUDA(cudaEventRecord(t->ev[1], s));
-    hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), t->nets[1].cst, self, es, t->lists.positions(), t->f4.as<float4>(),
-                             t->u.as<float>(), t->err.as<int>(), t->prof.as<unsigned long long>() + 6, t->num_sms, s);
-    HIGNN_CUDA(cudaEventRecord(t->ev[2], s));
-    int e = 0;
-    HIGNN_CUDA(cudaMemcpyAsync(u, t->u.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
-    HIGNN_CUDA(cudaMemcpyAsync(&e, t->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    HIGNN_CUDA(cudaStreamSynchronize(s));
-    float a = 0, b = 0;
-    HIGNN_CUDA(cudaEventElapsedTime(&a, t->ev[0], t->ev[1]));
-    HIGNN_CUDA(cudaEventElapsedTime(&b, t->ev[1], t->ev[2]));
-    t->ms_three = a;
-    t->ms_self = b;
-    if (e != 0)
-      throw Error(HIGNN_ERR_LIMIT, "three-body kernel: a wait timed out (code " + std::to_string(e) + ")");
+    tb_run(t, f, u, n, tri, e3, self, es);
+  });
+}
+
+int hignn_tb_velocity_edges(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n, const uint64_t* tri,
+                            int64_t e3, const uint64_t* self_edges, int64_t es) {
+  return guard([&] {
+    tb_check(t, xyz, f, u, n);
+    if (e3 < 0 || es < 0 || (e3 > 0 && !tri) || (es > 0 && !self_edges))
+      throw Error(HIGNN_ERR_ARG, "three-body: bad edge lists");
+    for (int64_t q = 0; q < 3 * e3; q++)
+      if (tri[q] >= (uint64_t)n) throw Error(HIGNN_ERR_ARG, "three-body: triplet index out of range");
+    for (int64_t q = 0; q < 2 * es; q++)
+      if (self_edges[q] >= (uint64_t)n) throw Error(HIGNN_ERR_ARG, "three-body: self-edge index out of range");
+    HIGNN_CUDA(cudaSetDevice(t->lists.device()));
+    cudaStream_t s = t->lists.stream();
+    t->lists.update_coord(xyz, n);
+    t->ms_lists = 0.0;
+    t->etri.ensure(sizeof(uint64_t) * 3 * (e3 > 0 ? e3 : 1));
+    t->eself.ensure(sizeof(uint64_t) * 2 * (es > 0 ? es : 1));
+    if (e3 > 0) HIGNN_CUDA(cudaMemcpyAsync(t->etri.p, tri, sizeof(uint64_t) * 3 * e3, cudaMemcpyHostToDevice, s));
+    if (es > 0)
+      HIGNN_CUDA(cudaMemcpyAsync(t->eself.p, self_edges, sizeof(uint64_t) * 2 * es, cudaMemcpyHostToDevice, s));
+    tb_run(t, f, u, n, t->etri.as<uint64_t>(), e3, t->eself.as<uint64_t>(), es);
   });
 }
 

@@ -327,6 +327,14 @@ int hignn_tb_set_epsilon(hignn_tb* t, float eps);
  * Builds the edge lists on the device, then runs both networks. */
 int hignn_tb_velocity(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n);
 
+/* As hignn_tb_velocity, on edge lists the caller gives instead of the internal ones: tri (3, e3)
+ * and self_edges (2, es), uint64 row-major host arrays with the rows of the reference's
+ * NeighborLists::GetThreeBodyEdgeInfo / GetThreeBodyEdgeSelfInfo (include/NeighborLists.hpp:
+ * 342-360, 405-422), in any edge order -- what python/gravity_field.py:31-52 passes to the torch
+ * model. Every index must be < n. */
+int hignn_tb_velocity_edges(hignn_tb* t, const float* xyz, const float* f, float* u, int64_t n, const uint64_t* tri,
+                            int64_t e3, const uint64_t* self_edges, int64_t es);
+
 /* Last call: ms of the list build, the three-body and the self kernels, and the edge counts. */
 int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
                    int64_t* pairs);

@@ -62,6 +62,24 @@ def test_matches_oracle_and_is_repeatable(tb):
     assert rel(u2, u) < 1e-5  # float atomics: only the order of the sums may differ
 
 
+def test_caller_edge_lists(tb):
+    # the reference's usage (python/gravity_field.py): edge lists from NeighborLists, any order
+    g = np.load(GOLD)
+    x, f, eps = g["filaments_x"], g["filaments_f"], float(g["filaments_eps"])
+    off, nbr = O.neighbour_csr(x, eps)
+    tri, _ = O.three_body_edge_info(off, nbr)
+    pairs = O.two_body_edge_info(off, nbr)
+    rng = np.random.default_rng(5)
+    tri = tri[:, rng.permutation(tri.shape[1])]
+    pairs = pairs[:, rng.permutation(pairs.shape[1])]
+    u = tb.velocity_edges(x, f, tri, pairs)
+    assert rel(u, g["filaments_v64"]) < TOL
+    tb.set_epsilon(eps)
+    assert rel(u, tb.velocity(x, f)) < 1e-5  # the same edges in another order: float sums only
+    with pytest.raises(capi.HignnError):
+        tb.velocity_edges(x, f, np.array([[0], [1], [len(x)]], np.uint64), pairs)
+
+
 def test_sparse_and_empty_lists(tb):
     tb.set_epsilon(5.0)
     x = np.array([[0, 0, 0], [100, 0, 0], [0, 100, 0]], np.float32)  # no neighbours at all
