@@ -9,7 +9,7 @@ from conftest import REPO
 def declared_symbols():
     src = open(os.path.join(REPO, "include", "hignn_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\bint\s+(hignn_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(?:int|void)\s+(hignn_\w+)\s*\(", src)))
 
 
 def test_header_declares_entry_points():
@@ -66,3 +66,21 @@ def test_bad_weight_file(tmp_path):
         raise AssertionError("malformed weights must be rejected")
     except capi.HignnError as e:
         assert e.code == -4
+
+
+def test_neighbour_lists_and_three_body_need_a_device():
+    import ctypes as C
+
+    import pytest
+
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from hignn_b200 import capi
+
+    h = C.c_void_p()
+    assert capi.lib.hignn_nbl_create(0, C.byref(h)) == -6  # HIGNN_ERR_NODEV
+    assert capi.lib.hignn_tb_create(0, C.byref(h)) == -6
+    assert not h.value
+    capi.lib.hignn_nbl_destroy(None)  # a null handle is accepted
+    capi.lib.hignn_tb_destroy(None)
