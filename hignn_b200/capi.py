@@ -97,6 +97,7 @@ SIGNATURES = {
     "hignn_pair_forces": ([_P, _fp, _fp, C.c_int64, _fp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
     "hignn_forces": ([_P, _fp, _fp, C.c_int64, C.c_void_p], C.c_int),
     "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
+    "hignn_run_rk2": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
     "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
@@ -317,6 +318,14 @@ class Model:
         fm = force_model(gravity=gravity, **model)
         check(lib.hignn_run_euler(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every),
                                   C.addressof(fm)))
+        return x
+
+    def run_rk2(self, x, steps, dt, rebuild_every=1, gravity=(0.0, 0.0, -1.0), **model):
+        """Explicit midpoint rule on the device with the forces of force_model(gravity, **model)."""
+        x = np.array(x, np.float32, copy=True)
+        fm = force_model(gravity=gravity, **model)
+        check(lib.hignn_run_rk2(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every),
+                                C.addressof(fm)))
         return x
 
     def set_shard(self, rank, world):

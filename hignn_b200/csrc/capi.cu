@@ -1159,40 +1159,66 @@ int hignn_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const hi
   });
 }
 
+namespace {
+
+// u (tree order, FP64) = M(x) F(x) at the device positions m->x4.
+void step_velocity(hignn_model* m, const hignn_force_model& fm) {
+  const int64_t n = m->n;
+  apply_forces(m, m->x4.as<float4>(), n, m->slot.as<int32_t>(), fm, m->f4.as<float4>(), nullptr);
+  HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
+  matvec_tree_order(m);
+  if (m->precision >= 1) check_device_error(m);
+}
+
+// The device time loop: method 0 = explicit Euler, 1 = explicit midpoint (RK2).
+void run_steps(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+               const hignn_force_model* fm, int method, const char* name) {
+  if (!m || !xyz || !fm) throw Error(HIGNN_ERR_ARG, "null argument");
+  if (n != m->n) throw Error(HIGNN_ERR_ARG, std::string(name) + ": particle count differs from the model's");
+  if (steps < 0 || !(dt > 0) || rebuild_every < 0)
+    throw Error(HIGNN_ERR_ARG, std::string(name) + ": need steps >= 0, dt > 0, rebuild_every >= 0");
+  check_force_model(*fm, n);
+  require_device(m);
+  require_weights(m);
+  require_student_if_needed(m);
+  if (m->shard_world != 1)
+    throw Error(HIGNN_ERR_STATE, std::string(name) + " needs the whole product (shard world 1): a sharded step "
+                                                     "would need the all-reduce of u between the matvec and the update");
+  for (int64_t i = 0; i < 3 * n; i++)
+    if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+  // start from xyz with a tree built for it
+  m->xyz.assign(xyz, xyz + 3 * n);
+  build_structures(m);
+  if (method == 1) m->tmp_x.ensure(sizeof(float4) * n);
+  for (int s = 0; s < steps; s++) {
+    if (s > 0 && rebuild_every > 0 && s % rebuild_every == 0) {
+      download_positions(m);  // m->xyz <- current positions
+      build_structures(m);
+    }
+    step_velocity(m, *fm);  // forces at the current positions, in tree order, into the matvec
+    if (method == 1) {
+      // midpoint: x_mid = x + (dt / 2) u(x) on the kept tree, then x += dt u(x_mid)
+      HIGNN_CUDA(cudaMemcpyAsync(m->tmp_x.p, m->x4.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, m->stream));
+      hignn::launch_advance(m->x4.as<float4>(), m->u.as<double>(), n, (float)(0.5 * dt), m->stream);
+      step_velocity(m, *fm);
+      HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, m->tmp_x.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, m->stream));
+    }
+    hignn::launch_advance(m->x4.as<float4>(), m->u.as<double>(), n, (float)dt, m->stream);
+  }
+  download_positions(m);
+  std::copy(m->xyz.begin(), m->xyz.end(), xyz);
+}
+
+}  // namespace
+
 int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
                     const hignn_force_model* fm) {
-  return guard([&] {
-    if (!m || !xyz || !fm) throw Error(HIGNN_ERR_ARG, "null argument");
-    if (n != m->n) throw Error(HIGNN_ERR_ARG, "run_euler: particle count differs from the model's");
-    if (steps < 0 || !(dt > 0) || rebuild_every < 0)
-      throw Error(HIGNN_ERR_ARG, "run_euler: need steps >= 0, dt > 0, rebuild_every >= 0");
-    check_force_model(*fm, n);
-    require_device(m);
-    require_weights(m);
-    require_student_if_needed(m);
-    if (m->shard_world != 1)
-      throw Error(HIGNN_ERR_STATE, "run_euler needs the whole product (shard world 1): a sharded step would "
-                                   "need the all-reduce of u between the matvec and the update");
-    for (int64_t i = 0; i < 3 * n; i++)
-      if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
-    // start from xyz with a tree built for it
-    m->xyz.assign(xyz, xyz + 3 * n);
-    build_structures(m);
-    for (int s = 0; s < steps; s++) {
-      if (s > 0 && rebuild_every > 0 && s % rebuild_every == 0) {
-        download_positions(m);  // m->xyz <- current positions
-        build_structures(m);
-      }
-      // forces at the current positions, in tree order, straight into the matvec's input
-      apply_forces(m, m->x4.as<float4>(), n, m->slot.as<int32_t>(), *fm, m->f4.as<float4>(), nullptr);
-      HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
-      matvec_tree_order(m);
-      hignn::launch_advance(m->x4.as<float4>(), m->u.as<double>(), n, (float)dt, m->stream);
-      if (m->precision >= 1) check_device_error(m);
-    }
-    download_positions(m);
-    std::copy(m->xyz.begin(), m->xyz.end(), xyz);
-  });
+  return guard([&] { run_steps(m, xyz, n, steps, dt, rebuild_every, fm, 0, "run_euler"); });
+}
+
+int hignn_run_rk2(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+                  const hignn_force_model* fm) {
+  return guard([&] { run_steps(m, xyz, n, steps, dt, rebuild_every, fm, 1, "run_rk2"); });
 }
 
 int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n) {

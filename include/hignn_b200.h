@@ -152,6 +152,12 @@ int hignn_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const hi
 int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
                     const hignn_force_model* fm);
 
+/* As hignn_run_euler with the explicit midpoint rule (second order; an addition -- the reference
+ * integrates with Euler or Dormand-Prince): x_mid = x + (dt/2) u(x) on the kept tree, then
+ * x += dt u(x_mid), each u = M F with the forces of fm at those positions. */
+int hignn_run_rk2(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
+                  const hignn_force_model* fm);
+
 /* Dot -- src/HignnModel.cpp:545-634: u = M(x) f through the H-matrix (close
  * field + ACA far field). Host pointers; u is written, its input ignored. */
 int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n);

@@ -114,6 +114,33 @@ def test_device_euler_matches_host_loop(precision):
     assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 1e-4)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_device_rk2_matches_host_loop(precision):
+    x0 = S.uniform_min_dist(6000, 0.1, 17)
+    steps, dt, k = 3, 1e-3, 2
+    m = make_model(x0, epsilon=1e-2, precision=precision)
+    xd = m.run_rk2(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE)
+    h = make_model(x0, epsilon=1e-2, precision=precision)
+    x = x0.copy()
+    for s in range(steps):
+        if s > 0 and s % k == 0:
+            h.update_coord(x)
+        elif s > 0:
+            h.update_coord_keep_tree(x)
+        u1 = h.dot(h.forces(x, gravity=G, **MORSE))
+        xm = (x + u1 * np.float32(0.5 * dt)).astype(np.float32)
+        h.update_coord_keep_tree(xm)
+        u2 = h.dot(h.forces(xm, gravity=G, **MORSE))
+        x = (x + u2 * np.float32(dt)).astype(np.float32)
+    disp = np.linalg.norm(x - x0)
+    assert disp > 0
+    assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 1e-4)
+    # a different integrator from Euler on the same forces
+    xe = make_model(x0, epsilon=1e-2, precision=precision).run_euler(x0, steps, dt, rebuild_every=k,
+                                                                      gravity=G, **MORSE)
+    assert np.linalg.norm(xe - xd) > 0
+
+
 def test_keep_tree_is_close_to_rebuild():
     x0 = S.uniform_min_dist(8000, 0.1, 8)
     f = S.sedimenting_forces(8000, 8)
