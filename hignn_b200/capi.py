@@ -98,6 +98,7 @@ SIGNATURES = {
     "hignn_forces": ([_P, _fp, _fp, C.c_int64, C.c_void_p], C.c_int),
     "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
     "hignn_run_rk2": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
+    "hignn_set_three_body": ([_P, _P], C.c_int),
     "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
@@ -327,6 +328,11 @@ class Model:
         check(lib.hignn_run_rk2(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every),
                                 C.addressof(fm)))
         return x
+
+    def set_three_body(self, tb):
+        """Add the three-body and self terms of `tb` (a ThreeBody, or None) to the device time loops."""
+        check(lib.hignn_set_three_body(self._h, tb._h if tb is not None else None))
+        self._tb = tb  # keep it alive while attached
 
     def set_shard(self, rank, world):
         """Compute only shard `rank` of `world` of the block lists; dot then returns partial velocities."""

@@ -112,6 +112,7 @@ struct hignn_model {
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
   hignn::CellList cells;  // neighbour search of the pair forces
+  hignn_tb* tb = nullptr;  // three-body near field added to the velocity of the device time loops
   int32_t* host_ctr = nullptr;
 
   // far-field plan: blocks in batch order; iters > 0 when every block's rank is known
@@ -1161,12 +1162,16 @@ int hignn_forces(hignn_model* m, const float* xyz, float* f, int64_t n, const hi
 
 namespace {
 
-// u (tree order, FP64) = M(x) F(x) at the device positions m->x4.
+void tb_add_device(hignn_tb* t, hignn_model* m);
+
+// u (tree order, FP64) = M(x) F(x) at the device positions m->x4, plus the three-body and self
+// terms when a three-body object is attached.
 void step_velocity(hignn_model* m, const hignn_force_model& fm) {
   const int64_t n = m->n;
   apply_forces(m, m->x4.as<float4>(), n, m->slot.as<int32_t>(), fm, m->f4.as<float4>(), nullptr);
   HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
   matvec_tree_order(m);
+  if (m->tb) tb_add_device(m->tb, m);
   if (m->precision >= 1) check_device_error(m);
 }
 
@@ -1691,6 +1696,51 @@ void tb_set(hignn_tb* t, int which, const std::vector<std::vector<float>>& W, co
 }
 
 }  // namespace
+
+namespace {
+
+// The three-body and self terms at the model's device positions (tree order), added into its
+// FP64 velocities: the edge lists are built from a copy of those positions, so their indices are
+// tree positions, as are the forces f4 and the velocities u.
+void tb_add_device(hignn_tb* t, hignn_model* m) {
+  const int64_t n = m->n;
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));  // positions, forces and the matvec are complete
+  const auto t0 = std::chrono::steady_clock::now();
+  t->lists.update_coord_device(m->x4.as<float4>(), n);
+  t->lists.set_three_body_epsilon(t->eps);
+  t->lists.build_three_body();
+  t->ms_lists = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  int64_t e3 = 0, es = 0;
+  const uint64_t* tri = t->lists.device_list(hignn::kEdgesThreeBody, &e3);
+  const uint64_t* self = t->lists.device_list(hignn::kEdgesThreeBodySelf, &es);
+  t->triplets = e3;
+  t->pairs = es;
+  t->err.ensure(sizeof(int));
+  HIGNN_CUDA(cudaMemsetAsync(t->err.p, 0, sizeof(int), m->stream));
+  hignn::launch_three_body(hignn::kTbThreeBody, t->nets[0].dev(), t->nets[0].cst, tri, e3, t->lists.positions(),
+                           m->f4.as<float4>(), m->u.as<double>(), t->err.as<int>(), nullptr, t->num_sms, m->stream);
+  hignn::launch_three_body(hignn::kTbSelf, t->nets[1].dev(), t->nets[1].cst, self, es, t->lists.positions(),
+                           m->f4.as<float4>(), m->u.as<double>(), t->err.as<int>(), nullptr, t->num_sms, m->stream);
+  int e = 0;
+  HIGNN_CUDA(cudaMemcpyAsync(&e, t->err.p, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  if (e != 0) throw Error(HIGNN_ERR_LIMIT, "three-body kernel: a wait timed out (code " + std::to_string(e) + ")");
+}
+
+}  // namespace
+
+int hignn_set_three_body(hignn_model* m, hignn_tb* t) {
+  return guard([&] {
+    if (!m) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (t) {
+      require_device(m);
+      if (t->lists.device() != m->device) throw Error(HIGNN_ERR_ARG, "three-body object on another device");
+      if (!t->nets[0].loaded || !t->nets[1].loaded)
+        throw Error(HIGNN_ERR_STATE, "three-body: load both the three-body and the self network");
+    }
+    m->tb = t;
+  });
+}
 
 int hignn_tb_create(int device, hignn_tb** out) {
   return guard([&] {

@@ -180,6 +180,16 @@ void NeighbourLists::update_coord(const float* xyz, int64_t n) {
   n_ = n;
 }
 
+void NeighbourLists::update_coord_device(const float4* x4, int64_t n) {
+  if (n < 0 || (n > 0 && !x4)) throw Error(-1, "neighbour lists: bad coordinates");
+  if (n > (int64_t)INT32_MAX - 1) throw Error(-1, "neighbour lists: more than 2^31 - 2 particles");
+  HIGNN_CUDA(cudaSetDevice(device_));
+  x4_.ensure(sizeof(float4) * (n > 0 ? n : 1));
+  if (n > 0) HIGNN_CUDA(cudaMemcpyAsync(x4_.p, x4, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream_));
+  HIGNN_CUDA(cudaStreamSynchronize(stream_));
+  n_ = n;
+}
+
 void NeighbourLists::build_csr(float eps, NeighbourCsr& c) {
   if (!(eps > 0.f)) throw Error(-1, "neighbour lists: the epsilon must be positive");
   const int64_t n = n_;

@@ -36,6 +36,8 @@ class NeighbourLists {
   NeighbourLists& operator=(const NeighbourLists&) = delete;
 
   void update_coord(const float* xyz, int64_t n);
+  // The same from device positions (float4, w unused); the caller's writes to x4 must be complete.
+  void update_coord_device(const float4* x4, int64_t n);
   void set_two_body_epsilon(float e) { eps2_ = e; }
   void set_three_body_epsilon(float e) { eps3_ = e; }
   void build_two_body();

@@ -164,7 +164,7 @@ __device__ __forceinline__ void edge_input(const uint64_t* __restrict__ edges, i
 __device__ __forceinline__ float norm3f(float a, float b, float c) { return sqrtf(a * a + b * b + c * c); }
 
 // ------------------------------------------------------------------ epilogue warps
-template <int KIND>
+template <int KIND, typename OUT>
 struct Epi {
   TbSmem& s;
   const TbConst& c;
@@ -173,7 +173,7 @@ struct Epi {
   int64_t E;
   const float4* x;
   const float4* f;
-  float* u;
+  OUT* u;
   int* err;
   int e, part;     // row of the tile, column part
   uint32_t tlane;  // TMEM address of this warp's lane quarter
@@ -306,7 +306,7 @@ struct Epi {
     const float4 fs = f[src];
 #pragma unroll
     for (int i = 0; i < 3; i++)
-      atomicAdd(&u[3 * dst + i], yy[3 * i] * fs.x + yy[3 * i + 1] * fs.y + yy[3 * i + 2] * fs.z);
+      atomicAdd(&u[3 * dst + i], (OUT)(yy[3 * i] * fs.x + yy[3 * i + 1] * fs.y + yy[3 * i + 2] * fs.z));
   }
 
   // The epilogue follows the MMA lane's order: per tile E2 of chunks 0..15, layer 3 of pass 0
@@ -486,11 +486,11 @@ __device__ void producer(TbSmem& s, const uint8_t* img, int64_t ntiles, int* err
   if (prof) atomicAdd(&prof[5], (unsigned long long)waited);
 }
 
-template <int KIND>
+template <int KIND, typename OUT>
 __global__ void __launch_bounds__(kThreads, 1)
     k_three_body(const __grid_constant__ TbConst cst, TbWeightsDev w, const uint64_t* __restrict__ edges, int64_t E,
                  int64_t ntiles,
-                 const float4* __restrict__ x, const float4* __restrict__ f, float* __restrict__ u, int* err,
+                 const float4* __restrict__ x, const float4* __restrict__ f, OUT* __restrict__ u, int* err,
                  unsigned long long* prof) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = saddr(smem_raw);
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   fence_after();
   if (warp < kMmaWarp) {
-    Epi<KIND> ep{s, cst, w, edges, E, x, f, u, err};
+    Epi<KIND, OUT> ep{s, cst, w, edges, E, x, f, u, err};
     ep.e = 32 * (warp & 3) + lane;
     ep.part = warp >> 2;
     ep.tlane = s.tmem_base + ((uint32_t)(32 * (warp & 3)) << 16);
@@ -540,13 +540,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-template <int KIND>
+template <int KIND, typename OUT>
 void launch_kind(const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t E, int64_t ntiles,
-                 const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
+                 const float4* x, const float4* f, OUT* u, int* err, unsigned long long* prof, int num_sms,
                  cudaStream_t s) {
-  HIGNN_CUDA(cudaFuncSetAttribute(k_three_body<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  HIGNN_CUDA(
+      cudaFuncSetAttribute(k_three_body<KIND, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   const int grid = (int)(ntiles < num_sms ? ntiles : num_sms);
-  k_three_body<KIND><<<grid, kThreads, kSmemBytes, s>>>(c, w, edges, E, ntiles, x, f, u, err, prof);
+  k_three_body<KIND, OUT><<<grid, kThreads, kSmemBytes, s>>>(c, w, edges, E, ntiles, x, f, u, err, prof);
   HIGNN_CHECK_LAUNCH();
 }
 
@@ -557,18 +558,31 @@ uint16_t f16_of(float v) {
   return b;
 }
 
+template <typename OUT>
+int64_t launch_any(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
+                   const float4* x, const float4* f, OUT* u, int* err, unsigned long long* prof, int num_sms,
+                   cudaStream_t s) {
+  const int64_t ntiles = (num_edges + 127) / 128;
+  if (ntiles == 0) return 0;
+  if (kind == kTbThreeBody)
+    launch_kind<kTbThreeBody, OUT>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
+  else
+    launch_kind<kTbSelf, OUT>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
+  return ntiles;
+}
+
 }  // namespace
 
 int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
                           const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
                           cudaStream_t s) {
-  const int64_t ntiles = (num_edges + 127) / 128;
-  if (ntiles == 0) return 0;
-  if (kind == kTbThreeBody)
-    launch_kind<kTbThreeBody>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
-  else
-    launch_kind<kTbSelf>(w, c, edges, num_edges, ntiles, x, f, u, err, prof, num_sms, s);
-  return ntiles;
+  return launch_any<float>(kind, w, c, edges, num_edges, x, f, u, err, prof, num_sms, s);
+}
+
+int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
+                          const float4* x, const float4* f, double* u, int* err, unsigned long long* prof, int num_sms,
+                          cudaStream_t s) {
+  return launch_any<double>(kind, w, c, edges, num_edges, x, f, u, err, prof, num_sms, s);
 }
 
 void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,

@@ -54,6 +54,10 @@ struct TbNet {
 int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
                           const float4* x, const float4* f, float* u, int* err, unsigned long long* prof, int num_sms,
                           cudaStream_t s);
+// The same, accumulating into FP64 velocities (the H-matvec's accumulator).
+int64_t launch_three_body(int kind, const TbWeightsDev& w, const TbConst& c, const uint64_t* edges, int64_t num_edges,
+                          const float4* x, const float4* f, double* u, int* err, unsigned long long* prof, int num_sms,
+                          cudaStream_t s);
 
 // Builds the device image of a network from its dense layers (W row-major out x in, b).
 void tb_upload(TbNet& net, int kin, const std::vector<std::vector<float>>& W, const std::vector<std::vector<float>>& B,

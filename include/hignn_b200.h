@@ -345,6 +345,13 @@ int hignn_tb_velocity_edges(hignn_tb* t, const float* xyz, const float* f, float
 int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
                    int64_t* pairs);
 
+/* Attach a three-body object to a model (t = NULL detaches): hignn_run_euler and hignn_run_rk2
+ * then add its three-body and self velocities (edge lists rebuilt at every evaluation at t's
+ * epsilon, from the current positions) to u = M F -- the whole velocity of the HIGNN model
+ * (python/HIGNN/model_structure.py:76-139 with the two-body part from the H-matrix). hignn_dot
+ * is unchanged. t must outlive the attachment and live on the model's device. */
+int hignn_set_three_body(hignn_model* m, hignn_tb* t);
+
 /* Where the last call's kernels waited, summed over CTAs (12 counters: three-body, then self):
  * clocks the MMA lane waited for layer-1 operands, weight stages, layer-2 epilogues and the
  * layer-3 accumulator; its total clocks; clocks the producer waited for free weight slots. */

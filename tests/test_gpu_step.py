@@ -141,6 +141,49 @@ def test_device_rk2_matches_host_loop(precision):
     assert np.linalg.norm(xe - xd) > 0
 
 
+def filament_suspension():
+    x0 = S.uniform_min_dist(8000, 0.1, 7)
+    # 100 slightly bent filaments along x on a 10 x 10 grid 6 apart, beside the free particles
+    yz = np.stack(np.meshgrid(np.arange(10), np.arange(10)), -1).reshape(100, 1, 2) * 6.0
+    fil = np.concatenate([np.broadcast_to(200.0 + 2.2 * np.arange(32)[None, :, None], (100, 32, 1)),
+                          np.broadcast_to(yz, (100, 32, 2))], axis=2).reshape(3200, 3)
+    x0[:3200] = fil + np.random.default_rng(3).normal(0, 0.05, fil.shape)
+    return x0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_device_rk2_with_three_body(precision):
+    # the whole HIGNN velocity in the device loop: H-matrix two-body term + three-body + self terms
+    x0 = filament_suspension()
+    steps, dt, k = 2, 1e-3, 2
+    tb = capi.ThreeBody(0, epsilon=5.0)
+    m = make_model(x0, epsilon=1e-2, precision=precision)
+    m.set_three_body(tb)
+    xd = m.run_rk2(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE, **FIL)
+    h = make_model(x0, epsilon=1e-2, precision=precision)
+    tbh = capi.ThreeBody(0, epsilon=5.0)
+
+    def vel(x):
+        f = h.forces(x, gravity=G, **MORSE, **FIL)
+        return h.dot(f) + tbh.velocity(x, f)
+
+    x = x0.copy()
+    for s in range(steps):
+        if s > 0 and s % k == 0:
+            h.update_coord(x)
+        elif s > 0:
+            h.update_coord_keep_tree(x)
+        xm = (x + vel(x) * np.float32(0.5 * dt)).astype(np.float32)
+        h.update_coord_keep_tree(xm)
+        x = (x + vel(xm) * np.float32(dt)).astype(np.float32)
+    disp = np.linalg.norm(x - x0)
+    assert tbh.stats()["triplets"] > 0
+    assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 1e-4)
+    m.set_three_body(None)  # detached: the two-body loop alone moves the particles differently
+    xn = m.run_rk2(x0, steps, dt, rebuild_every=k, gravity=G, **MORSE, **FIL)
+    assert np.linalg.norm(xn - xd) / disp > 1e-4
+
+
 def test_keep_tree_is_close_to_rebuild():
     x0 = S.uniform_min_dist(8000, 0.1, 8)
     f = S.sedimenting_forces(8000, 8)
