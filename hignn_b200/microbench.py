@@ -35,6 +35,7 @@ def main():
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
     ap.add_argument("--timing", type=int, default=2, help="2 = far-field breakdown by kernel category")
+    ap.add_argument("--pool-mb", type=int, default=0, help="ACA pool memory per batch (0: the default)")
     ap.add_argument("--student-steps", type=int, default=4000, help="training steps when --precision 2")
     ap.add_argument("--student-batch", type=int, default=16384)
     ap.add_argument("--student-samples", type=int, default=2_000_000)
@@ -84,6 +85,8 @@ def main():
         m.set(capi.P_FIELDS, a.fields)
         m.set(capi.P_EPSILON, a.epsilon)
         m.set(capi.P_TIMING, a.timing)
+        if a.pool_mb:
+            m.set(capi.P_FAR_POOL_MB, a.pool_mb)
         if a.precision == 2:
             import time
 
