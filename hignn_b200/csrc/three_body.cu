@@ -187,13 +187,23 @@ struct Epi {
   }
 
   // features and layer 1 of tile t into the tensor-memory A operand of layer 2 (this thread:
-  // outputs 64 part .. + 63 of row e, as FP16 pairs in columns 32 part .. + 31)
+  // outputs 64 part .. + 63 of row e, as FP16 pairs in columns 32 part .. + 31). The part is a
+  // template argument, so every weight is read at a constant offset of the kernel parameter.
   __device__ void layer1(int64_t t) {
+    switch (part) {
+      case 0: layer1_part<0>(t); break;
+      case 1: layer1_part<1>(t); break;
+      case 2: layer1_part<2>(t); break;
+      default: layer1_part<3>(t); break;
+    }
+  }
+  template <int PART>
+  __device__ void layer1_part(int64_t t) {
     const int64_t q = t * 128 + e;
     float in[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int64_t src, dst;
     if (q < E) edge_input<KIND>(edges, E, q, x, in, src, dst);
-#pragma unroll 1
+#pragma unroll
     for (int half = 0; half < 2; half++) {
       uint32_t pk[16];
 #pragma unroll
@@ -201,7 +211,7 @@ struct Epi {
         float acc[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const int n = 64 * part + 32 * half + 2 * pr + h;
+          const int n = 64 * PART + 32 * half + 2 * pr + h;
           const float* wr = c.w1 + 7 * n;
           float a = wr[6];  // b1
 #pragma unroll
@@ -210,7 +220,7 @@ struct Epi {
         }
         pk[pr] = tanh_f16x2(pack_f16(acc[0], acc[1]));
       }
-      tc::tmem_st16(tlane + kOffA1 + 32 * part + 16 * half, pk);
+      tc::tmem_st16(tlane + kOffA1 + 32 * PART + 16 * half, pk);
     }
     tc::tmem_wait_st();
     fence_before();
