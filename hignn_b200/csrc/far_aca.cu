@@ -93,6 +93,45 @@ __device__ void block_sum(double (&v)[N], double* scratch /* [32][N] */) {
   __syncthreads();
 }
 
+// block_argmax and block_sum<12> in one pass: the same per-warp and per-CTA orders, two barriers
+// instead of six (sv / si / scratch are not written again before the caller's next barrier).
+__device__ void block_argmax_sum(double& best, int& bi, double (&v)[12], double* sv, int* si,
+                                 double* scratch /* [32][12] */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, best, o);
+    int i2 = __shfl_down_sync(0xffffffffu, bi, o);
+    better(best, bi, v2, i2);
+  }
+#pragma unroll
+  for (int q = 0; q < 12; q++)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  if (lane == 0) {
+    sv[wid] = best;
+    si[wid] = bi;
+#pragma unroll
+    for (int q = 0; q < 12; q++) scratch[wid * 12 + q] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bv = sv[0];
+    int bj = si[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) better(bv, bj, sv[w], si[w]);
+    sv[0] = bv;
+    si[0] = bj;
+    for (int q = 0; q < 12; q++) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w * 12 + q];
+      scratch[q] = s;
+    }
+  }
+  __syncthreads();
+  best = sv[0];
+  bi = si[0];
+#pragma unroll
+  for (int q = 0; q < 12; q++) v[q] = scratch[q];
+}
+
 __global__ void k_far_init(FarArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b == 0) {
@@ -430,6 +469,9 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
   double best = -DBL_MAX;
   int bj = -1;
   pool_t* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
+  // nu2 = ||C_k Q_k||_F^2 from column norms/dots of C_k (v[0..5]) and row norms/dots of Q_k
+  // (v[6..11], accumulated as each row of Q_k is finished)
+  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
     double q[9];
 #pragma unroll
@@ -452,16 +494,19 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
         Qk[9 * j + e] = (pool_t)q[e];
       }
     }
+    v[6] += q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    v[7] += q[3] * q[3] + q[4] * q[4] + q[5] * q[5];
+    v[8] += q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
+    v[9] += q[0] * q[3] + q[1] * q[4] + q[2] * q[5];
+    v[10] += q[3] * q[6] + q[4] * q[7] + q[5] * q[8];
+    v[11] += q[6] * q[0] + q[7] * q[1] + q[8] * q[2];
     const double d = det3(q);
     if (!a.usedCol[bk.colOff + j] && (bj < 0 || d > best)) {
       best = d;
       bj = j;
     }
   }
-  block_argmax(best, bj, sv, si);  // contains __syncthreads: Q_k writes are visible below
-  // nu2 = ||C_k Q_k||_F^2 from column norms/dots of C_k and row norms/dots of Q_k
   const pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
-  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
     double c[9];
 #pragma unroll
@@ -473,18 +518,9 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
       v[3 + cc] += c[cc] * c[c1] + c[cc + 3] * c[c1 + 3] + c[cc + 6] * c[c1 + 6];
     }
   }
-  for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
-    double q[9];
-#pragma unroll
-    for (int e = 0; e < 9; e++) q[e] = Qk[9 * j + e];
-    v[6] += q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-    v[7] += q[3] * q[3] + q[4] * q[4] + q[5] * q[5];
-    v[8] += q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
-    v[9] += q[0] * q[3] + q[1] * q[4] + q[2] * q[5];
-    v[10] += q[3] * q[6] + q[4] * q[7] + q[5] * q[8];
-    v[11] += q[6] * q[0] + q[7] * q[1] + q[8] * q[2];
-  }
-  block_sum<12>(v, red);
+  // one reduction for the column pivot and the twelve sums (its barriers also make the Q_k
+  // writes visible to the cross terms below)
+  block_argmax_sum(best, bj, v, sv, si, red);
   const double nu2 = v[0] * v[6] + v[1] * v[7] + v[2] * v[8] + 2.0 * v[9] * v[3] + 2.0 * v[10] * v[4] +
                      2.0 * v[11] * v[5];
   double mu2 = a.state[b].mu2 + nu2;  // every thread tracks the same value; thread 0 stores it
