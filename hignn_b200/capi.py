@@ -99,6 +99,8 @@ SIGNATURES = {
     "hignn_run_euler": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
     "hignn_run_rk2": ([_P, _fp, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_void_p], C.c_int),
     "hignn_set_three_body": ([_P, _P], C.c_int),
+    "hignn_run_dp45": ([_P, _fp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p, _i64p],
+                       C.c_int),
     "hignn_get_shard": ([_P, _i64p], C.c_int),
     "hignn_get_far_pivots": ([_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int], C.c_int),
     "hignn_synchronize": ([_P], C.c_int),
@@ -328,6 +330,15 @@ class Model:
         check(lib.hignn_run_rk2(self._h, fptr(x), len(x), int(steps), float(dt), int(rebuild_every),
                                 C.addressof(fm)))
         return x
+
+    def run_dp45(self, x, tf, dt0, threshold=1e-3, rebuild_every=0, gravity=(0.0, 0.0, -1.0), **model):
+        """Adaptive Dormand-Prince on the device (the reference's ExplicitRk4); returns (positions, steps)."""
+        x = np.array(x, np.float32, copy=True)
+        fm = force_model(gravity=gravity, **model)
+        steps = C.c_int64()
+        check(lib.hignn_run_dp45(self._h, fptr(x), len(x), float(tf), float(dt0), float(threshold),
+                                 int(rebuild_every), C.addressof(fm), C.byref(steps)))
+        return x, steps.value
 
     def set_three_body(self, tb):
         """Add the three-body and self terms of `tb` (a ThreeBody, or None) to the device time loops."""

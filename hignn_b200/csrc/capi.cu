@@ -110,7 +110,7 @@ struct hignn_model {
   DevBuf x4, perm, slot, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
-  DevBuf tmp_work, tmp_x, tmp_u, tmp_pos;
+  DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err;
   hignn::CellList cells;  // neighbour search of the pair forces
   hignn_tb* tb = nullptr;  // three-body near field added to the velocity of the device time loops
   int32_t* host_ctr = nullptr;
@@ -909,7 +909,8 @@ int hignn_destroy(hignn_model* m) {
                       &m->weights_tc, &m->counter, &m->student,
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
-                      &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos})
+                      &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos,
+                      &m->dp_k, &m->dp_err})
       b->release();
     m->cells.release();
     for (auto& e : m->ev)
@@ -1224,6 +1225,93 @@ int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt,
 int hignn_run_rk2(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
                   const hignn_force_model* fm) {
   return guard([&] { run_steps(m, xyz, n, steps, dt, rebuild_every, fm, 1, "run_rk2"); });
+}
+
+// ExplicitRk4::Run (include/TimeIntegrator.hpp:602-860) with the velocity on the device: adaptive
+// Dormand-Prince 5(4), FSAL, the reference's float stage arithmetic and step control (k1 zero on
+// the first step; a grown step size is discarded because the next step starts from
+// min(h0, tf - t)). The initial velocity evaluation the reference makes for its output callback
+// is skipped (there is no callback).
+int hignn_run_dp45(hignn_model* m, float* xyz, int64_t n, double tf, double dt0, double threshold,
+                   int rebuild_every, const hignn_force_model* fm, int64_t* steps_taken) {
+  return guard([&] {
+    if (!m || !xyz || !fm) throw Error(HIGNN_ERR_ARG, "null argument");
+    if (n != m->n) throw Error(HIGNN_ERR_ARG, "run_dp45: particle count differs from the model's");
+    if (!(tf >= 0) || !(dt0 > 0) || !(threshold > 0) || rebuild_every < 0)
+      throw Error(HIGNN_ERR_ARG, "run_dp45: need tf >= 0, dt0 > 0, threshold > 0, rebuild_every >= 0");
+    check_force_model(*fm, n);
+    require_device(m);
+    require_weights(m);
+    require_student_if_needed(m);
+    if (m->shard_world != 1) throw Error(HIGNN_ERR_STATE, "run_dp45 needs the whole product (shard world 1)");
+    for (int64_t i = 0; i < 3 * n; i++)
+      if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
+    // Dormand-Prince tableau (include/TimeIntegrator.hpp:503-549), float constants
+    const float A[7][6] = {{0, 0, 0, 0, 0, 0},
+                           {1.f / 5.f, 0, 0, 0, 0, 0},
+                           {3.f / 40.f, 9.f / 40.f, 0, 0, 0, 0},
+                           {44.f / 45.f, -56.f / 15.f, 32.f / 9.f, 0, 0, 0},
+                           {19372.f / 6561.f, -25360.f / 2187.f, 64448.f / 6561.f, -212.f / 729.f, 0, 0},
+                           {9017.f / 3168.f, -355.f / 33.f, 46732.f / 5247.f, 49.f / 176.f, -5103.f / 18656.f, 0},
+                           {35.f / 384.f, 0.f, 500.f / 1113.f, 125.f / 192.f, -2187.f / 6784.f, 11.f / 84.f}};
+    const float b1 = 35.f / 384.f, b3 = 500.f / 1113.f, b4 = 125.f / 192.f, b5 = -2187.f / 6784.f, b6 = 11.f / 84.f;
+    const float dc[6] = {b1 - 5179.f / 57600.f, b3 - 7571.f / 16695.f, b4 - 393.f / 640.f,
+                         b5 - (-92097.f) / 339200.f, b6 - 187.f / 2100.f, -1.f / 40.f};
+    m->xyz.assign(xyz, xyz + 3 * n);
+    build_structures(m);
+    const size_t m3 = 3 * (size_t)n;
+    m->dp_k.ensure(sizeof(float) * 7 * m3);
+    m->dp_err.ensure(sizeof(double));
+    m->tmp_x.ensure(sizeof(float4) * n);
+    HIGNN_CUDA(cudaMemsetAsync(m->dp_k.p, 0, sizeof(float) * 7 * m3, m->stream));  // k1 = 0 on the first step
+    float* k = m->dp_k.as<float>();
+    double t = 0.0;
+    int64_t count = 0;
+    const double h0 = dt0;
+    while (t < tf - 1e-5) {
+      double dt = std::min(h0, tf - t);
+      if (count > 0 && rebuild_every > 0 && count % rebuild_every == 0) {
+        download_positions(m);
+        build_structures(m);
+      }
+      HIGNN_CUDA(cudaMemcpyAsync(m->tmp_x.p, m->x4.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, m->stream));
+      double err = 100.0;
+      while (err > threshold) {
+        for (int i = 1; i < 7; i++) {
+          hignn::Dp45Terms tm{};
+          for (int jj = 0; jj < 6; jj++) {
+            const float coef = A[i][jj];
+            if (i < 6 ? jj < i : coef != 0.f) {  // stage i uses k_1 .. k_i; the solution row skips k_2
+              tm.j[tm.n] = jj + 1;
+              tm.c[tm.n] = (float)(coef * dt);
+              tm.n++;
+            }
+          }
+          hignn::launch_dp45_stage(m->tmp_x.as<float4>(), k, n, tm, m->x4.as<float4>(), m->stream);
+          step_velocity(m, *fm);
+          hignn::launch_velocity_to_float(m->u.as<double>(), (int64_t)m3, k + (size_t)i * m3, m->stream);
+        }
+        const hignn::Dp45Error de{{dc[0], dc[1], dc[2], dc[3], dc[4], dc[5]}, (float)dt};
+        hignn::launch_dp45_error(k, n, de, m->dp_err.as<double>(), m->stream);
+        double e2 = 0.0;
+        HIGNN_CUDA(cudaMemcpyAsync(&e2, m->dp_err.p, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+        HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+        err = std::sqrt(e2);
+        if (!std::isfinite(err)) throw Error(HIGNN_ERR_LIMIT, "run_dp45: non-finite error estimate");
+        if (err > threshold) {
+          dt = dt * std::max(0.8 * std::pow(err / threshold, -0.2), 0.1);
+          dt = std::max(dt, 1e-6);
+        }
+      }
+      t += dt;
+      // first-same-as-last: k1 <- k7
+      HIGNN_CUDA(cudaMemcpyAsync(k, k + 6 * m3, sizeof(float) * m3, cudaMemcpyDeviceToDevice, m->stream));
+      count++;
+    }
+    download_positions(m);
+    std::copy(m->xyz.begin(), m->xyz.end(), xyz);
+    if (steps_taken) *steps_taken = count;
+  });
 }
 
 int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n) {

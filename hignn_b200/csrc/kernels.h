@@ -182,6 +182,21 @@ void launch_morse(const float4* x, int64_t n, const CellList& cl, const MorsePar
 void launch_neighbours(const float4* x, int64_t n, const CellList& cl, double cutoff, int64_t* count,
                        const int64_t* off, int* out, cudaStream_t s);
 void launch_advance(float4* x, const double* u, int64_t n, float dt, cudaStream_t s);
+
+// Dormand-Prince stage positions x = x0 + sum_t k[j_t] c_t (k: 7 stage velocities, float (n, 3)
+// each, k_j at offset (j - 1) 3n) and the error estimate (summed into *err, zeroed first).
+struct Dp45Terms {
+  int n;
+  int j[5];
+  float c[5];
+};
+struct Dp45Error {
+  float dc[6];  // k1, k3, k4, k5, k6, k7
+  float dt;
+};
+void launch_dp45_stage(const float4* x0, const float* k, int64_t n, const Dp45Terms& tm, float4* x, cudaStream_t s);
+void launch_velocity_to_float(const double* u, int64_t m, float* k, cudaStream_t s);
+void launch_dp45_error(const float* k, int64_t n, const Dp45Error& de, double* err, cudaStream_t s);
 // f += bending, then f += tension, for the filament rows (row -> slot of x and f: slot[row], or
 // the row itself when slot is null); f4 or f3 (n, 3) as in launch_morse.
 void launch_filaments(const float4* x, const int32_t* slot, const FilamentParams& fp, float4* f4, float* f3,

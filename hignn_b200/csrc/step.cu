@@ -379,6 +379,52 @@ __global__ void k_advance(float4* __restrict__ x, const double* __restrict__ u, 
   x[i] = p;
 }
 
+// ---- Dormand-Prince stages (ExplicitRk4::Run, include/TimeIntegrator.hpp:602-860): float
+// arithmetic in the reference's order, each product and sum rounded on its own.
+// x = x0 + k_j1 c_1 + k_j2 c_2 + ... (left to right), k_j the stage velocities (float, (n, 3)).
+__global__ void k_dp45_stage(const float4* __restrict__ x0, const float* __restrict__ k, int64_t n, Dp45Terms tm,
+                             float4* __restrict__ x) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = x0[i];
+  for (int t = 0; t < tm.n; t++) {
+    const float* kj = k + (size_t)(tm.j[t] - 1) * 3 * n + 3 * i;
+    p.x = __fadd_rn(p.x, __fmul_rn(kj[0], tm.c[t]));
+    p.y = __fadd_rn(p.y, __fmul_rn(kj[1], tm.c[t]));
+    p.z = __fadd_rn(p.z, __fmul_rn(kj[2], tm.c[t]));
+  }
+  x[i] = p;
+}
+
+__global__ void k_velocity_to_float(const double* __restrict__ u, int64_t m, float* __restrict__ k) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < m) k[q] = (float)u[q];
+}
+
+// Error estimate: ve = (k1 dc1 + k3 dc3 + k4 dc4 + k5 dc5 + k6 dc6 + k7 dc7) dt in float, |ve|^2 in
+// float (Vec3::SquareMag), summed in double.
+__global__ void k_dp45_error(const float* __restrict__ k, int64_t n, Dp45Error de, double* __restrict__ err) {
+  double acc = 0.0;
+  const size_t m = 3 * (size_t)n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float ve[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const size_t q = 3 * i + d;
+      float v = __fmul_rn(k[q], de.dc[0]);
+      v = __fadd_rn(v, __fmul_rn(k[2 * m + q], de.dc[1]));
+      v = __fadd_rn(v, __fmul_rn(k[3 * m + q], de.dc[2]));
+      v = __fadd_rn(v, __fmul_rn(k[4 * m + q], de.dc[3]));
+      v = __fadd_rn(v, __fmul_rn(k[5 * m + q], de.dc[4]));
+      v = __fadd_rn(v, __fmul_rn(k[6 * m + q], de.dc[5]));
+      ve[d] = __fmul_rn(v, de.dt);
+    }
+    acc += (double)__fadd_rn(__fadd_rn(__fmul_rn(ve[0], ve[0]), __fmul_rn(ve[1], ve[1])), __fmul_rn(ve[2], ve[2]));
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(err, acc);
+}
+
 __global__ void k_pack_positions(const float* __restrict__ xyz, int64_t n, float4* __restrict__ x4) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x4[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.f);
@@ -485,6 +531,26 @@ void launch_filaments(const float4* x, const int32_t* slot, const FilamentParams
   const int64_t rows = fp.n_filament * (int64_t)fp.n_chain;
   if (rows <= 0) return;
   k_filaments<<<nblk(rows, 128), 128, 0, s>>>(x, slot, fp, f4, f3);
+  HIGNN_CHECK_LAUNCH();
+}
+
+void launch_dp45_stage(const float4* x0, const float* k, int64_t n, const Dp45Terms& tm, float4* x, cudaStream_t s) {
+  if (n <= 0) return;
+  k_dp45_stage<<<nblk(n, 256), 256, 0, s>>>(x0, k, n, tm, x);
+  HIGNN_CHECK_LAUNCH();
+}
+
+void launch_velocity_to_float(const double* u, int64_t m, float* k, cudaStream_t s) {
+  if (m <= 0) return;
+  k_velocity_to_float<<<nblk(m, 256), 256, 0, s>>>(u, m, k);
+  HIGNN_CHECK_LAUNCH();
+}
+
+void launch_dp45_error(const float* k, int64_t n, const Dp45Error& de, double* err, cudaStream_t s) {
+  HIGNN_CUDA(cudaMemsetAsync(err, 0, sizeof(double), s));
+  if (n <= 0) return;
+  const unsigned g = nblk(n, 256) < 1184 ? nblk(n, 256) : 1184;
+  k_dp45_error<<<g, 256, 0, s>>>(k, n, de, err);
   HIGNN_CHECK_LAUNCH();
 }
 

@@ -158,6 +158,14 @@ int hignn_run_euler(hignn_model* m, float* xyz, int64_t n, int steps, double dt,
 int hignn_run_rk2(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int rebuild_every,
                   const hignn_force_model* fm);
 
+/* ExplicitRk4::Run (include/TimeIntegrator.hpp:602-860) with the velocity of fm (and of an
+ * attached three-body object) on the device: adaptive Dormand-Prince 5(4) from t = 0 to tf with
+ * the reference's float stage arithmetic, error norm and step control (initial step dt0, error
+ * threshold), tree rebuilt every `rebuild_every` accepted steps (0: never). *steps_taken (may be
+ * NULL) receives the number of accepted steps. */
+int hignn_run_dp45(hignn_model* m, float* xyz, int64_t n, double tf, double dt0, double threshold,
+                   int rebuild_every, const hignn_force_model* fm, int64_t* steps_taken);
+
 /* Dot -- src/HignnModel.cpp:545-634: u = M(x) f through the H-matrix (close
  * field + ACA far field). Host pointers; u is written, its input ignored. */
 int hignn_dot(hignn_model* m, float* u, const float* f, int64_t n);

@@ -184,6 +184,33 @@ def test_device_rk2_with_three_body(precision):
     assert np.linalg.norm(xn - xd) / disp > 1e-4
 
 
+@pytest.mark.parametrize("precision,morse", [(0, False), (0, True), (1, False)])
+def test_device_dp45_matches_reference_integrator(precision, morse):
+    # ExplicitRk4 (include/TimeIntegrator.hpp:602-860) as the oracle restates it, driven from the host
+    # through the C ABI on the same kept tree, against the device loop
+    x0 = S.uniform_min_dist(5000, 0.1, 23)
+    forces = dict(gravity=G, **(MORSE if morse else {}))
+    tf, dt0, thr = 4e-3, 1.5e-3, 2e-4
+    m = make_model(x0, epsilon=1e-2, precision=precision)
+    xd, steps = m.run_dp45(x0, tf, dt0, threshold=thr, **forces)
+    h = make_model(x0, epsilon=1e-2, precision=precision)
+
+    def velocity(t, inp):
+        p = np.ascontiguousarray(inp[:, :3])
+        h.update_coord_keep_tree(p)
+        return h.dot(h.forces(p, **forces))
+
+    x, count = O.dp45_run(x0, velocity, dt0, tf, threshold=thr)
+    assert steps == count >= 3
+    disp = np.linalg.norm(x - x0)
+    assert disp > 0
+    # FP32 network: last-bit differences only (FP64 atomic order of the matvec, order of the Morse
+    # sums). BF16 network: a last-bit difference of a stage position can flip the BF16 rounding of
+    # its network inputs, and six stages per accepted step compound it (1.4e-4 measured), so the
+    # bound is 3e-4; the step counts must still agree exactly.
+    assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 3e-4)
+
+
 def test_keep_tree_is_close_to_rebuild():
     x0 = S.uniform_min_dist(8000, 0.1, 8)
     f = S.sedimenting_forces(8000, 8)
