@@ -39,6 +39,10 @@ WEIGHTS = os.path.join(REPO, "hignn_b200", "data", "two_body_unbounded.hgnw")
 METRIC = "H-matvec particles/s at N=1M: mixed+batched+student vs plain FP32, err≤1e-3"
 FLOP_PER_EVAL = 2 * (3 * 128 + 128 * 512 + 512 * 9)  # 141,056
 TANH_PER_EVAL = 128 + 512
+# DRAM bytes of one k_near_tc launch in the committed full ncu capture (N = 131,072: 8.9 MB read,
+# nothing written; positions, forces and the pair list are read once, the FP64 accumulators stay
+# in L2). The reads are per particle, so the figure scales with N.
+NEAR_DRAM_BYTES_PER_PARTICLE = 8.9e6 / 131072
 PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor_cores", 2: "bf16_tensor_cores+student_far_field"}
 PREC_DTYPE = {0: "fp32", 1: "bf16", 2: "bf16"}
 WORKLOAD = ("N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, seed 2, "
@@ -437,7 +441,9 @@ def main():
         "roofline": {"bound": "tensor", "kernel": "k_near_tc (features + two-body network + contraction)",
                      "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
                      "peak_source": f"bf16_tflops of {src} MEASURED_PEAKS.json",
-                     "traffic": None,
+                     "traffic": NEAR_DRAM_BYTES_PER_PARTICLE * n,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of k_near_tc in the ncu "
+                                       "capture at N = 131,072 (profiles/k_near_tc_medium_n131k.md), scaled by N",
                      "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals / near-field time",
                      "mufu": {"achieved_evals_per_s": near_eps, "peak_evals_per_s": mufu_peak,
                               "frac": near_eps / mufu_peak,
