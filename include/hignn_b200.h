@@ -318,8 +318,8 @@ int hignn_nbl_get_stream(hignn_nbl* l, void** stream);
  *     u_c += (net3(x_b - x_a, x_c - x_b) / |x_b - x_a| / |x_c - x_b|) f_a
  * and for every self edge (a, b),  u_b += (net_self(x_a - x_b) / |x_a - x_b|^2) f_b
  * (the two-body term is the H-matrix product, hignn_dot). Networks kin -> 256 -> 1024 -> 512
- * -> 9 with tanh (kin 6 and 3); layers 2 and 3 on the tensor cores (BF16 operands, FP32
- * accumulation), layers 1 and 4 in FP32. */
+ * -> 9 with tanh (kin 6 and 3); layer 1 in FP32 on the CUDA cores, layers 2, 3 and 4 on the
+ * tensor cores (FP16 operands, FP32 accumulation). */
 typedef struct hignn_tb hignn_tb;
 
 #define HIGNN_TB_THREE_BODY 0
@@ -353,8 +353,8 @@ int hignn_tb_velocity_edges(hignn_tb* t, const float* xyz, const float* f, float
 int hignn_tb_stats(hignn_tb* t, double* ms_lists, double* ms_three, double* ms_self, int64_t* triplets,
                    int64_t* pairs);
 
-/* Attach a three-body object to a model (t = NULL detaches): hignn_run_euler and hignn_run_rk2
- * then add its three-body and self velocities (edge lists rebuilt at every evaluation at t's
+/* Attach a three-body object to a model (t = NULL detaches): hignn_run_euler, hignn_run_rk2 and
+ * hignn_run_dp45 then add its three-body and self velocities (edge lists rebuilt at every evaluation at t's
  * epsilon, from the current positions) to u = M F -- the whole velocity of the HIGNN model
  * (python/HIGNN/model_structure.py:76-139 with the two-body part from the H-matrix). hignn_dot
  * is unchanged. t must outlive the attachment and live on the model's device. */
