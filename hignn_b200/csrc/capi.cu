@@ -1026,11 +1026,14 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         m->precision = (int)v;
         break;
       case HIGNN_P_FAR_BATCH_ROWS:
-        if (v < 1024) throw Error(HIGNN_ERR_ARG, "far_batch_rows must be >= 1024");
+        // a batch's row offsets and prefix sums are 32-bit on the device
+        if (!(v >= 1024 && v <= (double)(int64_t(1) << 30)))
+          throw Error(HIGNN_ERR_ARG, "far_batch_rows must be in [1024, 2^30]");
         m->far_batch_rows = (int64_t)v;
         break;
       case HIGNN_P_FAR_POOL_MB:
-        if (v < 1) throw Error(HIGNN_ERR_ARG, "far_pool_mb must be >= 1");
+        if (!(v >= 1 && v <= (double)(int64_t(1) << 24)))
+          throw Error(HIGNN_ERR_ARG, "far_pool_mb must be in [1, 2^24]");
         m->far_pool_bytes = (int64_t)(v * 1048576.0);
         break;
       case HIGNN_P_RANK_HINT_OFFSET: m->rank_hint_offset = (int)v; break;

@@ -46,7 +46,7 @@ enum hignn_param {
   /* keys of this implementation */
   HIGNN_P_PRECISION = 100,       /* 0 = plain FP32 (default), 1 = BF16 tensor cores, 2 = BF16 + student far field;
                                     1 and 2 need block_size <= 128                               */
-  HIGNN_P_FAR_BATCH_ROWS = 101,  /* max rows (sum of |I|+|J|) per ACA batch, default 1<<26   */
+  HIGNN_P_FAR_BATCH_ROWS = 101,  /* max rows (sum of |I|+|J|) per ACA batch, default 1<<26, at most 1<<30 */
   HIGNN_P_TIMING = 102,          /* 1 = per-phase CUDA-event times in hignn_stats, 2 = also the
                                     far-field breakdown (events around every far launch)        */
   HIGNN_P_STUDENT_TOL = 103,     /* student fallback: a far block whose 64 sampled entries differ from
@@ -54,7 +54,7 @@ enum hignn_param {
                                     is recomputed with the teacher; default 1e-3                   */
   HIGNN_P_FIELDS = 104,          /* bit 0 = near field, bit 1 = far field (default 3), for diagnostics */
   HIGNN_P_RECORD_PIVOTS = 105,   /* 1 = keep every far block's ACA rank and pivots (hignn_get_far_pivots) */
-  HIGNN_P_FAR_POOL_MB = 106,     /* C + Q pool memory of one ACA batch in MiB, default 24576   */
+  HIGNN_P_FAR_POOL_MB = 106,     /* C + Q pool memory of one ACA batch in MiB, default 24576, at most 1<<24 */
   HIGNN_P_RANK_HINT_OFFSET = 107 /* added to the recorded ACA ranks when planning (default 0; a
                                     negative value exercises the deferral path in tests)        */
 };

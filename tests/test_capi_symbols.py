@@ -43,6 +43,14 @@ def test_version_and_errors_without_device():
         raise AssertionError("max_iter above the cap must be rejected")
     except capi.HignnError as e:
         assert e.code == -1
+    for key, bad in ((capi.P_FAR_BATCH_ROWS, 2.0 ** 31), (capi.P_FAR_BATCH_ROWS, float("nan")),
+                     (capi.P_FAR_BATCH_ROWS, 100), (capi.P_FAR_POOL_MB, 1e30), (capi.P_FAR_POOL_MB, 0)):
+        try:
+            m.set(key, bad)
+            raise AssertionError(f"key {key} = {bad} must be rejected")
+        except capi.HignnError as e:
+            assert e.code == -1
+    m.set(capi.P_FAR_BATCH_ROWS, 2.0 ** 30)
     try:
         m.set(12345, 1.0)
         raise AssertionError("unknown key must be rejected")
