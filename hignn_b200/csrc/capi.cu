@@ -1274,8 +1274,22 @@ int hignn_run_dp45(hignn_model* m, float* xyz, int64_t n, double tf, double dt0,
     while (t < tf - 1e-5) {
       double dt = std::min(h0, tf - t);
       if (count > 0 && rebuild_every > 0 && count % rebuild_every == 0) {
-        download_positions(m);
+        // k1 (the last step's k7) is stored in tree order: carry it over to the new tree's order
+        // through the caller's order, as the positions are
+        std::vector<float> kt(m3), kc(m3);
+        HIGNN_CUDA(cudaMemcpyAsync(kt.data(), k, sizeof(float) * m3, cudaMemcpyDeviceToHost, m->stream));
+        download_positions(m);  // synchronises the stream, so kt is complete
+        for (int64_t i = 0; i < n; i++) {
+          const int64_t p = m->tree.perm[i];
+          for (int c = 0; c < 3; c++) kc[3 * p + c] = kt[3 * i + c];
+        }
         build_structures(m);
+        for (int64_t i = 0; i < n; i++) {
+          const int64_t p = m->tree.perm[i];
+          for (int c = 0; c < 3; c++) kt[3 * i + c] = kc[3 * p + c];
+        }
+        HIGNN_CUDA(cudaMemcpyAsync(k, kt.data(), sizeof(float) * m3, cudaMemcpyHostToDevice, m->stream));
+        HIGNN_CUDA(cudaStreamSynchronize(m->stream));  // kt is released at the end of this block
       }
       HIGNN_CUDA(cudaMemcpyAsync(m->tmp_x.p, m->x4.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, m->stream));
       double err = 100.0;

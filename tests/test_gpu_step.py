@@ -211,6 +211,25 @@ def test_device_dp45_matches_reference_integrator(precision, morse):
     assert np.linalg.norm(xd - x) / disp < (1e-5 if precision == 0 else 3e-4)
 
 
+def test_device_dp45_with_tree_rebuilds():
+    """A rebuild between Dormand-Prince steps must carry the stage vector k1 (the previous step's
+    k7, first-same-as-last), which lives in tree order, over to the new tree's order. On this
+    workload one step of motion reorders 94 % of the tree (the root's PCA axis turns), and a k1
+    left in the old order errs by ~3e-3 of the displacement per rebuild (both figures from the
+    oracle's velocity field on the CPU; the velocity is mostly the collective sedimentation, so
+    particles' velocities differ little). Rebuilt every step, the run must agree with the
+    kept-tree run up to the two H-matrix approximations, which at eps 1e-5 are each within
+    ~2e-4 of the dense product."""
+    x0 = S.uniform_min_dist(5000, 0.1, 23)
+    forces = dict(gravity=G, **MORSE)
+    tf, dt0, thr = 4e-3, 1.5e-3, 2e-4
+    xa, na = make_model(x0, epsilon=1e-5).run_dp45(x0, tf, dt0, threshold=thr, rebuild_every=1, **forces)
+    xb, nb = make_model(x0, epsilon=1e-5).run_dp45(x0, tf, dt0, threshold=thr, rebuild_every=0, **forces)
+    disp = np.linalg.norm(xb - x0)
+    assert na >= 3 and nb >= 3 and disp > 0
+    assert np.linalg.norm(xa - xb) / disp < 1e-3, (np.linalg.norm(xa - xb) / disp, na, nb)
+
+
 def test_keep_tree_is_close_to_rebuild():
     x0 = S.uniform_min_dist(8000, 0.1, 8)
     f = S.sedimenting_forces(8000, 8)
