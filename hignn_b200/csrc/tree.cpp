@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <numeric>
 #include <utility>
 
@@ -73,8 +74,88 @@ void jacobi_dominant_axis(const double cov[3][3], double u[3]) {
 
 namespace {
 
+// Order-preserving unsigned image of a finite float; -0.0 and +0.0 share one image, as they
+// compare equal under operator<.
+inline uint32_t float_key(float f) {
+  uint32_t u;
+  if (f == 0.0f) f = 0.0f;
+  std::memcpy(&u, &f, 4);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Scratch of one thread's divisions, allocated once per tree build (fresh allocations of the
+// top nodes' sizes at every division cost more in first-touch page faults than the work).
+struct DivideScratch {
+  std::vector<float> vh, tv;
+  std::vector<uint32_t> kb, order;
+  std::vector<uint64_t> ra, rb;
+  std::vector<int64_t> pcopy;
+  std::vector<std::pair<float, int64_t>> key;
+};
+
+// Stable sort of positions 0..L-1 by kb (ascending), written to s.order: the permutation
+// std::stable_sort gives with operator< on the floats behind the keys. LSD radix, 8-bit
+// digits, digits on which all keys agree skipped. With `threads` > 1 each pass histograms
+// and scatters contiguous chunks per thread; the chunk-major prefix keeps it stable.
+void radix_order(DivideScratch& s, int64_t L, int threads) {
+  std::vector<uint64_t>& a = s.ra;
+  std::vector<uint64_t>& b = s.rb;
+  a.resize(L);
+  b.resize(L);
+  for (int64_t i = 0; i < L; i++) a[i] = ((uint64_t)s.kb[i] << 32) | (uint64_t)i;
+  const int T = threads > 1 ? threads : 1;
+  std::vector<int64_t> hist((size_t)T * 256);
+  for (int shift = 32; shift < 64; shift += 8) {
+    std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(T) if (T > 1)
+    {
+#ifdef _OPENMP
+      const int th = T > 1 ? omp_get_thread_num() : 0;
+#else
+      const int th = 0;
+#endif
+      const int64_t lo = L * th / T, hi = L * (th + 1) / T;
+      int64_t* h = &hist[(size_t)th * 256];
+      for (int64_t i = lo; i < hi; i++) h[(a[i] >> shift) & 255]++;
+    }
+    bool trivial = false;
+    for (int d = 0; d < 256 && !trivial; d++) {
+      int64_t c = 0;
+      for (int th = 0; th < T; th++) c += hist[(size_t)th * 256 + d];
+      trivial = (c == L);
+    }
+    if (trivial) continue;
+    int64_t run = 0;  // exclusive prefix over (digit, chunk)
+    for (int d = 0; d < 256; d++)
+      for (int th = 0; th < T; th++) {
+        const int64_t c = hist[(size_t)th * 256 + d];
+        hist[(size_t)th * 256 + d] = run;
+        run += c;
+      }
+#pragma omp parallel num_threads(T) if (T > 1)
+    {
+#ifdef _OPENMP
+      const int th = T > 1 ? omp_get_thread_num() : 0;
+#else
+      const int th = 0;
+#endif
+      const int64_t lo = L * th / T, hi = L * (th + 1) / T;
+      int64_t* h = &hist[(size_t)th * 256];
+      for (int64_t i = lo; i < hi; i++) b[h[(a[i] >> shift) & 255]++] = a[i];
+    }
+    a.swap(b);
+  }
+  s.order.resize(L);
+  for (int64_t i = 0; i < L; i++) s.order[i] = (uint32_t)(a[i] & 0xffffffffu);
+}
+
+// Nodes at least this large sort their projections by radix, smaller ones by comparison;
+// from kParallelSortMin on (the top divisions) the radix passes use several threads.
+constexpr int64_t kRadixMin = 4096;
+constexpr int64_t kParallelSortMin = int64_t(1) << 18;
+
 // HignnModel::Divide: returns the split index (first position with t > 0).
-int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last) {
+int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last, int sort_threads, DivideScratch& s) {
   const int64_t L = last - first;
   float mean[3] = {0.f, 0.f, 0.f};
   for (int64_t i = first; i < last; i++) {
@@ -84,7 +165,8 @@ int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last) {
     mean[2] += p[2];
   }
   for (int d = 0; d < 3; d++) mean[d] /= (float)L;
-  std::vector<float> vh(3 * L);
+  std::vector<float>& vh = s.vh;
+  vh.resize(3 * L);
   double cov[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   for (int64_t i = 0; i < L; i++) {
     const float* p = xyz + 3 * perm[first + i];
@@ -93,42 +175,77 @@ int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last) {
     q[1] = p[1] - mean[1];
     q[2] = p[2] - mean[2];
   }
-  for (int a = 0; a < 3; a++)
-    for (int b = a; b < 3; b++) {
-      double s = 0.0;
-      for (int64_t i = 0; i < L; i++) s += (double)vh[3 * i + a] * (double)vh[3 * i + b];
-      cov[a][b] = s;
-      cov[b][a] = s;
+  {
+    // six sums in one pass; each is still accumulated in index order
+    double s00 = 0.0, s01 = 0.0, s02 = 0.0, s11 = 0.0, s12 = 0.0, s22 = 0.0;
+    for (int64_t i = 0; i < L; i++) {
+      const double x = vh[3 * i], y = vh[3 * i + 1], z = vh[3 * i + 2];
+      s00 += x * x;
+      s01 += x * y;
+      s02 += x * z;
+      s11 += y * y;
+      s12 += y * z;
+      s22 += z * z;
     }
+    cov[0][0] = s00;
+    cov[0][1] = cov[1][0] = s01;
+    cov[0][2] = cov[2][0] = s02;
+    cov[1][1] = s11;
+    cov[1][2] = cov[2][1] = s12;
+    cov[2][2] = s22;
+  }
   double ud[3];
   jacobi_dominant_axis(cov, ud);
   const float u0 = (float)ud[0], u1 = (float)ud[1], u2 = (float)ud[2];
-  std::vector<std::pair<float, int64_t>> key(L);
-  for (int64_t i = 0; i < L; i++) {
+  auto project = [&](int64_t i) {
     const float* q = &vh[3 * i];
     float t = u0 * q[0];
     t = t + u1 * q[1];
     t = t + u2 * q[2];
-    key[i] = {t, perm[first + i]};
+    return t;
+  };
+  // upper_bound(t, 0) over the sorted projections: first position with t strictly above zero
+  auto first_positive = [L](auto&& sorted_t) {
+    int64_t lo = 0, hi = L;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) / 2;
+      if (0.0f < sorted_t(mid))
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    return lo;
+  };
+  int64_t split;
+  if (L >= kRadixMin) {
+    // the permutation a stable comparison sort gives (below), by radix; whole-machine threads
+    // for the top divisions, which run outside the per-level parallel loop
+    s.tv.resize(L);
+    s.kb.resize(L);
+    for (int64_t i = 0; i < L; i++) {
+      s.tv[i] = project(i);
+      s.kb[i] = float_key(s.tv[i]);
+    }
+#ifdef _OPENMP
+    const int threads = (omp_in_parallel() || L < kParallelSortMin) ? 1 : sort_threads;
+#else
+    const int threads = 1;
+#endif
+    radix_order(s, L, threads);
+    s.pcopy.assign(perm + first, perm + last);
+    for (int64_t i = 0; i < L; i++) perm[first + i] = s.pcopy[s.order[i]];
+    split = first_positive([&](int64_t k) { return s.tv[s.order[k]]; });
+  } else {
+    std::vector<std::pair<float, int64_t>>& key = s.key;
+    key.resize(L);
+    for (int64_t i = 0; i < L; i++) key[i] = {project(i), perm[first + i]};
+    std::stable_sort(key.begin(), key.end(),
+                     [](const std::pair<float, int64_t>& x, const std::pair<float, int64_t>& y) {
+                       return x.first < y.first;
+                     });
+    for (int64_t i = 0; i < L; i++) perm[first + i] = key[i].second;
+    split = first_positive([&](int64_t k) { return key[k].first; });
   }
-  std::stable_sort(key.begin(), key.end(),
-                   [](const std::pair<float, int64_t>& x, const std::pair<float, int64_t>& y) {
-                     return x.first < y.first;
-                   });
-  int64_t split = L;
-  for (int64_t i = 0; i < L; i++) {
-    perm[first + i] = key[i].second;
-  }
-  // upper_bound(t, 0): first element strictly greater than zero
-  int64_t lo = 0, hi = L;
-  while (lo < hi) {
-    int64_t mid = (lo + hi) / 2;
-    if (0.0f < key[mid].first)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  split = lo;
   return split + first;
 }
 
@@ -146,8 +263,9 @@ ClusterTree build_tree(const float* xyz, int64_t n, int64_t leaf, int num_thread
   std::iota(t.perm.begin(), t.perm.end(), (int64_t)0);
   // Sequential stage (src/Build.cpp:38-97): one rank => initialLevel 0, the root is divided once.
   TreeNode init[3] = {{0, 0, 0, n, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
+  std::vector<DivideScratch> scratch((size_t)std::max(1, num_threads));
   if (n > leaf) {
-    int64_t d = divide(xyz, t.perm.data(), 0, n);
+    int64_t d = divide(xyz, t.perm.data(), 0, n, num_threads, scratch[0]);
     if (split_ok(d, 0, n)) {
       init[0].child0 = 1;
       init[0].child1 = 2;
@@ -166,7 +284,12 @@ ClusterTree build_tree(const float* xyz, int64_t n, int64_t leaf, int num_thread
 #pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads) if (m > 1)
     for (int64_t i = 0; i < m; i++) {
       const TreeNode nd = local[frontier[i]];
-      split[i] = (nd.end - nd.start > leaf) ? divide(xyz, t.perm.data(), nd.start, nd.end) : 0;
+#ifdef _OPENMP
+      DivideScratch& sc = scratch[omp_in_parallel() ? omp_get_thread_num() : 0];
+#else
+      DivideScratch& sc = scratch[0];
+#endif
+      split[i] = (nd.end - nd.start > leaf) ? divide(xyz, t.perm.data(), nd.start, nd.end, num_threads, sc) : 0;
     }
     std::vector<int64_t> next;
     for (int64_t i = 0; i < m; i++) {
@@ -262,10 +385,12 @@ BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, b
   auto leafq = [&](int64_t nd) { return t.nodes[nd].child0 == 0; };
   std::vector<std::vector<int64_t>> farM(nn), closeM(nn);
   closeM[0].push_back(0);
-  // dual traversal (src/CloseFarCheck.cpp:186-290), BFS over the row tree
-  std::vector<int64_t> queue{0};
-  for (size_t qi = 0; qi < queue.size(); qi++) {
-    const int64_t i = queue[qi];
+  // dual traversal (src/CloseFarCheck.cpp:186-290), breadth first over the row tree. A FIFO
+  // queue visits the tree level by level, each level in the order its parents were visited;
+  // here the levels are taken one at a time in that order, and the nodes of a level in
+  // parallel (a node reads its own close list and writes only its own far list and its
+  // children's or its own close list), so every list comes out as the queue would build it.
+  auto visit = [&](int64_t i) {
     const float* ai = &L.aux[6 * i];
     if (!leafq(i)) {
       std::vector<int64_t> childClose;
@@ -281,9 +406,7 @@ BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, b
         }
       }
       closeM[t.nodes[i].child0] = childClose;
-      closeM[t.nodes[i].child1] = childClose;
-      queue.push_back(t.nodes[i].child0);
-      queue.push_back(t.nodes[i].child1);
+      closeM[t.nodes[i].child1] = std::move(childClose);
     } else {
       std::vector<int64_t> newClose;
       for (int64_t j : closeM[i]) {
@@ -320,8 +443,23 @@ BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, b
         }
       }
       closeM[i].swap(newClose);
-      L.leaves.push_back(i);
     }
+  };
+  std::vector<int64_t> level{0}, next;
+  while (!level.empty()) {
+    const int64_t m = (int64_t)level.size();
+#pragma omp parallel for schedule(dynamic, 16) if (m > 64)
+    for (int64_t q = 0; q < m; q++) visit(level[q]);
+    next.clear();
+    for (int64_t i : level) {
+      if (leafq(i)) {
+        L.leaves.push_back(i);
+      } else {
+        next.push_back(t.nodes[i].child0);
+        next.push_back(t.nodes[i].child1);
+      }
+    }
+    level.swap(next);
   }
   // flattening (src/CloseFarCheck.cpp:298-336, 385-408), one rank
   for (int64_t i : L.leaves)
