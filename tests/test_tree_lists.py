@@ -28,6 +28,11 @@ CASES = [
     ("clustered_30k", lambda: S.clustered(30000, 0.1, 2), 128),
     ("leaf_64", lambda: S.uniform(5000, 0.1, 3), 64),
     ("ragged_1001", lambda: S.uniform(1001, 0.2, 4), 50),
+    # exact ties and signed zeros among the projections: the sort must keep input order for equal keys
+    ("lattice_ties", lambda: (np.stack(np.meshgrid(*[np.arange(32)] * 3, indexing="ij"), -1)
+                              .reshape(-1, 3).astype(np.float32) - np.float32(15.5)), 100),
+    # the benchmark's workload: nodes of >= 2^18 particles take the threaded radix sort
+    ("clustered_1m", lambda: S.clustered(1048576, 0.10, 2), 128),
 ]
 
 
