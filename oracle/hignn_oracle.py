@@ -11,7 +11,12 @@ parts (tree, admissibility, CloseDot, FarDot/ACA, DenseDot) restate the C++
 sources line by line; the reference's own tests pin none of them (its only
 tests are docker smoke tests) and its C++ cannot be built here (Kokkos, Eigen,
 MPI, VTK are absent), so for those parts parity is unpinned against the
-reference binary and rests on this restatement.
+reference binary and rests on this restatement. Also pinned: the three-body and
+self terms against the reference's own model classes
+(python/HIGNN/model_structure.py; tests/golden/three_body_velocity.npz), the
+filament forces against its chain_bending / chain_tension (python/simulate.py;
+tests/golden/filament_forces.npz), and the Dormand-Prince integrator against
+scipy's DOP853 on a smooth system (tests/test_oracle_dp45.py).
 
 Declared choices where the reference is solver-defined:
 * PCA direction: the reference takes U(:,0) of an Eigen JacobiSVD of the
