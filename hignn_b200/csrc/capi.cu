@@ -781,6 +781,10 @@ void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
 // Dense product over all leaf pairs into m->u (tree order); f4 already gathered.
 void dense_tree_order(hignn_model* m, double* u_out) {
   const auto& lv = m->lists.leaves;
+  // one work item per leaf pair, counted in 32 bits on the device
+  if ((double)lv.size() * (double)lv.size() > 2147483647.0)
+    throw Error(HIGNN_ERR_ARG, "dense product: " + std::to_string(lv.size()) +
+                                   " leaves give more leaf pairs than one launch takes; use hignn_dense_rows");
   std::vector<hignn::PairWork> work;
   work.reserve(lv.size() * lv.size());
   for (int64_t I : lv)
@@ -984,6 +988,9 @@ int hignn_load_two_body_mem(hignn_model* m, int num_layers, const int32_t* dims,
   return guard([&] {
     if (!m || !dims || !params) throw Error(HIGNN_ERR_ARG, "null argument");
     if (activation != 1) throw Error(HIGNN_ERR_ARG, "two-body network activation must be tanh (1)");
+    // the shape is checked before any weight is read from `params`
+    if (num_layers != 3 || dims[0] != 3 || dims[1] != hignn::kH1 || dims[2] != hignn::kH2 || dims[3] != hignn::kOut)
+      throw Error(HIGNN_ERR_ARG, "two-body network must be 3 -> 128 -> 512 -> 9 (tanh)");
     std::vector<int> d(dims, dims + num_layers + 1);
     std::vector<std::vector<float>> W, B;
     const float* p = params;
@@ -1877,6 +1884,12 @@ int hignn_tb_load_mem(hignn_tb* t, int which, int num_layers, const int32_t* dim
   return guard([&] {
     if (!t || !dims || !params) throw Error(HIGNN_ERR_ARG, "null argument");
     if (num_layers != 4) throw Error(HIGNN_ERR_ARG, "three-body networks have 4 dense layers");
+    // the shape is checked before any weight is read from `params`
+    if (which != HIGNN_TB_THREE_BODY && which != HIGNN_TB_SELF) throw Error(HIGNN_ERR_ARG, "unknown network kind");
+    const int kin = which == HIGNN_TB_THREE_BODY ? 6 : 3;
+    if (dims[0] != kin || dims[1] != hignn::kTbH1 || dims[2] != hignn::kTbH2 || dims[3] != hignn::kTbH3 || dims[4] != 9)
+      throw Error(HIGNN_ERR_ARG, which == HIGNN_TB_THREE_BODY ? "three-body network must be 6 -> 256 -> 1024 -> 512 -> 9"
+                                                              : "self network must be 3 -> 256 -> 1024 -> 512 -> 9");
     std::vector<int> d(dims, dims + num_layers + 1);
     std::vector<std::vector<float>> W, B;
     const float* p = params;

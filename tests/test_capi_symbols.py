@@ -92,3 +92,29 @@ def test_neighbour_lists_and_three_body_need_a_device():
     assert not h.value
     capi.lib.hignn_nbl_destroy(None)  # a null handle is accepted
     capi.lib.hignn_tb_destroy(None)
+
+
+def test_weights_from_memory_are_shape_checked_first():
+    """hignn_load_two_body_mem checks the layer shapes before it reads any weight, so a wrong
+    shape is an error (not a read past the caller's array); the right shape loads on a
+    host-only model."""
+    import ctypes as C
+
+    import numpy as np
+
+    from hignn_b200 import capi
+
+    m = capi.Model(np.random.default_rng(1).uniform(0, 20, (400, 3)), 64, device=-1)
+    good = np.array([3, 128, 512, 9], np.int32)
+    params = np.random.default_rng(2).standard_normal(3 * 128 + 128 + 128 * 512 + 512 + 512 * 9 + 9).astype(np.float32)
+    fp = params.ctypes.data_as(C.POINTER(C.c_float))
+
+    def load(dims, layers, act=1):
+        d = np.ascontiguousarray(dims, np.int32)
+        return capi.lib.hignn_load_two_body_mem(m._h, layers, d.ctypes.data_as(C.POINTER(C.c_int32)), fp, act)
+
+    assert load(good, 3) == 0
+    assert load(good, 2) == -1
+    assert load(good, -5) == -1
+    assert load([3, 1 << 30, 512, 9], 3) == -1  # would read far past `params` if read first
+    assert load(good, 3, act=2) == -1
