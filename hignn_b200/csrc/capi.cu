@@ -1392,12 +1392,15 @@ int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64
     require_weights(m);
     ensure_tree(m);
     if (nrows <= 0) return;
+    const auto& lv = m->lists.leaves;
+    // one work item per (chunk of 128 rows, leaf), counted and offset in 32 bits on the device
+    if (nrows > 2147483647 - 128 || (double)((nrows + 127) / 128) * (double)lv.size() > 2147483647.0)
+      throw Error(HIGNN_ERR_ARG, "dense_rows: too many rows for one call; split the rows over several calls");
     std::vector<int32_t> pos(nrows);
     for (int64_t q = 0; q < nrows; q++) {
       if (rows[q] < 0 || rows[q] >= m->n) throw Error(HIGNN_ERR_ARG, "row index out of range");
       pos[q] = (int32_t)m->inv_perm[rows[q]];
     }
-    const auto& lv = m->lists.leaves;
     std::vector<hignn::PairWork> work;
     for (int64_t c0 = 0; c0 < nrows; c0 += 128)
       for (int64_t J : lv) {

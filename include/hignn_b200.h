@@ -181,7 +181,8 @@ int hignn_dense_dot(hignn_model* m, float* u, const float* f, int64_t n);
 
 /* Dense rows for accuracy checks: for each listed target row (caller's order)
  * u_row = sum over all j of 0.5 (M + M^T)(x_j - x_row) f_j, accumulated in FP64.
- * precision 0 = FP32 network, 2 = FP64 network. Host pointers; u_rows is (nrows, 3). */
+ * precision 0 (FP32 network) is the only one on the device. Host pointers; u_rows is (nrows, 3);
+ * rows may repeat. */
 int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
                      int precision);
 
