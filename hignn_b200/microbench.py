@@ -31,7 +31,7 @@ def main():
     ap.add_argument("--n", type=int, default=148 * 128 * 20)
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m"])
+    ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m", "uniform4m"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
     ap.add_argument("--timing", type=int, default=2, help="2 = far-field breakdown by kernel category")
@@ -75,6 +75,9 @@ def main():
     else:
         if a.workload == "uniform1m":
             x, f = S.uniform(1048576, 0.1, 2), S.sedimenting_forces(1048576, 2)
+        elif a.workload == "uniform4m":
+            # the learned-far-field workload: 4,194,304 spheres uniform at volume fraction 0.10, seed 4
+            x, f = S.uniform(4194304, 0.1, 4), S.sedimenting_forces(4194304, 4)
         elif a.workload == "large":
             x, f = S.clustered(1048576, 0.10, 2), S.sedimenting_forces(1048576, 2)
         else:
