@@ -18,6 +18,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hignn_b200.h"
@@ -55,10 +56,16 @@ int guard(F&& f) {
 
 using hignn::DevBuf;
 
+// Threads of the host tree build: the machine's cores shared among the ranks of this node
+// (LOCAL_WORLD_SIZE, as torchrun sets it), at most 32; HIGNN_HOST_THREADS overrides. The tree
+// and the lists do not depend on the thread count.
 int host_threads() {
-  int n = 8;
-  if (const char* e = std::getenv("HIGNN_HOST_THREADS")) n = std::max(1, std::atoi(e));
-  return n;
+  if (const char* e = std::getenv("HIGNN_HOST_THREADS")) return std::max(1, std::atoi(e));
+  int cores = (int)std::thread::hardware_concurrency();
+  if (cores <= 0) cores = 8;
+  int ranks = 1;
+  if (const char* w = std::getenv("LOCAL_WORLD_SIZE")) ranks = std::max(1, std::atoi(w));
+  return std::max(1, std::min(32, cores / ranks));
 }
 
 }  // namespace
