@@ -105,3 +105,17 @@ def test_edge_cases():
         capi.Model(np.zeros((0, 3), np.float32), 4, device=-1)
     with pytest.raises(capi.HignnError):
         capi.Model(np.array([[np.nan, 0, 0]], np.float32), 4, device=-1)
+
+
+def test_tree_does_not_depend_on_the_thread_count(monkeypatch):
+    # 300k particles: the root's divisions take the threaded radix sort (nodes of >= 2^18)
+    x = S.clustered(300000, 0.1, 6)
+    out = []
+    for threads in ("1", "5", "16"):
+        monkeypatch.setenv("HIGNN_HOST_THREADS", threads)
+        t, p, lists, _ = native(x, 128)
+        out.append((t, p, lists))
+    for t, p, lists in out[1:]:
+        assert np.array_equal(t, out[0][0]) and np.array_equal(p, out[0][1])
+        for a, b in zip(lists, out[0][2]):
+            assert np.array_equal(a, b)
