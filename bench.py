@@ -187,8 +187,44 @@ class ClockSampler:
                 "samples": len(rows), "samples_under_load": len(load), "power_w_max": max(pw)}
 
 
+class TorchCpuNet:
+    """The two-body network on torch's CPU FP32 path, the engine the reference evaluates it with
+    (libtorch, src/CloseDot.cpp:233), wrapped as the oracle's eval32 is (identity added, divided
+    by |r|, identity below |r| = 1e-5). Batches of 8,192 features, about the reference's
+    per-block batches."""
+
+    def __init__(self, net, threads):
+        import torch
+
+        self.torch = torch
+        torch.set_num_threads(threads)
+        self.layers = [(torch.from_numpy(w.copy()), torch.from_numpy(b.copy())) for w, b in zip(net.w32, net.b32)]
+
+    def eval32(self, r):
+        torch = self.torch
+        r = np.ascontiguousarray(r, np.float32)
+        y = np.empty((r.shape[0], 9), np.float32)
+        with torch.no_grad():
+            for s in range(0, r.shape[0], 8192):
+                h = torch.from_numpy(r[s:s + 8192])
+                for i, (w, b) in enumerate(self.layers):
+                    h = torch.addmm(b, h, w.T)
+                    if i + 1 < len(self.layers):
+                        h = torch.tanh(h)
+                y[s:s + 8192] = h.numpy()
+        y[:, 0] += np.float32(1)
+        y[:, 4] += np.float32(1)
+        y[:, 8] += np.float32(1)
+        nr = np.sqrt((r * r).sum(1, dtype=np.float32)).astype(np.float32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            y = y / nr[:, None]
+        y[nr < 1e-5] = np.eye(3, dtype=np.float32).reshape(9)
+        return y
+
+
 def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
-    """The oracle port (numpy restatement of the reference path) timed on a bounded sample.
+    """The oracle port (numpy restatement of the reference path, the network on torch's CPU path)
+    timed on a bounded sample.
 
     Near field: leading close pairs for ~seconds/2 of CPU work; far field: leading ACA
     blocks for the other half. Evaluations/s of each are extrapolated to the counted
@@ -197,7 +233,8 @@ def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
     """
     from oracle import hignn_oracle as O
 
-    net = O.TwoBody.from_hgnw(WEIGHTS)
+    cores = os.cpu_count() or 1
+    net = TorchCpuNet(O.TwoBody.from_hgnw(WEIGHTS), cores)
     t0 = time.time()
     tree, rmap = O.build_tree(x, 128)
     xt = x[rmap]
@@ -231,9 +268,9 @@ def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
     if far_evals is None:
         far_evals = float(np.mean(ranks)) * float(np.sum(sz[fi] + sz[fj])) if ranks else 0.0
     t_dot = close_evals / r_near + far_evals / r_far
-    cores = os.cpu_count() or 1
     return {"value": len(x) / t_dot, "unit": "particles/s", "cores": cores, "kind": "port",
-            "sample": (f"oracle numpy restatement on {cores} host threads: {p} close pairs ({done_e:.3g} evals, "
+            "sample": (f"oracle restatement (numpy) with the two-body network on torch's CPU FP32 path, as the "
+                       f"reference's libtorch, on {cores} host threads: {p} close pairs ({done_e:.3g} evals, "
                        f"{r_near:.3g} evals/s) and {b} ACA blocks ({far_e:.3g} evals, {r_far:.3g} evals/s), "
                        f"extrapolated to {close_evals:.3g} near + {far_evals:.3g} far evaluations of one "
                        f"H-matvec; tree+lists ({t_lists:.1f} s) not counted")}
@@ -258,7 +295,8 @@ def reference_arm(args, rank, world):
                              "sample": s["sample"]},
             "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent; "
-                    "not pip-installable); this arm times its restatement on the host cores"}
+                    "not pip-installable); this arm times its restatement on the host cores, the two-body "
+                    "network on torch's CPU FP32 path as the reference evaluates it with libtorch"}
     print(json.dumps(line), flush=True)
     return 0
 
