@@ -21,6 +21,10 @@
 #include <thread>
 #include <vector>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 #include "../../include/hignn_b200.h"
 #include "common.h"
 #include "kernels.h"
@@ -56,12 +60,17 @@ int guard(F&& f) {
 
 using hignn::DevBuf;
 
-// Threads of the host tree build: the machine's cores shared among the ranks of this node
+// Threads of the host tree build: the cores this process may run on (OpenMP's count, which
+// follows the affinity mask and OMP_NUM_THREADS) shared among the ranks of this node
 // (LOCAL_WORLD_SIZE, as torchrun sets it), at most 32; HIGNN_HOST_THREADS overrides. The tree
 // and the lists do not depend on the thread count.
 int host_threads() {
   if (const char* e = std::getenv("HIGNN_HOST_THREADS")) return std::max(1, std::atoi(e));
+#ifdef _OPENMP
+  int cores = omp_get_max_threads();
+#else
   int cores = (int)std::thread::hardware_concurrency();
+#endif
   if (cores <= 0) cores = 8;
   int ranks = 1;
   if (const char* w = std::getenv("LOCAL_WORLD_SIZE")) ranks = std::max(1, std::atoi(w));
