@@ -182,25 +182,45 @@ void require_device(hignn_model* m) {
   HIGNN_CUDA(cudaSetDevice(m->device));
 }
 
+// Builds the tree and lists of m->xyz and, on a device model, uploads the tree-order positions
+// and the close work list. Everything is built and checked before the model changes: a tree that
+// the device kernels cannot take (a leaf above kMaxLeaf particles, which coincident points can
+// give whatever the block size) leaves the model without a tree (tree_ready false), so that no
+// later call runs on lists that do not belong to the uploaded positions.
 void build_structures(hignn_model* m) {
   const auto t0 = std::chrono::steady_clock::now();
-  m->tree = hignn::build_tree(m->xyz.data(), m->n, m->block_size, host_threads());
-  m->xt.resize(3 * m->n);
-  m->inv_perm.resize(m->n);
-  for (int64_t i = 0; i < m->n; i++) {
-    const int64_t p = m->tree.perm[i];
-    m->xt[3 * i] = m->xyz[3 * p];
-    m->xt[3 * i + 1] = m->xyz[3 * p + 1];
-    m->xt[3 * i + 2] = m->xyz[3 * p + 2];
-    m->inv_perm[p] = i;
-  }
-  m->lists = hignn::build_lists(m->tree, m->xt.data(), m->max_relative_coord, m->use_symmetry);
-  m->lists_sym = m->use_symmetry;
-  m->lists_max_rel = m->max_relative_coord;
-  m->tree_ready = true;
+  m->tree_ready = false;
   m->plan_ready = false;
   m->hint_valid = false;
   m->shard_ready = false;
+  hignn::ClusterTree tree = hignn::build_tree(m->xyz.data(), m->n, m->block_size, host_threads());
+  std::vector<float> xt(3 * m->n);
+  std::vector<int64_t> inv_perm(m->n);
+  for (int64_t i = 0; i < m->n; i++) {
+    const int64_t p = tree.perm[i];
+    xt[3 * i] = m->xyz[3 * p];
+    xt[3 * i + 1] = m->xyz[3 * p + 1];
+    xt[3 * i + 2] = m->xyz[3 * p + 2];
+    inv_perm[p] = i;
+  }
+  hignn::BlockLists lists =
+      hignn::build_lists(tree, xt.data(), m->max_relative_coord, m->use_symmetry, host_threads());
+  if (m->device >= 0)
+    for (int64_t L : lists.leaves) {
+      const int64_t sz = tree.nodes[L].end - tree.nodes[L].start;
+      if (sz > hignn::kMaxLeaf)
+        throw Error(HIGNN_ERR_ARG, "leaf of " + std::to_string(sz) + " particles (more than " +
+                                       std::to_string(hignn::kMaxLeaf) +
+                                       "; coincident points or block_size > " + std::to_string(hignn::kMaxLeaf) +
+                                       "): the device kernels stage at most " + std::to_string(hignn::kMaxLeaf) +
+                                       " particles per leaf");
+    }
+  m->tree = std::move(tree);
+  m->xt = std::move(xt);
+  m->inv_perm = std::move(inv_perm);
+  m->lists = std::move(lists);
+  m->lists_sym = m->use_symmetry;
+  m->lists_max_rel = m->max_relative_coord;
   const auto t1 = std::chrono::steady_clock::now();
   m->stats.t_build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   m->stats.n = m->n;
@@ -208,7 +228,10 @@ void build_structures(hignn_model* m) {
   m->stats.num_leaves = (int64_t)m->lists.leaves.size();
   m->stats.num_close = (int64_t)m->lists.closeI.size();
   m->stats.num_far = (int64_t)m->lists.farI.size();
-  if (m->device < 0) return;
+  if (m->device < 0) {
+    m->tree_ready = true;
+    return;
+  }
   // device copies
   HIGNN_CUDA(cudaSetDevice(m->device));
   const int64_t n = m->n;
@@ -219,16 +242,6 @@ void build_structures(hignn_model* m) {
     perm[i] = (int32_t)m->tree.perm[i];
     slot[i] = (int32_t)m->inv_perm[i];
   }
-  m->x4.ensure(sizeof(float4) * n);
-  m->perm.ensure(sizeof(int32_t) * n);
-  m->slot.ensure(sizeof(int32_t) * n);
-  HIGNN_CUDA(cudaMemcpyAsync(m->slot.p, slot.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
-  m->f4.ensure(sizeof(float4) * n);
-  m->u.ensure(sizeof(double) * 3 * n);
-  m->io_f.ensure(sizeof(float) * 3 * n);
-  m->io_u.ensure(sizeof(float) * 3 * n);
-  HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
-  HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
   // close work list (src/CloseFarCheck.cpp:298-336 order)
   std::vector<hignn::PairWork> work(m->lists.closeI.size());
   int64_t evals = 0;
@@ -241,21 +254,29 @@ void build_structures(hignn_model* m) {
     w.sJ = (int32_t)J.start;
     w.nJ = (int32_t)(J.end - J.start);
     w.flags = (m->use_symmetry && m->lists.closeJ[q] > m->lists.closeI[q]) ? hignn::kPairTransposed : 0;
-    if (w.nI > hignn::kMaxLeaf || w.nJ > hignn::kMaxLeaf)
-      throw Error(HIGNN_ERR_ARG, "leaf larger than " + std::to_string(hignn::kMaxLeaf) +
-                                     " particles; use block_size <= " + std::to_string(hignn::kMaxLeaf));
     evals += (int64_t)w.nI * w.nJ;
     work[q] = w;
   }
   m->stats.close_evals = evals;
   m->max_leaf = 0;
   for (const auto& w : work) m->max_leaf = std::max(m->max_leaf, std::max(w.nI, w.nJ));
+  m->x4.ensure(sizeof(float4) * n);
+  m->perm.ensure(sizeof(int32_t) * n);
+  m->slot.ensure(sizeof(int32_t) * n);
+  m->f4.ensure(sizeof(float4) * n);
+  m->u.ensure(sizeof(double) * 3 * n);
+  m->io_f.ensure(sizeof(float) * 3 * n);
+  m->io_u.ensure(sizeof(float) * 3 * n);
   m->close_work.ensure(sizeof(hignn::PairWork) * std::max<size_t>(1, work.size()));
+  m->counter.ensure(64);
+  HIGNN_CUDA(cudaMemcpyAsync(m->slot.p, slot.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
+  HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
   if (!work.empty())
     HIGNN_CUDA(cudaMemcpyAsync(m->close_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
                                cudaMemcpyHostToDevice, m->stream));
-  m->counter.ensure(64);
   HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  m->tree_ready = true;
 }
 
 void ensure_tree(hignn_model* m) {
@@ -891,6 +912,9 @@ int hignn_create(const float* xyz, int64_t n, int block_size, int device, hignn_
     if (!xyz || n <= 0) throw Error(HIGNN_ERR_ARG, "coordinates must be a non-empty (n, 3) array");
     if (n >= (int64_t(1) << 31)) throw Error(HIGNN_ERR_ARG, "n must be below 2^31");
     if (block_size <= 0) throw Error(HIGNN_ERR_ARG, "block_size must be positive");
+    if (device >= 0 && block_size > hignn::kMaxLeaf)
+      throw Error(HIGNN_ERR_ARG, "block_size must be at most " + std::to_string(hignn::kMaxLeaf) +
+                                     " on a device (the near-field kernels stage one leaf in shared memory)");
     auto* m = new hignn_model();
     try {
       m->n = n;

@@ -15,8 +15,14 @@
 // (cudaGetSymbolAddress) with that device current; make that first call
 // before any stream capture. All calls share the array and it keeps the last
 // call's contents, so every call clears the accumulators and the counter
-// itself; calls whose GPU work overlaps (different streams or host threads on
-// one device) race on the array.
+// itself. Calls from one process are serialised by a process-wide lock that
+// is held until the call's GPU work has finished -- calls on different GPUs
+// included, since the host staging arrays are shared too -- so two calls of
+// this entry point never overlap on the GPU. What can race is other GPU work
+// that the caller issues, on another stream, against the same model's
+// buffers while a call runs: the call overwrites the model's force buffers
+// (the caller-order staging and the tree-order forces) and reads its
+// positions.
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -200,6 +206,9 @@ void dense_rows_noalloc(hignn_model* m, double* u_rows, const float* f, const in
   }
   for (int64_t l = 0; l < nleaves; l++) {
     const TreeNode& nd = (*v.nodes)[(*v.leaves)[l]];
+    if (nd.end - nd.start > kMaxLeaf)  // the kernel stages one source leaf in shared memory
+      throw Error(HIGNN_ERR_ARG, "dense_rows_noalloc: a leaf holds more than " + std::to_string(kMaxLeaf) +
+                                     " particles");
     g_na_leaf[l] = make_int2((int)nd.start, (int)(nd.end - nd.start));
   }
   int2* d_leaf = reinterpret_cast<int2*>(base + kNaOffLeaf);

@@ -349,7 +349,8 @@ bool is_far(const float* a, const float* b) {
   return (dist > d0) && (dist > d1);
 }
 
-BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, bool use_symmetry) {
+BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, bool use_symmetry, int num_threads) {
+  const int nthr = num_threads > 0 ? num_threads : 1;
   BlockLists L;
   const int64_t nn = (int64_t)t.nodes.size();
   L.aux.assign(6 * nn, 0.f);
@@ -368,7 +369,7 @@ BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, b
         st.push_back(t.nodes[nd].child1);
       }
     }
-#pragma omp parallel for schedule(dynamic, 16)
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthr)
     for (int64_t r = 0; r < (int64_t)reach.size(); r++) {
       const int64_t nd = reach[r];
       float bx[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
@@ -448,7 +449,7 @@ BlockLists build_lists(const ClusterTree& t, const float* xt, int64_t max_rel, b
   std::vector<int64_t> level{0}, next;
   while (!level.empty()) {
     const int64_t m = (int64_t)level.size();
-#pragma omp parallel for schedule(dynamic, 16) if (m > 64)
+#pragma omp parallel for schedule(dynamic, 16) if (m > 64) num_threads(nthr)
     for (int64_t q = 0; q < m; q++) visit(level[q]);
     next.clear();
     for (int64_t i : level) {

@@ -27,8 +27,9 @@ struct BlockLists {
 ClusterTree build_tree(const float* xyz, int64_t n, int64_t leaf, int num_threads);
 
 // ComputeAux + dual traversal + flattening, src/CloseFarCheck.cpp:11-454.
+// num_threads: OpenMP threads of the two parallel loops (the lists do not depend on it).
 BlockLists build_lists(const ClusterTree& t, const float* xyz_tree, int64_t max_relative_coord,
-                       bool use_symmetry);
+                       bool use_symmetry, int num_threads);
 
 // HignnModel::CloseFarCheck(aux, n1, n2), src/HignnModel.cpp:482-518.
 bool is_far(const float* a, const float* b);

@@ -197,8 +197,10 @@ int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64
  * (larger sizes return HIGNN_ERR_ARG); precision 0 only. The model must already
  * hold weights and a built tree (hignn_update_coord or hignn_dot once: those may
  * allocate). The first call on a device looks up the array's address; make it
- * before any stream capture. All calls share the array: calls whose GPU work
- * overlaps race. */
+ * before any stream capture. All calls share the array; a process-wide lock,
+ * held until a call's GPU work has finished, serialises the calls (on every GPU),
+ * so the race to avoid is with the caller's own GPU work on the same model's force
+ * and position buffers, issued on another stream while a call runs. */
 #define HIGNN_NOALLOC_MAX_ROWS 131072
 #define HIGNN_NOALLOC_MAX_LEAVES 65536
 int hignn_dense_rows_noalloc(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,

@@ -6,7 +6,7 @@ functions are compiled from its source (python/simulate.py:14-88) and called, pe
 way velocity_update assembles the force (python/simulate.py:130-142): a float32 body force,
 then += bending, then += tension. The outputs are committed as ``filament_forces.npz``.
 
-    python tests/golden/make_filament_golden.py [/path/to/reference]
+    python tests/golden/make_filament_golden.py /path/to/reference
 """
 import ast
 import os
@@ -31,7 +31,9 @@ def load_reference_forces(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python " + os.path.relpath(__file__) + " /path/to/reference  (the reference checkout)")
+    ref_root = sys.argv[1]
     bending, tension = load_reference_forces(ref_root)
     cases = {}
     rng = np.random.default_rng(7)

@@ -7,7 +7,7 @@ evaluates it in torch FP32 (the path libtorch runs in src/CloseDot.cpp:233,
 src/FarDot.cpp:414,739) and in FP64 on seeded inputs. The outputs are committed
 as ``two_body_net.npz`` next to this script.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 """
 import hashlib
 import importlib.util
@@ -54,7 +54,9 @@ def seeded_inputs(seed=20240):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python " + os.path.relpath(__file__) + " /path/to/reference  (the reference checkout)")
+    ref_root = sys.argv[1]
     Net, seq = load_reference_net(ref_root)
     r = seeded_inputs()
     with torch.no_grad():

@@ -8,7 +8,7 @@ evaluates the forward with no two-body edges -- as python/gravity_field.py:31-52
 seeded filament suspensions, in torch FP32 and FP64. The edge lists are the oracle's
 NeighborLists restatement at the three-body epsilon. Outputs: ``three_body_velocity.npz``.
 
-    python tests/golden/make_three_body_golden.py [/path/to/reference]
+    python tests/golden/make_three_body_golden.py /path/to/reference
 """
 import os
 import sys
@@ -32,7 +32,9 @@ def scatter(src, index, dim=0, dim_size=None, reduce="add"):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python " + os.path.relpath(__file__) + " /path/to/reference  (the reference checkout)")
+    ref = sys.argv[1]
     sys.modules["torch_scatter"] = types.SimpleNamespace(scatter=scatter)
     sys.path.insert(0, os.path.join(ref, "python"))
     import HIGNN.model_structure as ms

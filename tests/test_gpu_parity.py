@@ -192,3 +192,31 @@ def test_pybind_module_matches_capi(small_workload):
     assert rel(u, m.dot(f)) < 1e-6
     with pytest.raises(Exception):
         hm.dot(np.zeros((len(x), 3)), f)  # float64 output is rejected, not silently lost
+
+
+def test_failed_rebuild_leaves_model_unready():
+    """A tree the device kernels cannot take (here 300 coincident points: one leaf above the
+    256-particle staging limit whatever the block size) is refused on the host, before any
+    launch, and leaves the model without a tree: later calls are refused too, none runs on the
+    lists of the previous positions."""
+    n = 2000
+    x = S.uniform(n, 0.1, 7)
+    f = S.sedimenting_forces(n, 7)
+    m = make_model(x, epsilon=1e-2)
+    m.dot(f)
+    bad = x.copy()
+    bad[:300] = bad[0]
+    with pytest.raises(capi.HignnError) as e:
+        m.update_coord(bad)
+    assert e.value.code == -1
+    with pytest.raises(capi.HignnError) as e:
+        m.dense_rows_noalloc(f, np.arange(10))
+    assert e.value.code == -3
+    with pytest.raises(capi.HignnError) as e:
+        m.dot(f)  # the rebuild is tried again and refused again
+    assert e.value.code == -1
+    m.update_coord(x)  # good positions: the model works again
+    u = m.dot(f)
+    assert np.isfinite(u).all()
+    with pytest.raises(capi.HignnError):
+        capi.Model(x, 512, device=0)  # block_size above the staging limit

@@ -7,7 +7,8 @@ array that every call shares and that keeps the previous call's contents, so
 the test makes two calls in a row -- the second with other forces and fewer
 rows, over the first call's leftovers -- and checks each against the
 allocating entry point within the tolerance of the FP64-accumulated dense rows
-(only the order of FP64 atomic additions differs).
+(only the order of FP64 atomic additions differs), and that the device's free
+memory is the same before and after the second call.
 
 This file is named to be collected last.
 """
@@ -45,7 +46,12 @@ def test_noalloc_dense_rows_matches_allocating_entry_point_twice():
     out1 = m.dense_rows_noalloc(f1, rows1)
     ref1 = m.dense_rows(f1, rows1)
     assert rel(out1, ref1) < 1e-6
+    # the second call runs with every kernel loaded: the device's free memory must not change
+    torch.cuda.synchronize(0)
+    free_before = torch.cuda.mem_get_info(0)[0]
     out2 = m.dense_rows_noalloc(f2, rows2)
+    free_after = torch.cuda.mem_get_info(0)[0]
+    assert free_after == free_before, f"device free memory changed by {free_before - free_after} bytes"
     ref2 = m.dense_rows(f2, rows2)
     assert rel(out2, ref2) < 1e-6
 
