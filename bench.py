@@ -61,11 +61,15 @@ def parse():
     ap.add_argument("--student-samples", type=int, default=10_000_000)
     ap.add_argument("--n", type=int, default=1048576)
     ap.add_argument("--epsilon", type=float, default=1e-2)
-    ap.add_argument("--check-rows", type=int, default=2048, help="dense target rows for the error check")
+    ap.add_argument("--check-rows", type=int, default=16384,
+                    help="seeded target rows of the FP64 dense error check (all N sources each)")
+    ap.add_argument("--no-unplanned", action="store_true",
+                    help="skip the matvec on a freshly built tree (no recorded ACA ranks)")
     ap.add_argument("--no-plain", action="store_true", help="do not time the plain FP32 form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=6.0,
+                    help="CPU work of one sample step of the CPU baseline / reference arm")
     ap.add_argument("--no-next-rows", action="store_true",
                     help="skip the three-body near-field measurement added to the line")
     return ap.parse_args()
@@ -243,78 +247,118 @@ class TorchCpuNet:
         return y
 
 
-def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
+class CpuSample:
     """The oracle port (numpy restatement of the reference path, the network on torch's CPU path)
-    timed on a bounded sample.
+    on a bounded, fixed sample of one H-matvec: the leading close pairs worth about
+    seconds / 2 of CPU work and the leading ACA blocks worth the other half (chosen once, by a
+    first timed pass). Every step runs exactly that sample; its evaluations per second are
+    extrapolated to the counted evaluations of the whole H-matvec (far evaluations from the
+    sampled mean rank when not given)."""
 
-    Near field: leading close pairs for ~seconds/2 of CPU work; far field: leading ACA
-    blocks for the other half. Evaluations/s of each are extrapolated to the counted
-    evaluations of one full H-matvec (far evaluations from the sampled mean rank when
-    not given).
-    """
-    from oracle import hignn_oracle as O
+    def __init__(self, x, f, eps, seconds, close_evals=None, far_evals=None):
+        from oracle import hignn_oracle as O
 
-    cores = os.cpu_count() or 1
-    net = TorchCpuNet(O.TwoBody.from_hgnw(WEIGHTS), cores)
-    t0 = time.time()
-    tree, rmap = O.build_tree(x, 128)
-    xt = x[rmap]
-    aux = O.compute_aux(tree, xt)
-    ci, cj, fi, fj, _ = O.close_far_lists(tree, aux)
-    t_lists = time.time() - t0
-    ft = f[rmap]
-    sz = tree[:, 3] - tree[:, 2]
-    if close_evals is None:
-        close_evals = int(np.sum(sz[ci] * sz[cj]))
-    done_e, t_near, p = 0, 0.0, 0
-    while t_near < seconds / 2 and p < len(ci):
-        q = min(len(ci), p + 64)
-        t = time.time()
-        O.close_dot(tree, xt, ft, ci[p:q], cj[p:q], net)
-        t_near += time.time() - t
-        done_e += int(np.sum(sz[ci[p:q]] * sz[cj[p:q]]))
-        p = q
-    r_near = done_e / t_near
-    far_e, t_far, b, ranks = 0, 0.0, 0, []
-    while t_far < seconds / 2 and b < len(fi):
-        q = min(len(fi), b + 32)
-        t = time.time()
+        self.O = O
+        self.cores = os.cpu_count() or 1
+        self.net = TorchCpuNet(O.TwoBody.from_hgnw(WEIGHTS), self.cores)
+        self.eps = eps
+        self.n = len(x)
+        t0 = time.time()
+        tree, rmap = O.build_tree(x, 128)
+        self.tree = tree
+        self.xt = x[rmap]
+        aux = O.compute_aux(tree, self.xt)
+        self.ci, self.cj, self.fi, self.fj, _ = O.close_far_lists(tree, aux)
+        self.t_lists = time.time() - t0
+        self.ft = f[rmap]
+        self.sz = tree[:, 3] - tree[:, 2]
+        sz = self.sz
+        self.close_evals = int(np.sum(sz[self.ci] * sz[self.cj])) if close_evals is None else close_evals
+        # choose the sample: leading pairs / blocks until each half of the budget is used
+        p, t_near = 0, 0.0
+        while t_near < seconds / 2 and p < len(self.ci):
+            q = min(len(self.ci), p + 64)
+            t = time.time()
+            O.close_dot(tree, self.xt, self.ft, self.ci[p:q], self.cj[p:q], self.net)
+            t_near += time.time() - t
+            p = q
+        b, t_far, ranks = 0, 0.0, []
+        while t_far < seconds / 2 and b < len(self.fi):
+            q = min(len(self.fi), b + 32)
+            t = time.time()
+            col = []
+            O.far_dot(tree, self.xt, self.ft, self.fi[b:q], self.fj[b:q], self.net, eps, 100, collect=col)
+            t_far += time.time() - t
+            ranks += [c[2] for c in col]
+            b = q
+        self.p, self.b = p, b
+        self.near_sample = int(np.sum(sz[self.ci[:p]] * sz[self.cj[:p]]))
+        if far_evals is None:
+            far_evals = float(np.mean(ranks)) * float(np.sum(sz[self.fi] + sz[self.fj])) if ranks else 0.0
+        self.far_evals = far_evals
+
+    def step(self):
+        """One timed sample step: (seconds, near seconds, far seconds, far evaluations of the sample)."""
+        O, sz = self.O, self.sz
+        t0 = time.time()
+        O.close_dot(self.tree, self.xt, self.ft, self.ci[:self.p], self.cj[:self.p], self.net)
+        t1 = time.time()
         col = []
-        O.far_dot(tree, xt, ft, fi[b:q], fj[b:q], net, eps, 100, collect=col)
-        t_far += time.time() - t
-        far_e += sum(c[2] * (sz[c[0]] + sz[c[1]]) for c in col)
-        ranks += [c[2] for c in col]
-        b = q
-    r_far = far_e / t_far if t_far > 0 else r_near
-    if far_evals is None:
-        far_evals = float(np.mean(ranks)) * float(np.sum(sz[fi] + sz[fj])) if ranks else 0.0
-    t_dot = close_evals / r_near + far_evals / r_far
-    return {"value": len(x) / t_dot, "unit": "particles/s", "cores": cores, "kind": "port",
-            "sample": (f"oracle restatement (numpy) with the two-body network on torch's CPU FP32 path, as the "
-                       f"reference's libtorch, on {cores} host threads: {p} close pairs ({done_e:.3g} evals, "
-                       f"{r_near:.3g} evals/s) and {b} ACA blocks ({far_e:.3g} evals, {r_far:.3g} evals/s), "
-                       f"extrapolated to {close_evals:.3g} near + {far_evals:.3g} far evaluations of one "
-                       f"H-matvec; tree+lists ({t_lists:.1f} s) not counted")}
+        O.far_dot(self.tree, self.xt, self.ft, self.fi[:self.b], self.fj[:self.b], self.net, self.eps, 100, collect=col)
+        t2 = time.time()
+        far_e = sum(c[2] * (sz[c[0]] + sz[c[1]]) for c in col)
+        return t2 - t0, t1 - t0, t2 - t1, far_e
+
+    def estimate(self, t_near, t_far, far_e):
+        r_near = self.near_sample / t_near
+        r_far = far_e / t_far if t_far > 0 else r_near
+        t_dot = self.close_evals / r_near + self.far_evals / r_far
+        return {"value": self.n / t_dot, "unit": "particles/s", "cores": self.cores, "kind": "port",
+                "sample": (f"oracle restatement (numpy) with the two-body network on torch's CPU FP32 path, as the "
+                           f"reference's libtorch, on {self.cores} host threads (nproc {os.cpu_count()}); each step "
+                           f"runs the same sample: {self.p} close pairs ({self.near_sample:.3g} evals, "
+                           f"{r_near:.3g} evals/s) and {self.b} ACA blocks ({far_e:.3g} evals, {r_far:.3g} evals/s), "
+                           f"extrapolated to {self.close_evals:.3g} near + {self.far_evals:.3g} far evaluations of "
+                           f"one H-matvec; tree+lists ({self.t_lists:.1f} s) not counted")}
+
+
+def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
+    """One timed sample step of CpuSample, extrapolated to a whole H-matvec."""
+    cs = CpuSample(x, f, eps, seconds, close_evals, far_evals)
+    _, tn, tf, fe = cs.step()
+    return cs.estimate(tn, tf, fe)
 
 
 def reference_arm(args, rank, world):
-    """The reference algorithm (restated on the CPU, numpy) on the host cores, bounded samples."""
+    """The reference algorithm (restated on the CPU) on the host cores: every step runs the same
+    bounded sample of one H-matvec; ms_per_step is the measured time of that sample, value the
+    sample's rate extrapolated to the whole H-matvec."""
     if rank != 0:
         return 0
     x, f = workload(args.n)
-    vals = []
+    cs = CpuSample(x, f, args.epsilon, args.cpu_sample_seconds)
+    tot, near, far, fe = [], [], [], []
     for k in range(args.warmup + args.steps):
-        s = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds)
+        t, tn, tf, e = cs.step()
         if k >= args.warmup:
-            vals.append(s["value"])
-    v = float(np.mean(vals))
+            tot.append(t)
+            near.append(tn)
+            far.append(tf)
+            fe.append(e)
+    est = cs.estimate(float(np.sum(near)), float(np.sum(far)), float(np.sum(fe)))
+    v = est["value"]
+    frac = (cs.near_sample + float(np.mean(fe))) / (cs.close_evals + cs.far_evals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.n / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(tot)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": args.n, "epsilon": args.epsilon, "parallelism": "host cores"},
-            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": s["cores"], "kind": "port",
-                             "sample": s["sample"]},
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": est["cores"], "kind": "port",
+                             "sample": est["sample"]},
             "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "sample": {"fraction_of_matvec_evals": frac, "seconds_per_step": float(np.mean(tot)),
+                       "extrapolated_ms_per_matvec": 1e3 * args.n / v,
+                       "note": "ms_per_step is the measured time of one sample step; value extrapolates the "
+                               "sample's evaluations per second to the whole H-matvec"},
             "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent; "
                     "not pip-installable); this arm times its restatement on the host cores, the two-body "
                     "network on torch's CPU FP32 path as the reference evaluates it with libtorch"}
@@ -454,12 +498,29 @@ def main():
         e2e_ms = max_over_ranks(float(np.mean(e2e_times)))
     u = u_h.numpy().astype(np.float64)
 
-    # accuracy: dense rows (FP32 network, FP64 accumulation over all N sources)
+    # the reference rebuilds the tree before every product (python/simulate.py:129,
+    # src/HignnModel.cpp:744-762): a product on a freshly built tree has no recorded ACA ranks.
+    # One such product is timed here (same positions, so the same tree), the rebuild apart.
+    unplanned = None
+    if not args.no_unplanned:
+        t0 = time.perf_counter()
+        m.update_coord(x)
+        rebuild_ms = (time.perf_counter() - t0) * 1e3
+        ut, un, uf = timed(m, stream, flush, 1, lambda: step_device(u_d))
+        su = m.stats()
+        ums = max_over_ranks(float(ut[0]))
+        unplanned = {"ms_per_step": ums, "value": n / (ums / 1e3), "near_ms": float(un[0]), "far_ms": float(uf[0]),
+                     "far_iterations": su["far_iterations"], "rebuild_host_ms": rebuild_ms,
+                     "note": "first H-matvec after update_coord: ACA batches without recorded ranks, as every "
+                             "product of the reference's time loop; the host tree rebuild is timed apart"}
+        step_device(u_d)  # ranks recorded again for the forms timed below
+
+    # accuracy: FP64 dense rows on seeded target rows, each summed over all N sources
     rng = np.random.default_rng(12345)
     rows = np.sort(rng.choice(n, size=min(args.check_rows, n), replace=False))
     err = err_plain = None
     t0 = time.time()
-    ud = m.dense_rows(f, rows, 0) if len(rows) and rank == 0 else None
+    ud = m.dense_rows(f, rows, capi.DENSE_F64) if len(rows) and rank == 0 else None
     t_check = time.time() - t0
     if ud is not None:
         err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
@@ -502,7 +563,7 @@ def main():
                      "peak_source": f"bf16_tflops of {src} MEASURED_PEAKS.json",
                      "traffic": NEAR_DRAM_BYTES_PER_PARTICLE * n,
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of k_near_tc in the ncu "
-                                       "capture at N = 131,072 (profiles/k_near_tc_medium_n131k.md), scaled by N",
+                                       "capture at N = 131,072, scaled by N",
                      "algorithmic": f"{FLOP_PER_EVAL} FLOP/eval x {st['close_evals']} evals / near-field time",
                      "mufu": {"achieved_evals_per_s": near_eps, "peak_evals_per_s": mufu_peak,
                               "frac": near_eps / mufu_peak,
@@ -513,7 +574,10 @@ def main():
         "gpu_launches": int(st["gpu_launches"]),
         "clocks": ck,
         "error": {"rel_l2_vs_dense": err, "rows": int(len(rows)), "seconds": t_check,
-                  "oracle": "dense rows on the device, FP32 network, FP64 accumulation over all N sources"},
+                  "oracle": "FP64 dense rows on the device: the two-body network in FP64 (weights promoted "
+                            "from FP32), features and sums in FP64, every row summed over all N sources; "
+                            "rows drawn without replacement, seed 12345"},
+        "unplanned": unplanned,
         "plain_fp32": plain,
         "student": student,
         "breakdown_ms": {"near": float(np.mean(near_ms)), "far": float(np.mean(far_ms)),

@@ -34,6 +34,7 @@ CU_SOURCES = {
     "misc.cu": [],
     "tc_kernels.cu": [],
     "noalloc.cu": [],
+    "dense_f64.cu": [],
     "student.cu": [],
     "step.cu": [],
     "neighbors.cu": [],

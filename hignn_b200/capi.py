@@ -37,6 +37,7 @@ P_FIELDS = 104
 P_RECORD_PIVOTS = 105
 P_FAR_POOL_MB = 106
 P_RANK_HINT_OFFSET = 107
+DENSE_F64 = 64  # hignn_dense_rows precision: the network in FP64
 
 STUDENT_PARAMS = 2537
 
@@ -125,6 +126,7 @@ SIGNATURES = {
     "hignn_tb_velocity_edges": ([_P, _fp, _fp, _fp, C.c_int64, _u64p, C.c_int64, _u64p, C.c_int64], C.c_int),
     "hignn_tb_stats": ([_P, _dp, _dp, _dp, _i64p, _i64p], C.c_int),
     "hignn_tb_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
+    "hignn_near_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
 }
 
 for _name, (_args, _res) in SIGNATURES.items():
@@ -365,6 +367,15 @@ class Model:
     def set_student(self, params):
         p = np.ascontiguousarray(params, np.float32)
         check(lib.hignn_set_student(self._h, fptr(p), p.size))
+
+    def near_wait_profile(self):
+        """Wait cycles of the tensor-core near field by barrier (HIGNN_P_TIMING >= 3), then reset."""
+        c = (C.c_uint64 * 16)()
+        check(lib.hignn_near_wait_profile(self._h, c))
+        names = {0: "mma_a0", 1: "mma_a1", 2: "mma_a2_q0", 3: "mma_d3_free", 4: "mma_a2_q1", 5: "mma_a2_q2",
+                 6: "mma_a0_next", 7: "mma_a2_q3", 8: "epi_d1", 9: "epi_d2", 10: "epi_d3", 11: "epi_a2_free",
+                 12: "epi_total_warp0", 13: "tiles"}
+        return {names[i]: int(c[i]) for i in names}
 
     def get_student(self):
         p = np.empty(STUDENT_PARAMS, np.float32)

@@ -126,7 +126,7 @@ struct hignn_model {
   DevBuf x4, perm, slot, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
   DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
-  DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err;
+  DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err, near_prof;
   hignn::CellList cells;  // neighbour search of the pair forces
   hignn_tb* tb = nullptr;  // three-body near field added to the velocity of the device time loops
   int32_t* host_ctr = nullptr;
@@ -746,7 +746,15 @@ void near_field(hignn_model* m) {
       throw Error(HIGNN_ERR_ARG, "the tensor-core forms (precision 1, 2) need leaves of at most " +
                                      std::to_string(hignn::kTcMaxLeaf) + " particles (block_size <= " +
                                      std::to_string(hignn::kTcMaxLeaf) + ")");
-    hignn::launch_near_tc(a, m->wtc(), m->counter.as<int>(), m->err_flag(), m->num_sms, m->stream);
+    hignn::TcWeights tw = m->wtc();
+    if (m->timing >= 3) {  // wait profile of the engine, accumulated until hignn_near_wait_profile
+      if (!m->near_prof.p) {
+        m->near_prof.ensure(sizeof(unsigned long long) * 16);
+        HIGNN_CUDA(cudaMemsetAsync(m->near_prof.p, 0, sizeof(unsigned long long) * 16, m->stream));
+      }
+      tw.prof = m->near_prof.as<unsigned long long>();
+    }
+    hignn::launch_near_tc(a, tw, m->counter.as<int>(), m->err_flag(), m->num_sms, m->stream);
   }
   else
     hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
@@ -865,6 +873,7 @@ void post_check(hignn_model* m) {
     den += b[i] * b[i];
   }
   std::printf("relative error of the H-matrix product vs the dense product: %.6e\n", std::sqrt(num / den));
+  std::fflush(stdout);
   ud.release();
 }
 
@@ -954,7 +963,7 @@ int hignn_destroy(hignn_model* m) {
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
                       &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos,
-                      &m->dp_k, &m->dp_err})
+                      &m->dp_k, &m->dp_err, &m->near_prof})
       b->release();
     m->cells.release();
     for (auto& e : m->ev)
@@ -1427,7 +1436,8 @@ int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64
                      int precision) {
   return guard([&] {
     if (!m || !u_rows || !f || (!rows && nrows > 0)) throw Error(HIGNN_ERR_ARG, "null argument");
-    if (precision != 0) throw Error(HIGNN_ERR_ARG, "dense_rows on the device supports precision 0 (FP32 network)");
+    if (precision != 0 && precision != HIGNN_DENSE_F64)
+      throw Error(HIGNN_ERR_ARG, "dense_rows: precision must be 0 (FP32 network) or HIGNN_DENSE_F64 (FP64 network)");
     require_device(m);
     require_weights(m);
     ensure_tree(m);
@@ -1475,7 +1485,10 @@ int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64
     a.xJ = m->x4.as<float4>();
     a.fJ = m->f4.as<float4>();
     a.uJ = m->u.as<double>();
-    hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+    if (precision == HIGNN_DENSE_F64)
+      hignn::launch_dense_f64(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
+    else
+      hignn::launch_near_simt(a, m->wdev(), m->counter.as<int>(), m->num_sms, m->stream);
     HIGNN_CUDA(cudaMemcpyAsync(u_rows, m->tmp_u.p, sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, m->stream));
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
   });
@@ -1694,6 +1707,18 @@ int hignn_get_far_pivots(hignn_model* m, int32_t* ranks, int32_t* rows, int32_t*
         if (rows) rows[b * ld + l] = m->piv_rows[b * m->piv_ld + l];
         if (cols) cols[b * ld + l] = m->piv_cols[b * m->piv_ld + l];
       }
+  });
+}
+
+int hignn_near_wait_profile(hignn_model* m, uint64_t* counters) {
+  return guard([&] {
+    if (!m || !counters) throw Error(HIGNN_ERR_ARG, "null argument");
+    std::memset(counters, 0, sizeof(uint64_t) * 16);
+    if (!m->near_prof.p) return;
+    require_device(m);
+    HIGNN_CUDA(cudaMemcpyAsync(counters, m->near_prof.p, sizeof(uint64_t) * 16, cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaMemsetAsync(m->near_prof.p, 0, sizeof(uint64_t) * 16, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
   });
 }
 

@@ -70,6 +70,7 @@ struct TcWeights {
   const uint4* w1img;   // 128 x 64 BF16 slab, K 0-15 = [W_hi, W_hi, W_lo, b1_hi, b1_lo, 0...] (16384 B)
   const float* b2;      // [512]
   const float* b3;      // [9]
+  unsigned long long* prof = nullptr;  // optional wait profile of the engine (tc::kProfSlots counters)
 };
 
 // One unit of near-field (or dense) work: target range I against source range J.

@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF3
           if (r == c)
             dst[3 * r + c] = (double)y[3 * r + c];
           else
-            dst[3 * r + c] = 0.5 * (double)(y[3 * r + c] + y[3 * c + r]);
+            dst[3 * r + c] = 0.5 * (double)__fadd_rn(y[3 * r + c], y[3 * c + r]);
         }
     }
   }

@@ -33,6 +33,8 @@ struct NearArgs {
 
 size_t near_simt_smem_bytes();
 void launch_near_simt(const NearArgs& a, const MlpF32& w, int* work_counter, int num_sms, cudaStream_t s);
+// Dense rows with the network in FP64 (kPairSymmetrize items, I side only; dense_f64.cu).
+void launch_dense_f64(const NearArgs& a, const MlpF32& w, int* work_counter, int num_sms, cudaStream_t s);
 
 // ---------------------------------------------------------------- far field (ACA)
 struct FarBlock {

@@ -1,8 +1,14 @@
 // FP32 SIMT evaluation of the two-body network, 128 evaluations per tile.
 //
-// This is the "plain FP32" form: every layer in FP32 on the CUDA cores with
-// accurate tanhf, the same arithmetic class as the reference's libtorch FP32
-// forward (src/CloseDot.cpp:233). Layer widths 3 -> 128 -> 512 -> 9.
+// This is the "plain FP32" form: every layer in FP32 on the CUDA cores, the same
+// arithmetic class as the reference's libtorch FP32 forward (src/CloseDot.cpp:233).
+// Layer widths 3 -> 128 -> 512 -> 9. Every operation is a single correctly rounded
+// FP32 operation in a fixed order (explicit fused multiply-adds, _rn intrinsics,
+// the tanh of tanh_f32.cuh), so each output is a function of its feature alone:
+//   h1[k] = tanh(fma(W1[k][2], r_z, fma(W1[k][1], r_y, fma(W1[k][0], r_x, b1[k]))))
+//   h2[n] = tanh((sum_k fma(h1[k], W2[n][k], .), k ascending from 0) + b2[n])
+//   y[o]  = (sum_n fma(h2[n], W3[o][n], .), n ascending from 0) + b3[o] (+ 1 on the
+//           diagonal), divided by |r| = sqrt(fma(r_z, r_z, fma(r_y, r_y, r_x r_x))).
 //
 // Tile schedule (256 threads): layer 1 fills h1[k][e]; layer 2 runs in 8
 // chunks of 64 hidden units, each a 128x64x128 register-tiled GEMM (8 evals x
@@ -14,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "common.h"
+#include "tanh_f32.cuh"
 
 namespace hignn {
 namespace simt {
@@ -73,7 +80,7 @@ __device__ __forceinline__ void mlp_tile(Smem& s, const MlpF32& w) {
     const int k = idx / kTile, e = idx % kTile;
     const float4 wk = s.w1b1[k];
     const float4 r = s.r[e];
-    s.h1[k][e] = tanhf(fmaf(wk.z, r.z, fmaf(wk.y, r.y, fmaf(wk.x, r.x, wk.w))));
+    s.h1[k][e] = tanh_f32(__fmaf_rn(wk.z, r.z, __fmaf_rn(wk.y, r.y, __fmaf_rn(wk.x, r.x, wk.w))));
   }
   const int tn = t & 15, te = t >> 4;   // layer-2 micro tile: evals te*8..+8, units tn*4..+4
   const int e3 = t & (kTile - 1), og = t >> 7;  // layer-3 owner: eval e3, outputs og*5..
@@ -99,21 +106,21 @@ __device__ __forceinline__ void mlp_tile(Smem& s, const MlpF32& w) {
 #pragma unroll
       for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < 4; j++) acc[i][j] = __fmaf_rn(av[i], bv[j], acc[i][j]);
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int n = tn * 4 + j;
       const float bias = s.b2[c * kChunk + n];
       float4 v0, v1;
-      v0.x = tanhf(acc[0][j] + bias);
-      v0.y = tanhf(acc[1][j] + bias);
-      v0.z = tanhf(acc[2][j] + bias);
-      v0.w = tanhf(acc[3][j] + bias);
-      v1.x = tanhf(acc[4][j] + bias);
-      v1.y = tanhf(acc[5][j] + bias);
-      v1.z = tanhf(acc[6][j] + bias);
-      v1.w = tanhf(acc[7][j] + bias);
+      v0.x = tanh_f32(__fadd_rn(acc[0][j], bias));
+      v0.y = tanh_f32(__fadd_rn(acc[1][j], bias));
+      v0.z = tanh_f32(__fadd_rn(acc[2][j], bias));
+      v0.w = tanh_f32(__fadd_rn(acc[3][j], bias));
+      v1.x = tanh_f32(__fadd_rn(acc[4][j], bias));
+      v1.y = tanh_f32(__fadd_rn(acc[5][j], bias));
+      v1.z = tanh_f32(__fadd_rn(acc[6][j], bias));
+      v1.w = tanh_f32(__fadd_rn(acc[7][j], bias));
       *reinterpret_cast<float4*>(&s.h2[n][te * 8]) = v0;
       *reinterpret_cast<float4*>(&s.h2[n][te * 8 + 4]) = v1;
     }
@@ -124,17 +131,17 @@ __device__ __forceinline__ void mlp_tile(Smem& s, const MlpF32& w) {
       const float h = s.h2[n][e3];
 #pragma unroll
       for (int o = 0; o < 5; o++)
-        if (o < on) y3[o] = fmaf(h, s.w3[o0 + o][c * kChunk + n], y3[o]);
+        if (o < on) y3[o] = __fmaf_rn(h, s.w3[o0 + o][c * kChunk + n], y3[o]);
     }
   }
   // wrapper of python/convert.py:11-20: (y + b3 + I) / |r|, identity for |r| < 1e-5
   const float4 r = s.r[e3];
-  const float nr = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
+  const float nr = __fsqrt_rn(__fmaf_rn(r.z, r.z, __fmaf_rn(r.y, r.y, __fmul_rn(r.x, r.x))));
   for (int o = 0; o < on; o++) {
     const int oo = o0 + o;
-    float v = y3[o] + s.b3[oo];
-    if (oo == 0 || oo == 4 || oo == 8) v += 1.0f;
-    v = v / nr;
+    float v = __fadd_rn(y3[o], s.b3[oo]);
+    if (oo == 0 || oo == 4 || oo == 8) v = __fadd_rn(v, 1.0f);
+    v = __fdiv_rn(v, nr);
     if (nr < 1e-5f) v = (oo == 0 || oo == 4 || oo == 8) ? 1.0f : 0.0f;
     s.y[e3][oo] = v;
   }

@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (lane == 0) tc::mma_loop(S.tcs, err);
     __syncwarp();
   } else {
+    const long long t_start = clock64();
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
     NearTile prev{}, cur{};
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
                                                  [&](float (&M)[9]) { near_use(S, prev, p, M); })))
       near_flush(S, a, prev);
+    if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[12] += (unsigned long long)(clock64() - t_start);
   }
   tc::cta_teardown(S.tcs);
 }

@@ -66,6 +66,11 @@ constexpr int kW3Rows = 32;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 32768
 constexpr int kW1Bytes = kH1 * 64 * 2;       // 16384: 128 rows x one 64-wide K slab (K 0-15 used)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+// Wait profile (TcWeights::prof non-null): slot c - 13 sums the cycles that lane 0 of every warp
+// spent in bounded waits with code c (13-20 the MMA lane, 21-24 the epilogue warps: 21 layer-1
+// accumulator, 22 layer-2 accumulator, 23 layer-3 accumulator, 24 A2 buffer free); slot 12 the
+// cycles of warp 0's whole epilogue; slot 13 the tiles processed.
+constexpr int kProfSlots = 16;
 
 struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
@@ -75,6 +80,8 @@ struct alignas(1024) Smem {
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
+  unsigned long long* prof;          // optional wait profile (global, kProfSlots counters) or null
+  unsigned long long wprof[16];      // per-CTA wait cycles by barrier code (lane 0 of each warp)
   alignas(16) float b2[kH2];  // FP32 layer-2 bias, added before rounding to BF16
   float b3[16];
 };
@@ -244,7 +251,9 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   for (int i = t; i < kW1Bytes / 16; i += blockDim.x) dst1[i] = src1[i];
   for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
+  if (t < 16) s.wprof[t] = 0ull;
   if (t == 0) {
+    s.prof = w.prof;
     mbar_init(&s.a0_full, kEpiThreads);
     mbar_init(&s.d1_full, 1);
     mbar_init(&s.a1_full, kEpiThreads);
@@ -273,6 +282,7 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
   fence_before();
   __syncthreads();
   fence_after();
+  if (s.prof && threadIdx.x < kProfSlots) atomicAdd(&s.prof[threadIdx.x], s.wprof[threadIdx.x]);
   if ((threadIdx.x >> 5) == kMmaWarp) tmem_dealloc(s.tmem_base, 512);
 }
 
@@ -300,7 +310,9 @@ struct MmaLane {
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
     if (!ok) return false;
+    const long long t0 = s.prof ? clock64() : 0;
     ok = mbar_wait(b, parity, &s.abort_flag, err, code);
+    if (s.prof) atomicAdd(&s.wprof[code - 13], (unsigned long long)(clock64() - t0));
     if (ok) fence_after();
     return ok;
   }
@@ -422,7 +434,10 @@ struct Epi {
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
     if (!ok) return false;
+    const bool rec = s.prof && (threadIdx.x & 31) == 0;
+    const long long t0 = rec ? clock64() : 0;
     ok = mbar_wait(b, parity, &s.abort_flag, err, code);
+    if (rec) atomicAdd(&s.wprof[code - 13], (unsigned long long)(clock64() - t0));
     if (ok) fence_after();
     return ok;
   }
@@ -495,6 +510,7 @@ struct Epi {
     }
     fence_before();
     mbar_arrive(&s.a1_full);
+    if (s.prof && threadIdx.x == 0) s.wprof[13]++;
     if (tile > 0) {  // retire the previous tile while L2(tile, 0) runs on the tensor cores
       float M[9];
       if (!read_d3(tile - 1, px, py, pz, M)) return false;

@@ -34,7 +34,8 @@ def main():
     ap.add_argument("--workload", default="medium", choices=["small", "medium", "large", "uniform1m", "uniform4m"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--epsilon", type=float, default=1e-2)
-    ap.add_argument("--timing", type=int, default=2, help="2 = far-field breakdown by kernel category")
+    ap.add_argument("--timing", type=int, default=2,
+                    help="2 = far-field breakdown by kernel category, 3 = also the near-field wait profile")
     ap.add_argument("--pool-mb", type=int, default=0, help="ACA pool memory per batch (0: the default)")
     ap.add_argument("--student-steps", type=int, default=4000, help="training steps when --precision 2")
     ap.add_argument("--student-batch", type=int, default=16384)
@@ -108,6 +109,8 @@ def main():
             m.set(capi.P_STUDENT_TOL, a.student_tol[-1])
         m.dot(f)
         first = m.stats()
+        if a.timing >= 3:
+            m.near_wait_profile()  # reset: the profile below covers the timed repetitions only
         near, far = [], []
         for _ in range(a.reps):
             m.dot(f)
@@ -115,6 +118,8 @@ def main():
             near.append(st["t_close_ms"])
             far.append(st["t_far_ms"])
         st = m.stats()
+        if a.timing >= 3 and a.precision >= 1:
+            out["near_wait_profile"] = m.near_wait_profile()
         out["first_far_ms"] = first["t_far_ms"]
         out["first_far_iterations"] = first["far_iterations"]
         out.update(workload=a.workload, n=len(x), near_ms=float(np.min(near)), far_ms=float(np.min(far)),

@@ -179,10 +179,13 @@ int hignn_dot_device(hignn_model* m, float* d_u, const float* d_f, int64_t n);
  * FP64 accumulation. Host pointers. */
 int hignn_dense_dot(hignn_model* m, float* u, const float* f, int64_t n);
 
-/* Dense rows for accuracy checks: for each listed target row (caller's order)
- * u_row = sum over all j of 0.5 (M + M^T)(x_j - x_row) f_j, accumulated in FP64.
- * precision 0 (FP32 network) is the only one on the device. Host pointers; u_rows is (nrows, 3);
- * rows may repeat. */
+/* Dense rows for accuracy checks (PostCheckDot, src/PostCheckDot.cpp:351-376, on chosen rows):
+ * for each listed target row (caller's order) u_row = sum over all j of
+ * 0.5 (M + M^T)(x_j - x_row) f_j, accumulated in FP64. precision 0: the FP32 network;
+ * HIGNN_DENSE_F64: the network in FP64 (weights promoted from FP32, features x_j - x_row
+ * in FP64) -- the FP64 dense evaluation the H-matrix error is stated against. Host
+ * pointers; u_rows is (nrows, 3); rows may repeat. */
+#define HIGNN_DENSE_F64 64
 int hignn_dense_rows(hignn_model* m, double* u_rows, const float* f, const int64_t* rows, int64_t nrows,
                      int precision);
 
@@ -367,6 +370,13 @@ int hignn_set_three_body(hignn_model* m, hignn_tb* t);
  * clocks the MMA lane waited for layer-1 operands, weight stages, layer-2 epilogues and the
  * layer-3 accumulator; its total clocks; clocks the producer waited for free weight slots. */
 int hignn_tb_wait_profile(hignn_tb* t, uint64_t* counters);
+
+/* Wait profile of the tensor-core near field (no counterpart in the reference; a tuning aid),
+ * accumulated over the near fields run with HIGNN_P_TIMING >= 3 since the last call, then reset.
+ * counters[16]: [c - 13] cycles that lane 0 of every warp spent in bounded waits with code c
+ * (13-20 the MMA lane; 21 layer-1, 22 layer-2, 23 layer-3 accumulator, 24 A2 buffer free),
+ * [12] cycles of one epilogue warp's whole run summed over CTAs, [13] tiles. */
+int hignn_near_wait_profile(hignn_model* m, uint64_t* counters);
 
 #ifdef __cplusplus
 }

@@ -134,6 +134,60 @@ class TwoBody:
         return self._chunked(r, fn, np.float64)
 
 
+class TwoBodyF32Exact(TwoBody):
+    """TwoBody whose FP32 evaluation is the C restatement (oracle/twobody_f32.c) of the plain
+    device network: the same correctly rounded FP32 operations in the same order and the same
+    tanh, so its outputs equal the device's bit for bit. The FP64 evaluation is TwoBody's."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            import ctypes
+
+            import importlib
+
+            build = importlib.import_module("oracle.build")
+            path = build.build()
+            lib = ctypes.CDLL(path)
+            fp = ctypes.POINTER(ctypes.c_float)
+            lib.oracle_twobody_eval32.argtypes = [fp] * 7 + [ctypes.c_int64, fp, ctypes.c_int]
+            lib.oracle_twobody_eval32.restype = None
+            lib.oracle_tanh_f32.argtypes = [fp, ctypes.c_int64, fp]
+            lib.oracle_tanh_f32.restype = None
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, weights, biases, threads=None):
+        super().__init__(weights, biases)
+        self.threads = threads or os.cpu_count() or 1
+
+    def eval32(self, r):
+        import ctypes
+
+        fp = ctypes.POINTER(ctypes.c_float)
+        r = np.ascontiguousarray(r, np.float32)
+        y = np.empty((r.shape[0], 9), np.float32)
+        w = [np.ascontiguousarray(a, np.float32) for a in (self.w32[0], self.b32[0], self.w32[1], self.b32[1],
+                                                           self.w32[2], self.b32[2])]
+        if r.shape[0]:
+            self.lib().oracle_twobody_eval32(*[a.ctypes.data_as(fp) for a in w], r.ctypes.data_as(fp), r.shape[0],
+                                             y.ctypes.data_as(fp), int(self.threads))
+        return y
+
+
+def tanh_f32_exact(x):
+    """The plain form's FP32 tanh (oracle/twobody_f32.c) on an array."""
+    import ctypes
+
+    fp = ctypes.POINTER(ctypes.c_float)
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.empty_like(x)
+    TwoBodyF32Exact.lib().oracle_tanh_f32(x.ctypes.data_as(fp), x.size, t.ctypes.data_as(fp))
+    return t
+
+
 def symmetrize_f32(y32):
     """Far-field block symmetrisation, src/FarDot.cpp:445-456: diag copied, off-diag 0.5*(a+b).
 

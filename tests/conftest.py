@@ -24,6 +24,14 @@ def oracle_net():
 
 
 @pytest.fixture(scope="session")
+def oracle_net_exact():
+    """The oracle network whose FP32 evaluation reproduces the plain device network bit for bit."""
+    from oracle import hignn_oracle as O
+
+    return O.TwoBodyF32Exact.from_hgnw(WEIGHTS)
+
+
+@pytest.fixture(scope="session")
 def small_workload():
     from hignn_b200 import synthetic as S
 

@@ -23,3 +23,6 @@ def test_reference_arm_prints_one_contract_line():
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["config"]["n"] == 8192
+    # ms_per_step is the measured sample step, not an extrapolation: steps x ms_per_step fits the run
+    assert 0 < line["ms_per_step"] < 60e3
+    assert 0 < line["sample"]["fraction_of_matvec_evals"] <= 1.0
