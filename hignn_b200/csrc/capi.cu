@@ -32,6 +32,7 @@
 #include "neighbors.h"
 #include "three_body.h"
 #include "tree.h"
+#include "tree_dev.h"
 
 using hignn::Error;
 
@@ -128,6 +129,9 @@ struct hignn_model {
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err, near_prof;
   hignn::CellList cells;  // neighbour search of the pair forces
+  bool tree_on_device = true;     // HIGNN_P_TREE_DEVICE
+  bool tree_built_on_device = false;
+  hignn::TreeDevScratch tree_dev;
   hignn_tb* tb = nullptr;  // three-body near field added to the velocity of the device time loops
   int32_t* host_ctr = nullptr;
 
@@ -193,7 +197,18 @@ void build_structures(hignn_model* m) {
   m->plan_ready = false;
   m->hint_valid = false;
   m->shard_ready = false;
-  hignn::ClusterTree tree = hignn::build_tree(m->xyz.data(), m->n, m->block_size, host_threads());
+  const bool on_dev = m->device >= 0 && m->tree_on_device;
+  hignn::ClusterTree tree;
+  if (on_dev) {
+    HIGNN_CUDA(cudaSetDevice(m->device));
+    m->tree_dev.xyz.ensure(sizeof(float) * 3 * m->n);
+    HIGNN_CUDA(cudaMemcpyAsync(m->tree_dev.xyz.p, m->xyz.data(), sizeof(float) * 3 * m->n, cudaMemcpyHostToDevice,
+                               m->stream));
+    tree = hignn::build_tree_device(m->tree_dev.xyz.as<float>(), m->n, m->block_size, m->tree_dev, m->stream);
+  } else {
+    tree = hignn::build_tree(m->xyz.data(), m->n, m->block_size, host_threads());
+  }
+  m->tree_built_on_device = on_dev;
   std::vector<float> xt(3 * m->n);
   std::vector<int64_t> inv_perm(m->n);
   for (int64_t i = 0; i < m->n; i++) {
@@ -203,8 +218,10 @@ void build_structures(hignn_model* m) {
     xt[3 * i + 2] = m->xyz[3 * p + 2];
     inv_perm[p] = i;
   }
-  hignn::BlockLists lists =
-      hignn::build_lists(tree, xt.data(), m->max_relative_coord, m->use_symmetry, host_threads());
+  hignn::BlockLists lists;
+  if (!on_dev || !hignn::build_lists_device(tree, m->tree_dev.xt.as<float4>(), m->max_relative_coord,
+                                            m->use_symmetry, m->tree_dev, m->stream, lists))
+    lists = hignn::build_lists(tree, xt.data(), m->max_relative_coord, m->use_symmetry, host_threads());
   if (m->device >= 0)
     for (int64_t L : lists.leaves) {
       const int64_t sz = tree.nodes[L].end - tree.nodes[L].start;
@@ -270,8 +287,14 @@ void build_structures(hignn_model* m) {
   m->close_work.ensure(sizeof(hignn::PairWork) * std::max<size_t>(1, work.size()));
   m->counter.ensure(64);
   HIGNN_CUDA(cudaMemcpyAsync(m->slot.p, slot.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
-  HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
-  HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
+  if (on_dev) {  // tree-order positions and the permutation are already on the device
+    HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, m->tree_dev.xt.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, m->tree_dev.perm.p, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice,
+                               m->stream));
+  } else {
+    HIGNN_CUDA(cudaMemcpyAsync(m->x4.p, x4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(m->perm.p, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, m->stream));
+  }
   if (!work.empty())
     HIGNN_CUDA(cudaMemcpyAsync(m->close_work.p, work.data(), sizeof(hignn::PairWork) * work.size(),
                                cudaMemcpyHostToDevice, m->stream));
@@ -966,6 +989,7 @@ int hignn_destroy(hignn_model* m) {
                       &m->dp_k, &m->dp_err, &m->near_prof})
       b->release();
     m->cells.release();
+    m->tree_dev.release();
     for (auto& e : m->ev)
       if (e) cudaEventDestroy(e);
     if (m->host_ctr) cudaFreeHost(m->host_ctr);
@@ -1100,6 +1124,10 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         m->fields = (int)v;
         break;
       case HIGNN_P_RECORD_PIVOTS: m->record_pivots = v != 0; break;
+      case HIGNN_P_TREE_DEVICE:
+        if ((v != 0) != m->tree_on_device) m->tree_ready = false;  // rebuilt by the chosen builder
+        m->tree_on_device = v != 0;
+        break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });
@@ -1126,6 +1154,7 @@ int hignn_get_param(hignn_model* m, int key, double* v) {
       case HIGNN_P_STUDENT_TOL: *v = m->student_tol; break;
       case HIGNN_P_FIELDS: *v = m->fields; break;
       case HIGNN_P_RECORD_PIVOTS: *v = m->record_pivots; break;
+      case HIGNN_P_TREE_DEVICE: *v = m->tree_on_device; break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });

@@ -12,6 +12,7 @@
 // uses Eigen's JacobiSVD, whose sign is implementation-defined); the sort by
 // projection is stable (the reference's std::sort is not).
 #include "tree.h"
+#include "tree_math.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -26,62 +27,7 @@
 
 namespace hignn {
 
-void jacobi_dominant_axis(const double cov[3][3], double u[3]) {
-  double a[3][3], v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) a[i][j] = cov[i][j];
-  static const int P[3] = {0, 0, 1}, Q[3] = {1, 2, 2};
-  for (int sweep = 0; sweep < 50; sweep++) {
-    double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
-    double diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
-    if (off <= 1e-36 * diag || off == 0.0) break;
-    for (int r = 0; r < 3; r++) {
-      const int p = P[r], q = Q[r];
-      double apq = a[p][q];
-      if (apq == 0.0) continue;
-      double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
-      double t = 1.0 / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-      if (theta < 0.0) t = -t;
-      double c = 1.0 / std::sqrt(t * t + 1.0);
-      double s = t * c;
-      for (int k = 0; k < 3; k++) {
-        double akp = a[k][p], akq = a[k][q];
-        a[k][p] = c * akp - s * akq;
-        a[k][q] = s * akp + c * akq;
-      }
-      for (int k = 0; k < 3; k++) {
-        double apk = a[p][k], aqk = a[q][k];
-        a[p][k] = c * apk - s * aqk;
-        a[q][k] = s * apk + c * aqk;
-      }
-      for (int k = 0; k < 3; k++) {
-        double vkp = v[k][p], vkq = v[k][q];
-        v[k][p] = c * vkp - s * vkq;
-        v[k][q] = s * vkp + c * vkq;
-      }
-    }
-  }
-  int best = 0;
-  for (int k = 1; k < 3; k++)
-    if (a[k][k] > a[best][best]) best = k;
-  for (int k = 0; k < 3; k++) u[k] = v[k][best];
-  int big = 0;
-  for (int k = 1; k < 3; k++)
-    if (std::fabs(u[k]) > std::fabs(u[big])) big = k;
-  if (u[big] < 0.0)
-    for (int k = 0; k < 3; k++) u[k] = -u[k];
-}
-
 namespace {
-
-// Order-preserving unsigned image of a finite float; -0.0 and +0.0 share one image, as they
-// compare equal under operator<.
-inline uint32_t float_key(float f) {
-  uint32_t u;
-  if (f == 0.0f) f = 0.0f;
-  std::memcpy(&u, &f, 4);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
 
 // Scratch of one thread's divisions, allocated once per tree build (fresh allocations of the
 // top nodes' sizes at every division cost more in first-touch page faults than the work).
@@ -157,12 +103,20 @@ constexpr int64_t kParallelSortMin = int64_t(1) << 18;
 // HignnModel::Divide: returns the split index (first position with t > 0).
 int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last, int sort_threads, DivideScratch& s) {
   const int64_t L = last - first;
+  // the mean: blocks of kSumBlock consecutive particles summed sequentially, then the block sums
   float mean[3] = {0.f, 0.f, 0.f};
-  for (int64_t i = first; i < last; i++) {
-    const float* p = xyz + 3 * perm[i];
-    mean[0] += p[0];
-    mean[1] += p[1];
-    mean[2] += p[2];
+  for (int64_t b0 = first; b0 < last; b0 += kSumBlock) {
+    const int64_t b1 = std::min(last, b0 + kSumBlock);
+    float bs[3] = {0.f, 0.f, 0.f};
+    for (int64_t i = b0; i < b1; i++) {
+      const float* p = xyz + 3 * perm[i];
+      bs[0] += p[0];
+      bs[1] += p[1];
+      bs[2] += p[2];
+    }
+    mean[0] += bs[0];
+    mean[1] += bs[1];
+    mean[2] += bs[2];
   }
   for (int d = 0; d < 3; d++) mean[d] /= (float)L;
   std::vector<float>& vh = s.vh;
@@ -176,16 +130,26 @@ int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last, int
     q[2] = p[2] - mean[2];
   }
   {
-    // six sums in one pass; each is still accumulated in index order
+    // six sums, blocked as the mean: sequential within each block, then over the block sums
     double s00 = 0.0, s01 = 0.0, s02 = 0.0, s11 = 0.0, s12 = 0.0, s22 = 0.0;
-    for (int64_t i = 0; i < L; i++) {
-      const double x = vh[3 * i], y = vh[3 * i + 1], z = vh[3 * i + 2];
-      s00 += x * x;
-      s01 += x * y;
-      s02 += x * z;
-      s11 += y * y;
-      s12 += y * z;
-      s22 += z * z;
+    for (int64_t b0 = 0; b0 < L; b0 += kSumBlock) {
+      const int64_t b1 = std::min(L, b0 + kSumBlock);
+      double t00 = 0.0, t01 = 0.0, t02 = 0.0, t11 = 0.0, t12 = 0.0, t22 = 0.0;
+      for (int64_t i = b0; i < b1; i++) {
+        const double x = vh[3 * i], y = vh[3 * i + 1], z = vh[3 * i + 2];
+        t00 += x * x;
+        t01 += x * y;
+        t02 += x * z;
+        t11 += y * y;
+        t12 += y * z;
+        t22 += z * z;
+      }
+      s00 += t00;
+      s01 += t01;
+      s02 += t02;
+      s11 += t11;
+      s12 += t12;
+      s22 += t22;
     }
     cov[0][0] = s00;
     cov[0][1] = cov[1][0] = s01;
@@ -199,10 +163,7 @@ int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last, int
   const float u0 = (float)ud[0], u1 = (float)ud[1], u2 = (float)ud[2];
   auto project = [&](int64_t i) {
     const float* q = &vh[3 * i];
-    float t = u0 * q[0];
-    t = t + u1 * q[1];
-    t = t + u2 * q[2];
-    return t;
+    return project_axis(u0, u1, u2, q[0], q[1], q[2]);
   };
   // upper_bound(t, 0) over the sorted projections: first position with t strictly above zero
   auto first_positive = [L](auto&& sorted_t) {
@@ -249,87 +210,26 @@ int64_t divide(const float* xyz, int64_t* perm, int64_t first, int64_t last, int
   return split + first;
 }
 
-// The reference treats a split index of 0 as a leaf (src/Build.cpp:71,160). An
-// empty child (coincident points) would make it recurse forever; a leaf here.
-inline bool split_ok(int64_t d, int64_t first, int64_t last) {
-  return d != 0 && d != first && d != last;
-}
-
 }  // namespace
 
 ClusterTree build_tree(const float* xyz, int64_t n, int64_t leaf, int num_threads) {
   ClusterTree t;
   t.perm.resize(n);
   std::iota(t.perm.begin(), t.perm.end(), (int64_t)0);
-  // Sequential stage (src/Build.cpp:38-97): one rank => initialLevel 0, the root is divided once.
-  TreeNode init[3] = {{0, 0, 0, n, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
   std::vector<DivideScratch> scratch((size_t)std::max(1, num_threads));
-  if (n > leaf) {
-    int64_t d = divide(xyz, t.perm.data(), 0, n, num_threads, scratch[0]);
-    if (split_ok(d, 0, n)) {
-      init[0].child0 = 1;
-      init[0].child1 = 2;
-      init[1] = {0, 0, 0, d, 1};
-      init[2] = {0, 0, d, n, 1};
-    }
-  }
-  // Parallel stage (src/Build.cpp:108-180): the local tree restarts from node 0 and
-  // divides it again; children are numbered in BFS order.
-  std::vector<TreeNode> local;
-  local.push_back(init[0]);
-  std::vector<int64_t> frontier{0};
-  while (!frontier.empty()) {
-    const int64_t m = (int64_t)frontier.size();
-    std::vector<int64_t> split(m, 0);
+  t.nodes = build_tree_rows(n, leaf, [&](const std::vector<NodeRange>& rg, std::vector<int64_t>& split) {
+    const int64_t m = (int64_t)rg.size();
+    split.assign(m, 0);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads) if (m > 1)
     for (int64_t i = 0; i < m; i++) {
-      const TreeNode nd = local[frontier[i]];
 #ifdef _OPENMP
       DivideScratch& sc = scratch[omp_in_parallel() ? omp_get_thread_num() : 0];
 #else
       DivideScratch& sc = scratch[0];
 #endif
-      split[i] = (nd.end - nd.start > leaf) ? divide(xyz, t.perm.data(), nd.start, nd.end, num_threads, sc) : 0;
+      split[i] = divide(xyz, t.perm.data(), rg[i].start, rg[i].end, num_threads, sc);
     }
-    std::vector<int64_t> next;
-    for (int64_t i = 0; i < m; i++) {
-      const int64_t node = frontier[i];
-      TreeNode nd = local[node];
-      if (!split_ok(split[i], nd.start, nd.end)) {
-        local[node].child0 = local[node].child1 = 0;
-        continue;
-      }
-      const int64_t c0 = (int64_t)local.size();
-      local.push_back({0, 0, nd.start, split[i], nd.level + 1});
-      local.push_back({0, 0, split[i], nd.end, nd.level + 1});
-      local[node].child0 = c0;
-      local[node].child1 = c0 + 1;
-      next.push_back(c0);
-      next.push_back(c0 + 1);
-    }
-    frontier.swap(next);
-  }
-  const int64_t nloc = (int64_t)local.size() - 1;
-  if (nloc == 0) {
-    // N <= leaf: the reference points the root at rows 3, 4 of a 3-row tree
-    // (src/Build.cpp:239-240); here the root is a single leaf.
-    t.nodes.push_back({0, 0, 0, n, 0});
-    return t;
-  }
-  // Merge (src/Build.cpp:199-247): rows 0..2 from the sequential stage, local nodes from row 3
-  // with child ids shifted by +2, root re-pointed at rows 3, 4 (rows 1, 2 become orphans).
-  t.nodes.resize(nloc + 3);
-  for (int i = 0; i < 3; i++) t.nodes[i] = init[i];
-  for (int64_t i = 0; i < nloc; i++) {
-    TreeNode r = local[i + 1];
-    if (r.child0 != 0) {
-      r.child0 += 2;
-      r.child1 += 2;
-    }
-    t.nodes[3 + i] = r;
-  }
-  t.nodes[0].child0 = 3;
-  t.nodes[0].child1 = 4;
+  });
   return t;
 }
 

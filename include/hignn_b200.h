@@ -55,8 +55,10 @@ enum hignn_param {
   HIGNN_P_FIELDS = 104,          /* bit 0 = near field, bit 1 = far field (default 3), for diagnostics */
   HIGNN_P_RECORD_PIVOTS = 105,   /* 1 = keep every far block's ACA rank and pivots (hignn_get_far_pivots) */
   HIGNN_P_FAR_POOL_MB = 106,     /* C + Q pool memory of one ACA batch in MiB, default 24576, at most 1<<24 */
-  HIGNN_P_RANK_HINT_OFFSET = 107 /* added to the recorded ACA ranks when planning (default 0; a
+  HIGNN_P_RANK_HINT_OFFSET = 107, /* added to the recorded ACA ranks when planning (default 0; a
                                     negative value exercises the deferral path in tests)        */
+  HIGNN_P_TREE_DEVICE = 108       /* 1 (default on a device model) = build the cluster tree on the
+                                     device, 0 = on the host; both give the same tree and lists */
 };
 
 typedef struct hignn_stats {

@@ -258,23 +258,46 @@ def jacobi_dominant_axis(cov):
     return u
 
 
+SUM_BLOCK = 256
+
+
+def _blocked_sum(v, dtype):
+    """Column sums of v (L, k): each block of SUM_BLOCK consecutive rows is summed sequentially
+    from zero in ``dtype``, then the block sums are summed sequentially from zero."""
+    v = np.asarray(v, dtype)
+    L = v.shape[0]
+    nfull = L // SUM_BLOCK
+    parts = []
+    if nfull:
+        parts.append(np.cumsum(v[:nfull * SUM_BLOCK].reshape(nfull, SUM_BLOCK, -1), axis=1, dtype=dtype)[:, -1])
+    if L > nfull * SUM_BLOCK:
+        parts.append(np.cumsum(v[nfull * SUM_BLOCK:], axis=0, dtype=dtype)[-1:])
+    blocks = np.concatenate(parts, axis=0)
+    return np.cumsum(blocks, axis=0, dtype=dtype)[-1]
+
+
 def divide(coords, rmap, first, last):
     """Split [first,last) of ``rmap`` at the mean along the principal axis; returns the split index.
 
-    src/HignnModel.cpp:125-197: float mean (sequential sum in map order), centred
-    float coordinates, principal axis, float projection t_i, sort by t, split at
-    upper_bound(t, 0), i.e. the left child is {t <= 0}.
+    src/HignnModel.cpp:125-197: float mean (sum in map order), centred float coordinates,
+    principal axis, float projection t_i, sort by t, split at upper_bound(t, 0), i.e. the
+    left child is {t <= 0}. The reference sums the mean sequentially; here the mean and the
+    covariance sums run in blocks of SUM_BLOCK consecutive particles (see _blocked_sum), so a
+    parallel device build forms the same values.
     """
     L = last - first
     pts = coords[rmap[first:last]]  # float32 (L,3)
-    mean = (np.cumsum(pts, axis=0, dtype=np.float32)[-1] / np.float32(L)).astype(np.float32)
+    mean = (_blocked_sum(pts, np.float32) / np.float32(L)).astype(np.float32)
     vh = (pts - mean).astype(np.float32)
     vh64 = vh.astype(np.float64)
     cov = [[0.0] * 3 for _ in range(3)]
+    prods = np.stack([vh64[:, i] * vh64[:, j] for i in range(3) for j in range(i, 3)], axis=1)
+    sums = _blocked_sum(prods, np.float64)
+    q = 0
     for i in range(3):
         for j in range(i, 3):
-            cov[i][j] = float(np.cumsum(vh64[:, i] * vh64[:, j])[-1])
-            cov[j][i] = cov[i][j]
+            cov[i][j] = cov[j][i] = float(sums[q])
+            q += 1
     u = np.array(jacobi_dominant_axis(cov), np.float64).astype(np.float32)
     t = (u[0] * vh[:, 0]).astype(np.float32)
     t = (t + (u[1] * vh[:, 1]).astype(np.float32)).astype(np.float32)
