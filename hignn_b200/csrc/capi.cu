@@ -129,6 +129,14 @@ struct hignn_model {
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err, near_prof;
   hignn::CellList cells;  // neighbour search of the pair forces
+  // CUDA graph of the rank-planned H-matvec (HIGNN_P_GRAPH): captured once per plan and buffer
+  // layout, replayed by every later product on the same tree and settings
+  bool use_graph = true;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t graph_sig = 0;
+  int64_t graph_kernels = 0;
+  int graph_iters = 0;
+  DevBuf far_status;  // graph form: status[8], then the lists of blocks to rerun
   bool tree_on_device = true;     // HIGNN_P_TREE_DEVICE
   bool tree_built_on_device = false;
   hignn::TreeDevScratch tree_dev;
@@ -586,6 +594,37 @@ struct FarOutcome {
 // student network, each converged block applied only after its sampled residual against the
 // teacher passed (student_tol); otherwise queries by the teacher (tensor cores from precision 1
 // on, FP32 SIMT at precision 0).
+// Kernel arguments of ACA batch bt (device block table at d_blocks).
+hignn::FarArgs far_args(hignn_model* m, const hignn_model::Batch& bt, const hignn::FarBlock* d_blocks,
+                      bool student_pass) {
+  hignn::FarArgs a{};
+  a.blocks = d_blocks + bt.b0;
+  a.nb = bt.b1 - bt.b0;
+  a.state = m->far_state.as<hignn::FarState>();
+  a.rows = m->far_rows.as<int32_t>();
+  a.cols = m->far_cols.as<int32_t>();
+  a.ldr = m->max_iter + 1;
+  a.usedRow = m->far_used_row.as<uint8_t>();
+  a.usedCol = m->far_used_col.as<uint8_t>();
+  a.C = m->far_C.as<hignn::pool_t>();
+  a.Q = m->far_Q.as<hignn::pool_t>();
+  a.act = m->far_act.as<int32_t>();
+  a.preI = m->far_preI.as<int32_t>();
+  a.preJ = m->far_preJ.as<int32_t>();
+  a.ctr = m->far_ctr.as<int32_t>();
+  a.rank_sum = m->far_stats.as<unsigned long long>();
+  a.evals = m->far_stats.as<unsigned long long>() + 1;
+  a.rank_out = m->far_rank.as<int32_t>();
+  a.x = m->x4.as<float4>();
+  a.f = m->f4.as<float4>();
+  a.u = m->u.as<double>();
+  a.max_iter = m->max_iter;
+  a.eps2 = m->epsilon * m->epsilon;
+  a.use_symmetry = m->use_symmetry ? 1 : 0;
+  a.defer_apply = student_pass ? 1 : 0;
+  return a;
+}
+
 FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& plan,
                            const std::vector<hignn_model::Batch>& batches, const hignn::FarBlock* d_blocks,
                            bool student_pass, int* iterations) {
@@ -595,31 +634,7 @@ FarOutcome run_far_batches(hignn_model* m, const std::vector<hignn::FarBlock>& p
   FarOutcome out;
   std::vector<int>& deferred = out.deferred;
   for (const auto& bt : batches) {
-    hignn::FarArgs a{};
-    a.blocks = d_blocks + bt.b0;
-    a.nb = bt.b1 - bt.b0;
-    a.state = m->far_state.as<hignn::FarState>();
-    a.rows = m->far_rows.as<int32_t>();
-    a.cols = m->far_cols.as<int32_t>();
-    a.ldr = m->max_iter + 1;
-    a.usedRow = m->far_used_row.as<uint8_t>();
-    a.usedCol = m->far_used_col.as<uint8_t>();
-    a.C = m->far_C.as<hignn::pool_t>();
-    a.Q = m->far_Q.as<hignn::pool_t>();
-    a.act = m->far_act.as<int32_t>();
-    a.preI = m->far_preI.as<int32_t>();
-    a.preJ = m->far_preJ.as<int32_t>();
-    a.ctr = m->far_ctr.as<int32_t>();
-    a.rank_sum = m->far_stats.as<unsigned long long>();
-    a.evals = m->far_stats.as<unsigned long long>() + 1;
-    a.rank_out = m->far_rank.as<int32_t>();
-    a.x = m->x4.as<float4>();
-    a.f = m->f4.as<float4>();
-    a.u = m->u.as<double>();
-    a.max_iter = m->max_iter;
-    a.eps2 = m->epsilon * m->epsilon;
-    a.use_symmetry = m->use_symmetry ? 1 : 0;
-    a.defer_apply = student_pass ? 1 : 0;
+    const hignn::FarArgs a = far_args(m, bt, d_blocks, student_pass);
     const auto& last = plan[bt.b1 - 1];
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
@@ -837,7 +852,227 @@ void download_positions(hignn_model* m) {
   }
 }
 
+// ---------------------------------------------------------------- graph form of the planned matvec
+// The rank-planned H-matvec (every far block's ACA rank recorded by a previous product on the same
+// tree and settings) needs no host decision between its launches: each batch runs its known number
+// of iterations, and what would need the host -- blocks deferred past their recorded rank, blocks
+// the student check sends back to the teacher, error counters -- is collected on the device
+// (k_batch_end) and read once after the whole product. The launches from the force gather to the
+// velocity scatter are captured into one CUDA graph (caller-order staging io_f -> io_u) and
+// replayed; the rare reruns run eagerly afterwards.
+
+bool graph_eligible(hignn_model* m) {
+  return m->use_graph && m->device >= 0 && m->timing <= 1 && !m->record_pivots && !m->post_check &&
+         m->n > 0 && hints_usable(m);
+}
+
+// Pointers and settings baked into the captured launches: a change means a new capture.
+uint64_t graph_signature(hignn_model* m) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) {
+    h ^= v;
+    h *= 1099511628211ull;
+  };
+  for (const DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
+                          &m->weights_tc, &m->counter, &m->student, &m->far_blocks, &m->far_state, &m->far_rows,
+                          &m->far_cols, &m->far_used_row, &m->far_used_col, &m->far_C, &m->far_Q, &m->far_act,
+                          &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats, &m->far_rank, &m->far_check,
+                          &m->far_status})
+    mix((uint64_t)(uintptr_t)b->p);
+  mix((uint64_t)m->precision);
+  mix((uint64_t)m->fields);
+  mix((uint64_t)m->timing);
+  mix((uint64_t)m->max_iter);
+  mix((uint64_t)m->use_symmetry);
+  mix((uint64_t)m->has_student);
+  mix((uint64_t)m->sh_c0);
+  mix((uint64_t)m->sh_c1);
+  mix((uint64_t)m->batches.size());
+  for (const auto& bt : m->batches) mix(((uint64_t)bt.b0 << 40) ^ ((uint64_t)bt.b1 << 16) ^ (uint64_t)bt.iters);
+  uint64_t e, t;
+  std::memcpy(&e, &m->epsilon, 8);
+  const double tol = std::max(m->student_tol, m->epsilon);
+  std::memcpy(&t, &tol, 8);
+  mix(e);
+  mix(t);
+  return h;
+}
+
+void release_graph(hignn_model* m) {
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  m->gexec = nullptr;
+  m->graph_sig = 0;
+}
+
+// The launches of the graph (issued on the capturing stream).
+void graph_body(hignn_model* m) {
+  hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
+                              m->n, m->stream);
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
+  if ((m->fields & 1) && !m->lists.closeI.empty()) near_field(m);
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
+  if ((m->fields & 2) && !m->batches.empty()) {
+    const bool student_pass = m->precision == 2 && m->has_student;
+    const hignn::MlpF32 w = m->wdev();
+    const hignn::TcWeights tcw = m->wtc();
+    const float* student = student_pass ? m->student.as<float>() : nullptr;
+    int* status = m->far_status.as<int>();
+    int32_t* lists = status + 8;
+    const int cap = (int)(m->sh_f1 - m->sh_f0);
+    HIGNN_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 8, m->stream));
+    HIGNN_CUDA(cudaMemsetAsync(m->far_stats.p, 0, sizeof(unsigned long long) * 4, m->stream));
+    const hignn::FarBlock* d_blocks = m->far_blocks.as<hignn::FarBlock>();
+    for (const auto& bt : m->batches) {
+      const hignn::FarArgs a = far_args(m, bt, d_blocks, student_pass);
+      const auto& last = m->far_plan[bt.b1 - 1];
+      HIGNN_CUDA(cudaMemsetAsync(m->far_used_row.p, 0, (size_t)last.rOff + last.nI, m->stream));
+      HIGNN_CUDA(cudaMemsetAsync(m->far_used_col.p, 0, (size_t)last.colOff + last.nJ, m->stream));
+      hignn::far_batch_launch(a, w, m->precision >= 1 ? &tcw : nullptr, student, m->err_flag(), m->num_sms,
+                              m->stream, bt.iters);
+      if (student_pass) {
+        const size_t ns = (size_t)a.nb * hignn::kFarSamples;
+        float* feat = m->far_check.as<float>();
+        const float tol = (float)std::max(m->student_tol, m->epsilon);
+        hignn::far_student_check_launch(a, tcw, student, tol, feat, feat + 3 * ns, feat + 12 * ns,
+                                        reinterpret_cast<int*>(feat + 21 * ns), m->err_flag(), m->num_sms,
+                                        m->stream);
+      }
+      hignn::far_batch_end(a, status, lists, cap, m->stream);
+    }
+  }
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
+  hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n, m->stream);
+}
+
+// io_f -> io_u through the graph; returns false when the product has no complete rank plan yet
+// (the caller runs the eager form, which records the ranks).
+bool dot_graph(hignn_model* m) {
+  ensure_far_plan(m);
+  if (!m->plan_hinted) return false;
+  for (const auto& bt : m->batches)
+    if (bt.iters <= 0) return false;
+  const size_t nf = (size_t)(m->sh_f1 - m->sh_f0);
+  m->far_status.ensure(sizeof(int) * (8 + 2 * std::max<size_t>(nf, 1)));
+  if (m->precision == 2 && m->has_student) {
+    int maxnb = 1;
+    for (const auto& bt : m->batches) maxnb = std::max(maxnb, bt.b1 - bt.b0);
+    m->far_check.ensure(sizeof(float) * (size_t)maxnb * hignn::kFarSamples * 21 + 64);
+  }
+  const uint64_t sig = graph_signature(m);
+  if (!m->gexec || sig != m->graph_sig) {
+    release_graph(m);
+    cudaGraph_t g = nullptr;
+    HIGNN_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      graph_body(m);
+    } catch (...) {
+      cudaStreamEndCapture(m->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    HIGNN_CUDA(cudaStreamEndCapture(m->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&m->gexec, g, 0);
+    size_t nnodes = 0;
+    HIGNN_CUDA(cudaGraphGetNodes(g, nullptr, &nnodes));
+    std::vector<cudaGraphNode_t> nodes(nnodes);
+    if (nnodes) HIGNN_CUDA(cudaGraphGetNodes(g, nodes.data(), &nnodes));
+    m->graph_kernels = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType ty;
+      HIGNN_CUDA(cudaGraphNodeGetType(nd, &ty));
+      if (ty == cudaGraphNodeTypeKernel) m->graph_kernels++;
+    }
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      m->gexec = nullptr;
+      HIGNN_CUDA(e);
+    }
+    m->graph_sig = sig;
+    m->graph_iters = 0;
+    for (const auto& bt : m->batches) m->graph_iters += bt.iters;
+  }
+  HIGNN_CUDA(cudaGraphLaunch(m->gexec, m->stream));
+  // one read-back: the far-field status and statistics and the tensor-core error flag
+  int status[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long fst[2] = {0, 0};
+  int err = 0;
+  const bool far_on = (m->fields & 2) && !m->batches.empty();
+  if (far_on) {
+    HIGNN_CUDA(cudaMemcpyAsync(status, m->far_status.p, sizeof(status), cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaMemcpyAsync(fst, m->far_stats.p, sizeof(fst), cudaMemcpyDeviceToHost, m->stream));
+  }
+  HIGNN_CUDA(cudaMemcpyAsync(&err, m->err_flag(), sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  if (err != 0) {
+    HIGNN_CUDA(cudaMemsetAsync(m->err_flag(), 0, sizeof(int), m->stream));
+    throw Error(HIGNN_ERR_LIMIT, "tensor-core kernel: a bounded wait timed out (code " + std::to_string(err) + ")");
+  }
+  if (status[2] != 0) throw Error(-5, "ACA: pivot search found no unused row/column (non-finite block entries?)");
+  if (status[3] != 0) throw Error(-5, "ACA did not converge within max_iter iterations");
+  m->stats.gpu_launches = m->graph_kernels;
+  m->stats.far_rank_max = status[4];
+  m->stats.student_fallback_blocks = status[1];
+  m->stats.far_iterations = m->graph_iters;
+  if (m->timing) {
+    float a = 0, b = 0;
+    HIGNN_CUDA(cudaEventElapsedTime(&a, m->ev[0], m->ev[1]));
+    HIGNN_CUDA(cudaEventElapsedTime(&b, m->ev[1], m->ev[2]));
+    m->stats.t_close_ms = a;
+    m->stats.t_far_ms = b;
+    m->stats.t_dot_ms = a + b;
+  }
+  if (far_on && (status[0] > 0 || status[1] > 0)) {  // reruns, eagerly, then the scatter again
+    const int cap = (int)nf;
+    std::vector<int32_t> lists(2 * (size_t)cap);
+    HIGNN_CUDA(cudaMemcpyAsync(lists.data(), m->far_status.as<int>() + 8, sizeof(int32_t) * 2 * cap,
+                               cudaMemcpyDeviceToHost, m->stream));
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    std::vector<int> deferred(lists.begin(), lists.begin() + std::min(status[0], cap));
+    std::vector<int> fallback(lists.begin() + cap, lists.begin() + cap + std::min(status[1], cap));
+    std::sort(deferred.begin(), deferred.end());
+    std::sort(fallback.begin(), fallback.end());
+    const bool student_pass = m->precision == 2 && m->has_student;
+    int iters = 0;
+    if (!deferred.empty()) {
+      FarOutcome r2;
+      run_far_subset(m, deferred, student_pass, &iters, &r2);
+      if (!r2.deferred.empty()) throw Error(HIGNN_ERR_LIMIT, "ACA: a block was deferred at its full capacity");
+      fallback.insert(fallback.end(), r2.fallback.begin(), r2.fallback.end());
+    }
+    if (!fallback.empty()) {
+      FarOutcome r3;
+      run_far_subset(m, fallback, false, &iters, &r3);
+      if (!r3.deferred.empty()) throw Error(HIGNN_ERR_LIMIT, "ACA: a block was deferred at its full capacity");
+    }
+    m->stats.far_iterations += iters;
+    m->stats.gpu_launches += 5 * (int64_t)iters + 1;
+    hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n,
+                                     m->stream);
+    HIGNN_CUDA(cudaMemcpyAsync(fst, m->far_stats.p, sizeof(fst), cudaMemcpyDeviceToHost, m->stream));
+    if (!deferred.empty()) {  // ranks recorded again for the next plan
+      m->rank_hint.resize(m->lists.farI.size());
+      HIGNN_CUDA(cudaMemcpyAsync(m->rank_hint.data(), m->far_rank.p, sizeof(int32_t) * m->rank_hint.size(),
+                                 cudaMemcpyDeviceToHost, m->stream));
+    }
+    HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+    if (m->precision >= 1) check_device_error(m);
+  }
+  m->stats.far_rank_sum = (int64_t)fst[0];
+  m->stats.far_evals = (int64_t)fst[1];
+  return true;
+}
+
 void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
+  if (graph_eligible(m)) {  // the graph reads io_f and writes io_u
+    if (d_f != m->io_f.as<float>())
+      HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, d_f, sizeof(float) * 3 * m->n, cudaMemcpyDeviceToDevice, m->stream));
+    if (dot_graph(m)) {
+      if (d_u != m->io_u.as<float>())
+        HIGNN_CUDA(cudaMemcpyAsync(d_u, m->io_u.p, sizeof(float) * 3 * m->n, cudaMemcpyDeviceToDevice, m->stream));
+      return;
+    }
+  }
   m->stats.gpu_launches = 2;  // gather + scatter
   hignn::launch_gather_forces(d_f, m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(), m->n, m->stream);
   matvec_tree_order(m);
@@ -986,10 +1221,11 @@ int hignn_destroy(hignn_model* m) {
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
                       &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
                       &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos,
-                      &m->dp_k, &m->dp_err, &m->near_prof})
+                      &m->dp_k, &m->dp_err, &m->near_prof, &m->far_status})
       b->release();
     m->cells.release();
     m->tree_dev.release();
+    release_graph(m);
     for (auto& e : m->ev)
       if (e) cudaEventDestroy(e);
     if (m->host_ctr) cudaFreeHost(m->host_ctr);
@@ -1128,6 +1364,10 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         if ((v != 0) != m->tree_on_device) m->tree_ready = false;  // rebuilt by the chosen builder
         m->tree_on_device = v != 0;
         break;
+      case HIGNN_P_GRAPH:
+        m->use_graph = v != 0;
+        if (!m->use_graph) release_graph(m);
+        break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });
@@ -1155,6 +1395,7 @@ int hignn_get_param(hignn_model* m, int key, double* v) {
       case HIGNN_P_FIELDS: *v = m->fields; break;
       case HIGNN_P_RECORD_PIVOTS: *v = m->record_pivots; break;
       case HIGNN_P_TREE_DEVICE: *v = m->tree_on_device; break;
+      case HIGNN_P_GRAPH: *v = m->use_graph; break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });

@@ -24,6 +24,16 @@ struct Error : std::runtime_error {
 
 #define HIGNN_CHECK_LAUNCH() HIGNN_CUDA(cudaGetLastError())
 
+// Shared-memory size attribute of a kernel, set outside stream capture only: a graph is captured
+// after the same launches have run eagerly once, which set the attributes (they persist).
+template <class K>
+inline void set_max_dynamic_smem(K kernel, size_t bytes, cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  HIGNN_CUDA(cudaStreamIsCapturing(s, &st));
+  if (st == cudaStreamCaptureStatusNone)
+    HIGNN_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 // Device allocation owned by the model (grown on demand, never shrunk; contents not kept).
 struct DevBuf {
   void* p = nullptr;

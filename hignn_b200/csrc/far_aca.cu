@@ -706,22 +706,94 @@ FarTimer::~FarTimer() {
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
 }
 
-int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
-                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations,
-                    FarTimer* timer) {
+namespace {
+
+// One ACA iteration of every active block of a batch: active list, column queries, column pivot,
+// row queries, row pivot (with the stop test and, unless deferred, the apply).
+void far_iteration(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                   int num_sms, cudaStream_t s, FarTimer* timer) {
   auto mark = [&]() {
     if (timer) HIGNN_CUDA(cudaEventRecord(timer->next(), s));
   };
-  if (a.nb <= 0) return 0;
   const size_t eval_smem = sizeof(EvalSmem);
   const size_t row_smem = sizeof(double) * (9 + 3 + 3) * a.ldr;
   const size_t col_smem = sizeof(double) * 9 * a.ldr;
-  HIGNN_CUDA(cudaFuncSetAttribute(k_far_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem));
-  HIGNN_CUDA(cudaFuncSetAttribute(k_far_row_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
-  HIGNN_CUDA(cudaFuncSetAttribute(k_far_col_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
   const int piv_grid = a.nb < 16 * num_sms ? a.nb : 16 * num_sms;  // grid-stride over active blocks
+  mark();
+  k_far_active<<<1, 1024, 0, s>>>(a);
+  mark();
+  if (student)
+    launch_far_student(a, student, 0, err, num_sms, s);
+  else if (tcw)
+    launch_far_tc(a, *tcw, 0, err, num_sms, s);
+  else
+    k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
+  mark();
+  k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
+  mark();
+  if (student)
+    launch_far_student(a, student, 1, err, num_sms, s);
+  else if (tcw)
+    launch_far_tc(a, *tcw, 1, err, num_sms, s);
+  else
+    k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
+  mark();
+  k_far_row_pivot<<<piv_grid, kPivThreads, row_smem, s>>>(a);
+  mark();
+  HIGNN_CHECK_LAUNCH();
+}
+
+// Shared-memory attributes and the state of a batch (first column |J|/2, counters).
+void far_batch_start(const FarArgs& a, cudaStream_t s) {
+  const size_t eval_smem = sizeof(EvalSmem);
+  const size_t row_smem = sizeof(double) * (9 + 3 + 3) * a.ldr;
+  const size_t col_smem = sizeof(double) * 9 * a.ldr;
+  set_max_dynamic_smem(k_far_eval, eval_smem, s);
+  set_max_dynamic_smem(k_far_row_pivot, row_smem, s);
+  set_max_dynamic_smem(k_far_col_pivot, col_smem, s);
   k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   HIGNN_CHECK_LAUNCH();
+}
+
+// End of a batch in the graph form: its counters folded into the matvec's status and the blocks
+// to rerun (deferred: done 2; sent back to the teacher: done 3) appended to the status lists.
+// status: [0] deferred, [1] fallback, [2] pivot error, [3] blocks left unfinished, [4] largest
+// rank; lists: deferred far-list positions at [0, cap), fallback ones at [cap, 2 cap).
+__global__ void k_batch_end(FarArgs a, int* __restrict__ status, int32_t* __restrict__ lists, int cap) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0) {
+    if (a.ctr[kCtrError]) atomicOr(&status[2], a.ctr[kCtrError]);
+    atomicAdd(&status[3], a.ctr[kCtrRemaining]);
+    atomicMax(&status[4], a.ctr[kCtrRankMax]);
+  }
+  if (b >= a.nb) return;
+  const int d = a.state[b].done;
+  if (d == 2 || d == 3) {
+    const int q = atomicAdd(&status[d == 2 ? 0 : 1], 1);
+    if (q < cap) lists[(d == 2 ? 0 : cap) + q] = a.blocks[b].list_idx;
+  }
+}
+
+}  // namespace
+
+void far_batch_launch(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                      int num_sms, cudaStream_t s, int iters) {
+  if (a.nb <= 0) return;
+  far_batch_start(a, s);
+  for (int q = 0; q < iters; q++) far_iteration(a, w, tcw, student, err, num_sms, s, nullptr);
+}
+
+void far_batch_end(const FarArgs& a, int* status, int32_t* lists, int cap, cudaStream_t s) {
+  if (a.nb <= 0) return;
+  k_batch_end<<<(a.nb + 255) / 256, 256, 0, s>>>(a, status, lists, cap);
+  HIGNN_CHECK_LAUNCH();
+}
+
+int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                    int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations,
+                    FarTimer* timer) {
+  if (a.nb <= 0) return 0;
+  far_batch_start(a, s);
   // Without a known bound the counters are read back every kCheck iterations; the kernels of
   // an iteration with no active block return at once.
   constexpr int kCheck = 4;
@@ -730,30 +802,7 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
   bool finished = false;
   while (it < limit && !finished) {
     const int span = known_iters > 0 ? limit : (it + kCheck < limit ? kCheck : limit - it);
-    for (int q = 0; q < span; q++, it++) {
-      mark();
-      k_far_active<<<1, 1024, 0, s>>>(a);
-      mark();
-      if (student)
-        launch_far_student(a, student, 0, err, num_sms, s);
-      else if (tcw)
-        launch_far_tc(a, *tcw, 0, err, num_sms, s);
-      else
-        k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
-      mark();
-      k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
-      mark();
-      if (student)
-        launch_far_student(a, student, 1, err, num_sms, s);
-      else if (tcw)
-        launch_far_tc(a, *tcw, 1, err, num_sms, s);
-      else
-        k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
-      mark();
-      k_far_row_pivot<<<piv_grid, kPivThreads, row_smem, s>>>(a);
-      mark();
-      HIGNN_CHECK_LAUNCH();
-    }
+    for (int q = 0; q < span; q++, it++) far_iteration(a, w, tcw, student, err, num_sms, s, timer);
     HIGNN_CUDA(cudaMemcpyAsync(host_ctr, a.ctr, sizeof(int32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
     HIGNN_CUDA(cudaStreamSynchronize(s));
     if (timer) timer->collect();
@@ -766,9 +815,9 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
   return host_ctr[kCtrDeferred];
 }
 
-int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat, float* yt,
-                      float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s) {
-  if (a.nb <= 0) return 0;
+void far_student_check_launch(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat,
+                              float* yt, float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s) {
+  if (a.nb <= 0) return;
   const int64_t ns = (int64_t)a.nb * kFarSamples;
   HIGNN_CUDA(cudaMemsetAsync(nfail_dev, 0, sizeof(int), s));
   k_far_samples<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(a, feat);
@@ -781,6 +830,12 @@ int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* stude
   const int grid = a.nb < 8 * num_sms ? a.nb : 8 * num_sms;
   k_far_apply<<<grid, kApplyThreads, smem, s>>>(a);
   HIGNN_CHECK_LAUNCH();
+}
+
+int far_student_check(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat, float* yt,
+                      float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s) {
+  if (a.nb <= 0) return 0;
+  far_student_check_launch(a, tcw, student, tol, feat, yt, ys, nfail_dev, err, num_sms, s);
   int nfail = 0;
   HIGNN_CUDA(cudaMemcpyAsync(&nfail, nfail_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
   HIGNN_CUDA(cudaStreamSynchronize(s));

@@ -104,6 +104,16 @@ int far_batch_plain(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, con
                     int num_sms, int32_t* host_ctr, cudaStream_t s, int known_iters, int* iterations,
                     FarTimer* timer = nullptr);
 
+// Graph form of a batch (no host read-back): its state and `iters` iterations, every block's rank
+// known in advance; far_batch_end folds its counters into `status` and lists the blocks to rerun
+// (see k_batch_end in far_aca.cu).
+void far_batch_launch(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, const float* student, int* err,
+                      int num_sms, cudaStream_t s, int iters);
+void far_batch_end(const FarArgs& a, int* status, int32_t* lists, int cap, cudaStream_t s);
+// far_student_check without the read-back of the count of blocks sent back to the teacher.
+void far_student_check_launch(const FarArgs& a, const TcWeights& tcw, const float* student, float tol, float* feat,
+                              float* yt, float* ys, int* nfail_dev, int* err, int num_sms, cudaStream_t s);
+
 // Student residual check of a finished batch run with defer_apply = 1: kFarSamples entries per
 // converged block are evaluated by the student and by the teacher (tensor cores); blocks whose
 // relative residual exceeds tol are marked done = 3 (to be rerun with the teacher), the others

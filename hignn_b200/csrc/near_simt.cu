@@ -113,7 +113,7 @@ void launch_near_simt(const NearArgs& a, const MlpF32& w, int* work_counter, int
                       cudaStream_t stream) {
   if (a.nwork <= 0) return;
   const size_t smem = sizeof(NearSmem);
-  HIGNN_CUDA(cudaFuncSetAttribute(k_near_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  set_max_dynamic_smem(k_near_simt, smem, stream);
   HIGNN_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(int), stream));
   const int grid = a.nwork < num_sms ? a.nwork : num_sms;
   k_near_simt<<<grid, simt::kThreads, smem, stream>>>(a, w, work_counter);

@@ -611,7 +611,7 @@ void launch_student_eval(const float* params, const float* r, float* y, int64_t 
 }
 
 void launch_far_student(const FarArgs& a, const float* params, int which, int* err, int num_sms, cudaStream_t s) {
-  HIGNN_CUDA(cudaFuncSetAttribute(k_far_student_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStcSmemBytes));
+  set_max_dynamic_smem(k_far_student_tc, kStcSmemBytes, s);
   k_far_student_tc<<<8 * num_sms, kStcThreads, kStcSmemBytes, s>>>(a, params, which, err);
   HIGNN_CHECK_LAUNCH();
 }

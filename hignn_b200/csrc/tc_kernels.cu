@@ -374,8 +374,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
 }
 
 template <class K>
-void set_smem(K kernel, size_t bytes) {
-  HIGNN_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+void set_smem(K kernel, size_t bytes, cudaStream_t s) {
+  set_max_dynamic_smem(kernel, bytes, s);
 }
 
 }  // namespace
@@ -386,7 +386,7 @@ void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, in
                     cudaStream_t s) {
   if (a.nwork <= 0) return;
   const size_t smem = sizeof(NearTcSmem) + 1024;
-  set_smem(k_near_tc, smem);
+  set_smem(k_near_tc, smem, s);
   HIGNN_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(int), s));
   const int grid = a.nwork < num_sms ? a.nwork : num_sms;
   k_near_tc<<<grid, tc::kThreads, smem, s>>>(a, w, work_counter, err);
@@ -395,7 +395,7 @@ void launch_near_tc(const NearArgs& a, const TcWeights& w, int* work_counter, in
 
 void launch_far_tc(const FarArgs& a, const TcWeights& w, int which, int* err, int num_sms, cudaStream_t s) {
   const size_t smem = sizeof(FarTcSmem) + 1024;
-  set_smem(k_far_tc, smem);
+  set_smem(k_far_tc, smem, s);
   k_far_tc<<<num_sms, tc::kThreads, smem, s>>>(a, w, which, err);
   HIGNN_CHECK_LAUNCH();
 }
@@ -404,7 +404,7 @@ void launch_eval_tc(const float* r, float* y, int64_t n, const TcWeights& w, int
                     cudaStream_t s) {
   if (n <= 0) return;
   const size_t smem = sizeof(EvalTcSmem) + 1024;
-  set_smem(k_eval_tc, smem);
+  set_smem(k_eval_tc, smem, s);
   const int64_t tiles = (n + tc::kTile - 1) / tc::kTile;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
   k_eval_tc<<<grid, tc::kThreads, smem, s>>>(r, y, n, w, err);

@@ -57,8 +57,12 @@ enum hignn_param {
   HIGNN_P_FAR_POOL_MB = 106,     /* C + Q pool memory of one ACA batch in MiB, default 24576, at most 1<<24 */
   HIGNN_P_RANK_HINT_OFFSET = 107, /* added to the recorded ACA ranks when planning (default 0; a
                                     negative value exercises the deferral path in tests)        */
-  HIGNN_P_TREE_DEVICE = 108       /* 1 (default on a device model) = build the cluster tree on the
+  HIGNN_P_TREE_DEVICE = 108,      /* 1 (default on a device model) = build the cluster tree on the
                                      device, 0 = on the host; both give the same tree and lists */
+  HIGNN_P_GRAPH = 109             /* 1 (default) = a rank-planned H-matvec (the ACA ranks of every far
+                                     block recorded by a previous product on the same tree and
+                                     settings) runs as one captured CUDA graph with a single
+                                     read-back; 0 = every launch from the host */
 };
 
 typedef struct hignn_stats {
