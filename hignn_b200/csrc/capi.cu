@@ -179,7 +179,7 @@ struct hignn_model {
     w.w2img = weights_tc.as<uint4>();
     w.w3img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2);
     w.w1img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2 +
-                                             32 * hignn::kH2 * 2);
+                                             16 * hignn::kH2 * 2);
     w.b2 = f.b2;
     w.b3 = f.b3;
     return w;
@@ -489,6 +489,30 @@ uint16_t bf16_bits(float f) {
   u += 0x7fffu + ((u >> 16) & 1u);
   return (uint16_t)(u >> 16);
 }
+// IEEE binary16, round to nearest even (subnormals kept, overflow to infinity)
+uint16_t f16_bits(float f) {
+  uint32_t x;
+  std::memcpy(&x, &f, 4);
+  const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+  const uint32_t ax = x & 0x7fffffffu;
+  if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7e00u);  // NaN
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // rounds above 65504: infinity
+  if (ax < 0x38800000u) {                                     // below 2^-14: subnormal or zero
+    if (ax < 0x33000000u) return sign;                        // below half the smallest subnormal
+    const uint32_t e = ax >> 23, m = (ax & 0x7fffffu) | 0x800000u;
+    const uint32_t shift = 126 - e;                           // 14..24: value = m * 2^(e-150)
+    uint32_t q = m >> shift;
+    const uint32_t rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+    if (rem > half || (rem == half && (q & 1u))) q++;
+    return (uint16_t)(sign | q);
+  }
+  uint32_t r = ax - 0x38000000u;  // rebias the exponent (127 -> 15)
+  const uint32_t rem = r & 0x1fffu;
+  r >>= 13;
+  if (rem > 0x1000u || (rem == 0x1000u && (r & 1u))) r++;
+  return (uint16_t)(sign | r);
+}
+
 float bf16_value(uint16_t h) {
   const uint32_t u = (uint32_t)h << 16;
   float f;
@@ -544,20 +568,15 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
     return (size_t)slab * rows_per_slab * 128 + (size_t)(row >> 3) * 1024 + (row & 7) * 128 +
            (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
   };
-  const size_t w1off = (size_t)kH2 * kH1 * 2 + 32 * kH2 * 2;
+  // W2 (512 x 128) and W3 (rows 0-8 of 16 x 512) in FP16, W1 split in BF16
+  const size_t w1off = (size_t)kH2 * kH1 * 2 + 16 * kH2 * 2;
   std::vector<uint8_t> img(w1off + (size_t)kH1 * 64 * 2, 0);
   auto put = [&](size_t off, uint16_t v) { std::memcpy(img.data() + off, &v, 2); };
   for (int nn = 0; nn < kH2; nn++)
-    for (int k = 0; k < kH1; k++) put(swz(nn, k, kH2), bf16_bits(W[1][(size_t)nn * kH1 + k]));
+    for (int k = 0; k < kH1; k++) put(swz(nn, k, kH2), f16_bits(W[1][(size_t)nn * kH1 + k]));
   const size_t w3off = (size_t)kH2 * kH1 * 2;
   for (int o = 0; o < kOut; o++)
-    for (int k = 0; k < kH2; k++) {
-      const float v = W[2][(size_t)o * kH2 + k];
-      const uint16_t hi = bf16_bits(v);
-      const uint16_t lo = bf16_bits(v - bf16_value(hi));
-      put(w3off + swz(o, k, 32), hi);
-      put(w3off + swz(16 + o, k, 32), lo);
-    }
+    for (int k = 0; k < kH2; k++) put(w3off + swz(o, k, 16), f16_bits(W[2][(size_t)o * kH2 + k]));
   // layer 1 as one K = 16 MMA on split operands: row n = [W_hi(3), W_hi(3), W_lo(3), b1_hi, b1_lo, 0 x 5]
   // against the feature row [r_hi(3), r_lo(3), r_hi(3), 1, 1, 0 x 5]
   for (int nn = 0; nn < kH1; nn++) {

@@ -34,13 +34,14 @@ struct NearStage {
   float uI[kTcLeaf][3], uJ[kTcLeaf][3];
 };
 
-// Three staging buffers: the pair of the tile being retired, of the tile in flight and of the
-// next tile can all differ (pairs of a single tile).
+// Four staging buffers: the pairs of the tile being retired, of the tile in flight and of the two
+// tiles whose features are written ahead can all differ (pairs of a single tile).
+constexpr int kNearBufs = 4;
 struct NearTcSmem {
   tc::Smem tcs;
-  NearStage st[3];
-  PairWork pw[3];
-  int item[3];
+  NearStage st[kNearBufs];
+  PairWork pw[kNearBufs];
+  int item[kNearBufs];
 };
 static_assert(sizeof(NearTcSmem) + 1024 <= 232448, "near-field shared memory exceeds 227 KB per CTA");
 
@@ -166,7 +167,7 @@ __device__ __forceinline__ void near_flush(NearTcSmem& S, const NearArgs& a, con
       atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&G.uJ[0][0])[q]);
 }
 
-__global__ void __launch_bounds__(tc::kThreads, 1)
+__global__ void __maxnreg__(120)
     k_near_tc(NearArgs a, TcWeights w, int* work_counter, int* err) {
   extern __shared__ uint8_t smem_raw[];
   NearTcSmem& S = *reinterpret_cast<NearTcSmem*>(align1k(smem_raw));
@@ -179,36 +180,42 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const long long t_start = clock64();
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
-    NearTile prev{}, cur{};
+    NearTile prev{}, cur{}, nxt{}, nn{};
     int nbuf = 0;  // staging buffers are used in turn
-    const bool have = near_fetch(S, a, work_counter, nbuf, cur);
-    nbuf = (nbuf + 1) % 3;
-    if (have) near_row(S, cur, row);
-    eng.start(have, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true, has_prev = false;
-    while (have) {
-      // the next tile: the rest of this pair, or the next pair staged into the next buffer
-      NearTile nxt = cur;
-      nxt.t0 += tc::kTile;
-      bool has_next = true;
-      if (cur.last) {
-        has_next = near_fetch(S, a, work_counter, nbuf, nxt);
-        nbuf = (nbuf + 1) % 3;
-      }
-      if (has_next) near_row(S, nxt, row);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { near_use(S, prev, p, M); }));
+    // the tile after c: the rest of its pair, or the next pair staged into the next buffer
+    auto advance = [&](const NearTile& c, NearTile& out) -> bool {
+      out = c;
+      out.t0 += tc::kTile;
+      if (!c.last) return true;
+      const bool h = near_fetch(S, a, work_counter, nbuf, out);
+      nbuf = (nbuf + 1) % kNearBufs;
+      return h;
+    };
+    bool have_cur = near_fetch(S, a, work_counter, nbuf, cur);
+    nbuf = (nbuf + 1) % kNearBufs;
+    if (have_cur) near_row(S, cur, row);
+    bool have_nxt = have_cur && advance(cur, nxt);
+    if (have_nxt) near_row(S, nxt, row);
+    bool ok = tc::epi_all(eng.start(have_cur, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
+    bool has_prev = false;
+    while (ok && have_cur) {
+      const bool have_nn = have_nxt && advance(nxt, nn);
+      if (have_nn) near_row(S, nn, row);
+      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
+                                prev.r[2], [&](float (&M)[9]) { near_use(S, prev, p, M); }));
       if (!ok) break;
       if (has_prev && prev.last) near_flush(S, a, prev);
       prev = cur;
       has_prev = true;
-      if (!has_next) break;
       cur = nxt;
+      have_cur = have_nxt;
+      nxt = nn;
+      have_nxt = have_nn;
     }
     if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
                                                  [&](float (&M)[9]) { near_use(S, prev, p, M); })))
       near_flush(S, a, prev);
-    if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[12] += (unsigned long long)(clock64() - t_start);
+    if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[13] += (unsigned long long)(clock64() - t_start);
   }
   tc::cta_teardown(S.tcs);
 }
@@ -271,7 +278,7 @@ __device__ __forceinline__ void far_use(const FarArgs& a, int which, const FarRo
   }
 }
 
-__global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
+__global__ void __maxnreg__(120) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
   extern __shared__ uint8_t smem_raw[];
   FarTcSmem& S = *reinterpret_cast<FarTcSmem*>(align1k(smem_raw));
   const int nact = a.ctr[kCtrActive];
@@ -286,23 +293,29 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
     int tile = blockIdx.x;
-    FarRow prev{}, cur{};
+    FarRow prev{}, cur{}, nxt{}, nn{};
     far_row(a, which, nact, tot, tile, row, cur);
-    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true;
-    for (;;) {
-      const int nt = tile + gridDim.x;
-      const bool has_next = nt * tc::kTile < tot;
-      FarRow nxt{};
-      nxt.r[0] = 1.f;
-      if (has_next) far_row(a, which, nact, tot, nt, row, nxt);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
+    bool have_nxt = (tile + (int)gridDim.x) * tc::kTile < tot;
+    nxt.r[0] = 1.f;
+    if (have_nxt) far_row(a, which, nact, tot, tile + gridDim.x, row, nxt);
+    bool ok = tc::epi_all(eng.start(true, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
+    bool has_prev = false;
+    while (ok) {
+      const int t2 = tile + 2 * (int)gridDim.x;
+      const bool have_nn = have_nxt && t2 * tc::kTile < tot;
+      nn = FarRow{};
+      nn.r[0] = 1.f;
+      if (have_nn) far_row(a, which, nact, tot, t2, row, nn);
+      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
+                                prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
       if (!ok) break;
       prev = cur;
-      if (!has_next) break;
-      tile = nt;
+      has_prev = true;
+      if (!have_nxt) break;
+      tile += gridDim.x;
       cur = nxt;
+      nxt = nn;
+      have_nxt = have_nn;
     }
     if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
   }
@@ -331,7 +344,7 @@ __device__ __forceinline__ void eval_row(const float* __restrict__ r, int64_t n,
   f.r[2] = r[3 * f.g + 2];
 }
 
-__global__ void __launch_bounds__(tc::kThreads, 1)
+__global__ void __maxnreg__(120)
     k_eval_tc(const float* __restrict__ r, float* __restrict__ y, int64_t n, TcWeights w, int* err) {
   extern __shared__ uint8_t smem_raw[];
   EvalTcSmem& S = *reinterpret_cast<EvalTcSmem*>(align1k(smem_raw));
@@ -350,23 +363,29 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           if ((q & 1) == p) y[9 * f.g + q] = M[q];
     };
     int64_t tile = blockIdx.x;
-    EvalRow prev{}, cur{};
+    EvalRow prev{}, cur{}, nxt{}, nn{};
     eval_row(r, n, tile, row, cur);
-    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true;
-    for (;;) {
-      const int64_t nt = tile + gridDim.x;
-      const bool has_next = nt * tc::kTile < n;
-      EvalRow nxt{};
-      nxt.r[0] = 1.f;
-      if (has_next) eval_row(r, n, nt, row, nxt);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { use(prev, M); }));
+    bool have_nxt = (tile + gridDim.x) * tc::kTile < n;
+    nxt.r[0] = 1.f;
+    if (have_nxt) eval_row(r, n, tile + gridDim.x, row, nxt);
+    bool ok = tc::epi_all(eng.start(true, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
+    bool has_prev = false;
+    while (ok) {
+      const int64_t t2 = tile + 2 * (int64_t)gridDim.x;
+      const bool have_nn = have_nxt && t2 * tc::kTile < n;
+      nn = EvalRow{};
+      nn.r[0] = 1.f;
+      if (have_nn) eval_row(r, n, t2, row, nn);
+      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
+                                prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
       if (!ok) break;
       prev = cur;
-      if (!has_next) break;
-      tile = nt;
+      has_prev = true;
+      if (!have_nxt) break;
+      tile += gridDim.x;
       cur = nxt;
+      nxt = nn;
+      have_nxt = have_nn;
     }
     if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
   }

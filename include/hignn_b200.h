@@ -380,8 +380,9 @@ int hignn_tb_wait_profile(hignn_tb* t, uint64_t* counters);
 /* Wait profile of the tensor-core near field (no counterpart in the reference; a tuning aid),
  * accumulated over the near fields run with HIGNN_P_TIMING >= 3 since the last call, then reset.
  * counters[16]: [c - 13] cycles that lane 0 of every warp spent in bounded waits with code c
- * (13-20 the MMA lane; 21 layer-1, 22 layer-2, 23 layer-3 accumulator, 24 A2 buffer free),
- * [12] cycles of one epilogue warp's whole run summed over CTAs, [13] tiles. */
+ * (13-19 the MMA lane: features, layer-1 epilogue, quarters 0-3 read, layer-3 accumulator free;
+ * 21-25 the epilogue: layer-1, layer-2, layer-3 accumulator, A2 buffer free, quarter 3's MMA
+ * before the next A1), [13] cycles of one epilogue warp's whole run summed over CTAs, [15] tiles. */
 int hignn_near_wait_profile(hignn_model* m, uint64_t* counters);
 
 #ifdef __cplusplus
