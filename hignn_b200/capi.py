@@ -39,6 +39,7 @@ P_FAR_POOL_MB = 106
 P_RANK_HINT_OFFSET = 107
 P_TREE_DEVICE = 108
 P_GRAPH = 109
+P_KEEP_RANKS = 110
 DENSE_F64 = 64  # hignn_dense_rows precision: the network in FP64
 
 STUDENT_PARAMS = 2537

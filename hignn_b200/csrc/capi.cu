@@ -19,6 +19,7 @@
 #include <fstream>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #ifdef _OPENMP
@@ -132,6 +133,7 @@ struct hignn_model {
   // CUDA graph of the rank-planned H-matvec (HIGNN_P_GRAPH): captured once per plan and buffer
   // layout, replayed by every later product on the same tree and settings
   bool use_graph = true;
+  bool keep_ranks = true;  // HIGNN_P_KEEP_RANKS: ACA ranks carried across tree rebuilds
   cudaGraphExec_t gexec = nullptr;
   uint64_t graph_sig = 0;
   int64_t graph_kernels = 0;
@@ -201,6 +203,21 @@ void require_device(hignn_model* m) {
 // later call runs on lists that do not belong to the uploaded positions.
 void build_structures(hignn_model* m) {
   const auto t0 = std::chrono::steady_clock::now();
+  // ACA ranks of the previous far field, keyed by the two nodes of each block (ids and particle
+  // ranges): a block of the new lists that joins the same two nodes starts from that rank
+  struct Carried {
+    int64_t sI, eI, sJ, eJ;
+    int32_t rank;
+  };
+  std::unordered_map<uint64_t, Carried> carried;
+  const bool carry = m->keep_ranks && m->hint_valid && m->rank_hint.size() == m->lists.farI.size() && m->tree_ready;
+  if (carry)
+    for (size_t q = 0; q < m->lists.farI.size(); q++) {
+      const auto& I = m->tree.nodes[m->lists.farI[q]];
+      const auto& J = m->tree.nodes[m->lists.farJ[q]];
+      carried[((uint64_t)m->lists.farI[q] << 32) | (uint64_t)m->lists.farJ[q]] =
+          Carried{I.start, I.end, J.start, J.end, m->rank_hint[q]};
+    }
   m->tree_ready = false;
   m->plan_ready = false;
   m->hint_valid = false;
@@ -246,6 +263,18 @@ void build_structures(hignn_model* m) {
   m->lists = std::move(lists);
   m->lists_sym = m->use_symmetry;
   m->lists_max_rel = m->max_relative_coord;
+  if (carry) {  // hints for the new lists; -1 = not known (planned at full capacity)
+    m->rank_hint.assign(m->lists.farI.size(), -1);
+    for (size_t q = 0; q < m->lists.farI.size(); q++) {
+      const auto it = carried.find(((uint64_t)m->lists.farI[q] << 32) | (uint64_t)m->lists.farJ[q]);
+      if (it == carried.end()) continue;
+      const auto& I = m->tree.nodes[m->lists.farI[q]];
+      const auto& J = m->tree.nodes[m->lists.farJ[q]];
+      const Carried& c = it->second;
+      if (c.sI == I.start && c.eI == I.end && c.sJ == J.start && c.eJ == J.end) m->rank_hint[q] = c.rank;
+    }
+    m->hint_valid = true;
+  }
   const auto t1 = std::chrono::steady_clock::now();
   m->stats.t_build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   m->stats.n = m->n;
@@ -459,10 +488,12 @@ void ensure_far_plan(hignn_model* m) {
     full[q] = std::max(1, std::min(m->max_iter, std::min(nI, nJ)));
     idx[p] = (int)q;
   }
-  if (use_hints) {
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return m->rank_hint[x] > m->rank_hint[y]; });
-    for (size_t p = 0; p < nf; p++)
-      kcap[p] = std::max(1, std::min(full[idx[p]], m->rank_hint[idx[p]] + m->rank_hint_offset));
+  if (use_hints) {  // a block whose rank is not known (hint < 0) gets the full capacity
+    std::vector<int> kc(m->lists.farI.size());
+    for (int q : idx)
+      kc[q] = m->rank_hint[q] < 0 ? full[q] : std::max(1, std::min(full[q], m->rank_hint[q] + m->rank_hint_offset));
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return kc[x] > kc[y]; });
+    for (size_t p = 0; p < nf; p++) kcap[p] = kc[idx[p]];
   } else {
     for (size_t p = 0; p < nf; p++) kcap[p] = full[idx[p]];
   }
@@ -1387,6 +1418,7 @@ int hignn_set_param(hignn_model* m, int key, double v) {
         m->use_graph = v != 0;
         if (!m->use_graph) release_graph(m);
         break;
+      case HIGNN_P_KEEP_RANKS: m->keep_ranks = v != 0; break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });
@@ -1415,6 +1447,7 @@ int hignn_get_param(hignn_model* m, int key, double* v) {
       case HIGNN_P_RECORD_PIVOTS: *v = m->record_pivots; break;
       case HIGNN_P_TREE_DEVICE: *v = m->tree_on_device; break;
       case HIGNN_P_GRAPH: *v = m->use_graph; break;
+      case HIGNN_P_KEEP_RANKS: *v = m->keep_ranks; break;
       default: throw Error(HIGNN_ERR_ARG, "unknown parameter key " + std::to_string(key));
     }
   });

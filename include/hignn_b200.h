@@ -59,10 +59,16 @@ enum hignn_param {
                                     negative value exercises the deferral path in tests)        */
   HIGNN_P_TREE_DEVICE = 108,      /* 1 (default on a device model) = build the cluster tree on the
                                      device, 0 = on the host; both give the same tree and lists */
-  HIGNN_P_GRAPH = 109             /* 1 (default) = a rank-planned H-matvec (the ACA ranks of every far
+  HIGNN_P_GRAPH = 109,            /* 1 (default) = a rank-planned H-matvec (the ACA ranks of every far
                                      block recorded by a previous product on the same tree and
                                      settings) runs as one captured CUDA graph with a single
                                      read-back; 0 = every launch from the host */
+  HIGNN_P_KEEP_RANKS = 110        /* 1 (default) = a tree rebuild keeps the recorded ACA rank of every
+                                     far block that joins the same two nodes (ids and particle
+                                     ranges) as before, so the next product is planned; 0 = every
+                                     rebuild forgets the ranks, and the next product is a first one,
+                                     as every product of the reference's time loop. The result does
+                                     not depend on it. */
 };
 
 typedef struct hignn_stats {

@@ -119,3 +119,25 @@ def test_shards_sum_to_the_whole_product(workload):
         parts.append(m.dot(f).astype(np.float64))
     assert rel(parts[0] + parts[1], full) < 1e-6  # float32 partial results
     assert rel(parts[0], full) > 1e-2  # each shard alone is only part of the product
+
+
+def test_ranks_carried_across_a_rebuild(workload):
+    """A rebuild on moved positions keeps the recorded rank of every block that joins the same two
+    nodes (HIGNN_P_KEEP_RANKS, default on); the product on the new tree equals that of a model
+    that plans nothing (a fresh model, and the same model with the ranks forgotten)."""
+    x, f = workload
+    x2 = (x + np.random.default_rng(9).normal(0, 0.05, x.shape)).astype(np.float32)
+    for prec in (0, 1):
+        m = make_model(x, epsilon=1e-2, precision=prec)
+        m.dot(f)  # records the ranks on the first tree
+        m.update_coord(x2)
+        u_carried = m.dot(f)
+        fresh = make_model(x2, epsilon=1e-2, precision=prec)
+        u_fresh = fresh.dot(f)
+        assert rel(u_carried, u_fresh) < 1e-6
+        m.set(capi.P_KEEP_RANKS, 0)
+        m.update_coord(x)
+        m.update_coord(x2)
+        assert rel(m.dot(f), u_fresh) < 1e-6
+        m.close()
+        fresh.close()
