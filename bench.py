@@ -71,16 +71,17 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=6.0,
                     help="CPU work of one sample step of the CPU baseline / reference arm")
     ap.add_argument("--no-next-rows", action="store_true",
-                    help="skip the three-body near-field measurement added to the line")
+                    help="skip the time loops and the three-body near field added to the line")
+    ap.add_argument("--euler-steps", type=int, default=100, help="steps of the 1M Euler loop (next_rows)")
+    ap.add_argument("--filament-steps", type=int, default=200, help="RK2 steps of the filament loop (next_rows)")
     return ap.parse_args()
 
 
-def filament_steps(steps=4):
-    """Explicit midpoint steps of the filament suspension with the whole HIGNN velocity on the
-    device: filament bending and tension plus gravity, H-matrix two-body term (BF16 network,
-    eps 1e-2, leaf 128), three-body and self terms (cutoff 5); dt 5e-4, tree rebuilt every 2 steps."""
-    import time
-
+def filament_steps(steps=200):
+    """The filament suspension (4,096 filaments x 32 beads, bond 2.2, phi 0.05, seed 3) stepped on the
+    device with the whole HIGNN velocity: filament bending (k_b 10) and tension (k 100) plus
+    gravity, H-matrix two-body term (BF16 network, eps 1e-2, leaf 128), three-body and self terms
+    (cutoff 5); explicit midpoint rule (RK2), dt 5e-4, tree rebuilt every 2 steps."""
     from hignn_b200 import capi
     from hignn_b200 import synthetic as S
     from hignn_b200.weights import default_two_body_path
@@ -93,16 +94,20 @@ def filament_steps(steps=4):
     m.set(capi.P_EPSILON, 1e-2)
     m.set_three_body(tb)
     model = dict(gravity=(0.0, 0.0, -1.0), n_filament=4096, n_chain=32, rest_length=2.2, k_t=100.0, k_b=10.0)
-    x = m.run_rk2(x, 1, 5e-4, rebuild_every=2, **model)  # warm-up
+    m.run_rk2(x, 2, 5e-4, rebuild_every=2, **model)  # warm-up: module loading, allocations
     t0 = time.perf_counter()
     x1 = m.run_rk2(x, steps, 5e-4, rebuild_every=2, **model)
     dt = time.perf_counter() - t0
+    prof = m.loop_profile()
     m.set_three_body(None)
     m.close()
     tb.close()
-    return {"integrator": "explicit midpoint (hignn_run_rk2)", "steps": steps, "ms_per_step": dt / steps * 1e3,
+    return {"workload": "4,096 filaments x 32 beads, RK2 (explicit midpoint), dt 5e-4, tree rebuilt every 2 steps",
+            "integrator": "explicit midpoint (hignn_run_rk2)", "steps": steps, "ms_per_step": dt / steps * 1e3,
             "particle_steps_per_s": len(x) * steps / dt, "final_positions_finite": bool(np.isfinite(x1).all()),
-            "note": "wall clock of the whole call from host positions, tree rebuilds included"}
+            "phases_ms": prof,
+            "note": "wall clock of the whole call from host positions, tree rebuilds included; phases from "
+                    "hignn_loop_profile (device time of forces, matvecs, three-body terms; rebuilds by wall clock)"}
 
 
 def three_body_row(args):
@@ -143,7 +148,7 @@ def three_body_row(args):
             forward(z[s:s + 8192])
     dt = time.perf_counter() - t0
     row["workload"] = "4,096 filaments x 32 beads, bond 2.2, phi 0.05, seed 3, three-body cutoff 5"
-    row["time_step"] = filament_steps()
+    row["time_step"] = filament_steps(args.filament_steps)
     row["cpu_baseline"] = {"value": sample / dt, "unit": "triplets/s", "cores": os.cpu_count(), "kind": "port",
                            "sample": f"{sample} triplets through the three-body network on torch's CPU FP32 path "
                                      f"(the reference's engine), {os.cpu_count()} threads"}
@@ -593,9 +598,26 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds, st["close_evals"],
                                             st["far_evals"])
+    euler = None
+    if rank == 0 and world == 1 and not args.no_next_rows and args.euler_steps > 0:
+        # the batching workload's time loop on the benchmark model (BF16 + student, eps 1e-2):
+        # gravity + Morse (D 1, a 5, r0 2.1, cutoff 3), explicit Euler, dt 1e-3, rebuilt every 10 steps
+        m.set(capi.P_TIMING, 0)
+        morse = dict(De=1.0, a=5.0, re=2.1, cutoff=3.0)
+        m.run_euler(x, 1, 1e-3, rebuild_every=10, gravity=(0.0, 0.0, -1.0), **morse)  # warm-up
+        t0 = time.perf_counter()
+        x1 = m.run_euler(x, args.euler_steps, 1e-3, rebuild_every=10, gravity=(0.0, 0.0, -1.0), **morse)
+        dt_loop = time.perf_counter() - t0
+        euler = {"workload": "N=1,048,576 clustered (the benchmark's positions), gravity + Morse (D 1, a 5, r0 2.1, "
+                             "cutoff 3), BF16 + student far field, eps 1e-2, explicit Euler dt 1e-3, tree rebuilt "
+                             "every 10 steps",
+                 "steps": args.euler_steps, "ms_per_step": dt_loop / args.euler_steps * 1e3,
+                 "particle_steps_per_s": n * args.euler_steps / dt_loop,
+                 "final_positions_finite": bool(np.isfinite(x1).all()), "phases_ms": m.loop_profile(),
+                 "note": "wall clock of hignn_run_euler from host positions; rebuilds, forces, matvecs inside"}
     m.close()
     if rank == 0 and world == 1 and not args.no_next_rows:
-        line["next_rows"] = {"three_body": three_body_row(args)}
+        line["next_rows"] = {"three_body": three_body_row(args), "euler_1m": euler}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -130,6 +130,7 @@ SIGNATURES = {
     "hignn_tb_stats": ([_P, _dp, _dp, _dp, _i64p, _i64p], C.c_int),
     "hignn_tb_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
     "hignn_near_wait_profile": ([_P, C.POINTER(C.c_uint64)], C.c_int),
+    "hignn_loop_profile": ([_P, _dp], C.c_int),
 }
 
 for _name, (_args, _res) in SIGNATURES.items():
@@ -370,6 +371,14 @@ class Model:
     def set_student(self, params):
         p = np.ascontiguousarray(params, np.float32)
         check(lib.hignn_set_student(self._h, fptr(p), p.size))
+
+    def loop_profile(self):
+        """Phases of the last hignn_run_euler / hignn_run_rk2 call (milliseconds and counts)."""
+        v = np.zeros(8, np.float64)
+        check(lib.hignn_loop_profile(self._h, v.ctypes.data_as(_dp)))
+        keys = ("wall_ms", "rebuild_ms", "forces_ms", "matvec_ms", "three_body_ms", "steps", "evaluations",
+                "eager_matvecs")
+        return {k: float(x) for k, x in zip(keys, v)}
 
     def near_wait_profile(self):
         """Wait cycles of the tensor-core near field by barrier (HIGNN_P_TIMING >= 3), then reset."""

@@ -164,6 +164,10 @@ struct hignn_model {
 
   hignn_stats stats{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t lev[4] = {nullptr, nullptr, nullptr, nullptr};  // phases of the device time loops
+  // phases of the last time loop (hignn_loop_profile): wall, rebuild, forces, matvec, three-body,
+  // steps, velocity evaluations, matvecs that ran eagerly (no complete rank plan)
+  double loop_prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   hignn::MlpF32 wdev() const {
     hignn::MlpF32 w;
@@ -955,9 +959,10 @@ void release_graph(hignn_model* m) {
 }
 
 // The launches of the graph (issued on the capturing stream).
-void graph_body(hignn_model* m) {
-  hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
-                              m->n, m->stream);
+void graph_body(hignn_model* m, bool caller_order) {
+  if (caller_order)
+    hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
+                                m->n, m->stream);
   if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
   if ((m->fields & 1) && !m->lists.closeI.empty()) near_field(m);
   if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
@@ -991,12 +996,14 @@ void graph_body(hignn_model* m) {
     }
   }
   if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
-  hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n, m->stream);
+  if (caller_order)
+    hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n,
+                                     m->stream);
 }
 
 // io_f -> io_u through the graph; returns false when the product has no complete rank plan yet
 // (the caller runs the eager form, which records the ranks).
-bool dot_graph(hignn_model* m) {
+bool dot_graph(hignn_model* m, bool caller_order) {
   ensure_far_plan(m);
   if (!m->plan_hinted) return false;
   for (const auto& bt : m->batches)
@@ -1008,13 +1015,13 @@ bool dot_graph(hignn_model* m) {
     for (const auto& bt : m->batches) maxnb = std::max(maxnb, bt.b1 - bt.b0);
     m->far_check.ensure(sizeof(float) * (size_t)maxnb * hignn::kFarSamples * 21 + 64);
   }
-  const uint64_t sig = graph_signature(m);
+  const uint64_t sig = graph_signature(m) ^ (caller_order ? 0x9e3779b97f4a7c15ull : 0ull);
   if (!m->gexec || sig != m->graph_sig) {
     release_graph(m);
     cudaGraph_t g = nullptr;
     HIGNN_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
     try {
-      graph_body(m);
+      graph_body(m, caller_order);
     } catch (...) {
       cudaStreamEndCapture(m->stream, &g);
       if (g) cudaGraphDestroy(g);
@@ -1096,9 +1103,10 @@ bool dot_graph(hignn_model* m) {
       if (!r3.deferred.empty()) throw Error(HIGNN_ERR_LIMIT, "ACA: a block was deferred at its full capacity");
     }
     m->stats.far_iterations += iters;
-    m->stats.gpu_launches += 5 * (int64_t)iters + 1;
-    hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n,
-                                     m->stream);
+    m->stats.gpu_launches += 5 * (int64_t)iters + (caller_order ? 1 : 0);
+    if (caller_order)
+      hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n,
+                                       m->stream);
     HIGNN_CUDA(cudaMemcpyAsync(fst, m->far_stats.p, sizeof(fst), cudaMemcpyDeviceToHost, m->stream));
     if (!deferred.empty()) {  // ranks recorded again for the next plan
       m->rank_hint.resize(m->lists.farI.size());
@@ -1113,11 +1121,19 @@ bool dot_graph(hignn_model* m) {
   return true;
 }
 
+// The matvec of the time loops (forces already in f4, u zeroed, tree order) as a graph: the same
+// launches as graph_body without the gather and the scatter. Returns false when it cannot run
+// (no complete rank plan yet, or graphs off); the caller then runs the eager form.
+bool matvec_graph_tree_order(hignn_model* m) {
+  if (!graph_eligible(m)) return false;
+  return dot_graph(m, false);
+}
+
 void dot_impl(hignn_model* m, float* d_u, const float* d_f) {
   if (graph_eligible(m)) {  // the graph reads io_f and writes io_u
     if (d_f != m->io_f.as<float>())
       HIGNN_CUDA(cudaMemcpyAsync(m->io_f.p, d_f, sizeof(float) * 3 * m->n, cudaMemcpyDeviceToDevice, m->stream));
-    if (dot_graph(m)) {
+    if (dot_graph(m, true)) {
       if (d_u != m->io_u.as<float>())
         HIGNN_CUDA(cudaMemcpyAsync(d_u, m->io_u.p, sizeof(float) * 3 * m->n, cudaMemcpyDeviceToDevice, m->stream));
       return;
@@ -1248,7 +1264,10 @@ int hignn_create(const float* xyz, int64_t n, int block_size, int device, hignn_
         HIGNN_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
         HIGNN_CUDA(cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, device));
         HIGNN_CUDA(cudaMallocHost((void**)&m->host_ctr, sizeof(int32_t) * hignn::kCtrCount));
-        for (auto& e : m->ev) HIGNN_CUDA(cudaEventCreate(&e));
+        for (auto& e : m->lev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : m->ev) HIGNN_CUDA(cudaEventCreate(&e));
+        for (auto& e : m->lev) HIGNN_CUDA(cudaEventCreate(&e));
         m->counter.ensure(64);
         HIGNN_CUDA(cudaMemsetAsync(m->counter.p, 0, 64, m->stream));
       }
@@ -1550,11 +1569,27 @@ void tb_add_device(hignn_tb* t, hignn_model* m);
 // terms when a three-body object is attached.
 void step_velocity(hignn_model* m, const hignn_force_model& fm) {
   const int64_t n = m->n;
+  HIGNN_CUDA(cudaEventRecord(m->lev[0], m->stream));
   apply_forces(m, m->x4.as<float4>(), n, m->slot.as<int32_t>(), fm, m->f4.as<float4>(), nullptr);
   HIGNN_CUDA(cudaMemsetAsync(m->u.p, 0, sizeof(double) * 3 * n, m->stream));
-  matvec_tree_order(m);
+  HIGNN_CUDA(cudaEventRecord(m->lev[1], m->stream));
+  if (!matvec_graph_tree_order(m)) {
+    matvec_tree_order(m);
+    m->loop_prof[7] += 1;
+  }
+  HIGNN_CUDA(cudaEventRecord(m->lev[2], m->stream));
   if (m->tb) tb_add_device(m->tb, m);
+  HIGNN_CUDA(cudaEventRecord(m->lev[3], m->stream));
   if (m->precision >= 1) check_device_error(m);
+  HIGNN_CUDA(cudaEventSynchronize(m->lev[3]));
+  float a = 0, b = 0, c = 0;
+  HIGNN_CUDA(cudaEventElapsedTime(&a, m->lev[0], m->lev[1]));
+  HIGNN_CUDA(cudaEventElapsedTime(&b, m->lev[1], m->lev[2]));
+  HIGNN_CUDA(cudaEventElapsedTime(&c, m->lev[2], m->lev[3]));
+  m->loop_prof[2] += a;
+  m->loop_prof[3] += b;
+  m->loop_prof[4] += c;
+  m->loop_prof[6] += 1;
 }
 
 // The device time loop: method 0 = explicit Euler, 1 = explicit midpoint (RK2).
@@ -1574,13 +1609,17 @@ void run_steps(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int 
   for (int64_t i = 0; i < 3 * n; i++)
     if (!std::isfinite(xyz[i])) throw Error(HIGNN_ERR_ARG, "coordinates must be finite");
   // start from xyz with a tree built for it
+  const auto w0 = std::chrono::steady_clock::now();
+  for (double& v : m->loop_prof) v = 0.0;
   m->xyz.assign(xyz, xyz + 3 * n);
   build_structures(m);
   if (method == 1) m->tmp_x.ensure(sizeof(float4) * n);
   for (int s = 0; s < steps; s++) {
     if (s > 0 && rebuild_every > 0 && s % rebuild_every == 0) {
+      const auto r0 = std::chrono::steady_clock::now();
       download_positions(m);  // m->xyz <- current positions
       build_structures(m);
+      m->loop_prof[1] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r0).count();
     }
     step_velocity(m, *fm);  // forces at the current positions, in tree order, into the matvec
     if (method == 1) {
@@ -1594,6 +1633,8 @@ void run_steps(hignn_model* m, float* xyz, int64_t n, int steps, double dt, int 
   }
   download_positions(m);
   std::copy(m->xyz.begin(), m->xyz.end(), xyz);
+  m->loop_prof[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+  m->loop_prof[5] = steps;
 }
 
 }  // namespace
@@ -2041,6 +2082,13 @@ int hignn_near_wait_profile(hignn_model* m, uint64_t* counters) {
     HIGNN_CUDA(cudaMemcpyAsync(counters, m->near_prof.p, sizeof(uint64_t) * 16, cudaMemcpyDeviceToHost, m->stream));
     HIGNN_CUDA(cudaMemsetAsync(m->near_prof.p, 0, sizeof(uint64_t) * 16, m->stream));
     HIGNN_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int hignn_loop_profile(hignn_model* m, double* ms) {
+  return guard([&] {
+    if (!m || !ms) throw Error(HIGNN_ERR_ARG, "null argument");
+    for (int i = 0; i < 8; i++) ms[i] = m->loop_prof[i];
   });
 }
 

@@ -391,6 +391,12 @@ int hignn_tb_wait_profile(hignn_tb* t, uint64_t* counters);
  * before the next A1), [13] cycles of one epilogue warp's whole run summed over CTAs, [15] tiles. */
 int hignn_near_wait_profile(hignn_model* m, uint64_t* counters);
 
+/* Phases of the last device time loop (hignn_run_euler / hignn_run_rk2; no counterpart in the
+ * reference), ms[8]: wall milliseconds of the whole call, tree rebuilds (wall), forces, matvecs,
+ * three-body terms (device time), steps, velocity evaluations, evaluations whose matvec ran
+ * eagerly (no complete ACA rank plan yet; the others replayed a CUDA graph). */
+int hignn_loop_profile(hignn_model* m, double* ms);
+
 #ifdef __cplusplus
 }
 #endif
