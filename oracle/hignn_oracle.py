@@ -21,10 +21,18 @@ scipy's DOP853 on a smooth system (tests/test_oracle_dp45.py).
 Declared choices where the reference is solver-defined:
 * PCA direction: the reference takes U(:,0) of an Eigen JacobiSVD of the
   centred 3xL float matrix (src/HignnModel.cpp:149-151). Here it is the
-  dominant eigenvector of the 3x3 covariance (sequential FP64 sums of the float
-  centred coordinates) from a cyclic Jacobi solve, rounded to float, with the
-  sign fixed so that its largest-magnitude component is positive. Eigen's sign
-  is implementation-defined (it swaps child order and reverses in-node order).
+  dominant eigenvector of the 3x3 covariance (FP64 sums of the float centred
+  coordinates) from a cyclic Jacobi solve, rounded to float, with the sign
+  fixed so that its largest-magnitude component is positive. Eigen's sign is
+  implementation-defined (it swaps child order and reverses in-node order).
+* The mean (FP32) and the covariance (FP64) of a node are summed in blocks of
+  SUM_BLOCK consecutive particles, then over the block sums; the reference sums
+  the mean sequentially (src/HignnModel.cpp:130-135).
+* The ACA factors C_l, Q_l are stored in FP32 (the reference: FP64), every
+  operation on them in FP64.
+* The FP32 network of the plain form (TwoBodyF32Exact, oracle/twobody_f32.c)
+  performs the operations of the library's plain network in the same order,
+  with the same tanh; the FP64 network (TwoBody.eval64) is the dense oracle's.
 * ``std::sort`` with ``par_unseq`` is not stable (src/HignnModel.cpp:165-171);
   ties in the projection are ordered by position here (stable sort).
 * Team reductions (Kokkos MaxLoc / Sum) are sequential here; MaxLoc takes the
@@ -586,6 +594,13 @@ def _first_argmax(v, excluded):
     return int(np.argmax(vv))
 
 
+def _f32(v):
+    """Values rounded to FP32 and widened again: the ACA factors are stored in FP32 (the
+    reference stores FP64, src/FarDot.cpp:104-107; every operation on them is FP64 either way),
+    and the pivot searches, norms and the apply see the stored values."""
+    return np.asarray(v, np.float64).astype(np.float32).astype(np.float64)
+
+
 def _orth_col(C, Q, k, jk, Ck):
     """C_k(i) -= sum_{l<k} C_l(i) Q_l(jk)  (src/FarDot.cpp:502-511).
 
@@ -691,18 +706,18 @@ def aca_blocks(blocks, net, epsilon, max_iter, replays=None):
         Y = symmetrize_f32(net.eval32(np.concatenate(feats)))
         off = 0
         for s in act:
-            Ck = _orth_col(s.C, s.Q, s.k, s.cols[s.k], Y[off:off + s.nI])
+            Ck = _f32(_orth_col(s.C, s.Q, s.k, s.cols[s.k], Y[off:off + s.nI]))
             off += s.nI
             dets = det3(Ck)
             ik = _first_argmax(dets, set(s.rows)) if s.replay is None else int(s.replay[0][s.k])
             s.rows.append(ik)
-            s.Ck = _mul_inv(Ck, inv3(Ck[ik]))
+            s.Ck = _f32(_mul_inv(Ck, inv3(Ck[ik])))
         feats = [(s.xJ - s.xI[s.rows[s.k]][None, :]).astype(np.float32) for s in act]
         Y = symmetrize_f32(net.eval32(np.concatenate(feats)))
         off = 0
         for s in act:
             k = s.k
-            Qk = _orth_row(s.C, s.Q, k, s.rows[k], Y[off:off + s.nJ])
+            Qk = _f32(_orth_row(s.C, s.Q, k, s.rows[k], Y[off:off + s.nJ]))
             off += s.nJ
             if s.replay is None:
                 s.cols.append(_first_argmax(det3(Qk), set(s.cols[:k + 1])))
