@@ -217,44 +217,10 @@ class ClockSampler:
                 "samples": len(rows), "samples_under_load": len(load), "power_w_max": max(pw)}
 
 
-class TorchCpuNet:
-    """The two-body network on torch's CPU FP32 path, the engine the reference evaluates it with
-    (libtorch, src/CloseDot.cpp:233), wrapped as the oracle's eval32 is (identity added, divided
-    by |r|, identity below |r| = 1e-5). Batches of 8,192 features, about the reference's
-    per-block batches."""
-
-    def __init__(self, net, threads):
-        import torch
-
-        self.torch = torch
-        torch.set_num_threads(threads)
-        self.layers = [(torch.from_numpy(w.copy()), torch.from_numpy(b.copy())) for w, b in zip(net.w32, net.b32)]
-
-    def eval32(self, r):
-        torch = self.torch
-        r = np.ascontiguousarray(r, np.float32)
-        y = np.empty((r.shape[0], 9), np.float32)
-        with torch.no_grad():
-            for s in range(0, r.shape[0], 8192):
-                h = torch.from_numpy(r[s:s + 8192])
-                for i, (w, b) in enumerate(self.layers):
-                    h = torch.addmm(b, h, w.T)
-                    if i + 1 < len(self.layers):
-                        h = torch.tanh(h)
-                y[s:s + 8192] = h.numpy()
-        y[:, 0] += np.float32(1)
-        y[:, 4] += np.float32(1)
-        y[:, 8] += np.float32(1)
-        nr = np.sqrt((r * r).sum(1, dtype=np.float32)).astype(np.float32)
-        with np.errstate(divide="ignore", invalid="ignore"):
-            y = y / nr[:, None]
-        y[nr < 1e-5] = np.eye(3, dtype=np.float32).reshape(9)
-        return y
-
-
 class CpuSample:
-    """The oracle port (numpy restatement of the reference path, the network on torch's CPU path)
-    on a bounded, fixed sample of one H-matvec: the leading close pairs worth about
+    """The CPU baseline: the C++/OpenMP restatement of the reference path (oracle/hmatvec_cpu.cpp:
+    CloseDot and ACA FarDot, FP32 network, FP64 accumulation and bookkeeping) on all host threads,
+    timed on a bounded, fixed sample of one H-matvec: the leading close pairs worth about
     seconds / 2 of CPU work and the leading ACA blocks worth the other half (chosen once, by a
     first timed pass). Every step runs exactly that sample; its evaluations per second are
     extrapolated to the counted evaluations of the whole H-matvec (far evaluations from the
@@ -265,36 +231,34 @@ class CpuSample:
 
         self.O = O
         self.cores = os.cpu_count() or 1
-        self.net = TorchCpuNet(O.TwoBody.from_hgnw(WEIGHTS), self.cores)
+        net = O.TwoBodyF32Exact.from_hgnw(WEIGHTS)
         self.eps = eps
         self.n = len(x)
         t0 = time.time()
         tree, rmap = O.build_tree(x, 128)
-        self.tree = tree
-        self.xt = x[rmap]
-        aux = O.compute_aux(tree, self.xt)
+        xt = x[rmap]
+        aux = O.compute_aux(tree, xt)
         self.ci, self.cj, self.fi, self.fj, _ = O.close_far_lists(tree, aux)
         self.t_lists = time.time() - t0
         self.ft = f[rmap]
-        self.sz = tree[:, 3] - tree[:, 2]
-        sz = self.sz
+        self.cpu = O.CpuHMatvec(tree, xt, net, threads=self.cores)
+        sz = tree[:, 3] - tree[:, 2]
         self.close_evals = int(np.sum(sz[self.ci] * sz[self.cj])) if close_evals is None else close_evals
         # choose the sample: leading pairs / blocks until each half of the budget is used
         p, t_near = 0, 0.0
         while t_near < seconds / 2 and p < len(self.ci):
-            q = min(len(self.ci), p + 64)
+            q = min(len(self.ci), p + 256)
             t = time.time()
-            O.close_dot(tree, self.xt, self.ft, self.ci[p:q], self.cj[p:q], self.net)
+            self.cpu.close_dot(self.ft, self.ci, self.cj, p, q)
             t_near += time.time() - t
             p = q
         b, t_far, ranks = 0, 0.0, []
         while t_far < seconds / 2 and b < len(self.fi):
-            q = min(len(self.fi), b + 32)
+            q = min(len(self.fi), b + 256)
             t = time.time()
-            col = []
-            O.far_dot(tree, self.xt, self.ft, self.fi[b:q], self.fj[b:q], self.net, eps, 100, collect=col)
+            _, rk, _ = self.cpu.far_dot(self.ft, self.fi, self.fj, eps, 100, b, q)
             t_far += time.time() - t
-            ranks += [c[2] for c in col]
+            ranks += rk.tolist()
             b = q
         self.p, self.b = p, b
         self.near_sample = int(np.sum(sz[self.ci[:p]] * sz[self.cj[:p]]))
@@ -304,14 +268,11 @@ class CpuSample:
 
     def step(self):
         """One timed sample step: (seconds, near seconds, far seconds, far evaluations of the sample)."""
-        O, sz = self.O, self.sz
         t0 = time.time()
-        O.close_dot(self.tree, self.xt, self.ft, self.ci[:self.p], self.cj[:self.p], self.net)
+        self.cpu.close_dot(self.ft, self.ci, self.cj, 0, self.p)
         t1 = time.time()
-        col = []
-        O.far_dot(self.tree, self.xt, self.ft, self.fi[:self.b], self.fj[:self.b], self.net, self.eps, 100, collect=col)
+        _, _, far_e = self.cpu.far_dot(self.ft, self.fi, self.fj, self.eps, 100, 0, self.b)
         t2 = time.time()
-        far_e = sum(c[2] * (sz[c[0]] + sz[c[1]]) for c in col)
         return t2 - t0, t1 - t0, t2 - t1, far_e
 
     def estimate(self, t_near, t_far, far_e):
@@ -319,12 +280,13 @@ class CpuSample:
         r_far = far_e / t_far if t_far > 0 else r_near
         t_dot = self.close_evals / r_near + self.far_evals / r_far
         return {"value": self.n / t_dot, "unit": "particles/s", "cores": self.cores, "kind": "port",
-                "sample": (f"oracle restatement (numpy) with the two-body network on torch's CPU FP32 path, as the "
-                           f"reference's libtorch, on {self.cores} host threads (nproc {os.cpu_count()}); each step "
-                           f"runs the same sample: {self.p} close pairs ({self.near_sample:.3g} evals, "
-                           f"{r_near:.3g} evals/s) and {self.b} ACA blocks ({far_e:.3g} evals, {r_far:.3g} evals/s), "
-                           f"extrapolated to {self.close_evals:.3g} near + {self.far_evals:.3g} far evaluations of "
-                           f"one H-matvec; tree+lists ({self.t_lists:.1f} s) not counted")}
+                "sample": (f"C++/OpenMP restatement of the reference path (oracle/hmatvec_cpu.cpp: CloseDot and ACA "
+                           f"FarDot, FP32 network, FP64 accumulation) on {self.cores} host threads (nproc "
+                           f"{os.cpu_count()}; the reference fixes 10); each step runs the same sample: {self.p} "
+                           f"close pairs ({self.near_sample:.3g} evals, {r_near:.3g} evals/s) and {self.b} ACA blocks "
+                           f"({far_e:.3g} evals, {r_far:.3g} evals/s), extrapolated to {self.close_evals:.3g} near "
+                           f"+ {self.far_evals:.3g} far evaluations of one H-matvec; tree+lists "
+                           f"({self.t_lists:.1f} s) not counted")}
 
 
 def cpu_estimate(x, f, eps, seconds, close_evals=None, far_evals=None):
@@ -365,8 +327,7 @@ def reference_arm(args, rank, world):
                        "note": "ms_per_step is the measured time of one sample step; value extrapolates the "
                                "sample's evaluations per second to the whole H-matvec"},
             "note": "the reference's Kokkos/libtorch build cannot be built here (Kokkos, Eigen, MPI absent; "
-                    "not pip-installable); this arm times its restatement on the host cores, the two-body "
-                    "network on torch's CPU FP32 path as the reference evaluates it with libtorch"}
+                    "not pip-installable); this arm times its C++/OpenMP restatement on the host cores"}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -134,7 +134,8 @@ struct hignn_model {
   // layout, replayed by every later product on the same tree and settings
   bool use_graph = true;
   bool keep_ranks = true;  // HIGNN_P_KEEP_RANKS: ACA ranks carried across tree rebuilds
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr;       // near field (after the force gather)
+  cudaGraphExec_t gexec_far = nullptr;   // far field (before the velocity scatter)
   uint64_t graph_sig = 0;
   int64_t graph_kernels = 0;
   int graph_iters = 0;
@@ -954,18 +955,23 @@ uint64_t graph_signature(hignn_model* m) {
 
 void release_graph(hignn_model* m) {
   if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->gexec_far) cudaGraphExecDestroy(m->gexec_far);
   m->gexec = nullptr;
+  m->gexec_far = nullptr;
   m->graph_sig = 0;
 }
 
-// The launches of the graph (issued on the capturing stream).
-void graph_body(hignn_model* m, bool caller_order) {
+// The launches of the two graphs (issued on the capturing stream): the force gather (caller-order
+// products) and the near field; the far field and the velocity scatter. Two graphs rather than
+// one so that the near/far split can be timed with events between the launches.
+void graph_near_body(hignn_model* m, bool caller_order) {
   if (caller_order)
     hignn::launch_gather_forces(m->io_f.as<float>(), m->perm.as<int32_t>(), m->f4.as<float4>(), m->u.as<double>(),
                                 m->n, m->stream);
-  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
   if ((m->fields & 1) && !m->lists.closeI.empty()) near_field(m);
-  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
+}
+
+void graph_far_body(hignn_model* m, bool caller_order) {
   if ((m->fields & 2) && !m->batches.empty()) {
     const bool student_pass = m->precision == 2 && m->has_student;
     const hignn::MlpF32 w = m->wdev();
@@ -995,10 +1001,41 @@ void graph_body(hignn_model* m, bool caller_order) {
       hignn::far_batch_end(a, status, lists, cap, m->stream);
     }
   }
-  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
   if (caller_order)
     hignn::launch_scatter_velocities(m->u.as<double>(), m->perm.as<int32_t>(), m->io_u.as<float>(), m->n,
                                      m->stream);
+}
+
+// Captures body(m, caller_order) on the model's stream into an executable graph; returns its
+// kernel launches.
+template <class Body>
+cudaGraphExec_t capture_graph(hignn_model* m, bool caller_order, Body&& body, int64_t* kernels) {
+  cudaGraph_t g = nullptr;
+  HIGNN_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    body(m, caller_order);
+  } catch (...) {
+    cudaStreamEndCapture(m->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    (void)cudaGetLastError();
+    throw;
+  }
+  HIGNN_CUDA(cudaStreamEndCapture(m->stream, &g));
+  size_t nnodes = 0;
+  cudaError_t e = cudaGraphGetNodes(g, nullptr, &nnodes);
+  std::vector<cudaGraphNode_t> nodes(nnodes);
+  if (e == cudaSuccess && nnodes) e = cudaGraphGetNodes(g, nodes.data(), &nnodes);
+  int64_t k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType ty;
+    if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) k++;
+  }
+  cudaGraphExec_t x = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  HIGNN_CUDA(e);
+  *kernels += k;
+  return x;
 }
 
 // io_f -> io_u through the graph; returns false when the product has no complete rank plan yet
@@ -1016,40 +1053,20 @@ bool dot_graph(hignn_model* m, bool caller_order) {
     m->far_check.ensure(sizeof(float) * (size_t)maxnb * hignn::kFarSamples * 21 + 64);
   }
   const uint64_t sig = graph_signature(m) ^ (caller_order ? 0x9e3779b97f4a7c15ull : 0ull);
-  if (!m->gexec || sig != m->graph_sig) {
+  if (!m->gexec || !m->gexec_far || sig != m->graph_sig) {
     release_graph(m);
-    cudaGraph_t g = nullptr;
-    HIGNN_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-    try {
-      graph_body(m, caller_order);
-    } catch (...) {
-      cudaStreamEndCapture(m->stream, &g);
-      if (g) cudaGraphDestroy(g);
-      cudaGetLastError();
-      throw;
-    }
-    HIGNN_CUDA(cudaStreamEndCapture(m->stream, &g));
-    const cudaError_t e = cudaGraphInstantiate(&m->gexec, g, 0);
-    size_t nnodes = 0;
-    HIGNN_CUDA(cudaGraphGetNodes(g, nullptr, &nnodes));
-    std::vector<cudaGraphNode_t> nodes(nnodes);
-    if (nnodes) HIGNN_CUDA(cudaGraphGetNodes(g, nodes.data(), &nnodes));
     m->graph_kernels = 0;
-    for (auto nd : nodes) {
-      cudaGraphNodeType ty;
-      HIGNN_CUDA(cudaGraphNodeGetType(nd, &ty));
-      if (ty == cudaGraphNodeTypeKernel) m->graph_kernels++;
-    }
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-      m->gexec = nullptr;
-      HIGNN_CUDA(e);
-    }
+    m->gexec = capture_graph(m, caller_order, graph_near_body, &m->graph_kernels);
+    m->gexec_far = capture_graph(m, caller_order, graph_far_body, &m->graph_kernels);
     m->graph_sig = sig;
     m->graph_iters = 0;
     for (const auto& bt : m->batches) m->graph_iters += bt.iters;
   }
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[0], m->stream));
   HIGNN_CUDA(cudaGraphLaunch(m->gexec, m->stream));
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[1], m->stream));
+  HIGNN_CUDA(cudaGraphLaunch(m->gexec_far, m->stream));
+  if (m->timing) HIGNN_CUDA(cudaEventRecord(m->ev[2], m->stream));
   // one read-back: the far-field status and statistics and the tensor-core error flag
   int status[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   unsigned long long fst[2] = {0, 0};
@@ -1122,7 +1139,7 @@ bool dot_graph(hignn_model* m, bool caller_order) {
 }
 
 // The matvec of the time loops (forces already in f4, u zeroed, tree order) as a graph: the same
-// launches as graph_body without the gather and the scatter. Returns false when it cannot run
+// launches as graph_near_body and graph_far_body without the gather and the scatter. Returns false when it cannot run
 // (no complete rank plan yet, or graphs off); the caller then runs the eager form.
 bool matvec_graph_tree_order(hignn_model* m) {
   if (!graph_eligible(m)) return false;

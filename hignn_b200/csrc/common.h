@@ -14,12 +14,16 @@ struct Error : std::runtime_error {
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// A failed call throws; the runtime's record of a non-sticky error is cleared first, so that a
+// later, unrelated check (cudaGetLastError after a launch) does not report it again.
 #define HIGNN_CUDA(call)                                                                              \
   do {                                                                                                \
     cudaError_t _e = (call);                                                                          \
-    if (_e != cudaSuccess)                                                                            \
+    if (_e != cudaSuccess) {                                                                          \
+      (void)cudaGetLastError();                                                                       \
       throw ::hignn::Error(-2, std::string(#call " failed: ") + cudaGetErrorString(_e) + " at " +   \
                                    __FILE__ + ":" + std::to_string(__LINE__));                      \
+    }                                                                                                 \
   } while (0)
 
 #define HIGNN_CHECK_LAUNCH() HIGNN_CUDA(cudaGetLastError())

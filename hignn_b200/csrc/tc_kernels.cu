@@ -75,11 +75,17 @@ __device__ __forceinline__ void add_segmented(float (*uI)[3], int i, float v0, f
   }
 }
 
-// Position of one 128-evaluation tile in the near-field stream and this thread's row of it.
+// One 128-evaluation tile of the near-field stream: its pair (staging buffer), its first flat
+// evaluation index, and whether it is the pair's final tile (uniform over the CTA).
 struct NearTile {
-  int buf, t0;  // the pair itself is S.pw[buf]
+  int buf, t0;
+  bool last;
+};
+
+// This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
+struct NearRow {
   int i, j;
-  bool valid, last;  // last: the final tile of its pair
+  bool valid;
   float r[3];
 };
 
@@ -106,33 +112,34 @@ __device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int
   tc::epi_bar();
   c.buf = b;
   c.t0 = 0;
+  c.last = tc::kTile >= pw.nI * pw.nJ;
   return true;
 }
 
-// This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
-__device__ __forceinline__ void near_row(const NearTcSmem& S, NearTile& c, int row) {
+__device__ __forceinline__ NearRow near_row(const NearTcSmem& S, const NearTile& c, int row) {
+  NearRow w;
   const int nJ = S.pw[c.buf].nJ, total = S.pw[c.buf].nI * nJ;
   const int flat = c.t0 + row;
-  c.valid = flat < total;
-  c.last = c.t0 + tc::kTile >= total;
-  c.i = c.valid ? flat / nJ : 0;
-  c.j = c.valid ? flat - c.i * nJ : 0;
-  c.r[0] = 1.f;
-  c.r[1] = c.r[2] = 0.f;
-  if (c.valid) {
-    const float4 xi = S.st[c.buf].xI[c.i], xj = S.st[c.buf].xJ[c.j];
-    c.r[0] = xj.x - xi.x;
-    c.r[1] = xj.y - xi.y;
-    c.r[2] = xj.z - xi.z;
+  w.valid = flat < total;
+  w.i = w.valid ? flat / nJ : 0;
+  w.j = w.valid ? flat - w.i * nJ : 0;
+  w.r[0] = 1.f;
+  w.r[1] = w.r[2] = 0.f;
+  if (w.valid) {
+    const float4 xi = S.st[c.buf].xI[w.i], xj = S.st[c.buf].xJ[w.j];
+    w.r[0] = xj.x - xi.x;
+    w.r[1] = xj.y - xi.y;
+    w.r[2] = xj.z - xi.z;
   }
+  return w;
 }
 
 // Contraction of one retired tile: u_I += M f_J (part 0), u_J += M f_I for J > I (part 1)
 // (src/CloseDot.cpp:245-299), into the pair's shared-memory accumulators.
-__device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& c, int p, float (&M)[9]) {
+__device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& t, const NearRow& c, int p, float (&M)[9]) {
   if (!c.valid || p >= 2) return;
-  NearStage& G = S.st[c.buf];
-  const int flags = S.pw[c.buf].flags;
+  NearStage& G = S.st[t.buf];
+  const int flags = S.pw[t.buf].flags;
   if (flags & kPairSymmetrize) {
 #pragma unroll
     for (int q = 0; q < 3; q++)
@@ -167,7 +174,7 @@ __device__ __forceinline__ void near_flush(NearTcSmem& S, const NearArgs& a, con
       atomicAdd(&a.uJ[3 * (size_t)pw.sJ + q], (double)(&G.uJ[0][0])[q]);
 }
 
-__global__ void __maxnreg__(120)
+__global__ void __launch_bounds__(tc::kThreads, 1)
     k_near_tc(NearArgs a, TcWeights w, int* work_counter, int* err) {
   extern __shared__ uint8_t smem_raw[];
   NearTcSmem& S = *reinterpret_cast<NearTcSmem*>(align1k(smem_raw));
@@ -184,25 +191,32 @@ __global__ void __maxnreg__(120)
     int nbuf = 0;  // staging buffers are used in turn
     // the tile after c: the rest of its pair, or the next pair staged into the next buffer
     auto advance = [&](const NearTile& c, NearTile& out) -> bool {
-      out = c;
-      out.t0 += tc::kTile;
-      if (!c.last) return true;
+      if (!c.last) {
+        out.buf = c.buf;
+        out.t0 = c.t0 + tc::kTile;
+        out.last = out.t0 + tc::kTile >= S.pw[c.buf].nI * S.pw[c.buf].nJ;
+        return true;
+      }
       const bool h = near_fetch(S, a, work_counter, nbuf, out);
       nbuf = (nbuf + 1) % kNearBufs;
       return h;
     };
     bool have_cur = near_fetch(S, a, work_counter, nbuf, cur);
     nbuf = (nbuf + 1) % kNearBufs;
-    if (have_cur) near_row(S, cur, row);
     bool have_nxt = have_cur && advance(cur, nxt);
-    if (have_nxt) near_row(S, nxt, row);
-    bool ok = tc::epi_all(eng.start(have_cur, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
+    bool ok;
+    {
+      const NearRow r0 = have_cur ? near_row(S, cur, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
+      const NearRow r1 = have_nxt ? near_row(S, nxt, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
+      ok = tc::epi_all(eng.start(have_cur, r0.r[0], r0.r[1], r0.r[2], have_nxt, r1.r[0], r1.r[1], r1.r[2]));
+    }
     bool has_prev = false;
     while (ok && have_cur) {
       const bool have_nn = have_nxt && advance(nxt, nn);
-      if (have_nn) near_row(S, nn, row);
-      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
-                                prev.r[2], [&](float (&M)[9]) { near_use(S, prev, p, M); }));
+      const NearRow rn = have_nn ? near_row(S, nn, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
+      const NearRow rp = has_prev ? near_row(S, prev, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
+      ok = tc::epi_all(eng.step(have_nxt, have_nn, rn.r[0], rn.r[1], rn.r[2], has_prev, rp.r[0], rp.r[1], rp.r[2],
+                                [&](float (&M)[9]) { near_use(S, prev, rp, p, M); }));
       if (!ok) break;
       if (has_prev && prev.last) near_flush(S, a, prev);
       prev = cur;
@@ -212,9 +226,11 @@ __global__ void __maxnreg__(120)
       nxt = nn;
       have_nxt = have_nn;
     }
-    if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
-                                                 [&](float (&M)[9]) { near_use(S, prev, p, M); })))
-      near_flush(S, a, prev);
+    if (ok && has_prev) {
+      const NearRow rp = near_row(S, prev, row);
+      if (tc::epi_all(eng.finish(rp.r[0], rp.r[1], rp.r[2], [&](float (&M)[9]) { near_use(S, prev, rp, p, M); })))
+        near_flush(S, a, prev);
+    }
     if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[13] += (unsigned long long)(clock64() - t_start);
   }
   tc::cta_teardown(S.tcs);
@@ -278,7 +294,7 @@ __device__ __forceinline__ void far_use(const FarArgs& a, int which, const FarRo
   }
 }
 
-__global__ void __maxnreg__(120) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
+__global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights w, int which, int* err) {
   extern __shared__ uint8_t smem_raw[];
   FarTcSmem& S = *reinterpret_cast<FarTcSmem*>(align1k(smem_raw));
   const int nact = a.ctr[kCtrActive];
@@ -344,7 +360,7 @@ __device__ __forceinline__ void eval_row(const float* __restrict__ r, int64_t n,
   f.r[2] = r[3 * f.g + 2];
 }
 
-__global__ void __maxnreg__(120)
+__global__ void __launch_bounds__(tc::kThreads, 1)
     k_eval_tc(const float* __restrict__ r, float* __restrict__ y, int64_t n, TcWeights w, int* err) {
   extern __shared__ uint8_t smem_raw[];
   EvalTcSmem& S = *reinterpret_cast<EvalTcSmem*>(align1k(smem_raw));

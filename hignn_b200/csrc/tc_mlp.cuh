@@ -316,14 +316,16 @@ struct MmaLane {
   uint32_t tb, w1, w2, w3;
   bool ok = true;
   uint32_t u = 0;  // fills issued
-  uint32_t ph_a0 = 0, ph_a1 = 0, ph_a2[2] = {0, 0}, ph_d3f[2] = {0, 0};
+  // phase bits of the barriers this thread waits on, one bit per barrier (registers, no arrays)
+  uint32_t ph_a0 = 0, ph_a1 = 0, ph_a2 = 0, ph_d3f = 0;
 
-  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, int code) {
+  // waits for phase bit `bit` of `ph` of barrier b, then flips that bit
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, uint32_t bit, int code) {
     if (!ok) return false;
     const long long t0 = s.prof ? clock64() : 0;
-    ok = mbar_wait(b, ph, &s.abort_flag, err, code);
+    ok = mbar_wait(b, (ph >> bit) & 1u, &s.abort_flag, err, code);
     if (s.prof) atomicAdd(&s.wprof[code - 13], (unsigned long long)(clock64() - t0));
-    ph ^= 1u;
+    ph ^= 1u << bit;
     if (ok) fence_after();
     return ok;
   }
@@ -358,31 +360,31 @@ struct MmaLane {
   }
 
   __device__ void run() {
-    if (!wait(&s.a0_full, ph_a0, 13)) return;  // tile 0's features, or the end
+    if (!wait(&s.a0_full, ph_a0, 0, 13)) return;  // tile 0's features, or the end
     if (*(volatile int*)&s.exit_flag) return;
-    l1();                                        // fill 0
-    if (!wait(&s.a1_full, ph_a1, 14)) return;   // A1 of tile 0
+    l1();                                           // fill 0
+    if (!wait(&s.a1_full, ph_a1, 0, 14)) return;   // A1 of tile 0
     l2(0);
     l2(1);
     for (uint32_t t = 0;; t++) {
       const uint32_t tp = t & 1;
-      if (!wait(&s.a2_full[0], ph_a2[0], 15)) return;  // quarter 0 of t read
+      if (!wait(&s.a2_full[0], ph_a2, 0, 15)) return;  // quarter 0 of t read
       l2(2);
-      if (!wait(&s.a2_full[1], ph_a2[1], 16)) return;  // quarter 1 of t read
-      if (!wait(&s.a0_full, ph_a0, 13)) return;        // tile t + 1's features, or the end
+      if (!wait(&s.a2_full[1], ph_a2, 1, 16)) return;  // quarter 1 of t read
+      if (!wait(&s.a0_full, ph_a0, 0, 13)) return;     // tile t + 1's features, or the end
       const bool more = !*(volatile int*)&s.exit_flag;
       if (more) l1();
-      if (t >= 2 && !wait(&s.d3_free[tp], ph_d3f[tp], 19)) return;  // tile t - 2 retired
+      if (t >= 2 && !wait(&s.d3_free[tp], ph_d3f, tp, 19)) return;  // tile t - 2 retired
       l3(0, tp);
       l3(1, tp);
-      if (!wait(&s.a2_full[0], ph_a2[0], 17)) return;  // quarter 2 of t read
+      if (!wait(&s.a2_full[0], ph_a2, 0, 17)) return;  // quarter 2 of t read
       l2(3);
       l3(2, tp);
       if (more) {
-        if (!wait(&s.a1_full, ph_a1, 14)) return;  // A1 of tile t + 1
+        if (!wait(&s.a1_full, ph_a1, 0, 14)) return;  // A1 of tile t + 1
         l2(0);
       }
-      if (!wait(&s.a2_full[1], ph_a2[1], 18)) return;  // quarter 3 of t read
+      if (!wait(&s.a2_full[1], ph_a2, 1, 18)) return;  // quarter 3 of t read
       if (more) l2(1);
       l3(3, tp);
       mma_commit(&s.d3_full[tp]);
@@ -445,8 +447,9 @@ struct Epi {
   int p;
   uint32_t tile = 0;
   uint32_t u = 0;  // accumulator fills consumed
-  uint32_t ph_d1 = 0, ph_d2[2] = {0, 0}, ph_a2f[2] = {0, 0}, ph_d3[2] = {0, 0};
-  bool a2_used[2] = {false, false};
+  // phase bits of the barriers this thread waits on, one bit per barrier (registers, no arrays)
+  uint32_t ph_d1 = 0, ph_d2 = 0, ph_a2f = 0, ph_d3 = 0;
+  uint32_t a2_used = 0;  // bit b: A2 buffer b has been written once
   bool ok = true;
 
   __device__ __forceinline__ bool wait_ph(uint64_t* b, uint32_t ph, int code) {
@@ -458,9 +461,10 @@ struct Epi {
     if (ok) fence_after();
     return ok;
   }
-  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, int code) {
-    const bool r = wait_ph(b, ph, code);
-    ph ^= 1u;
+  // waits for phase bit `bit` of `ph` of barrier b, then flips that bit
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, uint32_t bit, int code) {
+    const bool r = wait_ph(b, (ph >> bit) & 1u, code);
+    ph ^= 1u << bit;
     return r;
   }
   // threads that receive M: parts 0 and 1 (both hold all nine entries)
@@ -498,7 +502,7 @@ struct Epi {
                                         float z1) {
     put_features(has0, x0, y0, z0);
     if (!has0) return true;
-    if (!wait(&s.d1_full, ph_d1, 21)) return false;
+    if (!wait(&s.d1_full, ph_d1, 0, 21)) return false;
     put_features(has1, x1, y1, z1);  // A0 was read by L1(0)
     uint32_t out[16];
     layer1(out);
@@ -510,7 +514,7 @@ struct Epi {
   // layer-2 quarter q of the current tile: accumulator -> tanh(. + b2) -> A2[q % 2]
   __device__ __forceinline__ bool quarter(uint32_t q) {
     const uint32_t sl = u & 1;
-    if (!wait(&s.d2_full[sl], ph_d2[sl], 22)) return false;
+    if (!wait(&s.d2_full[sl], ph_d2, sl, 22)) return false;
     uint32_t v[32], out[16];
     tmem_ld32(slot() + 32 * p, v);
     tmem_wait_ld();
@@ -522,9 +526,9 @@ struct Epi {
       out[2 * k + 1] =
           tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
     }
-    const int b = q & 1;
-    if (a2_used[b] && !wait(&s.a2_free[b], ph_a2f[b], 24)) return false;  // L3 of quarter q - 2 done
-    a2_used[b] = true;
+    const uint32_t b = q & 1;
+    if (((a2_used >> b) & 1u) && !wait(&s.a2_free[b], ph_a2f, b, 24)) return false;  // L3 of quarter q - 2 done
+    a2_used |= 1u << b;
     tmem_st16(tl + (b ? kOffA2b : kOffA2a) + 16 * p, out);
     tmem_wait_st();
     fence_before();
@@ -536,7 +540,7 @@ struct Epi {
   // M (row-major 3x3) of tile t from its layer-3 accumulator (parts 0 and 1 read it)
   __device__ __forceinline__ bool read_d3(uint32_t t, float rx, float ry, float rz, float (&M)[9]) {
     const uint32_t b = t & 1;
-    if (!wait(&s.d3_full[b], ph_d3[b], 23)) return false;
+    if (!wait(&s.d3_full[b], ph_d3, b, 23)) return false;
     if (p < 2) {
       uint32_t v[16];
       tmem_ld16(tl + (b ? kOffD3b : kOffD3a), v);
@@ -573,14 +577,14 @@ struct Epi {
     }
     if (!quarter(2)) return false;
     if (has_next) {
-      if (!wait(&s.d1_full, ph_d1, 21)) return false;
+      if (!wait(&s.d1_full, ph_d1, 0, 21)) return false;
       put_features(has_next2, nx, ny, nz);  // A0 was read by L1(tile + 1)
       uint32_t out[16];
       layer1(out);
       u++;
       // A1 is still read by quarter 3's MMAs of this tile: store once they completed (the
       // accumulator consumed next; waited here without consuming its phase)
-      if (!wait_ph(&s.d2_full[u & 1], ph_d2[u & 1], 25)) return false;
+      if (!wait_ph(&s.d2_full[u & 1], (ph_d2 >> (u & 1)) & 1u, 25)) return false;
       store_a1(out);
     }
     if (!quarter(3)) return false;

@@ -185,6 +185,76 @@ class TwoBodyF32Exact(TwoBody):
         return y
 
 
+def _cpu_lib():
+    import ctypes
+
+    lib = TwoBodyF32Exact.lib()
+    if not getattr(lib, "_hmatvec_ready", False):
+        fp, dp, lp = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
+        i64, c_int = ctypes.c_int64, ctypes.c_int
+        lib.oracle_close_dot.argtypes = [fp] * 8 + [lp] * 4 + [i64, i64, c_int, c_int, dp]
+        lib.oracle_close_dot.restype = None
+        lib.oracle_far_dot.argtypes = ([fp] * 8 + [lp] * 4 + [i64, i64, ctypes.c_double, c_int, c_int, c_int, dp,
+                                       ctypes.POINTER(ctypes.c_int32)])
+        lib.oracle_far_dot.restype = ctypes.c_int64
+        lib._hmatvec_ready = True
+    return lib
+
+
+class CpuHMatvec:
+    """The C++/OpenMP restatement of the H-matvec (oracle/hmatvec_cpu.cpp) on a built tree: the
+    same blocks and ACA rules as close_dot / aca_blocks / aca_apply, the FP32 network of
+    TwoBodyF32Exact, every block on one host thread (dynamic schedule over the threads)."""
+
+    def __init__(self, tree, xt, net, threads=None):
+        self.tree = tree
+        self.xt = np.ascontiguousarray(xt, np.float32)
+        self.net = net
+        self.threads = int(threads or os.cpu_count() or 1)
+        self.nstart = np.ascontiguousarray(tree[:, 2], np.int64)
+        self.nend = np.ascontiguousarray(tree[:, 3], np.int64)
+        self.w = [np.ascontiguousarray(a, np.float32) for a in (net.w32[0], net.b32[0], net.w32[1], net.b32[1],
+                                                               net.w32[2], net.b32[2])]
+
+    def _common(self, ft):
+        import ctypes
+
+        fp = ctypes.POINTER(ctypes.c_float)
+        lp = ctypes.POINTER(ctypes.c_int64)
+        self._ft = np.ascontiguousarray(ft, np.float32)
+        return ([a.ctypes.data_as(fp) for a in self.w] + [self.xt.ctypes.data_as(fp), self._ft.ctypes.data_as(fp),
+                self.nstart.ctypes.data_as(lp), self.nend.ctypes.data_as(lp)])
+
+    def close_dot(self, ft, closeI, closeJ, p0=0, p1=None, use_symmetry=True, u=None):
+        import ctypes
+
+        ci = np.ascontiguousarray(closeI, np.int64)
+        cj = np.ascontiguousarray(closeJ, np.int64)
+        p1 = len(ci) if p1 is None else p1
+        u = np.zeros((self.xt.shape[0], 3), np.float64) if u is None else u
+        lp = ctypes.POINTER(ctypes.c_int64)
+        _cpu_lib().oracle_close_dot(*self._common(ft), ci.ctypes.data_as(lp), cj.ctypes.data_as(lp), int(p0), int(p1),
+                                    int(bool(use_symmetry)), self.threads,
+                                    u.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return u
+
+    def far_dot(self, ft, farI, farJ, epsilon, max_iter=100, p0=0, p1=None, use_symmetry=True, u=None):
+        """Adds the far field of far pairs [p0, p1) into u; returns (u, ranks, ACA evaluations)."""
+        import ctypes
+
+        fi = np.ascontiguousarray(farI, np.int64)
+        fj = np.ascontiguousarray(farJ, np.int64)
+        p1 = len(fi) if p1 is None else p1
+        u = np.zeros((self.xt.shape[0], 3), np.float64) if u is None else u
+        ranks = np.zeros(max(0, p1 - p0), np.int32)
+        lp = ctypes.POINTER(ctypes.c_int64)
+        ev = _cpu_lib().oracle_far_dot(*self._common(ft), fi.ctypes.data_as(lp), fj.ctypes.data_as(lp), int(p0),
+                                       int(p1), float(epsilon), int(max_iter), int(bool(use_symmetry)), self.threads,
+                                       u.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       ranks.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        return u, ranks, int(ev)
+
+
 def tanh_f32_exact(x):
     """The plain form's FP32 tanh (oracle/twobody_f32.c) on an array."""
     import ctypes

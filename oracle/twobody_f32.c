@@ -71,7 +71,7 @@ static inline float own_tanh(float x) {
 }
 
 /* One batch of up to BATCH features. */
-__attribute__((target_clones("arch=x86-64-v3", "default")))
+__attribute__((target_clones("arch=x86-64-v4", "arch=x86-64-v3", "default")))
 static void eval_batch(const float* W1, const float* b1, const float* W2, const float* b2, const float* W3,
                        const float* b3, const float* r, int nb, float* y) {
   float rx[BATCH], ry[BATCH], rz[BATCH];
@@ -89,20 +89,31 @@ static void eval_batch(const float* W1, const float* b1, const float* W2, const 
   }
   for (int o = 0; o < NOUT; o++)
     for (int e = 0; e < BATCH; e++) y3[o][e] = 0.0f;
-  for (int n = 0; n < H2; n++) {
-    float acc[BATCH];
-    for (int e = 0; e < BATCH; e++) acc[e] = 0.0f;
-    const float* wn = W2 + (size_t)n * H1;
+  /* four hidden units at a time (each accumulation still runs over k in order) */
+  for (int n0 = 0; n0 < H2; n0 += 4) {
+    float acc[4][BATCH];
+    for (int j = 0; j < 4; j++)
+      for (int e = 0; e < BATCH; e++) acc[j][e] = 0.0f;
+    const float* w0 = W2 + (size_t)n0 * H1;
     for (int k = 0; k < H1; k++) {
-      const float w = wn[k];
-      for (int e = 0; e < BATCH; e++) acc[e] = fmaf(h1[k][e], w, acc[e]);
+      const float a0 = w0[k], a1 = w0[H1 + k], a2 = w0[2 * H1 + k], a3 = w0[3 * H1 + k];
+      for (int e = 0; e < BATCH; e++) {
+        const float h = h1[k][e];
+        acc[0][e] = fmaf(h, a0, acc[0][e]);
+        acc[1][e] = fmaf(h, a1, acc[1][e]);
+        acc[2][e] = fmaf(h, a2, acc[2][e]);
+        acc[3][e] = fmaf(h, a3, acc[3][e]);
+      }
     }
-    const float bn = b2[n];
-    float h2[BATCH];
-    for (int e = 0; e < BATCH; e++) h2[e] = own_tanh(acc[e] + bn);
-    for (int o = 0; o < NOUT; o++) {
-      const float w = W3[(size_t)o * H2 + n];
-      for (int e = 0; e < BATCH; e++) y3[o][e] = fmaf(h2[e], w, y3[o][e]);
+    for (int j = 0; j < 4; j++) {
+      const int n = n0 + j;
+      const float bn = b2[n];
+      float h2[BATCH];
+      for (int e = 0; e < BATCH; e++) h2[e] = own_tanh(acc[j][e] + bn);
+      for (int o = 0; o < NOUT; o++) {
+        const float w = W3[(size_t)o * H2 + n];
+        for (int e = 0; e < BATCH; e++) y3[o][e] = fmaf(h2[e], w, y3[o][e]);
+      }
     }
   }
   for (int e = 0; e < nb; e++) {
@@ -133,4 +144,10 @@ void oracle_twobody_eval32(const float* W1, const float* b1, const float* W2, co
 /* tanh of the plain form for an array (tests of the method against a double tanh). */
 void oracle_tanh_f32(const float* x, int64_t n, float* t) {
   for (int64_t i = 0; i < n; i++) t[i] = own_tanh(x[i]);
+}
+
+/* One batch of nb <= 16 features (the C++ restatement of the H-matvec evaluates through this). */
+void oracle_twobody_batch(const float* W1, const float* b1, const float* W2, const float* b2, const float* W3,
+                          const float* b3, const float* r, int nb, float* y) {
+  eval_batch(W1, b1, W2, b2, W3, b3, r, nb, y);
 }
