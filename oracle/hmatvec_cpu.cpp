@@ -228,18 +228,24 @@ void oracle_close_dot(const float* W1, const float* b1, const float* W2, const f
     for (int64_t p = p0; p < p1; p++) {
       const int64_t I = closeI[p], J = closeJ[p];
       const int64_t sI = nstart[I], nI = nend[I] - sI, sJ = nstart[J], nJ = nend[J] - sJ;
-      r.resize(3 * nI * nJ);
-      y.resize(9 * nI * nJ);
-      for (int64_t i = 0; i < nI; i++)
-        for (int64_t j = 0; j < nJ; j++)
-          for (int d = 0; d < 3; d++) r[3 * (i * nJ + j) + d] = xt[3 * (sJ + j) + d] - xt[3 * (sI + i) + d];
-      net.eval(r.data(), nI * nJ, y.data());
       uI.assign(3 * nI, 0.0);
       const bool tr = use_symmetry && J > I;
       uJ.assign(tr ? 3 * nJ : 0, 0.0);
-      for (int64_t i = 0; i < nI; i++)
-        for (int64_t j = 0; j < nJ; j++) {
-          const float* m = &y[9 * (i * nJ + j)];
+      // in chunks of kChunk evaluations, so that features and outputs stay in the core's cache
+      constexpr int64_t kChunk = 256;
+      r.resize(3 * kChunk);
+      y.resize(9 * kChunk);
+      const int64_t total = nI * nJ;
+      for (int64_t c0 = 0; c0 < total; c0 += kChunk) {
+        const int64_t cn = total - c0 < kChunk ? total - c0 : kChunk;
+        for (int64_t e = 0; e < cn; e++) {
+          const int64_t i = (c0 + e) / nJ, j = (c0 + e) - i * nJ;
+          for (int d = 0; d < 3; d++) r[3 * e + d] = xt[3 * (sJ + j) + d] - xt[3 * (sI + i) + d];
+        }
+        net.eval(r.data(), cn, y.data());
+        for (int64_t e = 0; e < cn; e++) {
+          const int64_t i = (c0 + e) / nJ, j = (c0 + e) - i * nJ;
+          const float* m = &y[9 * e];
           const double fj[3] = {ft[3 * (sJ + j)], ft[3 * (sJ + j) + 1], ft[3 * (sJ + j) + 2]};
           for (int rr = 0; rr < 3; rr++)
             uI[3 * i + rr] += (double)m[3 * rr] * fj[0] + (double)m[3 * rr + 1] * fj[1] + (double)m[3 * rr + 2] * fj[2];
@@ -250,6 +256,7 @@ void oracle_close_dot(const float* W1, const float* b1, const float* W2, const f
                   (double)m[3 * rr] * fi[0] + (double)m[3 * rr + 1] * fi[1] + (double)m[3 * rr + 2] * fi[2];
           }
         }
+      }
       for (int64_t q = 0; q < 3 * nI; q++) atomic_add(&u[3 * sI + q], uI[q]);
       if (tr)
         for (int64_t q = 0; q < 3 * nJ; q++) atomic_add(&u[3 * sJ + q], uJ[q]);
