@@ -384,9 +384,9 @@ class Model:
         """Wait cycles of the tensor-core near field by barrier (HIGNN_P_TIMING >= 3), then reset."""
         c = (C.c_uint64 * 16)()
         check(lib.hignn_near_wait_profile(self._h, c))
-        names = {0: "mma_features", 1: "mma_a1", 2: "mma_q0_read", 3: "mma_q1_read", 4: "mma_q2_read",
-                 5: "mma_q3_read", 6: "mma_d3_free", 8: "epi_layer1_acc", 9: "epi_layer2_acc", 10: "epi_layer3_acc",
-                 11: "epi_a2_free", 12: "epi_q3_before_a1", 13: "epi_total_warp0", 15: "tiles"}
+        names = {0: "mma_first_features", 1: "mma_a1", 2: "mma_q0_in_a2", 3: "mma_d3_free", 4: "mma_q1_in_a2",
+                 5: "mma_q2_in_a2", 6: "mma_next_features", 7: "mma_q3_in_a2", 8: "epi_layer1_acc",
+                 9: "epi_layer2_acc", 10: "epi_layer3_acc", 11: "epi_a2_free", 12: "epi_total_warp0", 13: "tiles"}
         return {names[i]: int(c[i]) for i in names}
 
     def get_student(self):

@@ -34,14 +34,13 @@ struct NearStage {
   float uI[kTcLeaf][3], uJ[kTcLeaf][3];
 };
 
-// Four staging buffers: the pairs of the tile being retired, of the tile in flight and of the two
-// tiles whose features are written ahead can all differ (pairs of a single tile).
-constexpr int kNearBufs = 4;
+// Three staging buffers: the pair of the tile being retired, of the tile in flight and of the
+// next tile can all differ (pairs of a single tile).
 struct NearTcSmem {
   tc::Smem tcs;
-  NearStage st[kNearBufs];
-  PairWork pw[kNearBufs];
-  int item[kNearBufs];
+  NearStage st[3];
+  PairWork pw[3];
+  int item[3];
 };
 static_assert(sizeof(NearTcSmem) + 1024 <= 232448, "near-field shared memory exceeds 227 KB per CTA");
 
@@ -75,17 +74,11 @@ __device__ __forceinline__ void add_segmented(float (*uI)[3], int i, float v0, f
   }
 }
 
-// One 128-evaluation tile of the near-field stream: its pair (staging buffer), its first flat
-// evaluation index, and whether it is the pair's final tile (uniform over the CTA).
+// Position of one 128-evaluation tile in the near-field stream and this thread's row of it.
 struct NearTile {
-  int buf, t0;
-  bool last;
-};
-
-// This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
-struct NearRow {
+  int buf, t0;  // the pair itself is S.pw[buf]
   int i, j;
-  bool valid;
+  bool valid, last;  // last: the final tile of its pair
   float r[3];
 };
 
@@ -112,34 +105,33 @@ __device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int
   tc::epi_bar();
   c.buf = b;
   c.t0 = 0;
-  c.last = tc::kTile >= pw.nI * pw.nJ;
   return true;
 }
 
-__device__ __forceinline__ NearRow near_row(const NearTcSmem& S, const NearTile& c, int row) {
-  NearRow w;
+// This thread's row of a tile: (i, j) and the feature r = x_j - x_i (a dummy for padding rows).
+__device__ __forceinline__ void near_row(const NearTcSmem& S, NearTile& c, int row) {
   const int nJ = S.pw[c.buf].nJ, total = S.pw[c.buf].nI * nJ;
   const int flat = c.t0 + row;
-  w.valid = flat < total;
-  w.i = w.valid ? flat / nJ : 0;
-  w.j = w.valid ? flat - w.i * nJ : 0;
-  w.r[0] = 1.f;
-  w.r[1] = w.r[2] = 0.f;
-  if (w.valid) {
-    const float4 xi = S.st[c.buf].xI[w.i], xj = S.st[c.buf].xJ[w.j];
-    w.r[0] = xj.x - xi.x;
-    w.r[1] = xj.y - xi.y;
-    w.r[2] = xj.z - xi.z;
+  c.valid = flat < total;
+  c.last = c.t0 + tc::kTile >= total;
+  c.i = c.valid ? flat / nJ : 0;
+  c.j = c.valid ? flat - c.i * nJ : 0;
+  c.r[0] = 1.f;
+  c.r[1] = c.r[2] = 0.f;
+  if (c.valid) {
+    const float4 xi = S.st[c.buf].xI[c.i], xj = S.st[c.buf].xJ[c.j];
+    c.r[0] = xj.x - xi.x;
+    c.r[1] = xj.y - xi.y;
+    c.r[2] = xj.z - xi.z;
   }
-  return w;
 }
 
 // Contraction of one retired tile: u_I += M f_J (part 0), u_J += M f_I for J > I (part 1)
 // (src/CloseDot.cpp:245-299), into the pair's shared-memory accumulators.
-__device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& t, const NearRow& c, int p, float (&M)[9]) {
+__device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& c, int p, float (&M)[9]) {
   if (!c.valid || p >= 2) return;
-  NearStage& G = S.st[t.buf];
-  const int flags = S.pw[t.buf].flags;
+  NearStage& G = S.st[c.buf];
+  const int flags = S.pw[c.buf].flags;
   if (flags & kPairSymmetrize) {
 #pragma unroll
     for (int q = 0; q < 3; q++)
@@ -187,51 +179,36 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const long long t_start = clock64();
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
-    NearTile prev{}, cur{}, nxt{}, nn{};
+    NearTile prev{}, cur{};
     int nbuf = 0;  // staging buffers are used in turn
-    // the tile after c: the rest of its pair, or the next pair staged into the next buffer
-    auto advance = [&](const NearTile& c, NearTile& out) -> bool {
-      if (!c.last) {
-        out.buf = c.buf;
-        out.t0 = c.t0 + tc::kTile;
-        out.last = out.t0 + tc::kTile >= S.pw[c.buf].nI * S.pw[c.buf].nJ;
-        return true;
+    const bool have = near_fetch(S, a, work_counter, nbuf, cur);
+    nbuf = (nbuf + 1) % 3;
+    if (have) near_row(S, cur, row);
+    eng.start(have, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true, has_prev = false;
+    while (have) {
+      // the next tile: the rest of this pair, or the next pair staged into the next buffer
+      NearTile nxt = cur;
+      nxt.t0 += tc::kTile;
+      bool has_next = true;
+      if (cur.last) {
+        has_next = near_fetch(S, a, work_counter, nbuf, nxt);
+        nbuf = (nbuf + 1) % 3;
       }
-      const bool h = near_fetch(S, a, work_counter, nbuf, out);
-      nbuf = (nbuf + 1) % kNearBufs;
-      return h;
-    };
-    bool have_cur = near_fetch(S, a, work_counter, nbuf, cur);
-    nbuf = (nbuf + 1) % kNearBufs;
-    bool have_nxt = have_cur && advance(cur, nxt);
-    bool ok;
-    {
-      const NearRow r0 = have_cur ? near_row(S, cur, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
-      const NearRow r1 = have_nxt ? near_row(S, nxt, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
-      ok = tc::epi_all(eng.start(have_cur, r0.r[0], r0.r[1], r0.r[2], have_nxt, r1.r[0], r1.r[1], r1.r[2]));
-    }
-    bool has_prev = false;
-    while (ok && have_cur) {
-      const bool have_nn = have_nxt && advance(nxt, nn);
-      const NearRow rn = have_nn ? near_row(S, nn, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
-      const NearRow rp = has_prev ? near_row(S, prev, row) : NearRow{0, 0, false, {1.f, 0.f, 0.f}};
-      ok = tc::epi_all(eng.step(have_nxt, have_nn, rn.r[0], rn.r[1], rn.r[2], has_prev, rp.r[0], rp.r[1], rp.r[2],
-                                [&](float (&M)[9]) { near_use(S, prev, rp, p, M); }));
+      if (has_next) near_row(S, nxt, row);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { near_use(S, prev, p, M); }));
       if (!ok) break;
       if (has_prev && prev.last) near_flush(S, a, prev);
       prev = cur;
       has_prev = true;
+      if (!has_next) break;
       cur = nxt;
-      have_cur = have_nxt;
-      nxt = nn;
-      have_nxt = have_nn;
     }
-    if (ok && has_prev) {
-      const NearRow rp = near_row(S, prev, row);
-      if (tc::epi_all(eng.finish(rp.r[0], rp.r[1], rp.r[2], [&](float (&M)[9]) { near_use(S, prev, rp, p, M); })))
-        near_flush(S, a, prev);
-    }
-    if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[13] += (unsigned long long)(clock64() - t_start);
+    if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
+                                                 [&](float (&M)[9]) { near_use(S, prev, p, M); })))
+      near_flush(S, a, prev);
+    if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[12] += (unsigned long long)(clock64() - t_start);
   }
   tc::cta_teardown(S.tcs);
 }
@@ -309,29 +286,23 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
     const int row = tc::epi_row(), p = tc::epi_part();
     tc::Epi eng{S.tcs, err, S.tcs.tmem_base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16), p};
     int tile = blockIdx.x;
-    FarRow prev{}, cur{}, nxt{}, nn{};
+    FarRow prev{}, cur{};
     far_row(a, which, nact, tot, tile, row, cur);
-    bool have_nxt = (tile + (int)gridDim.x) * tc::kTile < tot;
-    nxt.r[0] = 1.f;
-    if (have_nxt) far_row(a, which, nact, tot, tile + gridDim.x, row, nxt);
-    bool ok = tc::epi_all(eng.start(true, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
-    bool has_prev = false;
-    while (ok) {
-      const int t2 = tile + 2 * (int)gridDim.x;
-      const bool have_nn = have_nxt && t2 * tc::kTile < tot;
-      nn = FarRow{};
-      nn.r[0] = 1.f;
-      if (have_nn) far_row(a, which, nact, tot, t2, row, nn);
-      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
-                                prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
+    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true;
+    for (;;) {
+      const int nt = tile + gridDim.x;
+      const bool has_next = nt * tc::kTile < tot;
+      FarRow nxt{};
+      nxt.r[0] = 1.f;
+      if (has_next) far_row(a, which, nact, tot, nt, row, nxt);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
       if (!ok) break;
       prev = cur;
-      has_prev = true;
-      if (!have_nxt) break;
-      tile += gridDim.x;
+      if (!has_next) break;
+      tile = nt;
       cur = nxt;
-      nxt = nn;
-      have_nxt = have_nn;
     }
     if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
   }
@@ -379,29 +350,23 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           if ((q & 1) == p) y[9 * f.g + q] = M[q];
     };
     int64_t tile = blockIdx.x;
-    EvalRow prev{}, cur{}, nxt{}, nn{};
+    EvalRow prev{}, cur{};
     eval_row(r, n, tile, row, cur);
-    bool have_nxt = (tile + gridDim.x) * tc::kTile < n;
-    nxt.r[0] = 1.f;
-    if (have_nxt) eval_row(r, n, tile + gridDim.x, row, nxt);
-    bool ok = tc::epi_all(eng.start(true, cur.r[0], cur.r[1], cur.r[2], have_nxt, nxt.r[0], nxt.r[1], nxt.r[2]));
-    bool has_prev = false;
-    while (ok) {
-      const int64_t t2 = tile + 2 * (int64_t)gridDim.x;
-      const bool have_nn = have_nxt && t2 * tc::kTile < n;
-      nn = EvalRow{};
-      nn.r[0] = 1.f;
-      if (have_nn) eval_row(r, n, t2, row, nn);
-      ok = tc::epi_all(eng.step(have_nxt, have_nn, nn.r[0], nn.r[1], nn.r[2], has_prev, prev.r[0], prev.r[1],
-                                prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
+    eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
+    bool ok = true;
+    for (;;) {
+      const int64_t nt = tile + gridDim.x;
+      const bool has_next = nt * tc::kTile < n;
+      EvalRow nxt{};
+      nxt.r[0] = 1.f;
+      if (has_next) eval_row(r, n, nt, row, nxt);
+      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+                                [&](float (&M)[9]) { use(prev, M); }));
       if (!ok) break;
       prev = cur;
-      has_prev = true;
-      if (!have_nxt) break;
-      tile += gridDim.x;
+      if (!has_next) break;
+      tile = nt;
       cur = nxt;
-      nxt = nn;
-      have_nxt = have_nn;
     }
     if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
   }

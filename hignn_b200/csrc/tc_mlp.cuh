@@ -13,15 +13,14 @@
 // round to FP16 pairs and apply tanh.approx.f16x2, and write the pairs back into tensor memory as
 // the next A operand.
 //
-// The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM, i.e. 40 clocks per
-// evaluation per SM, against ~33 clocks of tensor-pipe occupancy (every MMA holds the pipe >= ~64
-// cycles whatever its N). The schedule keeps the epilogue -- and so the MUFU -- from waiting on
-// the tensor core: per tile t the epilogue consumes the layer-2 quarters 0, 1, 2 of t, then the
-// layer-1 accumulator of tile t + 1, then quarter 3 of t, so that the next tile's first quarter
-// is on the tensor cores while quarter 3 is in the epilogue. The layer-1 result of tile t + 1 is
-// computed into registers and stored as the next A1 once quarter 3's MMA (the last reader of A1)
-// has completed. Tile t - 1 is retired (its layer-3 output read, M formed and handed to the
-// caller) after quarter 1 of tile t, from the other of two layer-3 accumulators.
+// The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM (the packed f16x2
+// form issues at half the rate of tanh.approx.f32, so packing saves issue slots, not MUFU time),
+// i.e. 40 clocks per evaluation per SM, against ~33 clocks of tensor-pipe occupancy (every MMA
+// holds the pipe >= ~64 cycles whatever its N). The pipeline is therefore
+// built to keep the MUFU busy: one tile stream per CTA, two FP32 accumulator
+// slots, separate buffers for layer 3's operand, and an MMA lane that runs a
+// quarter ahead of the epilogue without ever waiting for an MMA of its own (an
+// MMA's result reaches a waiting thread ~500 cycles after issue, measured).
 //
 // CTA = 17 warps:
 //   warps 0-15  epilogue; warp w reaches TMEM lanes 32 (w % 4) .. + 31, so the
@@ -31,16 +30,18 @@
 //   warp 16     allocates tensor memory; one lane issues every MMA.
 // Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed FP16 pairs (A operand of layer 2)
-//   [ 64,192)  slot 0 and [192,320) slot 1: FP32 accumulators, filled in turn (fill u uses slot
-//              u % 2) by the layer-1 MMA and the layer-2 quarters, in the epilogue's order
-//   [320,384)  and [384,448): A2 of even / odd quarters (A operand of layer 3)
-//   [448,464)  and [464,480): layer-3 accumulators of even / odd tiles
+//   [ 64,192)  slot 0 and [192,320) slot 1: FP32 accumulators, used in turn by
+//              layer 1 and the four layer-2 quarters of each tile
+//   [320,384)  and [384,448): A2 of even / odd quarters, the tanh'd FP16 pairs
+//              of a quarter (A operand of layer 3)
+//   [448,464)  layer-3 accumulator (M in columns 0-8)
 //   [480,488)  A0: the split features (K = 16 BF16) of layer 1
 // Shared memory: W2 (512 x 128) and W3 (16 x 512) as FP16 and W1 (128 x 16, in a 64-wide slab)
 // as BF16, canonical K-major 128-byte-swizzle layout, loaded once per CTA; FP32 biases b2, b3;
-// mbarriers. Every thread tracks the phase of each barrier it waits on. Every wait is bounded
-// (about two seconds of clock): on a timeout the CTA records an error, stops issuing work, drains
-// its MMAs and frees its tensor memory.
+// mbarriers. A barrier that completes twice per tile (the per-slot and per-buffer ones) is waited
+// with the parity of its position in the tile, and no waiter can fall two phases behind. Every wait is
+// bounded (about two seconds of clock): on a timeout the CTA records an error,
+// stops issuing work, drains its MMAs and frees its tensor memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -58,18 +59,17 @@ constexpr int kTile = 128;
 constexpr int kEpiThreads = 512;
 constexpr int kThreads = 544;
 constexpr int kMmaWarp = 16;
-constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffA2a = 320, kOffA2b = 384, kOffD3a = 448,
-                   kOffD3b = 464, kOffA0 = 480;
+constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffA2a = 320, kOffA2b = 384, kOffD3 = 448, kOffA0 = 480;
 constexpr int kW2Bytes = kH2 * kH1 * 2;      // 131072
 constexpr int kW3Rows = 16;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 16384
 constexpr int kW1Bytes = kH1 * 64 * 2;       // 16384: 128 rows x one 64-wide K slab (K 0-15 used)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // Wait profile (TcWeights::prof non-null): slot c - 13 sums the cycles that lane 0 of every warp
-// spent in bounded waits with code c (13-19 the MMA lane: 13 features, 14 layer-1 epilogue,
-// 15-18 quarters 0-3 read, 19 layer-3 accumulator free; 21-25 the epilogue warps: 21 layer-1
-// accumulator, 22 layer-2 accumulator, 23 layer-3 accumulator, 24 A2 buffer free, 25 quarter 3's
-// MMA before the next A1 is stored); slot 13 the cycles of warp 0's whole epilogue; slot 15 the
+// spent in bounded waits with code c (13-20 the MMA lane: 13 first features, 14 layer-1 epilogue,
+// 15 quarter 0 in A2, 16 D3 free, 17 quarter 1, 18 quarter 2, 19 next features, 20 quarter 3;
+// 21-24 the epilogue warps: 21 layer-1 accumulator, 22 layer-2 accumulator, 23 layer-3
+// accumulator, 24 A2 buffer free); slot 12 the cycles of warp 0's whole epilogue; slot 13 the
 // tiles processed.
 constexpr int kProfSlots = 16;
 
@@ -77,7 +77,7 @@ struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
   uint8_t w3[kW3Bytes];
   uint8_t w1[kW1Bytes];
-  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], a2_free[2], d3_full[2], d3_free[2], drain;
+  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], a2_free[2], d3_full, d3_free, drain;
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
@@ -274,10 +274,8 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
     mbar_init(&s.a2_full[1], kEpiThreads);
     mbar_init(&s.a2_free[0], 1);
     mbar_init(&s.a2_free[1], 1);
-    mbar_init(&s.d3_full[0], 1);
-    mbar_init(&s.d3_full[1], 1);
-    mbar_init(&s.d3_free[0], kEpiThreads);
-    mbar_init(&s.d3_free[1], kEpiThreads);
+    mbar_init(&s.d3_full, 1);
+    mbar_init(&s.d3_free, kEpiThreads);
     mbar_init(&s.drain, 1);
     s.exit_flag = 0;
     s.abort_flag = 0;
@@ -300,94 +298,92 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
 }
 
 // ------------------------------------------------------------------ MMA lane
-// One thread issues every MMA. Fills of the two accumulator slots are counted by u (fill u goes to
-// slot u % 2 and may start once the epilogue has read fill u - 2); the epilogue consumes them in
-// the same order. Per tile t (fills in brackets exist only when a tile t + 1 follows):
-//   after quarter 0 of t is read:  L2(t, 2)
-//   after quarter 1 of t is read:  [L1(t + 1)], then L3(t, 0), L3(t, 1) into D3[t % 2] once
-//                                  tile t - 2 has been retired from it
-//   after quarter 2 of t is read:  L2(t, 3), L3(t, 2), [L2(t + 1, 0) once A1 of t + 1 is stored]
-//   after quarter 3 of t is read:  [L2(t + 1, 1)], L3(t, 3), commit D3[t % 2]
-// so the tensor core holds the accumulator the epilogue needs next, and the layer-3 MMAs (needed
-// only at retirement) fill the gaps.
+// One thread issues every MMA, per tile t (u = 5t; accumulator slot of a use = u & 1; A2 buffer
+// of quarter q = q & 1), in this order:
+//   L2(t,0)->slot(u+1)  L2(t,1)->slot(u+2)          after a1_full(t): A1 written, L1 slot read
+//   L2(t,2)->slot(u+3)  L3(t,0)<-A2[0]               after a2(q0): slot(u+1) read, A2[0] written
+//   L2(t,3)->slot(u+4)  L3(t,1)<-A2[1]               after a2(q1)
+//   L1(t+1)->slot(u+5)  L3(t,2)<-A2[0]               after a2(q2) and a0_full(t+1)
+//   L3(t,3)<-A2[1]  commit d3_full                   after a2(q3)
+// Every MMA holds the tensor pipe >= ~64 cycles whatever its N, so the eight layer-3 MMAs of a
+// quarter cost as much as its eight layer-2 MMAs; the accumulator the epilogue waits for next
+// is therefore queued ahead of the layer-3 MMAs, whose result is needed only at retirement.
+// An accumulator slot is reused as soon as the epilogue has read it (its tanh'd pairs go to a
+// separate A2 buffer), so the lane never waits for an MMA of its own: the ~500-cycle latency
+// from an MMA's issue to its commit reaching a waiting thread is paid only by threads that have
+// other work queued. L3(t,0) overwrites D3, so it also waits until the epilogue has read D3 of
+// tile t-1 (d3_free).
 struct MmaLane {
   Smem& s;
   int* err;
   uint32_t tb, w1, w2, w3;
   bool ok = true;
-  uint32_t u = 0;  // fills issued
-  // phase bits of the barriers this thread waits on, one bit per barrier (registers, no arrays)
-  uint32_t ph_a0 = 0, ph_a1 = 0, ph_a2 = 0, ph_d3f = 0;
 
-  // waits for phase bit `bit` of `ph` of barrier b, then flips that bit
-  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, uint32_t bit, int code) {
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
     if (!ok) return false;
     const long long t0 = s.prof ? clock64() : 0;
-    ok = mbar_wait(b, (ph >> bit) & 1u, &s.abort_flag, err, code);
+    ok = mbar_wait(b, parity, &s.abort_flag, err, code);
     if (s.prof) atomicAdd(&s.wprof[code - 13], (unsigned long long)(clock64() - t0));
-    ph ^= 1u << bit;
     if (ok) fence_after();
     return ok;
   }
-  __device__ __forceinline__ uint32_t slot() const { return tb + (u & 1 ? kOffS1 : kOffS0); }
-  __device__ __forceinline__ void l1() {
-    mma_ts(slot(), tb + kOffA0, sdesc(w1), idesc_bf16(128, 128), 0u);
+  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tb + (u & 1 ? kOffS1 : kOffS0); }
+  __device__ __forceinline__ void l1(uint32_t u) {
+    mma_ts(slot(u), tb + kOffA0, sdesc(w1), idesc_bf16(128, 128), 0u);
     mma_commit(&s.d1_full);
-    u++;
   }
-  __device__ __forceinline__ void l2(uint32_t q) {
+  __device__ __forceinline__ void l2(uint32_t u, uint32_t q) {
     const uint32_t id = idesc_f16x(128, 128);
 #pragma unroll
     for (uint32_t kk = 0; kk < 8; kk++) {
       const uint32_t bb = w2 + (kk >> 2) * (kH2 * 128) + q * (128 * 128) + (kk & 3) * 32;
-      mma_ts(slot(), tb + kOffA1 + 8 * kk, sdesc(bb), id, kk > 0);
+      mma_ts(slot(u), tb + kOffA1 + 8 * kk, sdesc(bb), id, kk > 0);
     }
     mma_commit(&s.d2_full[u & 1]);
-    u++;
   }
-  // layer 3 of quarter q (A2 buffer q % 2) into the layer-3 accumulator of tile parity tp
-  __device__ __forceinline__ void l3(uint32_t q, uint32_t tp) {
+  // layer 3 of quarter q from its A2 buffer into D3
+  __device__ __forceinline__ void l3(uint32_t q) {
     const uint32_t id = idesc_f16x(128, kW3Rows);
     const uint32_t a2 = tb + (q & 1 ? kOffA2b : kOffA2a);
-    const uint32_t d3 = tb + (tp ? kOffD3b : kOffD3a);
 #pragma unroll
     for (uint32_t kk = 0; kk < 8; kk++) {
       const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
       const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-      mma_ts(d3, a2 + 8 * kk, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
+      mma_ts(tb + kOffD3, a2 + 8 * kk, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
     }
     mma_commit(&s.a2_free[q & 1]);
   }
+  // the epilogue wrote the A2 pairs of quarter q. Each of the two a2_full barriers completes
+  // twice per tile (quarters q and q + 2), so the phase parity is q / 2.
+  __device__ __forceinline__ bool a2(uint32_t u, uint32_t q, int code) {
+    return wait(&s.a2_full[(u + 1 + q) & 1], q >> 1, code);
+  }
 
   __device__ void run() {
-    if (!wait(&s.a0_full, ph_a0, 0, 13)) return;  // tile 0's features, or the end
+    // tile 0: layer 1 once its features are in A0
+    if (!wait(&s.a0_full, 0, 13)) return;
     if (*(volatile int*)&s.exit_flag) return;
-    l1();                                           // fill 0
-    if (!wait(&s.a1_full, ph_a1, 0, 14)) return;   // A1 of tile 0
-    l2(0);
-    l2(1);
+    l1(0);
     for (uint32_t t = 0;; t++) {
-      const uint32_t tp = t & 1;
-      if (!wait(&s.a2_full[0], ph_a2, 0, 15)) return;  // quarter 0 of t read
-      l2(2);
-      if (!wait(&s.a2_full[1], ph_a2, 1, 16)) return;  // quarter 1 of t read
-      if (!wait(&s.a0_full, ph_a0, 0, 13)) return;     // tile t + 1's features, or the end
+      const uint32_t u = 5 * t;
+      if (!wait(&s.a1_full, t & 1, 14)) return;
+      l2(u + 1, 0);
+      l2(u + 2, 1);
+      if (!a2(u, 0, 15)) return;
+      l2(u + 3, 2);  // the next accumulator first: the epilogue waits for it, D3 only at retirement
+      if (t > 0 && !wait(&s.d3_free, (t - 1) & 1, 16)) return;
+      l3(0);
+      if (!a2(u, 1, 17)) return;
+      l2(u + 4, 3);
+      l3(1);
+      if (!a2(u, 2, 18)) return;
+      if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;  // the next tile's features, or the end
       const bool more = !*(volatile int*)&s.exit_flag;
-      if (more) l1();
-      if (t >= 2 && !wait(&s.d3_free[tp], ph_d3f, tp, 19)) return;  // tile t - 2 retired
-      l3(0, tp);
-      l3(1, tp);
-      if (!wait(&s.a2_full[0], ph_a2, 0, 17)) return;  // quarter 2 of t read
-      l2(3);
-      l3(2, tp);
-      if (more) {
-        if (!wait(&s.a1_full, ph_a1, 0, 14)) return;  // A1 of tile t + 1
-        l2(0);
-      }
-      if (!wait(&s.a2_full[1], ph_a2, 1, 18)) return;  // quarter 3 of t read
-      if (more) l2(1);
-      l3(3, tp);
-      mma_commit(&s.d3_full[tp]);
+      if (more) l1(u + 5);
+      l3(2);
+      if (!a2(u, 3, 20)) return;
+      l3(3);
+      mma_commit(&s.d3_full);
       if (!more) return;
     }
   }
@@ -435,43 +431,33 @@ __device__ __forceinline__ void write_features(uint32_t ta0, int p, float rx, fl
   }
 }
 
-// The tile engine seen from the epilogue threads (all 512 call every member). Per tile t, step()
-// consumes quarters 0 and 1 of t, retires tile t - 1 (use(M) with its features), consumes quarter
-// 2, the layer-1 accumulator of t + 1 (writing the features of t + 2 into A0), and quarter 3.
-// start() writes the features of tiles 0 and 1 and runs layer 1 of tile 0; finish() retires the
-// last tile.
+// The tile engine seen from the epilogue threads. Tiles are retired one step late: step(t)
+// computes the network of tile t up to its layer-3 MMAs and hands the finished M of tile t-1 to
+// `use`, called between the layer-1 epilogue of tile t and its first quarter -- the time the
+// first layer-2 quarter of tile t spends on the tensor cores. finish() retires the last tile.
 struct Epi {
   Smem& s;
   int* err;
   uint32_t tl;  // TMEM base with this warp's lane field
   int p;
   uint32_t tile = 0;
-  uint32_t u = 0;  // accumulator fills consumed
-  // phase bits of the barriers this thread waits on, one bit per barrier (registers, no arrays)
-  uint32_t ph_d1 = 0, ph_d2 = 0, ph_a2f = 0, ph_d3 = 0;
-  uint32_t a2_used = 0;  // bit b: A2 buffer b has been written once
   bool ok = true;
 
-  __device__ __forceinline__ bool wait_ph(uint64_t* b, uint32_t ph, int code) {
+  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
     if (!ok) return false;
     const bool rec = s.prof && (threadIdx.x & 31) == 0;
     const long long t0 = rec ? clock64() : 0;
-    ok = mbar_wait(b, ph, &s.abort_flag, err, code);
+    ok = mbar_wait(b, parity, &s.abort_flag, err, code);
     if (rec) atomicAdd(&s.wprof[code - 13], (unsigned long long)(clock64() - t0));
     if (ok) fence_after();
     return ok;
   }
-  // waits for phase bit `bit` of `ph` of barrier b, then flips that bit
-  __device__ __forceinline__ bool wait(uint64_t* b, uint32_t& ph, uint32_t bit, int code) {
-    const bool r = wait_ph(b, (ph >> bit) & 1u, code);
-    ph ^= 1u << bit;
-    return r;
-  }
   // threads that receive M: parts 0 and 1 (both hold all nine entries)
   __device__ __forceinline__ bool has_m() const { return p < 2; }
-  __device__ __forceinline__ uint32_t slot() const { return tl + (u & 1 ? kOffS1 : kOffS0); }
+  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tl + (u & 1 ? kOffS1 : kOffS0); }
 
-  __device__ __forceinline__ void put_features(bool has, float rx, float ry, float rz) {
+  // features of the first tile (has = false: nothing to do at all)
+  __device__ __forceinline__ void start(bool has, float rx, float ry, float rz) {
     if (has) {
       write_features(tl + kOffA0, p, rx, ry, rz);
       tmem_wait_st();
@@ -482,68 +468,12 @@ struct Epi {
     mbar_arrive(&s.a0_full);
   }
 
-  // tanh(layer 1) of the current fill as 16 packed FP16 pairs (this thread's 32 columns)
-  __device__ __forceinline__ void layer1(uint32_t (&out)[16]) {
-    uint32_t v[32];
-    tmem_ld32(slot() + 32 * p, v);
-    tmem_wait_ld();
-#pragma unroll
-    for (int k = 0; k < 16; k++) out[k] = tanh_f16x2(pack_f16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
-  }
-  __device__ __forceinline__ void store_a1(const uint32_t (&out)[16]) {
-    tmem_st16(tl + kOffA1 + 16 * p, out);
-    tmem_wait_st();
-    fence_before();
-    mbar_arrive(&s.a1_full);
-  }
-
-  // features of tiles 0 and 1 (has0 = false: nothing to do at all); layer 1 of tile 0
-  __device__ __forceinline__ bool start(bool has0, float x0, float y0, float z0, bool has1, float x1, float y1,
-                                        float z1) {
-    put_features(has0, x0, y0, z0);
-    if (!has0) return true;
-    if (!wait(&s.d1_full, ph_d1, 0, 21)) return false;
-    put_features(has1, x1, y1, z1);  // A0 was read by L1(0)
-    uint32_t out[16];
-    layer1(out);
-    u++;
-    store_a1(out);
-    return true;
-  }
-
-  // layer-2 quarter q of the current tile: accumulator -> tanh(. + b2) -> A2[q % 2]
-  __device__ __forceinline__ bool quarter(uint32_t q) {
-    const uint32_t sl = u & 1;
-    if (!wait(&s.d2_full[sl], ph_d2, sl, 22)) return false;
-    uint32_t v[32], out[16];
-    tmem_ld32(slot() + 32 * p, v);
-    tmem_wait_ld();
-    const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const float4 bv = bb[k];
-      out[2 * k] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
-      out[2 * k + 1] =
-          tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
-    }
-    const uint32_t b = q & 1;
-    if (((a2_used >> b) & 1u) && !wait(&s.a2_free[b], ph_a2f, b, 24)) return false;  // L3 of quarter q - 2 done
-    a2_used |= 1u << b;
-    tmem_st16(tl + (b ? kOffA2b : kOffA2a) + 16 * p, out);
-    tmem_wait_st();
-    fence_before();
-    mbar_arrive(&s.a2_full[b]);
-    u++;
-    return true;
-  }
-
-  // M (row-major 3x3) of tile t from its layer-3 accumulator (parts 0 and 1 read it)
+  // M (row-major 3x3) of the tile retired now, from D3 (parts 0 and 1 read it)
   __device__ __forceinline__ bool read_d3(uint32_t t, float rx, float ry, float rz, float (&M)[9]) {
-    const uint32_t b = t & 1;
-    if (!wait(&s.d3_full[b], ph_d3, b, 23)) return false;
+    if (!wait(&s.d3_full, t & 1, 23)) return false;
     if (p < 2) {
-      uint32_t v[16];
-      tmem_ld16(tl + (b ? kOffD3b : kOffD3a), v);
+      uint32_t v[32];
+      tmem_ld32(tl + kOffD3, v);
       tmem_wait_ld();
       const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
       const float inv = __frcp_rn(nr);
@@ -558,37 +488,68 @@ struct Epi {
       }
     }
     fence_before();
-    mbar_arrive(&s.d3_free[b]);
+    mbar_arrive(&s.d3_free);
     return true;
   }
 
-  // Tile `tile`: quarters 0 and 1; retirement of tile - 1 (use(M) with its features px, py, pz,
-  // when has_prev); quarter 2; if has_next, the layer-1 epilogue of tile + 1, which writes the
-  // features of tile + 2 (has_next2: nx, ny, nz) or the end of the stream; quarter 3. Returns
-  // false if the CTA aborted.
+  // Tile `tile`: layer-1 epilogue (and the next tile's features, or the end of the stream),
+  // retirement of the previous tile (use(M) with its features (px, py, pz)), then the four
+  // layer-2 quarters. Returns false if the CTA aborted. All 512 epilogue threads call it.
   template <class Use>
-  __device__ __forceinline__ bool step(bool has_next, bool has_next2, float nx, float ny, float nz, bool has_prev,
-                                       float px, float py, float pz, Use&& use) {
-    if (!quarter(0) || !quarter(1)) return false;
-    if (has_prev) {
+  __device__ __forceinline__ bool step(bool has_next, float nx, float ny, float nz, float px, float py, float pz,
+                                       Use&& use) {
+    const uint32_t u = 5 * tile;
+    if (!wait(&s.d1_full, tile & 1, 21)) return false;
+    // A0 was consumed by L1(tile): the next tile's features (or the end of the stream)
+    if (has_next) {
+      write_features(tl + kOffA0, p, nx, ny, nz);
+      tmem_wait_st();
+    } else if (threadIdx.x == 0) {
+      *(volatile int*)&s.exit_flag = 1;  // released by this thread's arrival below
+    }
+    fence_before();
+    mbar_arrive(&s.a0_full);
+    {  // layer 1: tanh(W1 r + b1) -> A1
+      uint32_t v[32], out[16];
+      tmem_ld32(slot(u) + 32 * p, v);
+      tmem_wait_ld();
+#pragma unroll
+      for (int k = 0; k < 16; k++)
+        out[k] = tanh_f16x2(pack_f16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
+      tmem_st16(tl + kOffA1 + 16 * p, out);
+      tmem_wait_st();
+    }
+    fence_before();
+    mbar_arrive(&s.a1_full);
+    if (s.prof && threadIdx.x == 0) s.wprof[13]++;
+    if (tile > 0) {  // retire the previous tile while L2(tile, 0) runs on the tensor cores
       float M[9];
       if (!read_d3(tile - 1, px, py, pz, M)) return false;
       use(M);
     }
-    if (!quarter(2)) return false;
-    if (has_next) {
-      if (!wait(&s.d1_full, ph_d1, 0, 21)) return false;
-      put_features(has_next2, nx, ny, nz);  // A0 was read by L1(tile + 1)
-      uint32_t out[16];
-      layer1(out);
-      u++;
-      // A1 is still read by quarter 3's MMAs of this tile: store once they completed (the
-      // accumulator consumed next; waited here without consuming its phase)
-      if (!wait_ph(&s.d2_full[u & 1], (ph_d2 >> (u & 1)) & 1u, 25)) return false;
-      store_a1(out);
+    for (uint32_t q = 0; q < 4; q++) {
+      // each d2 / a2_full barrier completes twice per tile (quarters q and q + 2): parity q / 2
+      const uint32_t sl = (u + 1 + q) & 1;
+      if (!wait(&s.d2_full[sl], q >> 1, 22)) return false;
+      uint32_t v[32], out[16];
+      tmem_ld32(slot(u + 1 + q) + 32 * p, v);
+      tmem_wait_ld();
+      const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const float4 bv = bb[k];
+        out[2 * k] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
+        out[2 * k + 1] =
+            tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
+      }
+      // A2 buffer q % 2 was last read by L3 of quarter q - 2 (this tile, first commit on its
+      // barrier: parity 0) or of quarter q + 2 of the previous tile (second commit: parity 1)
+      if ((tile > 0 || q >= 2) && !wait(&s.a2_free[q & 1], q >= 2 ? 0u : 1u, 24)) return false;
+      tmem_st16(tl + (q & 1 ? kOffA2b : kOffA2a) + 16 * p, out);
+      tmem_wait_st();
+      fence_before();
+      mbar_arrive(&s.a2_full[sl]);
     }
-    if (!quarter(3)) return false;
-    if (s.prof && threadIdx.x == 0) s.wprof[15]++;
     tile++;
     return true;
   }
