@@ -185,8 +185,7 @@ struct hignn_model {
     hignn::TcWeights w;
     w.w2img = weights_tc.as<uint4>();
     w.w3img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2);
-    w.w1img = reinterpret_cast<const uint4*>(weights_tc.as<uint8_t>() + hignn::kH2 * hignn::kH1 * 2 +
-                                             16 * hignn::kH2 * 2);
+    w.w1b1 = f.w1b1;
     w.b2 = f.b2;
     w.b3 = f.b3;
     return w;
@@ -517,14 +516,6 @@ void ensure_far_plan(hignn_model* m) {
   m->plan_offset = m->rank_hint_offset;
 }
 
-// BF16 round-to-nearest-even
-uint16_t bf16_bits(float f) {
-  uint32_t u;
-  std::memcpy(&u, &f, 4);
-  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
-  u += 0x7fffu + ((u >> 16) & 1u);
-  return (uint16_t)(u >> 16);
-}
 // IEEE binary16, round to nearest even (subnormals kept, overflow to infinity)
 uint16_t f16_bits(float f) {
   uint32_t x;
@@ -547,13 +538,6 @@ uint16_t f16_bits(float f) {
   r >>= 13;
   if (rem > 0x1000u || (rem == 0x1000u && (r & 1u))) r++;
   return (uint16_t)(sign | r);
-}
-
-float bf16_value(uint16_t h) {
-  const uint32_t u = (uint32_t)h << 16;
-  float f;
-  std::memcpy(&f, &u, 4);
-  return f;
 }
 
 void check_device_error(hignn_model* m) {
@@ -597,38 +581,21 @@ void upload_weights(hignn_model* m, const std::vector<std::vector<float>>& W, co
   for (int q = 0; q < kOut * kH2; q++) w3[q] = W[2][q];
   float* b3 = w3 + kOut * kH2;
   for (int q = 0; q < kOut; q++) b3[q] = B[2][q];
-  // tensor-core images: K-major rows of 64 BF16 (128 B) per 64-wide K slab, 8-row groups of
+  // tensor-core images: K-major rows of 64 FP16 (128 B) per 64-wide K slab, 8-row groups of
   // 1024 B, 16-byte chunk c of row r stored at chunk position c ^ (r % 8) (128-byte swizzle)
   auto swz = [](int row, int k, int rows_per_slab) -> size_t {
     const int slab = k >> 6, kc = k & 63;
     return (size_t)slab * rows_per_slab * 128 + (size_t)(row >> 3) * 1024 + (row & 7) * 128 +
            (size_t)(((kc >> 3) ^ (row & 7)) * 16) + (kc & 7) * 2;
   };
-  // W2 (512 x 128) and W3 (rows 0-8 of 16 x 512) in FP16, W1 split in BF16
-  const size_t w1off = (size_t)kH2 * kH1 * 2 + 16 * kH2 * 2;
-  std::vector<uint8_t> img(w1off + (size_t)kH1 * 64 * 2, 0);
+  // W2 (512 x 128) and W3 (rows 0-8 of 16 x 512) in FP16; layer 1 stays FP32 (MlpF32::w1b1)
+  const size_t w3off = (size_t)kH2 * kH1 * 2;
+  std::vector<uint8_t> img(w3off + (size_t)16 * kH2 * 2, 0);
   auto put = [&](size_t off, uint16_t v) { std::memcpy(img.data() + off, &v, 2); };
   for (int nn = 0; nn < kH2; nn++)
     for (int k = 0; k < kH1; k++) put(swz(nn, k, kH2), f16_bits(W[1][(size_t)nn * kH1 + k]));
-  const size_t w3off = (size_t)kH2 * kH1 * 2;
   for (int o = 0; o < kOut; o++)
     for (int k = 0; k < kH2; k++) put(w3off + swz(o, k, 16), f16_bits(W[2][(size_t)o * kH2 + k]));
-  // layer 1 as one K = 16 MMA on split operands: row n = [W_hi(3), W_hi(3), W_lo(3), b1_hi, b1_lo, 0 x 5]
-  // against the feature row [r_hi(3), r_lo(3), r_hi(3), 1, 1, 0 x 5]
-  for (int nn = 0; nn < kH1; nn++) {
-    uint16_t row[16] = {0};
-    for (int d = 0; d < 3; d++) {
-      const float v = W[0][3 * nn + d];
-      const uint16_t hi = bf16_bits(v);
-      row[d] = hi;
-      row[3 + d] = hi;
-      row[6 + d] = bf16_bits(v - bf16_value(hi));
-    }
-    const uint16_t bh = bf16_bits(B[0][nn]);
-    row[9] = bh;
-    row[10] = bf16_bits(B[0][nn] - bf16_value(bh));
-    for (int k = 0; k < 16; k++) put(w1off + swz(nn, k, kH1), row[k]);
-  }
   m->has_weights = true;
   m->hint_valid = false;  // ACA ranks depend on the network
   if (m->device < 0) return;

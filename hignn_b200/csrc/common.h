@@ -76,12 +76,12 @@ struct MlpF32 {
   const float* b3;     // [kOut]
 };
 
-// Tensor-core weights: swizzled images of W1 (BF16, split, bias folded in), W2 and W3 (FP16)
-// plus FP32 biases of layers 2 and 3.
+// Tensor-core weights: swizzled FP16 images of W2 and W3 plus FP32 layer 1 (W1, b1) and FP32
+// biases of layers 2 and 3.
 struct TcWeights {
   const uint4* w2img;   // 512 x 128 FP16, K-major 128-byte swizzle (131072 B)
   const uint4* w3img;   // 16 x 512 FP16 (rows 0-8 W3, rows 9-15 zero) (16384 B)
-  const uint4* w1img;   // 128 x 64 BF16 slab, K 0-15 = [W_hi, W_hi, W_lo, b1_hi, b1_lo, 0...] (16384 B)
+  const float4* w1b1;   // [128]: (W1[k][0], W1[k][1], W1[k][2], b1[k])
   const float* b2;      // [512]
   const float* b3;      // [9]
   unsigned long long* prof = nullptr;  // optional wait profile of the engine (tc::kProfSlots counters)

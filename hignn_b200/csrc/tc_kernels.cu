@@ -85,7 +85,8 @@ struct NearTile {
 // Next close pair from the global counter, staged into buffer b (all epilogue threads).
 __device__ __forceinline__ bool near_fetch(NearTcSmem& S, const NearArgs& a, int* counter, int b, NearTile& c) {
   const int e = threadIdx.x;
-  if (e == 0) S.item[b] = atomicAdd(counter, 1);
+  // after an abort the stream ends here for every thread (the item is broadcast)
+  if (e == 0) S.item[b] = *(volatile int*)&S.tcs.abort_flag ? a.nwork : atomicAdd(counter, 1);
   tc::epi_bar();  // also: every thread is done with the pair last staged in buffer b
   const int item = S.item[b];
   if (item >= a.nwork) return false;
@@ -157,6 +158,7 @@ __device__ __forceinline__ void near_use(NearTcSmem& S, const NearTile& c, int p
 // The pair of a retired last tile is complete: flush its velocities (all epilogue threads).
 __device__ __forceinline__ void near_flush(NearTcSmem& S, const NearArgs& a, const NearTile& c) {
   tc::epi_bar();
+  if (*(volatile int*)&S.tcs.abort_flag) return;  // the launch reports an error; nothing is added
   const NearStage& G = S.st[c.buf];
   const PairWork pw = S.pw[c.buf];
   for (int q = threadIdx.x; q < 3 * pw.nI; q += tc::kEpiThreads)
@@ -185,7 +187,10 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     nbuf = (nbuf + 1) % 3;
     if (have) near_row(S, cur, row);
     eng.start(have, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true, has_prev = false;
+    bool has_prev = false;
+    // The control flow is uniform over the epilogue threads (tile positions and work items are
+    // shared), so the named barriers of near_fetch / near_flush are always reached by all of them;
+    // after an abort the engine calls return at once and near_fetch ends the stream.
     while (have) {
       // the next tile: the rest of this pair, or the next pair staged into the next buffer
       NearTile nxt = cur;
@@ -196,18 +201,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         nbuf = (nbuf + 1) % 3;
       }
       if (has_next) near_row(S, nxt, row);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { near_use(S, prev, p, M); }));
-      if (!ok) break;
+      eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+               [&](float (&M)[9]) { near_use(S, prev, p, M); });
       if (has_prev && prev.last) near_flush(S, a, prev);
       prev = cur;
       has_prev = true;
       if (!has_next) break;
       cur = nxt;
     }
-    if (ok && has_prev && tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2],
-                                                 [&](float (&M)[9]) { near_use(S, prev, p, M); })))
+    if (has_prev) {
+      eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { near_use(S, prev, p, M); });
       near_flush(S, a, prev);
+    }
     if (S.tcs.prof && threadIdx.x == 0) S.tcs.wprof[12] += (unsigned long long)(clock64() - t_start);
   }
   tc::cta_teardown(S.tcs);
@@ -289,22 +294,20 @@ __global__ void __launch_bounds__(tc::kThreads, 1) k_far_tc(FarArgs a, TcWeights
     FarRow prev{}, cur{};
     far_row(a, which, nact, tot, tile, row, cur);
     eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true;
-    for (;;) {
+    for (;;) {  // uniform over the epilogue threads; after an abort the engine calls return at once
       const int nt = tile + gridDim.x;
       const bool has_next = nt * tc::kTile < tot;
       FarRow nxt{};
       nxt.r[0] = 1.f;
       if (has_next) far_row(a, which, nact, tot, nt, row, nxt);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
-      if (!ok) break;
+      eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+               [&](float (&M)[9]) { far_use(a, which, prev, p, M); });
       prev = cur;
       if (!has_next) break;
       tile = nt;
       cur = nxt;
     }
-    if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); }));
+    eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { far_use(a, which, prev, p, M); });
   }
   tc::cta_teardown(S.tcs);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(a.evals, (unsigned long long)tot);
@@ -353,22 +356,20 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     EvalRow prev{}, cur{};
     eval_row(r, n, tile, row, cur);
     eng.start(true, cur.r[0], cur.r[1], cur.r[2]);
-    bool ok = true;
-    for (;;) {
+    for (;;) {  // uniform over the epilogue threads; after an abort the engine calls return at once
       const int64_t nt = tile + gridDim.x;
       const bool has_next = nt * tc::kTile < n;
       EvalRow nxt{};
       nxt.r[0] = 1.f;
       if (has_next) eval_row(r, n, nt, row, nxt);
-      ok = tc::epi_all(eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
-                                [&](float (&M)[9]) { use(prev, M); }));
-      if (!ok) break;
+      eng.step(has_next, nxt.r[0], nxt.r[1], nxt.r[2], prev.r[0], prev.r[1], prev.r[2],
+               [&](float (&M)[9]) { use(prev, M); });
       prev = cur;
       if (!has_next) break;
       tile = nt;
       cur = nxt;
     }
-    if (ok) tc::epi_all(eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { use(prev, M); }));
+    eng.finish(prev.r[0], prev.r[1], prev.r[2], [&](float (&M)[9]) { use(prev, M); });
   }
   tc::cta_teardown(S.tcs);
 }

@@ -1,47 +1,51 @@
 // Two-body network on the 5th-generation tensor cores (tcgen05, TMEM), 128 evaluations per tile.
 //
-// All three layers are tcgen05 MMAs with FP32 accumulation in tensor memory:
-//   layer 1 (3 -> 128): one K = 16 BF16 MMA on split operands. Each feature r is
-//       written as r_hi + r_lo (two BF16 numbers) and each W1 entry as W_hi + W_lo,
-//       so the row [r_hi, r_lo, r_hi, 1, 1] against [W_hi, W_hi, W_lo, b1_hi, b1_lo]
-//       gives W1 r + b1 to about 2^-16 relative, bias included;
+// Layer 1 (3 -> 128) runs on the CUDA cores in FP32 (three FMAs per hidden unit from the
+// features in registers); layers 2 and 3 are tcgen05 MMAs with FP32 accumulation in tensor
+// memory:
 //   layer 2 (128 -> 512): four quarters of N = 128, K = 128, FP16 operands;
 //   layer 3 (512 -> 9): N = 16, K = 512, FP16 operands (W3 rows 0-8, rows 9-15 zero).
 // FP16 rather than BF16 for layers 2 and 3: their operands are tanh outputs in [-1, 1] and
 // weights well inside FP16's range, so the 11-bit significand costs no range and rounds 8x finer.
-// Between layers the epilogue warps read the accumulator (tcgen05.ld), add the FP32 layer-2 bias,
-// round to FP16 pairs and apply tanh.approx.f16x2, and write the pairs back into tensor memory as
-// the next A operand.
+// The epilogue warps read a layer-2 accumulator (tcgen05.ld), add the FP32 bias, round to FP16
+// pairs, apply tanh.approx.f16x2 and write the pairs back into tensor memory as layer 3's A
+// operand; layer 1's tanh'd pairs go the same way into layer 2's A operand.
 //
-// The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM (the packed f16x2
-// form issues at half the rate of tanh.approx.f32, so packing saves issue slots, not MUFU time),
-// i.e. 40 clocks per evaluation per SM, against ~33 clocks of tensor-pipe occupancy (every MMA
-// holds the pipe >= ~64 cycles whatever its N). The pipeline is therefore
-// built to keep the MUFU busy: one tile stream per CTA, two FP32 accumulator
-// slots, separate buffers for layer 3's operand, and an MMA lane that runs a
-// quarter ahead of the epilogue without ever waiting for an MMA of its own (an
-// MMA's result reaches a waiting thread ~500 cycles after issue, measured).
+// The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM (tanh.approx.f16x2
+// issues at half the rate of tanh.approx.f32, measured on B200: packing saves issue slots, not
+// MUFU time), i.e. 40 clocks per evaluation per SM, against ~32 clocks of tensor-pipe occupancy
+// (every MMA holds the pipe >= ~64 cycles whatever its N). The schedule keeps the epilogue -- and
+// so the MUFU -- from waiting on the tensor core. Per tile t the epilogue handles
+//   quarter 0, quarter 1, the retirement of tile t-1, quarter 2, layer 1 of tile t+1, quarter 3
+// and the MMA lane issues each layer-2 quarter two epilogue phases before it is read:
+//   L2(t,0), L2(t,1) after layer 1 of t and quarter 3 of t-1; L2(t,2) after quarter 0;
+//   L2(t,3) after quarter 1; L3(t,q) after quarter q, behind the layer-2 MMA issued with it.
+// Layer 1 of tile t+1 is stored into A1 once quarter 3's accumulator is complete (the last MMA
+// reading A1), so no layer-2 quarter of t+1 waits for a layer-1 MMA and its epilogue, and the
+// first quarter of t+1 is on the tensor cores while quarter 3 of t is in the epilogue. Tile t-1
+// is retired from the other of two layer-3 accumulators.
 //
 // CTA = 17 warps:
 //   warps 0-15  epilogue; warp w reaches TMEM lanes 32 (w % 4) .. + 31, so the
 //               evaluation (row) e = 32 (w % 4) + lane is handled by four
-//               threads (part p = w / 4 owns columns 32p .. 32p + 31 of every
-//               128-column accumulator);
+//               threads (part p = w / 4 owns hidden units 32p .. 32p + 31 of layer 1
+//               and columns 32p .. 32p + 31 of every layer-2 quarter);
 //   warp 16     allocates tensor memory; one lane issues every MMA.
 // Tensor memory (512 columns allocated):
 //   [  0, 64)  A1: tanh(layer 1) as packed FP16 pairs (A operand of layer 2)
-//   [ 64,192)  slot 0 and [192,320) slot 1: FP32 accumulators, used in turn by
-//              layer 1 and the four layer-2 quarters of each tile
-//   [320,384)  and [384,448): A2 of even / odd quarters, the tanh'd FP16 pairs
-//              of a quarter (A operand of layer 3)
-//   [448,464)  layer-3 accumulator (M in columns 0-8)
-//   [480,488)  A0: the split features (K = 16 BF16) of layer 1
-// Shared memory: W2 (512 x 128) and W3 (16 x 512) as FP16 and W1 (128 x 16, in a 64-wide slab)
-// as BF16, canonical K-major 128-byte-swizzle layout, loaded once per CTA; FP32 biases b2, b3;
-// mbarriers. A barrier that completes twice per tile (the per-slot and per-buffer ones) is waited
-// with the parity of its position in the tile, and no waiter can fall two phases behind. Every wait is
-// bounded (about two seconds of clock): on a timeout the CTA records an error,
-// stops issuing work, drains its MMAs and frees its tensor memory.
+//   [ 64,192)  slot 0 (quarters 0, 2) and [192,320) slot 1 (quarters 1, 3): FP32 accumulators
+//   [320,384)  and [384,448): A2 of even / odd quarters, the tanh'd FP16 pairs of a quarter
+//              (A operand of layer 3)
+//   [448,464)  and [464,480): layer-3 accumulators of even / odd tiles (M in columns 0-8)
+// Shared memory: W2 (512 x 128) and W3 (16 x 512) as FP16, canonical K-major 128-byte-swizzle
+// layout, loaded once per CTA; FP32 (W1, b1) per hidden unit and biases b2, b3; mbarriers. A
+// barrier that completes twice per tile (the per-slot and per-buffer ones) is waited with the
+// parity of its position in the tile, and no waiter can fall two phases behind: every phase
+// needs the arrival of all epilogue threads or follows one that did. Every wait is bounded
+// (about two seconds of clock): on a timeout the CTA records an error, every later wait of the
+// CTA returns at once, and the CTA drains its MMAs and frees its tensor memory. The callers keep
+// their control flow uniform across the epilogue threads (tile counts and work items are
+// broadcast), so no named barrier is left waiting for a thread that gave up.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -59,31 +63,30 @@ constexpr int kTile = 128;
 constexpr int kEpiThreads = 512;
 constexpr int kThreads = 544;
 constexpr int kMmaWarp = 16;
-constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffA2a = 320, kOffA2b = 384, kOffD3 = 448, kOffA0 = 480;
+constexpr uint32_t kOffA1 = 0, kOffS0 = 64, kOffS1 = 192, kOffA2a = 320, kOffA2b = 384, kOffD3a = 448,
+                   kOffD3b = 464;
 constexpr int kW2Bytes = kH2 * kH1 * 2;      // 131072
 constexpr int kW3Rows = 16;
 constexpr int kW3Bytes = kW3Rows * kH2 * 2;  // 16384
-constexpr int kW1Bytes = kH1 * 64 * 2;       // 16384: 128 rows x one 64-wide K slab (K 0-15 used)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // Wait profile (TcWeights::prof non-null): slot c - 13 sums the cycles that lane 0 of every warp
-// spent in bounded waits with code c (13-20 the MMA lane: 13 first features, 14 layer-1 epilogue,
-// 15 quarter 0 in A2, 16 D3 free, 17 quarter 1, 18 quarter 2, 19 next features, 20 quarter 3;
-// 21-24 the epilogue warps: 21 layer-1 accumulator, 22 layer-2 accumulator, 23 layer-3
-// accumulator, 24 A2 buffer free); slot 12 the cycles of warp 0's whole epilogue; slot 13 the
-// tiles processed.
+// spent in bounded waits with code c (13-18 the MMA lane: 13 layer 1 in A1, 14-17 quarters 0-3
+// in A2, 18 layer-3 accumulator free; 21-24 the epilogue warps: 21 layer-2 accumulator of
+// quarters 0-2, 22 quarter 3's accumulator (A1 free), 23 layer-3 accumulator, 24 A2 buffer
+// free); slot 12 the cycles of warp 0's whole epilogue; slot 13 the tiles processed.
 constexpr int kProfSlots = 16;
 
 struct alignas(1024) Smem {
   uint8_t w2[kW2Bytes];
   uint8_t w3[kW3Bytes];
-  uint8_t w1[kW1Bytes];
-  uint64_t a0_full, d1_full, a1_full, d2_full[2], a2_full[2], a2_free[2], d3_full, d3_free, drain;
+  uint64_t a1_full, d2_full[2], a2_full[2], a2_free[2], d3_full[2], d3_free[2], drain;
   uint32_t tmem_base;
   int exit_flag;
   int abort_flag;
   unsigned long long* prof;          // optional wait profile (global, kProfSlots counters) or null
   unsigned long long wprof[16];      // per-CTA wait cycles by barrier code (lane 0 of each warp)
-  alignas(16) float b2[kH2];  // FP32 layer-2 bias, added before rounding to BF16
+  alignas(16) float4 w1b1[kH1];      // FP32 layer 1: (W1[k][0..2], b1[k]) per hidden unit
+  alignas(16) float b2[kH2];         // FP32 layer-2 bias, added before rounding to FP16
   float b3[16];
 };
 
@@ -257,25 +260,20 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   const uint4* src3 = w.w3img;
   uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
   for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
-  const uint4* src1 = w.w1img;
-  uint4* dst1 = reinterpret_cast<uint4*>(s.w1);
-  for (int i = t; i < kW1Bytes / 16; i += blockDim.x) dst1[i] = src1[i];
+  for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
   for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t < 16) s.wprof[t] = 0ull;
   if (t == 0) {
     s.prof = w.prof;
-    mbar_init(&s.a0_full, kEpiThreads);
-    mbar_init(&s.d1_full, 1);
     mbar_init(&s.a1_full, kEpiThreads);
-    mbar_init(&s.d2_full[0], 1);
-    mbar_init(&s.d2_full[1], 1);
-    mbar_init(&s.a2_full[0], kEpiThreads);
-    mbar_init(&s.a2_full[1], kEpiThreads);
-    mbar_init(&s.a2_free[0], 1);
-    mbar_init(&s.a2_free[1], 1);
-    mbar_init(&s.d3_full, 1);
-    mbar_init(&s.d3_free, kEpiThreads);
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&s.d2_full[i], 1);
+      mbar_init(&s.a2_full[i], kEpiThreads);
+      mbar_init(&s.a2_free[i], 1);
+      mbar_init(&s.d3_full[i], 1);
+      mbar_init(&s.d3_free[i], kEpiThreads);
+    }
     mbar_init(&s.drain, 1);
     s.exit_flag = 0;
     s.abort_flag = 0;
@@ -298,25 +296,23 @@ __device__ __forceinline__ void cta_teardown(Smem& s) {
 }
 
 // ------------------------------------------------------------------ MMA lane
-// One thread issues every MMA, per tile t (u = 5t; accumulator slot of a use = u & 1; A2 buffer
-// of quarter q = q & 1), in this order:
-//   L2(t,0)->slot(u+1)  L2(t,1)->slot(u+2)          after a1_full(t): A1 written, L1 slot read
-//   L2(t,2)->slot(u+3)  L3(t,0)<-A2[0]               after a2(q0): slot(u+1) read, A2[0] written
-//   L2(t,3)->slot(u+4)  L3(t,1)<-A2[1]               after a2(q1)
-//   L1(t+1)->slot(u+5)  L3(t,2)<-A2[0]               after a2(q2) and a0_full(t+1)
-//   L3(t,3)<-A2[1]  commit d3_full                   after a2(q3)
-// Every MMA holds the tensor pipe >= ~64 cycles whatever its N, so the eight layer-3 MMAs of a
-// quarter cost as much as its eight layer-2 MMAs; the accumulator the epilogue waits for next
-// is therefore queued ahead of the layer-3 MMAs, whose result is needed only at retirement.
-// An accumulator slot is reused as soon as the epilogue has read it (its tanh'd pairs go to a
-// separate A2 buffer), so the lane never waits for an MMA of its own: the ~500-cycle latency
-// from an MMA's issue to its commit reaching a waiting thread is paid only by threads that have
-// other work queued. L3(t,0) overwrites D3, so it also waits until the epilogue has read D3 of
-// tile t-1 (d3_free).
+// One thread issues every MMA; quarter q of a tile reads accumulator slot q % 2 and A2 buffer
+// q % 2, tile t writes layer-3 accumulator t % 2. Per tile t, in this order:
+//   L2(t,2)->slot 0, L3(t,0)<-A2[0]         after a2(q0): slot 0 read, A2[0] written
+//   L2(t,3)->slot 1, L3(t,1)<-A2[1]         after a2(q1)
+//   L3(t,2)<-A2[0]                          after a2(q2)
+//   L2(t+1,0)->slot 0                       after a1_full(t+1): layer 1 of t+1 in A1
+//   L2(t+1,1)->slot 1, L3(t,3)<-A2[1], commit d3_full[t % 2]   after a2(q3)
+// A layer-2 quarter is queued ahead of the layer-3 MMAs issued with it: the epilogue reads it two
+// phases later, while layer 3 is needed only at retirement. An accumulator slot is reused as soon
+// as the epilogue has read it (its tanh'd pairs go to a separate A2 buffer), so the lane never
+// waits for an MMA of its own: the ~500-cycle latency from an MMA's issue to its commit reaching
+// a waiting thread is paid only by threads that have other work queued. L3(t,0) overwrites the
+// layer-3 accumulator of tile t - 2, so it also waits until the epilogue has read that (d3_free).
 struct MmaLane {
   Smem& s;
   int* err;
-  uint32_t tb, w1, w2, w3;
+  uint32_t tb, w2, w3;
   bool ok = true;
 
   __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, int code) {
@@ -327,70 +323,64 @@ struct MmaLane {
     if (ok) fence_after();
     return ok;
   }
-  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tb + (u & 1 ? kOffS1 : kOffS0); }
-  __device__ __forceinline__ void l1(uint32_t u) {
-    mma_ts(slot(u), tb + kOffA0, sdesc(w1), idesc_bf16(128, 128), 0u);
-    mma_commit(&s.d1_full);
-  }
-  __device__ __forceinline__ void l2(uint32_t u, uint32_t q) {
+  __device__ __forceinline__ uint32_t slot(uint32_t q) const { return tb + (q & 1 ? kOffS1 : kOffS0); }
+  // layer-2 quarter q of the tile whose layer 1 is in A1
+  __device__ __forceinline__ void l2(uint32_t q) {
     const uint32_t id = idesc_f16x(128, 128);
 #pragma unroll
     for (uint32_t kk = 0; kk < 8; kk++) {
       const uint32_t bb = w2 + (kk >> 2) * (kH2 * 128) + q * (128 * 128) + (kk & 3) * 32;
-      mma_ts(slot(u), tb + kOffA1 + 8 * kk, sdesc(bb), id, kk > 0);
+      mma_ts(slot(q), tb + kOffA1 + 8 * kk, sdesc(bb), id, kk > 0);
     }
-    mma_commit(&s.d2_full[u & 1]);
+    mma_commit(&s.d2_full[q & 1]);
   }
-  // layer 3 of quarter q from its A2 buffer into D3
-  __device__ __forceinline__ void l3(uint32_t q) {
+  // layer 3 of quarter q of tile t from its A2 buffer into the tile's layer-3 accumulator
+  __device__ __forceinline__ void l3(uint32_t t, uint32_t q) {
     const uint32_t id = idesc_f16x(128, kW3Rows);
     const uint32_t a2 = tb + (q & 1 ? kOffA2b : kOffA2a);
+    const uint32_t d3 = tb + (t & 1 ? kOffD3b : kOffD3a);
 #pragma unroll
     for (uint32_t kk = 0; kk < 8; kk++) {
       const uint32_t kg = q * 128 + kk * 16;  // global K of layer 3
       const uint32_t bb = w3 + (kg >> 6) * (kW3Rows * 128) + ((kg & 63) >> 3) * 16;
-      mma_ts(tb + kOffD3, a2 + 8 * kk, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
+      mma_ts(d3, a2 + 8 * kk, sdesc(bb), id, (q > 0 || kk > 0) ? 1u : 0u);
     }
     mma_commit(&s.a2_free[q & 1]);
   }
-  // the epilogue wrote the A2 pairs of quarter q. Each of the two a2_full barriers completes
-  // twice per tile (quarters q and q + 2), so the phase parity is q / 2.
-  __device__ __forceinline__ bool a2(uint32_t u, uint32_t q, int code) {
-    return wait(&s.a2_full[(u + 1 + q) & 1], q >> 1, code);
-  }
+  // the epilogue wrote the A2 pairs of quarter q. Each a2_full barrier completes twice per tile
+  // (quarters q and q + 2), so the phase parity is q / 2.
+  __device__ __forceinline__ bool a2(uint32_t q) { return wait(&s.a2_full[q & 1], q >> 1, 14 + (int)q); }
 
   __device__ void run() {
-    // tile 0: layer 1 once its features are in A0
-    if (!wait(&s.a0_full, 0, 13)) return;
+    // tile 0: its layer 1 in A1, or the end of an empty stream
+    if (!wait(&s.a1_full, 0, 13)) return;
     if (*(volatile int*)&s.exit_flag) return;
-    l1(0);
+    l2(0);
+    l2(1);
     for (uint32_t t = 0;; t++) {
-      const uint32_t u = 5 * t;
-      if (!wait(&s.a1_full, t & 1, 14)) return;
-      l2(u + 1, 0);
-      l2(u + 2, 1);
-      if (!a2(u, 0, 15)) return;
-      l2(u + 3, 2);  // the next accumulator first: the epilogue waits for it, D3 only at retirement
-      if (t > 0 && !wait(&s.d3_free, (t - 1) & 1, 16)) return;
-      l3(0);
-      if (!a2(u, 1, 17)) return;
-      l2(u + 4, 3);
-      l3(1);
-      if (!a2(u, 2, 18)) return;
-      if (!wait(&s.a0_full, (t + 1) & 1, 19)) return;  // the next tile's features, or the end
+      if (!a2(0)) return;
+      l2(2);
+      if (t >= 2 && !wait(&s.d3_free[t & 1], ((t - 2) >> 1) & 1, 18)) return;
+      l3(t, 0);
+      if (!a2(1)) return;
+      l2(3);
+      l3(t, 1);
+      if (!a2(2)) return;
+      l3(t, 2);
+      if (!wait(&s.a1_full, (t + 1) & 1, 13)) return;  // layer 1 of the next tile, or the end
       const bool more = !*(volatile int*)&s.exit_flag;
-      if (more) l1(u + 5);
-      l3(2);
-      if (!a2(u, 3, 20)) return;
-      l3(3);
-      mma_commit(&s.d3_full);
+      if (more) l2(0);
+      if (!a2(3)) return;
+      if (more) l2(1);
+      l3(t, 3);
+      mma_commit(&s.d3_full[t & 1]);
       if (!more) return;
     }
   }
 };
 
 __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
-  MmaLane lane{s, err, s.tmem_base, saddr(s.w1), saddr(s.w2), saddr(s.w3)};
+  MmaLane lane{s, err, s.tmem_base, saddr(s.w2), saddr(s.w3)};
   lane.run();
   // drain: every MMA issued so far completes before tensor memory is released
   mma_commit(&s.drain);
@@ -401,40 +391,17 @@ __device__ __forceinline__ void mma_loop(Smem& s, int* err) {
 
 // ------------------------------------------------------------------ epilogue side
 // Warp w (0-15) reaches TMEM lanes 32 (w % 4) ..; the evaluation (row) e = 32 (w % 4) + lane is
-// handled by four threads (warps w % 4 + 4 p, p = 0..3), thread p owning columns 32p..32p+31
-// of every 128-column accumulator and packed columns 16p..16p+15 of A1 and of the A2 buffers.
+// handled by four threads (warps w % 4 + 4 p, p = 0..3), thread p owning hidden units
+// 32p..32p+31 of layer 1, columns 32p..32p+31 of every layer-2 quarter and packed columns
+// 16p..16p+15 of A1 and of the A2 buffers.
 __device__ __forceinline__ int epi_row() { return 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31); }
 __device__ __forceinline__ int epi_part() { return (threadIdx.x >> 7) & 3; }
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 512;\n" ::: "memory"); }
 
-// All 512 epilogue threads agree on ok (false if any thread's bounded wait gave up).
-__device__ __forceinline__ bool epi_all(bool ok) {
-  uint32_t r;
-  asm volatile("{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, 512, p;\nselp.u32 %0, 1, 0, q;\n}\n"
-               : "=r"(r)
-               : "r"((uint32_t)ok)
-               : "memory");
-  return r != 0;
-}
-
-__device__ __forceinline__ float bf16_round(float x) { return __uint_as_float(pack_bf16(x, 0.f) << 16); }
-
-// Layer-1 operand of one row: K = 16 BF16 values [r_hi(3), r_lo(3), r_hi(3), 1, 1, 0 x 5] packed in
-// pairs; part 0 writes columns 0-3, part 1 columns 4-7.
-__device__ __forceinline__ void write_features(uint32_t ta0, int p, float rx, float ry, float rz) {
-  const float hx = bf16_round(rx), hy = bf16_round(ry), hz = bf16_round(rz);
-  if (p == 0) {
-    const float lx = rx - hx, ly = ry - hy, lz = rz - hz;  // exact in FP32
-    tmem_st4(ta0, pack_bf16(hx, hy), pack_bf16(hz, lx), pack_bf16(ly, lz), pack_bf16(hx, hy));
-  } else if (p == 1) {
-    tmem_st4(ta0 + 4, pack_bf16(hz, 1.f), pack_bf16(1.f, 0.f), 0u, 0u);
-  }
-}
-
 // The tile engine seen from the epilogue threads. Tiles are retired one step late: step(t)
-// computes the network of tile t up to its layer-3 MMAs and hands the finished M of tile t-1 to
-// `use`, called between the layer-1 epilogue of tile t and its first quarter -- the time the
-// first layer-2 quarter of tile t spends on the tensor cores. finish() retires the last tile.
+// computes the network of tile t up to its layer-3 MMAs, layer 1 of tile t + 1, and hands the
+// finished M of tile t - 1 to `use`, called between quarters 1 and 2 of tile t. finish() retires
+// the last tile. Every call returns false once the CTA has aborted (and then does nothing).
 struct Epi {
   Smem& s;
   int* err;
@@ -452,28 +419,71 @@ struct Epi {
     if (ok) fence_after();
     return ok;
   }
-  // threads that receive M: parts 0 and 1 (both hold all nine entries)
-  __device__ __forceinline__ bool has_m() const { return p < 2; }
-  __device__ __forceinline__ uint32_t slot(uint32_t u) const { return tl + (u & 1 ? kOffS1 : kOffS0); }
+  __device__ __forceinline__ uint32_t slot(uint32_t q) const { return tl + (q & 1 ? kOffS1 : kOffS0); }
 
-  // features of the first tile (has = false: nothing to do at all)
-  __device__ __forceinline__ void start(bool has, float rx, float ry, float rz) {
+  // tanh(W1 r + b1) of this thread's 32 hidden units as FP16 pairs (FP32 FMAs, bias first)
+  __device__ __forceinline__ void layer1(float rx, float ry, float rz, uint32_t (&out)[16]) const {
+    const float4* w = s.w1b1 + 32 * p;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const float4 a = w[2 * k], b = w[2 * k + 1];
+      const float h0 = fmaf(a.z, rz, fmaf(a.y, ry, fmaf(a.x, rx, a.w)));
+      const float h1 = fmaf(b.z, rz, fmaf(b.y, ry, fmaf(b.x, rx, b.w)));
+      out[k] = tanh_f16x2(pack_f16(h0, h1));
+    }
+  }
+  // A1 <- out, then the lane may issue the tile's layer-2 quarters (or learns of the end)
+  __device__ __forceinline__ void publish_a1(bool has, const uint32_t (&out)[16]) {
     if (has) {
-      write_features(tl + kOffA0, p, rx, ry, rz);
+      tmem_st16(tl + kOffA1 + 16 * p, out);
       tmem_wait_st();
     } else if (threadIdx.x == 0) {
       *(volatile int*)&s.exit_flag = 1;  // released by this thread's arrival below
     }
     fence_before();
-    mbar_arrive(&s.a0_full);
+    mbar_arrive(&s.a1_full);
   }
 
-  // M (row-major 3x3) of the tile retired now, from D3 (parts 0 and 1 read it)
+  // layer 1 of the first tile (has = false: nothing to do at all)
+  __device__ __forceinline__ void start(bool has, float rx, float ry, float rz) {
+    uint32_t out[16];
+    if (has) layer1(rx, ry, rz, out);
+    publish_a1(has, out);
+  }
+
+  // Quarter q: accumulator slot q % 2 (+ FP32 bias) -> tanh -> A2 buffer q % 2. Quarter 3's
+  // accumulator was already waited for (before A1 was rewritten).
+  __device__ __forceinline__ bool quarter(uint32_t q) {
+    // each d2_full / a2_full barrier completes twice per tile (quarters q and q + 2): parity q / 2
+    if (q != 3 && !wait(&s.d2_full[q & 1], q >> 1, 21)) return false;
+    uint32_t v[32], out[16];
+    tmem_ld32(slot(q) + 32 * p, v);
+    tmem_wait_ld();
+    const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float4 bv = bb[k];
+      out[2 * k] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
+      out[2 * k + 1] =
+          tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
+    }
+    // A2 buffer q % 2 was last read by L3 of quarter q - 2 (this tile, first commit on its
+    // barrier: parity 0) or of quarter q + 2 of the previous tile (second commit: parity 1)
+    if ((tile > 0 || q >= 2) && !wait(&s.a2_free[q & 1], q >= 2 ? 0u : 1u, 24)) return false;
+    tmem_st16(tl + (q & 1 ? kOffA2b : kOffA2a) + 16 * p, out);
+    tmem_wait_st();
+    fence_before();
+    mbar_arrive(&s.a2_full[q & 1]);
+    return true;
+  }
+
+  // M (row-major 3x3) of tile t, from its layer-3 accumulator (parts 0 and 1 read it; both end
+  // up with all nine entries)
   __device__ __forceinline__ bool read_d3(uint32_t t, float rx, float ry, float rz, float (&M)[9]) {
-    if (!wait(&s.d3_full, t & 1, 23)) return false;
+    if (!wait(&s.d3_full[t & 1], (t >> 1) & 1, 23)) return false;
     if (p < 2) {
-      uint32_t v[32];
-      tmem_ld32(tl + kOffD3, v);
+      uint32_t v[16];
+      tmem_ld16(tl + (t & 1 ? kOffD3b : kOffD3a), v);
       tmem_wait_ld();
       const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
       const float inv = __frcp_rn(nr);
@@ -488,68 +498,32 @@ struct Epi {
       }
     }
     fence_before();
-    mbar_arrive(&s.d3_free);
+    mbar_arrive(&s.d3_free[t & 1]);
     return true;
   }
 
-  // Tile `tile`: layer-1 epilogue (and the next tile's features, or the end of the stream),
-  // retirement of the previous tile (use(M) with its features (px, py, pz)), then the four
-  // layer-2 quarters. Returns false if the CTA aborted. All 512 epilogue threads call it.
+  // Tile `tile`: quarters 0 and 1, retirement of the previous tile (use(M) with its features
+  // (px, py, pz)), quarter 2, layer 1 of the next tile (features nx, ny, nz; has_next = false:
+  // the end of the stream), quarter 3. All 512 epilogue threads call it.
   template <class Use>
   __device__ __forceinline__ bool step(bool has_next, float nx, float ny, float nz, float px, float py, float pz,
                                        Use&& use) {
-    const uint32_t u = 5 * tile;
-    if (!wait(&s.d1_full, tile & 1, 21)) return false;
-    // A0 was consumed by L1(tile): the next tile's features (or the end of the stream)
-    if (has_next) {
-      write_features(tl + kOffA0, p, nx, ny, nz);
-      tmem_wait_st();
-    } else if (threadIdx.x == 0) {
-      *(volatile int*)&s.exit_flag = 1;  // released by this thread's arrival below
-    }
-    fence_before();
-    mbar_arrive(&s.a0_full);
-    {  // layer 1: tanh(W1 r + b1) -> A1
-      uint32_t v[32], out[16];
-      tmem_ld32(slot(u) + 32 * p, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int k = 0; k < 16; k++)
-        out[k] = tanh_f16x2(pack_f16(__uint_as_float(v[2 * k]), __uint_as_float(v[2 * k + 1])));
-      tmem_st16(tl + kOffA1 + 16 * p, out);
-      tmem_wait_st();
-    }
-    fence_before();
-    mbar_arrive(&s.a1_full);
-    if (s.prof && threadIdx.x == 0) s.wprof[13]++;
-    if (tile > 0) {  // retire the previous tile while L2(tile, 0) runs on the tensor cores
+    if (!quarter(0) || !quarter(1)) return false;
+    if (tile > 0) {  // retire the previous tile while L2(tile, 2) and L3(tile, 0) run
       float M[9];
       if (!read_d3(tile - 1, px, py, pz, M)) return false;
       use(M);
     }
-    for (uint32_t q = 0; q < 4; q++) {
-      // each d2 / a2_full barrier completes twice per tile (quarters q and q + 2): parity q / 2
-      const uint32_t sl = (u + 1 + q) & 1;
-      if (!wait(&s.d2_full[sl], q >> 1, 22)) return false;
-      uint32_t v[32], out[16];
-      tmem_ld32(slot(u + 1 + q) + 32 * p, v);
-      tmem_wait_ld();
-      const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const float4 bv = bb[k];
-        out[2 * k] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
-        out[2 * k + 1] =
-            tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
-      }
-      // A2 buffer q % 2 was last read by L3 of quarter q - 2 (this tile, first commit on its
-      // barrier: parity 0) or of quarter q + 2 of the previous tile (second commit: parity 1)
-      if ((tile > 0 || q >= 2) && !wait(&s.a2_free[q & 1], q >= 2 ? 0u : 1u, 24)) return false;
-      tmem_st16(tl + (q & 1 ? kOffA2b : kOffA2a) + 16 * p, out);
-      tmem_wait_st();
-      fence_before();
-      mbar_arrive(&s.a2_full[sl]);
+    if (!quarter(2)) return false;
+    {
+      uint32_t out[16];
+      if (has_next) layer1(nx, ny, nz, out);
+      // quarter 3's accumulator complete: every layer-2 MMA of this tile has read A1
+      if (!wait(&s.d2_full[1], 1, 22)) return false;
+      publish_a1(has_next, out);
     }
+    if (!quarter(3)) return false;
+    if (s.prof && threadIdx.x == 0) s.wprof[13]++;
     tile++;
     return true;
   }
