@@ -42,11 +42,18 @@ inline void set_max_dynamic_smem(K kernel, size_t bytes, cudaStream_t s) {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
-  void ensure(size_t b) {
+  // the caller's file and line go into the error of a failed allocation
+  void ensure(size_t b, const char* file = __builtin_FILE(), int line = __builtin_LINE()) {
     if (b <= bytes && p) return;
     release();
     if (b == 0) return;
-    HIGNN_CUDA(cudaMalloc(&p, b));
+    const cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+      throw Error(-2, std::string("cudaMalloc of ") + std::to_string(b) + " bytes failed: " + cudaGetErrorString(e) +
+                          " (buffer grown at " + file + ":" + std::to_string(line) + ")");
+    }
     bytes = b;
   }
   void release() {

@@ -461,16 +461,18 @@ void CellList::build(const float4* x, int64_t n, double cutoff, cudaStream_t s) 
   // cells no smaller than the cutoff (a little larger, so rounding never splits a neighbour pair
   // across non-adjacent cells), at most kMaxCells of them
   double size = cutoff * (1.0 + 1e-5);
+  // counts in double: a far-flung position must coarsen the grid, not overflow the product
   auto dims = [&](double sz, int* nd) {
-    int64_t tot = 1;
+    double tot = 1.0;
     for (int d = 0; d < 3; d++) {
-      nd[d] = std::max(1, (int)std::floor((double)(hi[d] - lo[d]) / sz) + 1);
-      tot *= nd[d];
+      const double c = std::floor((double)(hi[d] - lo[d]) / sz) + 1.0;
+      tot *= c;
+      nd[d] = (int)std::min(c, (double)kMaxCells);
     }
     return tot;
   };
   int nd[3];
-  while (dims(size, nd) > kMaxCells) size *= 1.26;
+  while (dims(size, nd) > (double)kMaxCells) size *= 1.26;
   grid.lo = make_double3(lo[0], lo[1], lo[2]);
   grid.inv = 1.0 / size;
   grid.nx = nd[0];
