@@ -644,6 +644,7 @@ hignn::FarArgs far_args(hignn_model* m, const hignn_model::Batch& bt, const hign
   a.eps2 = m->epsilon * m->epsilon;
   a.use_symmetry = m->use_symmetry ? 1 : 0;
   a.defer_apply = student_pass ? 1 : 0;
+  a.fast_pivots = m->precision >= 1 ? 1 : 0;
   return a;
 }
 

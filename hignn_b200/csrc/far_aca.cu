@@ -31,25 +31,38 @@ namespace {
 // pivots at N = 1M, against 527 ms for 256-thread CTAs at ~126 registers, two per SM; a cap of
 // 40 registers spills too much and is slower).
 constexpr int kPivThreads = 128;
+// FP32 bookkeeping (the fast forms): 64 registers, no spills; 10 or 12 CTAs per SM spill and ran
+// slower at N = 1M (287 ms of pivots at 8, 297 at 10, 315 at 12, 337 for the FP64 form)
+constexpr int kPivBlocksF32 = 8;
 constexpr int kApplyThreads = 256;  // the deferred apply: few phases, wider CTAs
 
-__device__ __forceinline__ double det3(const double* m) {
+template <typename T>
+__device__ __forceinline__ T det3(const T* m) {
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
          m[2] * (m[3] * m[7] - m[4] * m[6]);
 }
 
+template <typename T>
+__device__ __forceinline__ T lowest();
+template <>
+__device__ __forceinline__ double lowest<double>() { return -DBL_MAX; }
+template <>
+__device__ __forceinline__ float lowest<float>() { return -FLT_MAX; }
+
 // argmax with the first index winning ties (Kokkos MaxLoc over a strict '>').
-__device__ __forceinline__ void better(double& v, int& i, double v2, int i2) {
+template <typename T>
+__device__ __forceinline__ void better(T& v, int& i, T v2, int i2) {
   if (i2 >= 0 && (i < 0 || v2 > v || (v2 == v && i2 < i))) {
     v = v2;
     i = i2;
   }
 }
 
-__device__ void block_argmax(double& v, int& i, double* sv, int* si) {
+template <typename T>
+__device__ void block_argmax(T& v, int& i, T* sv, int* si) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
-    double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    T v2 = __shfl_down_sync(0xffffffffu, v, o);
     int i2 = __shfl_down_sync(0xffffffffu, i, o);
     better(v, i, v2, i2);
   }
@@ -59,7 +72,7 @@ __device__ void block_argmax(double& v, int& i, double* sv, int* si) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double bv = sv[0];
+    T bv = sv[0];
     int bi = si[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) better(bv, bi, sv[w], si[w]);
     sv[0] = bv;
@@ -71,8 +84,8 @@ __device__ void block_argmax(double& v, int& i, double* sv, int* si) {
   __syncthreads();
 }
 
-template <int N>
-__device__ void block_sum(double (&v)[N], double* scratch /* [32][N] */) {
+template <int N, typename T>
+__device__ void block_sum(T (&v)[N], T* scratch /* [32][N] */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < N; q++)
@@ -83,7 +96,7 @@ __device__ void block_sum(double (&v)[N], double* scratch /* [32][N] */) {
   __syncthreads();
   if (threadIdx.x == 0)
     for (int q = 0; q < N; q++) {
-      double s = 0.0;
+      T s = 0;
       for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w * N + q];
       scratch[q] = s;
     }
@@ -95,11 +108,11 @@ __device__ void block_sum(double (&v)[N], double* scratch /* [32][N] */) {
 
 // block_argmax and block_sum<12> in one pass: the same per-warp and per-CTA orders, two barriers
 // instead of six (sv / si / scratch are not written again before the caller's next barrier).
-__device__ void block_argmax_sum(double& best, int& bi, double (&v)[12], double* sv, int* si,
-                                 double* scratch /* [32][12] */) {
+template <typename T>
+__device__ void block_argmax_sum(T& best, int& bi, T (&v)[12], T* sv, int* si, T* scratch /* [32][12] */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
-    double v2 = __shfl_down_sync(0xffffffffu, best, o);
+    T v2 = __shfl_down_sync(0xffffffffu, best, o);
     int i2 = __shfl_down_sync(0xffffffffu, bi, o);
     better(best, bi, v2, i2);
   }
@@ -114,13 +127,13 @@ __device__ void block_argmax_sum(double& best, int& bi, double (&v)[12], double*
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double bv = sv[0];
+    T bv = sv[0];
     int bj = si[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) better(bv, bj, sv[w], si[w]);
     sv[0] = bv;
     si[0] = bj;
     for (int q = 0; q < 12; q++) {
-      double s = 0.0;
+      T s = 0;
       for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w * 12 + q];
       scratch[q] = s;
     }
@@ -289,10 +302,11 @@ __global__ void __launch_bounds__(simt::kThreads, 1) k_far_eval(FarArgs a, MlpF3
 }
 
 // Orthogonalise the new column, pick the pivot row, normalise (one CTA per active block).
-__global__ void __launch_bounds__(kPivThreads, 8) k_far_col_pivot(FarArgs a) {
+template <typename T, int MinBlocks>
+__global__ void __launch_bounds__(kPivThreads, MinBlocks) k_far_col_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
-  double* qj = dsm;  // [k][9]
-  __shared__ double sv[32], inv[9];
+  T* qj = reinterpret_cast<T*>(dsm);  // [k][9]
+  __shared__ T sv[32], inv[9];
   __shared__ int si[32];
   const int nact = a.ctr[kCtrActive];
   for (int ai = blockIdx.x; ai < nact; ai += gridDim.x) {
@@ -305,18 +319,18 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_col_pivot(FarArgs a) {
     qj[q] = a.Q[9 * (bk.qOff + (int64_t)l * bk.nJ + jk) + e];
   }
   __syncthreads();
-  double best = -DBL_MAX;
+  T best = lowest<T>();
   int bi = -1;
   pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
-    double c[9];
+    T c[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
     if (k > 0) {
-      double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      T s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int l = 0; l < k; l++) {
         const pool_t* cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
-        const double* ql = qj + 9 * l;
+        const T* ql = qj + 9 * l;
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
@@ -326,11 +340,11 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_col_pivot(FarArgs a) {
       }
 #pragma unroll
       for (int q = 0; q < 9; q++) {  // stored rounded; the pivot search sees the stored value
-        c[q] = (double)(pool_t)(c[q] - s[q]);
+        c[q] = (T)(pool_t)(c[q] - s[q]);
         Ck[9 * i + q] = (pool_t)c[q];
       }
     }
-    const double d = det3(c);
+    const T d = det3(c);
     if (!a.usedRow[bk.rOff + i] && (bi < 0 || d > best)) {
       best = d;
       bi = i;
@@ -351,26 +365,26 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_col_pivot(FarArgs a) {
     const pool_t* m = Ck + 9 * bi;
     const double A = m[0], B = m[1], C = m[2], D = m[3], E = m[4], F = m[5], G = m[6], H = m[7], I = m[8];
     const double det = A * (E * I - F * H) - B * (D * I - F * G) + C * (D * H - E * G);
-    inv[0] = (E * I - F * H) / det;
-    inv[1] = -(B * I - C * H) / det;
-    inv[2] = (B * F - C * E) / det;
-    inv[3] = -(D * I - F * G) / det;
-    inv[4] = (A * I - C * G) / det;
-    inv[5] = -(A * F - C * D) / det;
-    inv[6] = (D * H - E * G) / det;
-    inv[7] = -(A * H - B * G) / det;
-    inv[8] = (A * E - B * D) / det;
+    inv[0] = (T)((E * I - F * H) / det);
+    inv[1] = (T)(-(B * I - C * H) / det);
+    inv[2] = (T)((B * F - C * E) / det);
+    inv[3] = (T)(-(D * I - F * G) / det);
+    inv[4] = (T)((A * I - C * G) / det);
+    inv[5] = (T)(-(A * F - C * D) / det);
+    inv[6] = (T)((D * H - E * G) / det);
+    inv[7] = (T)(-(A * H - B * G) / det);
+    inv[8] = (T)((A * E - B * D) / det);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
-    double c[9], o[9];
+    T c[9], o[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
       for (int cc = 0; cc < 3; cc++) {
-        double acc = c[3 * r] * inv[cc];
+        T acc = c[3 * r] * inv[cc];
         acc = acc + c[3 * r + 1] * inv[3 + cc];
         acc = acc + c[3 * r + 2] * inv[6 + cc];
         o[3 * r + cc] = acc;
@@ -445,12 +459,13 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
 }
 
 // Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
-__global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
+template <typename T, int MinBlocks>
+__global__ void __launch_bounds__(kPivThreads, MinBlocks) k_far_row_pivot(FarArgs a) {
   extern __shared__ __align__(16) double dsm[];
-  double* ci = dsm;                          // [k][9]
-  double* mid = dsm + 9 * a.ldr;            // [rank][3]
-  double* mid2 = mid + 3 * a.ldr;            // [rank][3]
-  __shared__ double sv[32], cross[8][18], red[32 * 12];
+  T* ci = reinterpret_cast<T*>(dsm);  // [k][9]
+  double* mid = dsm + 9 * a.ldr;      // [rank][3]
+  double* mid2 = mid + 3 * a.ldr;     // [rank][3]
+  __shared__ T sv[32], cross[8][18], red[32 * 12];
   __shared__ int si[32];
   __shared__ int s_done, s_rank;
   const int nact = a.ctr[kCtrActive];
@@ -466,21 +481,21 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
   }
   if (threadIdx.x == 0) a.usedCol[bk.colOff + a.cols[(size_t)b * a.ldr + k]] = 1;
   __syncthreads();
-  double best = -DBL_MAX;
+  T best = lowest<T>();
   int bj = -1;
   pool_t* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
   // nu2 = ||C_k Q_k||_F^2 from column norms/dots of C_k (v[0..5]) and row norms/dots of Q_k
   // (v[6..11], accumulated as each row of Q_k is finished)
-  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  T v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int j = threadIdx.x; j < bk.nJ; j += blockDim.x) {
-    double q[9];
+    T q[9];
 #pragma unroll
     for (int e = 0; e < 9; e++) q[e] = Qk[9 * j + e];
     if (k > 0) {
-      double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      T s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int l = 0; l < k; l++) {
         const pool_t* ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
-        const double* cl = ci + 9 * l;
+        const T* cl = ci + 9 * l;
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
@@ -490,7 +505,7 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
       }
 #pragma unroll
       for (int e = 0; e < 9; e++) {  // stored rounded; the pivot search sees the stored value
-        q[e] = (double)(pool_t)(q[e] - s[e]);
+        q[e] = (T)(pool_t)(q[e] - s[e]);
         Qk[9 * j + e] = (pool_t)q[e];
       }
     }
@@ -500,7 +515,7 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
     v[9] += q[0] * q[3] + q[1] * q[4] + q[2] * q[5];
     v[10] += q[3] * q[6] + q[4] * q[7] + q[5] * q[8];
     v[11] += q[6] * q[0] + q[7] * q[1] + q[8] * q[2];
-    const double d = det3(q);
+    const T d = det3(q);
     if (!a.usedCol[bk.colOff + j] && (bj < 0 || d > best)) {
       best = d;
       bj = j;
@@ -508,7 +523,7 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
   }
   const pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
   for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
-    double c[9];
+    T c[9];
 #pragma unroll
     for (int e = 0; e < 9; e++) c[e] = Ck[9 * i + e];
 #pragma unroll
@@ -521,21 +536,21 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
   // one reduction for the column pivot and the twelve sums (its barriers also make the Q_k
   // writes visible to the cross terms below)
   block_argmax_sum(best, bj, v, sv, si, red);
-  const double nu2 = v[0] * v[6] + v[1] * v[7] + v[2] * v[8] + 2.0 * v[9] * v[3] + 2.0 * v[10] * v[4] +
-                     2.0 * v[11] * v[5];
+  const double nu2 = (T)(v[0] * v[6] + v[1] * v[7] + v[2] * v[8] + T(2) * v[9] * v[3] + T(2) * v[10] * v[4] +
+                        T(2) * v[11] * v[5]);
   double mu2 = a.state[b].mu2 + nu2;  // every thread tracks the same value; thread 0 stores it
   // cross terms for l < k - 1 (src/FarDot.cpp:1041-1077), eight l per pass, one warp per l
   const int nw = blockDim.x >> 5;  // at most 8 (cross)
   for (int lb = 0; lb < k - 1; lb += nw) {
     const int l = lb + wid;
     if (l < k - 1) {
-      double acc[18];
+      T acc[18];
 #pragma unroll
       for (int q = 0; q < 18; q++) acc[q] = 0.0;
       const pool_t* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI);
       const pool_t* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ);
       for (int i = lane; i < bk.nI; i += 32) {
-        double c[9], d[9];
+        T c[9], d[9];
 #pragma unroll
         for (int e = 0; e < 9; e++) {
           c[e] = Ck[9 * i + e];
@@ -548,7 +563,7 @@ __global__ void __launch_bounds__(kPivThreads, 8) k_far_row_pivot(FarArgs a) {
             acc[3 * d1 + d2] += c[d1] * d[d2] + c[d1 + 3] * d[d2 + 3] + c[d1 + 6] * d[d2 + 6];
       }
       for (int j = lane; j < bk.nJ; j += 32) {
-        double q[9], p[9];
+        T q[9], p[9];
 #pragma unroll
         for (int e = 0; e < 9; e++) {
           q[e] = Qk[9 * j + e];
@@ -729,7 +744,10 @@ void far_iteration(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, cons
   else
     k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
   mark();
-  k_far_col_pivot<<<piv_grid, kPivThreads, col_smem, s>>>(a);
+  if (a.fast_pivots)
+    k_far_col_pivot<float, kPivBlocksF32><<<piv_grid, kPivThreads, col_smem, s>>>(a);
+  else
+    k_far_col_pivot<double, 8><<<piv_grid, kPivThreads, col_smem, s>>>(a);
   mark();
   if (student)
     launch_far_student(a, student, 1, err, num_sms, s);
@@ -738,7 +756,10 @@ void far_iteration(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, cons
   else
     k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
   mark();
-  k_far_row_pivot<<<piv_grid, kPivThreads, row_smem, s>>>(a);
+  if (a.fast_pivots)
+    k_far_row_pivot<float, kPivBlocksF32><<<piv_grid, kPivThreads, row_smem, s>>>(a);
+  else
+    k_far_row_pivot<double, 8><<<piv_grid, kPivThreads, row_smem, s>>>(a);
   mark();
   HIGNN_CHECK_LAUNCH();
 }
@@ -749,8 +770,10 @@ void far_batch_start(const FarArgs& a, cudaStream_t s) {
   const size_t row_smem = sizeof(double) * (9 + 3 + 3) * a.ldr;
   const size_t col_smem = sizeof(double) * 9 * a.ldr;
   set_max_dynamic_smem(k_far_eval, eval_smem, s);
-  set_max_dynamic_smem(k_far_row_pivot, row_smem, s);
-  set_max_dynamic_smem(k_far_col_pivot, col_smem, s);
+  set_max_dynamic_smem(k_far_row_pivot<double, 8>, row_smem, s);
+  set_max_dynamic_smem(k_far_col_pivot<double, 8>, col_smem, s);
+  set_max_dynamic_smem(k_far_row_pivot<float, kPivBlocksF32>, row_smem, s);
+  set_max_dynamic_smem(k_far_col_pivot<float, kPivBlocksF32>, col_smem, s);
   k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   HIGNN_CHECK_LAUNCH();
 }

@@ -80,6 +80,8 @@ struct FarArgs {
   double eps2;
   int use_symmetry;
   int defer_apply;  // 1: converged blocks are applied later by far_student_check
+  int fast_pivots;  // 1: orthogonalisation, pivot search and stopping norms in FP32 (the fast
+                    // forms); 0: in FP64, as the restated reference
 };
 
 constexpr int kFarSamples = 64;  // sampled entries per block in the student residual check
