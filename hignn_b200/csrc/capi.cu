@@ -126,7 +126,7 @@ struct hignn_model {
   DevBuf student;         // 2537 FP32 parameters of the far-field student network
 
   DevBuf x4, perm, slot, f4, u, io_f, io_u, close_work, weights, weights_tc, counter;
-  DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_act,
+  DevBuf far_blocks, far_state, far_rows, far_cols, far_used_row, far_used_col, far_C, far_Q, far_xc, far_act,
       far_preI, far_preJ, far_ctr, far_stats, far_rank, far_retry, far_check;
   DevBuf tmp_work, tmp_x, tmp_u, tmp_pos, dp_k, dp_err, near_prof;
   hignn::CellList cells;  // neighbour search of the pair forces
@@ -401,7 +401,7 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
                                             bool known, std::vector<hignn_model::Batch>& batches) {
   std::vector<hignn::FarBlock> out(idx.size());
   batches.clear();
-  int64_t rows = 0, cE = 0, qE = 0, maxC = 0, maxQ = 0;
+  int64_t rows = 0, cE = 0, qE = 0, xE = 0, maxC = 0, maxQ = 0, maxX = 0;
   int32_t rOff = 0, colOff = 0, maxR = 0, maxCol = 0;
   int b0 = 0, maxNb = 0, iters = 0;
   for (size_t p = 0; p < idx.size(); p++) {
@@ -416,7 +416,7 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
       batches.push_back({b0, (int)p, known ? iters : 0});
       maxNb = std::max(maxNb, cnt);
       b0 = (int)p;
-      rows = cE = qE = 0;
+      rows = cE = qE = xE = 0;
       rOff = colOff = 0;
       iters = 0;
     }
@@ -429,16 +429,19 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
     fb.list_idx = q;
     fb.cOff = cE;
     fb.qOff = qE;
+    fb.xOff = xE;
     fb.rOff = rOff;
     fb.colOff = colOff;
     cE += (int64_t)fb.kcap * nI;
     qE += (int64_t)fb.kcap * nJ;
+    xE += hignn::kXcHead + 9 * (int64_t)fb.kcap;
     rOff += nI;
     colOff += nJ;
     rows += nI + nJ;
     iters = std::max(iters, fb.kcap);
     maxC = std::max(maxC, cE);
     maxQ = std::max(maxQ, qE);
+    maxX = std::max(maxX, xE);
     maxR = std::max(maxR, rOff);
     maxCol = std::max(maxCol, colOff);
     out[p] = fb;
@@ -456,6 +459,7 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
     m->far_used_col.ensure((size_t)maxCol + 16);
     m->far_C.ensure(sizeof(hignn::pool_t) * 9 * (size_t)maxC);
     m->far_Q.ensure(sizeof(hignn::pool_t) * 9 * (size_t)maxQ);
+    m->far_xc.ensure(sizeof(float) * (size_t)maxX);
     m->far_act.ensure(sizeof(int32_t) * (maxNb + 1));
     m->far_preI.ensure(sizeof(int32_t) * (maxNb + 1));
     m->far_preJ.ensure(sizeof(int32_t) * (maxNb + 1));
@@ -630,6 +634,7 @@ hignn::FarArgs far_args(hignn_model* m, const hignn_model::Batch& bt, const hign
   a.usedCol = m->far_used_col.as<uint8_t>();
   a.C = m->far_C.as<hignn::pool_t>();
   a.Q = m->far_Q.as<hignn::pool_t>();
+  a.xc = m->far_xc.as<float>();
   a.act = m->far_act.as<int32_t>();
   a.preI = m->far_preI.as<int32_t>();
   a.preJ = m->far_preJ.as<int32_t>();
@@ -898,7 +903,7 @@ uint64_t graph_signature(hignn_model* m) {
   };
   for (const DevBuf* b : {&m->x4, &m->perm, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
                           &m->weights_tc, &m->counter, &m->student, &m->far_blocks, &m->far_state, &m->far_rows,
-                          &m->far_cols, &m->far_used_row, &m->far_used_col, &m->far_C, &m->far_Q, &m->far_act,
+                          &m->far_cols, &m->far_used_row, &m->far_used_col, &m->far_C, &m->far_Q, &m->far_xc, &m->far_act,
                           &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats, &m->far_rank, &m->far_check,
                           &m->far_status})
     mix((uint64_t)(uintptr_t)b->p);
@@ -1273,7 +1278,7 @@ int hignn_destroy(hignn_model* m) {
     for (DevBuf* b : {&m->x4, &m->perm, &m->slot, &m->f4, &m->u, &m->io_f, &m->io_u, &m->close_work, &m->weights,
                       &m->weights_tc, &m->counter, &m->student,
                       &m->far_blocks, &m->far_state, &m->far_rows, &m->far_cols, &m->far_used_row, &m->far_used_col,
-                      &m->far_C, &m->far_Q, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
+                      &m->far_C, &m->far_Q, &m->far_xc, &m->far_act, &m->far_preI, &m->far_preJ, &m->far_ctr, &m->far_stats,
                       &m->far_rank, &m->far_retry, &m->far_check, &m->tmp_work, &m->tmp_x, &m->tmp_u, &m->tmp_pos,
                       &m->dp_k, &m->dp_err, &m->near_prof, &m->far_status})
       b->release();

@@ -458,6 +458,39 @@ __device__ void apply_block(const FarArgs& a, const FarBlock& bk, int rank, doub
     }
 }
 
+// Stopping rule of iteration k (src/FarDot.cpp:1079-1109) and the block's state update, by one
+// thread; done_out: the block converged (apply it), rank_out: its rank.
+__device__ void stop_test(const FarArgs& a, int b, const FarBlock& bk, int k, int bj, double nu2, double mu2,
+                        int& done_out, int& rank_out) {
+  const int k1 = k + 1;
+  const int mn = bk.nI < bk.nJ ? bk.nI : bk.nJ;
+  int done = (nu2 < mu2 * a.eps2) || k1 >= a.max_iter || k1 >= mn;
+  if (!done && bj < 0) {  // no unused column left: cannot continue
+    done = 1;
+    a.ctr[kCtrError] = 2;
+  }
+  a.state[b].nu2 = nu2;
+  a.state[b].mu2 = mu2;
+  a.state[b].k = k1;
+  if (k1 < a.ldr) a.cols[(size_t)b * a.ldr + k1] = bj < 0 ? 0 : bj;
+  int deferred = 0;
+  if (!done && k1 >= bk.kcap) {  // the next term would not fit this block's pool share
+    deferred = 1;
+    a.state[b].done = 2;
+    atomicSub(&a.ctr[kCtrRemaining], 1);
+    atomicAdd(&a.ctr[kCtrDeferred], 1);
+  }
+  if (done) {
+    a.state[b].done = 1;
+    atomicSub(&a.ctr[kCtrRemaining], 1);
+    atomicMax(&a.ctr[kCtrRankMax], k1);
+    atomicAdd(a.rank_sum, (unsigned long long)k1);
+    if (a.rank_out) a.rank_out[bk.list_idx] = k1;
+  }
+  done_out = done && !deferred;
+  rank_out = k1;
+}
+
 // Orthogonalise the new row, pick the next column, stop test, and apply a finished block.
 template <typename T, int MinBlocks>
 __global__ void __launch_bounds__(kPivThreads, MinBlocks) k_far_row_pivot(FarArgs a) {
@@ -588,39 +621,292 @@ __global__ void __launch_bounds__(kPivThreads, MinBlocks) k_far_row_pivot(FarArg
       for (int q = 0; q < 9; q++) mu2 += 2.0 * fabs(cross[ww][q]) * fabs(cross[ww][9 + q]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const int k1 = k + 1;
-    const int mn = bk.nI < bk.nJ ? bk.nI : bk.nJ;
-    int done = (nu2 < mu2 * a.eps2) || k1 >= a.max_iter || k1 >= mn;
-    if (!done && bj < 0) {  // no unused column left: cannot continue
-      done = 1;
-      a.ctr[kCtrError] = 2;
-    }
-    a.state[b].nu2 = nu2;
-    a.state[b].mu2 = mu2;
-    a.state[b].k = k1;
-    if (k1 < a.ldr) a.cols[(size_t)b * a.ldr + k1] = bj < 0 ? 0 : bj;
-    int deferred = 0;
-    if (!done && k1 >= bk.kcap) {  // the next term would not fit this block's pool share
-      deferred = 1;
-      a.state[b].done = 2;
-      atomicSub(&a.ctr[kCtrRemaining], 1);
-      atomicAdd(&a.ctr[kCtrDeferred], 1);
-    }
-    if (done) {
-      a.state[b].done = 1;
-      atomicSub(&a.ctr[kCtrRemaining], 1);
-      atomicMax(&a.ctr[kCtrRankMax], k1);
-      atomicAdd(a.rank_sum, (unsigned long long)k1);
-      if (a.rank_out) a.rank_out[bk.list_idx] = k1;
-    }
-    s_done = done && !deferred;
-    s_rank = k1;
-  }
+  if (threadIdx.x == 0) stop_test(a, b, bk, k, bj, nu2, mu2, s_done, s_rank);
   __syncthreads();
   if (!s_done) continue;  // CTA-uniform; the loop-end barrier protects the shared state
   if (!a.defer_apply) apply_block(a, bk, s_rank, mid, mid2);
   __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- FP32 bookkeeping (fast forms)
+// The pivot kernels of the fast forms keep the orthogonalisation, the pivot search and the
+// stopping norms in FP32 and read every earlier factor once per iteration. The |.| cross terms of
+// the stopping norm (column d1 of C_k . column d2 of C_l and row d1 of Q_k . row d2 of Q_l, for
+// l < k - 1; src/FarDot.cpp:1036-1078) are summed chunk by chunk (128 entries) right after the
+// orthogonalisation of the same entries: the new entries are staged in shared memory and the
+// earlier factors, just read, come from L1 / L2; one warp per l. The C side is summed in the
+// column kernel on the orthogonalised column and mapped through the pivot inverse (C_k = c inv,
+// so column d1 of C_k is sum_e inv[e][d1] column e of c); it reaches the row kernel of the same
+// iteration through the block's scratch at FarBlock::xOff: [0, 6) the column norms and
+// adjacent-column dots of C_k, [kXcHead + 9 l, + 9) the cross terms with C_l.
+
+__device__ __forceinline__ void warp_sum9(float (&v)[9]) {
+#pragma unroll
+  for (int q = 0; q < 9; q++)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+}
+
+size_t col_smem_f32(int ldr) { return sizeof(float) * (18 * (size_t)ldr + 9 * kPivThreads); }
+size_t row_smem_f32(int ldr) { return sizeof(double) * 6 * (size_t)ldr + col_smem_f32(ldr); }
+
+__global__ void __launch_bounds__(kPivThreads, kPivBlocksF32) k_far_col_pivot_f32(FarArgs a) {
+  extern __shared__ __align__(16) float fsm[];
+  float* qj = fsm;             // [k][9]: Q_l[j_k]
+  float* xo = qj + 9 * a.ldr;  // [k - 1][9]: cross terms of the orthogonalised column with C_l
+  float* cs = xo + 9 * a.ldr;  // [128][9]: the chunk's orthogonalised entries
+  __shared__ float sv[32], inv[9], red[32 * 6];
+  __shared__ int si[32];
+  const int nact = a.ctr[kCtrActive];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int ai = blockIdx.x; ai < nact; ai += gridDim.x) {
+    const int b = a.act[ai];
+    const FarBlock bk = a.blocks[b];
+    const int k = a.state[b].k;
+    const int jk = a.cols[(size_t)b * a.ldr + k];
+    const int ncross = k > 1 ? k - 1 : 0;
+    for (int q = threadIdx.x; q < 9 * k; q += blockDim.x) {
+      const int l = q / 9, e = q - (q / 9) * 9;
+      qj[q] = a.Q[9 * (bk.qOff + (int64_t)l * bk.nJ + jk) + e];
+    }
+    for (int q = threadIdx.x; q < 9 * ncross; q += blockDim.x) xo[q] = 0.f;
+    __syncthreads();
+    float best = -FLT_MAX;
+    int bi = -1;
+    pool_t* Ck = a.C + 9 * (bk.cOff + (int64_t)k * bk.nI);
+    for (int i0 = 0; i0 < bk.nI; i0 += blockDim.x) {
+      const int i = i0 + threadIdx.x;
+      if (i < bk.nI) {
+        float c[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
+        if (k > 0) {
+          float s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+          for (int l = 0; l < k; l++) {
+            const pool_t* cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i);
+            const float* ql = qj + 9 * l;
+            float cv[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) cv[q] = cl[q];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+              for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+                for (int m = 0; m < 3; m++) s[3 * r + cc] += cv[3 * r + m] * ql[3 * m + cc];
+          }
+#pragma unroll
+          for (int q = 0; q < 9; q++) {
+            c[q] = c[q] - s[q];
+            Ck[9 * i + q] = c[q];
+          }
+        }
+        const float d = det3(c);
+        if (!a.usedRow[bk.rOff + i] && (bi < 0 || d > best)) {
+          best = d;
+          bi = i;
+        }
+        if (ncross > 0)
+#pragma unroll
+          for (int q = 0; q < 9; q++) cs[9 * threadIdx.x + q] = c[q];
+      }
+      if (ncross > 0) {  // CTA-uniform
+        __syncthreads();
+        const int cnt = bk.nI - i0 < (int)blockDim.x ? bk.nI - i0 : (int)blockDim.x;
+        for (int l = wid; l < ncross; l += nw) {
+          float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+          const pool_t* Cl = a.C + 9 * (bk.cOff + (int64_t)l * bk.nI + i0);
+          for (int r = lane; r < cnt; r += 32) {
+            const float* c = cs + 9 * r;
+            float dv[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) dv[q] = Cl[9 * r + q];
+#pragma unroll
+            for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+              for (int d2 = 0; d2 < 3; d2++)
+                acc[3 * d1 + d2] += c[d1] * dv[d2] + c[d1 + 3] * dv[d2 + 3] + c[d1 + 6] * dv[d2 + 6];
+          }
+          warp_sum9(acc);
+          if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 9; q++) xo[9 * l + q] += acc[q];
+        }
+        __syncthreads();
+      }
+    }
+    block_argmax(best, bi, sv, si);
+    if (bi < 0) {  // CTA-uniform
+      if (threadIdx.x == 0) {
+        a.ctr[kCtrError] = 1;
+        a.rows[(size_t)b * a.ldr + k] = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (threadIdx.x == 0) {
+      a.rows[(size_t)b * a.ldr + k] = bi;
+      a.usedRow[bk.rOff + bi] = 1;
+      const pool_t* m = Ck + 9 * bi;
+      const double A = m[0], B = m[1], C = m[2], D = m[3], E = m[4], F = m[5], G = m[6], H = m[7], I = m[8];
+      const double det = A * (E * I - F * H) - B * (D * I - F * G) + C * (D * H - E * G);
+      inv[0] = (float)((E * I - F * H) / det);
+      inv[1] = (float)(-(B * I - C * H) / det);
+      inv[2] = (float)((B * F - C * E) / det);
+      inv[3] = (float)(-(D * I - F * G) / det);
+      inv[4] = (float)((A * I - C * G) / det);
+      inv[5] = (float)(-(A * F - C * D) / det);
+      inv[6] = (float)((D * H - E * G) / det);
+      inv[7] = (float)(-(A * H - B * G) / det);
+      inv[8] = (float)((A * E - B * D) / det);
+    }
+    __syncthreads();
+    float* xc = a.xc + bk.xOff;
+    for (int q = threadIdx.x; q < 9 * ncross; q += blockDim.x) {  // cross terms of the final C_k
+      const int l = q / 9, e = q - (q / 9) * 9, d1 = e / 3, d2 = e - (e / 3) * 3;
+      const float* x = xo + 9 * l;
+      xc[kXcHead + q] = inv[d1] * x[d2] + inv[3 + d1] * x[3 + d2] + inv[6 + d1] * x[6 + d2];
+    }
+    float v[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < bk.nI; i += blockDim.x) {
+      float c[9], o[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) c[q] = Ck[9 * i + q];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++) {
+          float acc = c[3 * r] * inv[cc];
+          acc = acc + c[3 * r + 1] * inv[3 + cc];
+          acc = acc + c[3 * r + 2] * inv[6 + cc];
+          o[3 * r + cc] = acc;
+        }
+#pragma unroll
+      for (int q = 0; q < 9; q++) Ck[9 * i + q] = o[q];
+#pragma unroll
+      for (int cc = 0; cc < 3; cc++) {  // column norms and adjacent-column dots of the final C_k
+        const int c1 = (cc + 1) % 3;
+        v[cc] += o[cc] * o[cc] + o[cc + 3] * o[cc + 3] + o[cc + 6] * o[cc + 6];
+        v[3 + cc] += o[cc] * o[c1] + o[cc + 3] * o[c1 + 3] + o[cc + 6] * o[c1 + 6];
+      }
+    }
+    block_sum<6>(v, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 6; q++) xc[q] = v[q];
+    __syncthreads();  // shared state is reused by the next active block
+  }
+}
+
+__global__ void __launch_bounds__(kPivThreads, kPivBlocksF32) k_far_row_pivot_f32(FarArgs a) {
+  extern __shared__ __align__(16) double dsm[];
+  double* mid = dsm;                                       // [rank][3] (apply)
+  double* mid2 = mid + 3 * a.ldr;                          // [rank][3]
+  float* ci = reinterpret_cast<float*>(mid2 + 3 * a.ldr);  // [k][9]: C_l[i_k]
+  float* xq = ci + 9 * a.ldr;                              // [k - 1][9]: cross terms of Q_k with Q_l
+  float* qs = xq + 9 * a.ldr;                              // [128][9]: the chunk's orthogonalised entries
+  __shared__ float sv[32], red[32 * 6];
+  __shared__ int si[32];
+  __shared__ int s_done, s_rank;
+  const int nact = a.ctr[kCtrActive];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int ai = blockIdx.x; ai < nact; ai += gridDim.x) {
+    const int b = a.act[ai];
+    const FarBlock bk = a.blocks[b];
+    const int k = a.state[b].k;
+    const int ik = a.rows[(size_t)b * a.ldr + k];
+    const int ncross = k > 1 ? k - 1 : 0;
+    for (int q = threadIdx.x; q < 9 * k; q += blockDim.x) {
+      const int l = q / 9, e = q - (q / 9) * 9;
+      ci[q] = a.C[9 * (bk.cOff + (int64_t)l * bk.nI + ik) + e];
+    }
+    for (int q = threadIdx.x; q < 9 * ncross; q += blockDim.x) xq[q] = 0.f;
+    if (threadIdx.x == 0) a.usedCol[bk.colOff + a.cols[(size_t)b * a.ldr + k]] = 1;
+    __syncthreads();
+    float best = -FLT_MAX;
+    int bj = -1;
+    float v[6] = {0, 0, 0, 0, 0, 0};  // row norms and adjacent-row dots of Q_k
+    pool_t* Qk = a.Q + 9 * (bk.qOff + (int64_t)k * bk.nJ);
+    for (int j0 = 0; j0 < bk.nJ; j0 += blockDim.x) {
+      const int j = j0 + threadIdx.x;
+      if (j < bk.nJ) {
+        float q[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) q[e] = Qk[9 * j + e];
+        if (k > 0) {
+          float s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+          for (int l = 0; l < k; l++) {
+            const pool_t* ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j);
+            const float* cl = ci + 9 * l;
+            float qv[9];
+#pragma unroll
+            for (int e = 0; e < 9; e++) qv[e] = ql[e];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+              for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+                for (int m = 0; m < 3; m++) s[3 * r + cc] += cl[3 * r + m] * qv[3 * m + cc];
+          }
+#pragma unroll
+          for (int e = 0; e < 9; e++) {
+            q[e] = q[e] - s[e];
+            Qk[9 * j + e] = q[e];
+          }
+        }
+        v[0] += q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        v[1] += q[3] * q[3] + q[4] * q[4] + q[5] * q[5];
+        v[2] += q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
+        v[3] += q[0] * q[3] + q[1] * q[4] + q[2] * q[5];
+        v[4] += q[3] * q[6] + q[4] * q[7] + q[5] * q[8];
+        v[5] += q[6] * q[0] + q[7] * q[1] + q[8] * q[2];
+        const float d = det3(q);
+        if (!a.usedCol[bk.colOff + j] && (bj < 0 || d > best)) {
+          best = d;
+          bj = j;
+        }
+        if (ncross > 0)
+#pragma unroll
+          for (int e = 0; e < 9; e++) qs[9 * threadIdx.x + e] = q[e];
+      }
+      if (ncross > 0) {  // CTA-uniform
+        __syncthreads();
+        const int cnt = bk.nJ - j0 < (int)blockDim.x ? bk.nJ - j0 : (int)blockDim.x;
+        for (int l = wid; l < ncross; l += nw) {
+          float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+          const pool_t* Ql = a.Q + 9 * (bk.qOff + (int64_t)l * bk.nJ + j0);
+          for (int r = lane; r < cnt; r += 32) {
+            const float* q = qs + 9 * r;
+            float p[9];
+#pragma unroll
+            for (int e = 0; e < 9; e++) p[e] = Ql[9 * r + e];
+#pragma unroll
+            for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+              for (int d2 = 0; d2 < 3; d2++)
+                acc[3 * d1 + d2] += q[3 * d1] * p[3 * d2] + q[3 * d1 + 1] * p[3 * d2 + 1] + q[3 * d1 + 2] * p[3 * d2 + 2];
+          }
+          warp_sum9(acc);
+          if (lane == 0)
+#pragma unroll
+            for (int e = 0; e < 9; e++) xq[9 * l + e] += acc[e];
+        }
+        __syncthreads();
+      }
+    }
+    block_argmax(best, bj, sv, si);
+    block_sum<6>(v, red);
+    const float* xc = a.xc + bk.xOff;  // written by this iteration's column kernel
+    const double nu2 = (float)(xc[0] * v[0] + xc[1] * v[1] + xc[2] * v[2] + 2.f * v[3] * xc[3] + 2.f * v[4] * xc[4] +
+                               2.f * v[5] * xc[5]);
+    double mu2 = a.state[b].mu2 + nu2;  // every thread tracks the same value; thread 0 stores it
+    for (int l = 0; l < ncross; l++)
+      for (int e = 0; e < 9; e++) mu2 += 2.0 * fabs((double)xc[kXcHead + 9 * l + e]) * fabs((double)xq[9 * l + e]);
+    if (threadIdx.x == 0) stop_test(a, b, bk, k, bj, nu2, mu2, s_done, s_rank);
+    __syncthreads();
+    if (!s_done) continue;  // CTA-uniform; the loop-end barrier protects the shared state
+    if (!a.defer_apply) apply_block(a, bk, s_rank, mid, mid2);
+    __syncthreads();
   }
 }
 
@@ -745,7 +1031,7 @@ void far_iteration(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, cons
     k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 0);
   mark();
   if (a.fast_pivots)
-    k_far_col_pivot<float, kPivBlocksF32><<<piv_grid, kPivThreads, col_smem, s>>>(a);
+    k_far_col_pivot_f32<<<piv_grid, kPivThreads, col_smem_f32(a.ldr), s>>>(a);
   else
     k_far_col_pivot<double, 8><<<piv_grid, kPivThreads, col_smem, s>>>(a);
   mark();
@@ -757,7 +1043,7 @@ void far_iteration(const FarArgs& a, const MlpF32& w, const TcWeights* tcw, cons
     k_far_eval<<<num_sms, simt::kThreads, eval_smem, s>>>(a, w, 1);
   mark();
   if (a.fast_pivots)
-    k_far_row_pivot<float, kPivBlocksF32><<<piv_grid, kPivThreads, row_smem, s>>>(a);
+    k_far_row_pivot_f32<<<piv_grid, kPivThreads, row_smem_f32(a.ldr), s>>>(a);
   else
     k_far_row_pivot<double, 8><<<piv_grid, kPivThreads, row_smem, s>>>(a);
   mark();
@@ -772,8 +1058,8 @@ void far_batch_start(const FarArgs& a, cudaStream_t s) {
   set_max_dynamic_smem(k_far_eval, eval_smem, s);
   set_max_dynamic_smem(k_far_row_pivot<double, 8>, row_smem, s);
   set_max_dynamic_smem(k_far_col_pivot<double, 8>, col_smem, s);
-  set_max_dynamic_smem(k_far_row_pivot<float, kPivBlocksF32>, row_smem, s);
-  set_max_dynamic_smem(k_far_col_pivot<float, kPivBlocksF32>, col_smem, s);
+  set_max_dynamic_smem(k_far_row_pivot_f32, row_smem_f32(a.ldr), s);
+  set_max_dynamic_smem(k_far_col_pivot_f32, col_smem_f32(a.ldr), s);
   k_far_init<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   HIGNN_CHECK_LAUNCH();
 }

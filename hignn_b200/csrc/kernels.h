@@ -37,12 +37,15 @@ void launch_near_simt(const NearArgs& a, const MlpF32& w, int* work_counter, int
 void launch_dense_f64(const NearArgs& a, const MlpF32& w, int* work_counter, int num_sms, cudaStream_t s);
 
 // ---------------------------------------------------------------- far field (ACA)
+constexpr int kXcHead = 8;  // FP32 pivot scratch of a block: 8 norm terms, then 9 floats per term
+
 struct FarBlock {
   int32_t sI, nI, sJ, nJ;
   int64_t cOff, qOff;      // batch-relative entry offsets into the C / Q pools
   int32_t rOff, colOff;    // batch-relative offsets into the used-row / used-column flags
   int32_t kcap;            // pool capacity in ACA terms, <= min(max_iter, nI, nJ)
   int32_t list_idx;        // position in the far list (ranks are recorded there)
+  int64_t xOff;            // batch-relative offset into the FP32 pivot scratch (kXcHead + 9 kcap floats)
 };
 
 // done: 0 = iterating, 1 = converged (applied to u), 2 = deferred (reached its pool
@@ -66,6 +69,7 @@ struct FarArgs {
   uint8_t* usedCol;
   pool_t* C;          // [entries][9]
   pool_t* Q;
+  float* xc;          // per-block scratch of the FP32 pivot kernels (C-side norm terms)
   int32_t* act;       // active block list
   int32_t* preI;      // exclusive prefix of nI over active blocks (nact + 1)
   int32_t* preJ;
