@@ -536,18 +536,19 @@ __global__ void __launch_bounds__(kStcThreads, 8) k_far_student_tc(FarArgs a, co
       } else {
         float y[9];
         rpy_inner(rx, ry, rz, y);
+        const float inv_nr = 1.0f / nr;  // one division, not nine: the MUFU is this kernel's busiest unit
 #pragma unroll
         for (int o = 0; o < 9; o++) {
           float z = y[o] + __uint_as_float(v[o]) + S.b4[o];
           if (o == 0 || o == 4 || o == 8) z += 1.0f;
-          M[o] = z / nr;
+          M[o] = z * inv_nr;
         }
       }
 #pragma unroll
       for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++)
-          cur.dst[3 * r + c] = (r == c) ? (double)M[3 * r + c] : 0.5 * (double)(M[3 * r + c] + M[3 * c + r]);
+          cur.dst[3 * r + c] = (r == c) ? M[3 * r + c] : 0.5f * (M[3 * r + c] + M[3 * c + r]);  // as FP64, exact
     }
     cur = nxt;
   }

@@ -272,7 +272,7 @@ __device__ __forceinline__ void far_use(const FarArgs& a, int which, const FarRo
   for (int q = 0; q < 9; q++) {
     if ((q & 1) != p) continue;
     const int rr = q / 3, c = q % 3;
-    dst[q] = (rr == c) ? (double)M[q] : 0.5 * (double)(M[3 * rr + c] + M[3 * c + rr]);
+    dst[q] = (rr == c) ? M[q] : 0.5f * (M[3 * rr + c] + M[3 * c + rr]);  // the FP32 half-sum is exact in FP64 too
   }
 }
 
