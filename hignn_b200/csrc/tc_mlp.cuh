@@ -86,7 +86,7 @@ struct alignas(1024) Smem {
   unsigned long long* prof;          // optional wait profile (global, kProfSlots counters) or null
   unsigned long long wprof[16];      // per-CTA wait cycles by barrier code (lane 0 of each warp)
   alignas(16) float4 w1b1[kH1];      // FP32 layer 1: (W1[k][0..2], b1[k]) per hidden unit
-  alignas(16) float b2[kH2];         // FP32 layer-2 bias, added before rounding to FP16
+  alignas(16) uint32_t b2h[kH2 / 2];  // layer-2 bias as FP16 pairs, added to the rounded accumulator
   float b3[16];
 };
 
@@ -212,6 +212,11 @@ __device__ __forceinline__ uint32_t tanh_f16x2(uint32_t x) {
   asm("tanh.approx.f16x2 %0, %1;\n" : "=r"(y) : "r"(x));
   return y;
 }
+__device__ __forceinline__ uint32_t add_f16x2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("add.rn.f16x2 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
 __device__ __forceinline__ uint32_t add_bf16x2(uint32_t a, uint32_t b) {
   uint32_t r;
   asm("add.rn.bf16x2 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(b));
@@ -261,7 +266,7 @@ __device__ __forceinline__ void cta_setup(Smem& s, const TcWeights& w) {
   uint4* dst3 = reinterpret_cast<uint4*>(s.w3);
   for (int i = t; i < kW3Bytes / 16; i += blockDim.x) dst3[i] = src3[i];
   for (int i = t; i < kH1; i += blockDim.x) s.w1b1[i] = w.w1b1[i];
-  for (int i = t; i < kH2; i += blockDim.x) s.b2[i] = w.b2[i];
+  for (int i = t; i < kH2 / 2; i += blockDim.x) s.b2h[i] = pack_f16(w.b2[2 * i], w.b2[2 * i + 1]);
   if (t < 16) s.b3[t] = t < kOut ? w.b3[t] : 0.f;
   if (t < 16) s.wprof[t] = 0ull;
   if (t == 0) {
@@ -459,13 +464,19 @@ struct Epi {
     uint32_t v[32], out[16];
     tmem_ld32(slot(q) + 32 * p, v);
     tmem_wait_ld();
-    const float4* bb = reinterpret_cast<const float4*>(s.b2 + q * 128 + 32 * p);
+    // one rounding to FP16 pairs, the FP16 bias added to the pairs (one instruction per pair
+    // instead of two FP32 adds)
+    const uint4* bb = reinterpret_cast<const uint4*>(s.b2h + (q * 128 + 32 * p) / 2);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const float4 bv = bb[k];
-      out[2 * k] = tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 0]) + bv.x, __uint_as_float(v[4 * k + 1]) + bv.y));
-      out[2 * k + 1] =
-          tanh_f16x2(pack_f16(__uint_as_float(v[4 * k + 2]) + bv.z, __uint_as_float(v[4 * k + 3]) + bv.w));
+    for (int k = 0; k < 4; k++) {
+      const uint4 bv = bb[k];
+      out[4 * k] = tanh_f16x2(add_f16x2(pack_f16(__uint_as_float(v[8 * k]), __uint_as_float(v[8 * k + 1])), bv.x));
+      out[4 * k + 1] =
+          tanh_f16x2(add_f16x2(pack_f16(__uint_as_float(v[8 * k + 2]), __uint_as_float(v[8 * k + 3])), bv.y));
+      out[4 * k + 2] =
+          tanh_f16x2(add_f16x2(pack_f16(__uint_as_float(v[8 * k + 4]), __uint_as_float(v[8 * k + 5])), bv.z));
+      out[4 * k + 3] =
+          tanh_f16x2(add_f16x2(pack_f16(__uint_as_float(v[8 * k + 6]), __uint_as_float(v[8 * k + 7])), bv.w));
     }
     // A2 buffer q % 2 was last read by L3 of quarter q - 2 (this tile, first commit on its
     // barrier: parity 0) or of quarter q + 2 of the previous tile (second commit: parity 1)
