@@ -471,13 +471,19 @@ std::vector<hignn::FarBlock> layout_batches(hignn_model* m, const std::vector<in
 }
 
 // ACA plan of the far list. Without rank information every block gets the pool capacity
-// min(max_iter, |I|, |J|) and the batches follow the list order (src/FarDot.cpp:191-340
-// batches the list in order). When the previous far field on the same tree and settings
+// min(max_iter, |I|, |J|, kFirstPlanCap) and the batches follow the list order
+// (src/FarDot.cpp:191-340 batches the list in order); a block that needs more terms is deferred
+// and rerun with min(max_iter, |I|, |J|), so the cap only decides how many blocks share a batch. When the previous far field on the same tree and settings
 // recorded every block's rank, each block gets exactly that capacity, the blocks are sorted by
 // rank (batches of similar ranks need fewer iterations) and each batch runs its known
 // iteration count without reading counters back; a block that would need more terms than
 // recorded is deferred and rerun with the full capacity, so the result never depends on the
 // hint.
+// Pool capacity of a block without a recorded rank: about twice the largest rank of the
+// benchmark's far blocks at epsilon 1e-2 (14-18), so that the first far field on a tree packs up to
+// three times more blocks per batch than at the full capacity of max_iter = 100 terms.
+constexpr int kFirstPlanCap = 32;
+
 void ensure_far_plan(hignn_model* m) {
   ensure_shard(m);
   const bool use_hints = hints_usable(m);
@@ -503,7 +509,7 @@ void ensure_far_plan(hignn_model* m) {
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return kc[x] > kc[y]; });
     for (size_t p = 0; p < nf; p++) kcap[p] = kc[idx[p]];
   } else {
-    for (size_t p = 0; p < nf; p++) kcap[p] = full[idx[p]];
+    for (size_t p = 0; p < nf; p++) kcap[p] = std::min(full[idx[p]], kFirstPlanCap);
   }
   m->far_plan = layout_batches(m, idx, kcap, use_hints, m->batches);
   if (m->device >= 0 && nf > 0) {

@@ -7,9 +7,9 @@
 //   layer 3 (512 -> 9): N = 16, K = 512, FP16 operands (W3 rows 0-8, rows 9-15 zero).
 // FP16 rather than BF16 for layers 2 and 3: their operands are tanh outputs in [-1, 1] and
 // weights well inside FP16's range, so the 11-bit significand costs no range and rounds 8x finer.
-// The epilogue warps read a layer-2 accumulator (tcgen05.ld), add the FP32 bias, round to FP16
-// pairs, apply tanh.approx.f16x2 and write the pairs back into tensor memory as layer 3's A
-// operand; layer 1's tanh'd pairs go the same way into layer 2's A operand.
+// The epilogue warps read a layer-2 accumulator (tcgen05.ld), round it to FP16 pairs, add the
+// bias as FP16 pairs, apply tanh.approx.f16x2 and write the pairs back into tensor memory as
+// layer 3's A operand; layer 1's tanh'd pairs go the same way into layer 2's A operand.
 //
 // The bound is the MUFU: 640 tanh per evaluation at 16 tanh per clock per SM (tanh.approx.f16x2
 // issues at half the rate of tanh.approx.f32, measured on B200: packing saves issue slots, not
@@ -38,7 +38,7 @@
 //              (A operand of layer 3)
 //   [448,464)  and [464,480): layer-3 accumulators of even / odd tiles (M in columns 0-8)
 // Shared memory: W2 (512 x 128) and W3 (16 x 512) as FP16, canonical K-major 128-byte-swizzle
-// layout, loaded once per CTA; FP32 (W1, b1) per hidden unit and biases b2, b3; mbarriers. A
+// layout, loaded once per CTA; FP32 (W1, b1) per hidden unit, b2 as FP16 pairs, FP32 b3; mbarriers. A
 // barrier that completes twice per tile (the per-slot and per-buffer ones) is waited with the
 // parity of its position in the tile, and no waiter can fall two phases behind: every phase
 // needs the arrival of all epilogue threads or follows one that did. Every wait is bounded
