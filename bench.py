@@ -6,8 +6,8 @@ volume fraction 0.10, 64 Gaussian clusters (sigma 8 radii) + 50% uniform
 background (seed 2), forces (0,0,-1) + N(0, 0.1^2); leaf size 128, ACA
 tolerance 1e-2 (the reference's production value, python/simulate.py:198),
 max_iter 100, tree prebuilt (its host build time is reported apart). One step =
-one H-matvec (near field + ACA far field). The headline form is BF16 tensor
-cores + rank-planned ACA batches + the far-field student network (trained on
+one H-matvec (near field + ACA far field). The headline form is FP16 tensor
+cores (FP32 layer 1 and accumulation) + rank-planned ACA batches + the far-field student network (trained on
 the device before timing; its training time is reported apart); the plain FP32
 form is timed in the same run for the mixed-vs-plain ratio of the metric, and
 both are checked against the dense product on sampled target rows.
@@ -43,8 +43,8 @@ TANH_PER_EVAL = 128 + 512
 # nothing written; positions, forces and the pair list are read once, the FP64 accumulators stay
 # in L2). The reads are per particle, so the figure scales with N.
 NEAR_DRAM_BYTES_PER_PARTICLE = 8.9e6 / 131072
-PREC_NAME = {0: "plain_fp32", 1: "bf16_tensor_cores", 2: "bf16_tensor_cores+student_far_field"}
-PREC_DTYPE = {0: "fp32", 1: "bf16", 2: "bf16"}
+PREC_NAME = {0: "plain_fp32", 1: "fp16_tensor_cores", 2: "fp16_tensor_cores+student_far_field"}
+PREC_DTYPE = {0: "fp32", 1: "fp16", 2: "fp16"}  # layers 2-3 on the tensor cores in FP16 (FP32 accumulation)
 WORKLOAD = ("N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, seed 2, "
             "leaf 128, eps 1e-2, max_iter 100, tree prebuilt")
 
@@ -80,7 +80,7 @@ def parse():
 def filament_steps(steps=200):
     """The filament suspension (4,096 filaments x 32 beads, bond 2.2, phi 0.05, seed 3) stepped on the
     device with the whole HIGNN velocity: filament bending (k_b 10) and tension (k 100) plus
-    gravity, H-matrix two-body term (BF16 network, eps 1e-2, leaf 128), three-body and self terms
+    gravity, H-matrix two-body term (tensor-core network, eps 1e-2, leaf 128), three-body and self terms
     (cutoff 5); explicit midpoint rule (RK2), dt 5e-4, tree rebuilt every 2 steps."""
     from hignn_b200 import capi
     from hignn_b200 import synthetic as S
@@ -561,7 +561,7 @@ def main():
                                             st["far_evals"])
     euler = None
     if rank == 0 and world == 1 and not args.no_next_rows and args.euler_steps > 0:
-        # the batching workload's time loop on the benchmark model (BF16 + student, eps 1e-2):
+        # the batching workload's time loop on the benchmark model (tensor cores + student, eps 1e-2):
         # gravity + Morse (D 1, a 5, r0 2.1, cutoff 3), explicit Euler, dt 1e-3, rebuilt every 10 steps
         # The 64 Gaussian clusters of the matvec positions overlap (their cores hold about ten
         # times the spheres that fit), and Morse repulsion between overlapping spheres blows the
@@ -583,7 +583,7 @@ def main():
         euler = {"workload": "N=1,048,576 spheres uniform at volume fraction 0.10 with minimum separation 2.05 "
                              "(seed 2; the matvec's clustered positions overlap), Morse (D 1, a 5, r0 2.1, cutoff "
                              "3) without gravity (with it the unbounded collective flow drives neighbours into the "
-                             "Morse wall and explicit Euler at dt 1e-3 becomes unstable), BF16 + student far field, "
+                             "Morse wall and explicit Euler at dt 1e-3 becomes unstable), tensor cores + student far field, "
                              "eps 1e-2, explicit Euler dt 1e-3, tree rebuilt every 10 steps",
                  "steps": args.euler_steps, "ms_per_step": dt_loop / args.euler_steps * 1e3,
                  "particle_steps_per_s": n * args.euler_steps / dt_loop,
