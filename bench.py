@@ -45,6 +45,14 @@ TANH_PER_EVAL = 128 + 512
 NEAR_DRAM_BYTES_PER_PARTICLE = 8.9e6 / 131072
 PREC_NAME = {0: "plain_fp32", 1: "fp16_tensor_cores", 2: "fp16_tensor_cores+student_far_field"}
 PREC_DTYPE = {0: "fp32", 1: "fp16", 2: "fp16"}  # layers 2-3 on the tensor cores in FP16 (FP32 accumulation)
+_T0 = time.time()
+
+
+def note(msg):
+    """Progress of a run on stderr (stdout carries only the result line)."""
+    print(f"[bench {time.time() - _T0:8.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 WORKLOAD = ("N=1,048,576 clustered (64 Gaussian clusters sigma 8 + 50% uniform), phi 0.10, seed 2, "
             "leaf 128, eps 1e-2, max_iter 100, tree prebuilt")
 
@@ -124,6 +132,7 @@ def three_body_row(args):
     import torch
 
     row = three_body(SimpleNamespace(filaments=4096, reps=3))
+    note("three-body kernel timed")
     # the reference runs this network in torch (python/HIGNN/model_structure.py:41-55): its CPU
     # FP32 path on the oracle's weights, batches of 8,192 triplets
     net = O.DenseTanh.from_hgnw(default_three_body_paths()[0])
@@ -148,7 +157,9 @@ def three_body_row(args):
             forward(z[s:s + 8192])
     dt = time.perf_counter() - t0
     row["workload"] = "4,096 filaments x 32 beads, bond 2.2, phi 0.05, seed 3, three-body cutoff 5"
+    note("three-body CPU baseline timed")
     row["time_step"] = filament_steps(args.filament_steps)
+    note("filament loop done")
     row["cpu_baseline"] = {"value": sample / dt, "unit": "triplets/s", "cores": os.cpu_count(), "kind": "port",
                            "sample": f"{sample} triplets through the three-body network on torch's CPU FP32 path "
                                      f"(the reference's engine), {os.cpu_count()} threads"}
@@ -391,6 +402,7 @@ def main():
     if world > 1:
         m.set_shard(rank, world)
     st0 = m.stats()  # builds the tree and lists
+    note("tree and lists built")
     student = None
     if args.precision == 2:  # the far-field student network, trained on the device from teacher samples
         t0 = time.time()
@@ -425,8 +437,10 @@ def main():
             dist.all_reduce(u_d)
             u_h.copy_(u_d, non_blocking=True)
 
+    note("student trained" if student else "model ready")
     for _ in range(args.warmup):
         step_device(u_d)
+    note("warm-up products done")
     props = torch.cuda.get_device_properties(local)
     bus = None
     try:
@@ -440,6 +454,7 @@ def main():
     times, near_ms, far_ms = timed(m, stream, flush, args.steps, lambda: step_device(u_d))
     torch.cuda.synchronize()
     ck = clocks.stop()
+    note("timed products done")
     if dist:
         dist.barrier()
     st = m.stats()
@@ -483,6 +498,7 @@ def main():
                              "recorded ranks, as every product of the reference's time loop; the tree rebuild is "
                              "timed apart"}
         step_device(u_d)  # ranks recorded again for the forms timed below
+        note("unplanned product done")
 
     # accuracy: FP64 dense rows on seeded target rows, each summed over all N sources
     rng = np.random.default_rng(12345)
@@ -491,6 +507,7 @@ def main():
     t0 = time.time()
     ud = m.dense_rows(f, rows, capi.DENSE_F64) if len(rows) and rank == 0 else None
     t_check = time.time() - t0
+    note("FP64 dense-row check done")
     if ud is not None:
         err = float(np.linalg.norm(u[rows] - ud) / np.linalg.norm(ud))
 
@@ -559,6 +576,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_estimate(x, f, args.epsilon, args.cpu_sample_seconds, st["close_evals"],
                                             st["far_evals"])
+    note("plain form and CPU baseline done")
     euler = None
     if rank == 0 and world == 1 and not args.no_next_rows and args.euler_steps > 0:
         # the batching workload's time loop on the benchmark model (tensor cores + student, eps 1e-2):
@@ -574,12 +592,14 @@ def main():
         from hignn_b200 import synthetic as S
 
         xe = S.uniform_min_dist(n, 0.10, 2)
+        note("Euler loop: positions placed")
         m.set(capi.P_TIMING, 0)
         morse = dict(De=1.0, a=5.0, re=2.1, cutoff=3.0)
         m.run_euler(xe, 1, 1e-3, rebuild_every=10, gravity=(0.0, 0.0, 0.0), **morse)  # warm-up
         t0 = time.perf_counter()
         x1 = m.run_euler(xe, args.euler_steps, 1e-3, rebuild_every=10, gravity=(0.0, 0.0, 0.0), **morse)
         dt_loop = time.perf_counter() - t0
+        note(f"Euler loop done: {dt_loop / args.euler_steps * 1e3:.0f} ms per step")
         euler = {"workload": "N=1,048,576 spheres uniform at volume fraction 0.10 with minimum separation 2.05 "
                              "(seed 2; the matvec's clustered positions overlap), Morse (D 1, a 5, r0 2.1, cutoff "
                              "3) without gravity (with it the unbounded collective flow drives neighbours into the "
